@@ -1,0 +1,233 @@
+/*
+ * pasta_b200.h -- C ABI of the B200 (sm_100a) implementation of PASTA's
+ * per-particle model-evaluation and chi2 hot path.
+ *
+ * Every entry point returns an int status: 0 on success, a negative
+ * PASTA_E_* code on failure, with a message from pasta_last_error()
+ * (thread-local).  All array arguments are caller-owned HOST pointers; the
+ * library copies them to the device and back.  Handles own device memory
+ * until destroyed.  No torch or C++ types cross this boundary.
+ *
+ * Reference interface that each entry point replaces is cited as
+ * file:line in SimonVanSchuylenbergh/PASTA (Rust + PyO3).
+ */
+#ifndef PASTA_B200_H
+#define PASTA_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PASTA_B200_ABI_VERSION 1
+
+/* wavelength grid kinds (interpolate.rs:672-679) */
+enum { PASTA_WL_LINSPACE = 0, PASTA_WL_LOGSPACE = 1, PASTA_WL_NONUNIFORM = 2 };
+/* dispersion kinds (lib.rs:655-662) */
+enum { PASTA_DISP_NONE = 0, PASTA_DISP_FIXED = 1, PASTA_DISP_VARIABLE = 2 };
+/* continuum fitter kinds (lib.rs:800-807) */
+enum { PASTA_CONT_CHUNK = 0, PASTA_CONT_LINEAR = 1, PASTA_CONT_FIXED = 2, PASTA_CONT_CONSTANT = 3 };
+/* fit execution forms */
+enum { PASTA_FIT_BATCHED = 0, PASTA_FIT_PLAIN = 1 };
+
+/* error codes */
+enum {
+  PASTA_OK = 0,
+  PASTA_E_ARG = -1,            /* invalid argument / length mismatch      */
+  PASTA_E_CUDA = -2,           /* CUDA runtime error                      */
+  PASTA_E_NOMEM = -3,          /* device memory or HBM budget exhausted   */
+  PASTA_E_OUT_OF_GRID = -10,   /* label outside the grid (interpolate.rs:425-430) */
+  PASTA_E_NEIGHBORS = -11,     /* neighbour search failed (interpolate.rs:105-159, cubic.rs:155) */
+  PASTA_E_VSINI = -12,         /* vsini < 0 (convolve_rv.rs:489-491)      */
+  PASTA_E_KERNEL_WIDTH = -13,  /* rotation kernel > 2048 (convolve_rv.rs:512-519) */
+  PASTA_E_RV_RANGE = -14,      /* shifted window leaves the synthetic grid (convolve_rv.rs:549-567) */
+  PASTA_E_RESAMPLE = -15,      /* resampling reads one pixel past the grid (convolve_rv.rs:572) */
+  PASTA_E_BOUNDS = -16,        /* PSO particle outside the bounds (particleswarm.rs:267-275) */
+  PASTA_E_CLAMP = -17,         /* clamp limits invalid (bounds.rs:13-16)  */
+  PASTA_E_CONTINUUM = -18,     /* continuum fitter cannot run on this spectrum */
+  PASTA_E_NAN = -19,           /* NaN label                                */
+  PASTA_E_UNSUPPORTED = -20,   /* e.g. rotation on a non-uniform grid (convolve_rv.rs:506) */
+  PASTA_E_INTERNAL = -99
+};
+
+typedef struct pasta_grid pasta_grid;
+typedef struct pasta_dispersion pasta_dispersion;
+typedef struct pasta_continuum pasta_continuum;
+typedef struct pasta_server pasta_server;
+
+typedef struct {
+  int32_t num_particles;
+  int32_t max_iters;
+  double inertia_factor, cognitive_factor, social_factor, delta;
+  double vsini_lo, vsini_hi, rv_lo, rv_hi;
+  /* per-parameter constraint: 0 none, 1 fixed at a, 2 range [a, b] (lib.rs:817-835) */
+  int32_t ckind[5];
+  double ca[5], cb[5];
+} pasta_pso_settings;
+
+typedef struct {
+  double label[5]; /* teff, m, logg, vsini, rv */
+  double chi2;
+  double time;     /* seconds from submission to result */
+  int32_t iterations;
+  int32_t status;  /* 0 ok, else PASTA_E_* of the failing particle */
+  int32_t n_params;
+  int32_t _pad;
+} pasta_fit_result;
+
+/* ------------------------------------------------------------ library */
+int pasta_abi_version(void);
+const char *pasta_last_error(void);
+/* Select the CUDA device used by handles created afterwards on this thread. */
+int pasta_set_device(int device);
+/* Number of launches of this library's kernels since load (all threads). */
+int64_t pasta_kernel_launch_count(void);
+
+/* ----------------------------------------------------------- the grid
+ * Replaces InMemFetcher::new / from_tar_zstd + GridInterpolator::new
+ * (model_fetchers.rs:136-226, interpolate.rs:905) and the PyO3
+ * constructors InMemInterpolator/OnDiskInterpolator/CachedInterpolator
+ * (lib.rs:1875-1931).  labels: n x (teff, m, logg) in any order; spectra:
+ * n x n_px uint16, row i for labels[i]; maxima: the includes_factor f32
+ * maxima (model_fetchers.rs:53-63) or NULL.  The grid is uploaded once and
+ * stays resident in HBM. */
+int pasta_grid_create(const double *labels, const uint16_t *spectra,
+                      const float *maxima, int64_t n_models, int64_t n_px,
+                      int wl_kind, double wl_a, double wl_b,
+                      const double *wl_values, pasta_grid **out);
+int pasta_grid_destroy(pasta_grid *g);
+/* sizes: n_teff, n_m, n_logg, n_px, n_models (lib.rs:1436-1461) */
+int pasta_grid_shape(const pasta_grid *g, int64_t *out5);
+int pasta_grid_axis(const pasta_grid *g, int axis, double *out);
+int pasta_grid_logg_limits(const pasta_grid *g, int64_t *lo, int64_t *hi);
+int pasta_grid_cumulative_size(const pasta_grid *g, int64_t *out);
+/* Grid::clamp_1d (interpolate.rs:625-628, lib.rs:1377-1382) */
+int pasta_grid_clamp_1d(const pasta_grid *g, double teff, double m,
+                        double logg, int index, double *out);
+/* Grid::is_teff_logg_between_bounds (interpolate.rs:351-369, lib.rs:1463) */
+int pasta_grid_is_teff_logg_between_bounds(const pasta_grid *g, double teff,
+                                           double logg, int *out);
+/* neighbour columns (-1 = missing) and f32 weights of the 4x4x4 cube plus
+ * the flat factors (lib.rs:1388-1433, cubic.rs:159-243) */
+int pasta_grid_coefficients(const pasta_grid *g, double teff, double m,
+                            double logg, int64_t *cols64, float *w64,
+                            double *teff16, double *logg16, double *m4);
+
+/* GridInterpolator::interpolate (interpolate.rs:930-983, lib.rs:1111):
+ * tml L x 3, out L x n_px float, status[L]. */
+int pasta_interpolate(const pasta_grid *g, const double *tml, int64_t L,
+                      float *out, int32_t *status);
+
+/* ----------------------------------------------------- dispersions
+ * NoConvolutionDispersion / FixedResolutionDispersion /
+ * VariableResolutionDispersion (lib.rs:763-797; convolve_rv.rs:72-431).
+ * The synthetic wavelength grid is passed like WlGrid (lib.rs:636-648).
+ * disp: per observed pixel Gaussian sigma in Angstrom (variable kind). */
+int pasta_dispersion_create(int synth_kind, double synth_a, double synth_b,
+                            int64_t synth_n, const double *synth_values,
+                            int kind, const double *wl_obs, int64_t n_obs,
+                            double resolution, const float *disp,
+                            pasta_dispersion **out);
+int pasta_dispersion_destroy(pasta_dispersion *d);
+/* PyWavelengthDispersion.convolve (lib.rs:671-680): in/out n = synth n */
+int pasta_dispersion_convolve(const pasta_dispersion *d, const float *in,
+                              int64_t n, float *out);
+/* kernel width (odd) and, if out != NULL, the kernels width x n_synth
+ * row-major as get_kernels returns them (lib.rs:1043-1060) */
+int pasta_dispersion_kernels(const pasta_dispersion *d, int64_t *width,
+                             float *out);
+
+/* ------------------------------------------------------ continuum
+ * ChunkContinuumFitter / LinearModelContinuumFitter / FixedContinuum /
+ * ConstantContinuum (lib.rs:945-983; continuum_fitting.rs:44-505).
+ * design: n x k row-major f32. */
+int pasta_continuum_create(int kind, const double *wl, int64_t n,
+                           int n_chunks, int p_order, double overlap,
+                           const float *design, int k,
+                           const float *continuum, int ignore_first_and_last,
+                           pasta_continuum **out);
+int pasta_continuum_destroy(pasta_continuum *c);
+int pasta_continuum_nparams(const pasta_continuum *c);
+/* ContinuumFitter::fit_continuum (continuum_fitting.rs:13-17; lib.rs:862) */
+int pasta_continuum_fit(const pasta_continuum *c, const float *model,
+                        const float *flux, const float *var, int64_t n,
+                        float *params, double *chi2);
+/* ContinuumFitter::build_continuum (lib.rs:927-939); out has n values
+ * (1 for the constant fitter) */
+int pasta_continuum_build(const pasta_continuum *c, const float *params,
+                          int64_t n_params, float *out);
+
+/* ------------------------------------------------------ model / chi2
+ * Interpolator::produce_model (interpolate.rs:1068-1090; lib.rs:993-1011,
+ * 1064-1089): labels L x 5, out L x n_obs. */
+int pasta_produce_model(const pasta_grid *g, const pasta_dispersion *d,
+                        const double *labels, int64_t L, float *out,
+                        int32_t *status);
+/* interpolate_and_convolve (interpolate.rs:1030-1047; lib.rs:1141):
+ * labels L x 4 (teff, m, logg, vsini), out L x n_synth. */
+int pasta_interpolate_and_convolve(const pasta_grid *g,
+                                   const pasta_dispersion *d,
+                                   const double *labels, int64_t L,
+                                   float *out, int32_t *status);
+/* SingleFitter::chi2 via CostFunction::cost (fitting.rs:313-326, 460-478;
+ * lib.rs:1603-1627): out[L] chi2 (NaN where status != 0). */
+int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d,
+               const pasta_continuum *c, const float *flux, const float *var,
+               int64_t n, const double *labels, int64_t L, double *out,
+               int32_t *status);
+
+/* ------------------------------------------------------------- fit
+ * SingleFitter::fit / fit_bulk (fitting.rs:399-458; lib.rs:1478-1540) with
+ * the particle swarm of particleswarm.rs:111-307.  S stars share the
+ * dispersion and continuum fitter; flux/var are S x n.  seeds[S] select the
+ * counter-based draw stream.  mode PASTA_FIT_BATCHED runs every star's
+ * swarm on the device in one launch sequence per iteration captured in a
+ * CUDA graph; PASTA_FIT_PLAIN runs one star at a time with the swarm update
+ * on the host (the comparison baseline).  params: S x nparams floats.
+ * trace (optional): (max_iters + 1) x num_particles x 6 doubles for star 0
+ * (position, cost) after initialisation and after every iteration. */
+int pasta_fit(const pasta_grid *g, const pasta_dispersion *d,
+              const pasta_continuum *c, const pasta_pso_settings *settings,
+              const float *flux, const float *var, int64_t n, int64_t S,
+              const uint64_t *seeds, int mode, pasta_fit_result *results,
+              float *params, double *trace);
+
+/* Batched fit of S stars with their own dispersion, continuum fitter,
+ * settings and pixel count (ragged batches: every star its own observed
+ * wavelength grid).  params[i] receives pasta_continuum_nparams(c[i]) floats
+ * (or is NULL). */
+int pasta_fit_many(const pasta_grid *g, int64_t S,
+                   const pasta_dispersion *const *d,
+                   const pasta_continuum *const *c,
+                   const pasta_pso_settings *settings,
+                   const float *const *flux, const float *const *var,
+                   const int64_t *n, const uint64_t *seeds, int mode,
+                   pasta_fit_result *results, float *const *params);
+
+/* ------------------------------------------------------- serving
+ * Continuous batching: requests are admitted into device slots as slots and
+ * HBM budget free up, every admitted star advances one PSO iteration per
+ * device step, finished stars leave and new ones join without draining.
+ * Each request carries its own dispersion and continuum fitter. */
+int pasta_server_create(const pasta_grid *g, int max_slots,
+                        int64_t hbm_budget_bytes, pasta_server **out);
+int pasta_server_submit(pasta_server *s, const pasta_dispersion *d,
+                        const pasta_continuum *c,
+                        const pasta_pso_settings *settings, const float *flux,
+                        const float *var, int64_t n, uint64_t seed,
+                        int64_t *request_id);
+/* advance the device loop by one step (admit, iterate, retire); returns the
+ * number of active slots after the step */
+int pasta_server_step(pasta_server *s);
+/* collect up to max finished results (non-blocking) */
+int pasta_server_poll(pasta_server *s, int64_t *ids, pasta_fit_result *results,
+                      float *params, int64_t params_stride, int max,
+                      int *n_out);
+int pasta_server_pending(const pasta_server *s, int64_t *queued,
+                         int64_t *active, int64_t *done);
+int pasta_server_destroy(pasta_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

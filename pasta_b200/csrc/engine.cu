@@ -1,0 +1,1895 @@
+// engine.cu -- host engine and C ABI of pasta_b200.
+//
+// Owns device memory for grids, dispersions, continuum fitters and
+// evaluation workspaces; runs the evaluation pipeline
+//   prep -> rotation spectra -> interpolation -> rotation FFT ->
+//   instrument profile -> resampling + continuum + chi2
+// over batches of (star, label) evaluations; drives the particle swarm
+// either fully on the device (batched form, one CUDA graph per PSO step)
+// or with the swarm on the host one star at a time (plain form).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pasta_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace pb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct PErr : std::runtime_error {
+  int code;
+  PErr(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] void fail(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  throw PErr(code, buf);
+}
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) fail(PASTA_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class F>
+int guard(F &&f) {
+  try {
+    f();
+    return PASTA_OK;
+  } catch (const PErr &e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return PASTA_E_NOMEM;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return PASTA_E_INTERNAL;
+  }
+}
+
+const char *status_message(int s) {
+  switch (s) {
+    case S_OUT_OF_GRID: return "label outside the grid";
+    case S_NEIGHBORS: return "not enough grid neighbours for cubic interpolation";
+    case S_VSINI: return "vsini must be positive";
+    case S_KERNEL_WIDTH: return "rotation kernel is larger than FFTSIZE (2048)";
+    case S_RV_RANGE: return "shifted observed wavelengths leave the synthetic grid";
+    case S_RESAMPLE: return "resampling index out of range";
+    case S_BOUNDS: return "particle is not within bounds";
+    case S_CLAMP: return "clamp limits are invalid";
+    case S_CONTINUUM: return "continuum fitter cannot evaluate chi2 on this spectrum";
+    case S_NAN: return "NaN label";
+    case S_UNSUPPORTED: return "non-equidistant wavelength grid not supported";
+    default: return "error";
+  }
+}
+
+// ---------------------------------------------------------------- memory
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      fail(PASTA_E_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+    n = count;
+  }
+  void upload(const T *h, size_t count) {
+    alloc(count);
+    if (count) CK(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void upload(const std::vector<T> &v) { upload(v.data(), v.size()); }
+};
+
+struct Ctx {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  DBuf<float2> tw;  // W_2048^k
+};
+std::mutex g_ctx_mu;
+std::map<int, std::unique_ptr<Ctx>> g_ctx;
+thread_local int g_dev = -1;
+
+Ctx &ctx() {
+  if (g_dev < 0) {
+    int d;
+    CK(cudaGetDevice(&d));
+    g_dev = d;
+  }
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  auto &c = g_ctx[g_dev];
+  if (!c) {
+    c.reset(new Ctx());
+    c->dev = g_dev;
+    CK(cudaSetDevice(g_dev));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    std::vector<float2> t(FFTN);
+    for (int k = 0; k < FFTN; k++) {
+      double a = -2.0 * M_PI * (double)k / (double)FFTN;
+      t[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    c->tw.upload(t);
+  }
+  CK(cudaSetDevice(c->dev));
+  return *c;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+// =================================================================== grid
+struct Workspace {
+  int64_t cap = 0, stride = 0;
+  int64_t gen = 0;  // bumped on every reallocation (captured graphs compare it)
+  DBuf<float> A, B;
+  DBuf<float2> H;
+  DBuf<EvalPrep> prep;
+  void ensure(int64_t want, int64_t str) {
+    if (want <= cap && str == stride) return;
+    A.release(); B.release(); H.release(); prep.release();
+    cap = 0;
+    A.alloc((size_t)want * str);
+    B.alloc((size_t)want * str);
+    H.alloc((size_t)want * 1025);
+    prep.alloc((size_t)want);
+    cap = want;
+    stride = str;
+    gen++;
+  }
+};
+
+struct pasta_grid {
+  int dev = 0;
+  DevGrid d{};
+  GridGeom hg{};
+  std::vector<double> tv, mv, lv, wl_vals;
+  std::vector<int> llo, lhi;
+  std::vector<int64_t> cum;
+  int64_t n_cols = 0, npx = 0, stride = 0;
+  int wl_kind = WL_LOG;
+  double wl_a = 0, wl_b = 0;
+  DBuf<uint16_t> spectra;
+  DBuf<float> factor;
+  DBuf<double> dtv, dmv, dlv, dwl;
+  DBuf<int> dllo, dlhi;
+  DBuf<int64_t> dcum;
+  std::mutex mu;
+  Workspace ws;
+};
+
+namespace {
+
+int64_t workspace_cap(const pasta_grid *g, int64_t want) {
+  // per evaluation: two spectrum rows + rotation half spectrum + prep record
+  const int64_t per = g->stride * 8 + 1025 * 8 + (int64_t)sizeof(EvalPrep);
+  int64_t budget = 24ll << 30;
+  if (const char *e = getenv("PASTA_WORKSPACE_BYTES")) budget = atoll(e);
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+    const int64_t avail = (int64_t)fr - (2ll << 30) + (int64_t)g->ws.cap * per;
+    if (avail < budget) budget = avail;
+  }
+  int64_t cap = std::max<int64_t>(1, budget / per);
+  return std::min<int64_t>(cap, std::max<int64_t>(want, 1));
+}
+
+}  // namespace
+
+// ============================================================ dispersion
+struct pasta_dispersion {
+  int kind = PASTA_DISP_NONE, dev_kind = DISP_NONE;
+  int synth_kind = WL_LOG;
+  double synth_a = 0, synth_b = 0;
+  int64_t synth_n = 0;
+  std::vector<double> synth_vals, wl, fidx;
+  double wl_first = 0, wl_last = 0, wl_min = 0, wl_max = 0, fidx_min = 0, fidx_max = 0;
+  int gw = 0;
+  std::vector<float> gk;  // fixed: [gw]; per pixel: [synth_n][gw]
+  DBuf<double> dfidx, dwl;
+  DBuf<float> dgk;
+};
+
+namespace {
+
+// WlGrid helpers (interpolate.rs:681-743)
+double wl_at(int kind, double a, double b, const std::vector<double> &v, int64_t i) {
+  if (kind == WL_LIN) return a + b * (double)i;
+  if (kind == WL_LOG) return std::pow(10.0, a + b * (double)i);
+  return v[i];
+}
+double wl_float_index(int kind, double a, double b, const std::vector<double> &v, double wl) {
+  if (kind == WL_LIN) return (wl - a) / b;
+  if (kind == WL_LOG) return (std::log10(wl) - a) / b;
+  auto it = std::lower_bound(v.begin(), v.end(), wl);
+  int64_t i = it - v.begin();
+  if (i < (int64_t)v.size() && v[i] == wl) return (double)i;
+  if (i == 0) return 0.0;
+  if (i == (int64_t)v.size()) return (double)v.size() - 1.0;
+  return (wl - v[i - 1]) / (v[i] - v[i - 1]) + (double)i - 1.0;
+}
+
+// convolve_rv.rs:107-118 (f32)
+void make_gaussian(float *arr, int n, float sigma) {
+  int mid = (n - 1) / 2;
+  for (int i = 0; i < n; i++) {
+    float x = ((float)i - (float)mid) / sigma;
+    arr[i] = std::exp(-0.5f * x * x);
+  }
+  float s = 0.0f;
+  for (int i = 0; i < n; i++) s = s + arr[i];
+  for (int i = 0; i < n; i++) arr[i] = arr[i] / s;
+}
+int odd_width(double six_sigma) {
+  double c = std::ceil(six_sigma);
+  int64_t nme = c > 0 ? (int64_t)c : 0;
+  return (int)(nme + 1 - nme % 2);
+}
+
+void disp_per_pixel(pasta_dispersion *d, const std::vector<float> &sig) {
+  float largest = sig[0];
+  for (float s : sig) if (s > largest) largest = s;
+  int w = odd_width((double)(largest * 6.0f));
+  if (w > 2 * 255 + 1) fail(PASTA_E_UNSUPPORTED, "instrument kernel of %d taps exceeds the supported 511", w);
+  d->gw = w;
+  d->dev_kind = DISP_PIXEL;
+  d->gk.assign((size_t)w * sig.size(), 0.0f);
+  for (size_t i = 0; i < sig.size(); i++) make_gaussian(&d->gk[i * w], w, sig[i]);
+}
+
+}  // namespace
+
+// ============================================================= continuum
+struct pasta_continuum {
+  int kind = PASTA_CONT_CHUNK;
+  int64_t n = 0;
+  int bad = 0;
+  std::string bad_msg;
+  // chunk
+  int nc = 0, p1 = 0;
+  std::vector<int> cstart, cstop;
+  std::vector<float> xa, xb, fac;
+  std::vector<double> chol;  // nc x p1 x p1
+  // linear
+  int k = 0;
+  std::vector<float> qcol;  // k x n column-major
+  std::vector<double> R;    // k x k upper (row-major)
+  // fixed
+  std::vector<float> cont;
+  int ignore = 0;
+  DBuf<int> dcs, dce;
+  DBuf<float> dxa, dxb, dfac, dq, dcont;
+  DBuf<double> dchol;
+};
+
+namespace {
+
+template <class F>
+F map_range(F x, F fl, F fh, F tl, F th, bool clamp) {  // continuum_fitting.rs:109-116
+  F v = (x - fl) / (fh - fl) * (th - tl) + tl;
+  if (clamp) v = std::min(std::max(v, tl), th);
+  return v;
+}
+float poly_blend(float x) {  // continuum_fitting.rs:119-123
+  float xc = std::min(std::max(x, 0.0f), 1.0f);
+  float s = std::sin(xc * (float)M_PI / 2.0f);
+  return s * s;
+}
+void legendre_host(double x, int p1, double *P) {
+  P[0] = 1.0;
+  if (p1 > 1) P[1] = x;
+  for (int k = 1; k + 1 < p1; k++) {
+    const double a = (double)(2 * k + 1) / (double)(k + 1), c = (double)k / (double)(k + 1);
+    P[k + 1] = a * x * P[k] - c * P[k - 1];
+  }
+}
+// monomial coefficients of P_0..P_{p1-1}: T[k][j]
+std::vector<double> legendre_to_monomial(int p1) {
+  std::vector<double> T((size_t)p1 * p1, 0.0);
+  T[0] = 1.0;
+  if (p1 > 1) T[(size_t)1 * p1 + 1] = 1.0;
+  for (int k = 1; k + 1 < p1; k++) {
+    const double a = (double)(2 * k + 1) / (double)(k + 1), c = (double)k / (double)(k + 1);
+    for (int j = 0; j < p1; j++) {
+      double v = -c * T[(size_t)(k - 1) * p1 + j];
+      if (j > 0) v += a * T[(size_t)k * p1 + j - 1];
+      T[(size_t)(k + 1) * p1 + j] = v;
+    }
+  }
+  return T;
+}
+
+// ChunkFitter::new (continuum_fitting.rs:140-214) plus the Legendre Gram
+// Cholesky factors used by the device solve.
+void chunk_setup(pasta_continuum *c, const double *wl, int n_chunks, int p_order, double overlap) {
+  const int64_t n = c->n;
+  if (n_chunks < 1) fail(PASTA_E_ARG, "n_chunks must be >= 1");
+  if (n_chunks > MAX_CHUNKS) fail(PASTA_E_UNSUPPORTED, "at most %d chunks are supported", MAX_CHUNKS);
+  if (p_order < 0 || p_order + 1 > MAX_P1) fail(PASTA_E_UNSUPPORTED, "polynomial order must be 0..%d", MAX_P1 - 1);
+  if (n < 2) fail(PASTA_E_ARG, "wavelength array too short");
+  c->nc = n_chunks;
+  c->p1 = p_order + 1;
+  c->cstart.resize(n_chunks);
+  c->cstop.resize(n_chunks);
+  for (int i = 0; i < n_chunks; i++) {
+    double s = map_range((double)i - overlap, 0.0, (double)n_chunks, wl[0], wl[n - 1], true);
+    double e = map_range((double)i + 1.0 + overlap, 0.0, (double)n_chunks, wl[0], wl[n - 1], true);
+    int64_t a = -1, b = -1;
+    for (int64_t j = 0; j < n; j++) if (wl[j] > s) { a = j; break; }
+    for (int64_t j = n - 1; j >= 0; j--) if (wl[j] < e) { b = j; break; }
+    if (a < 0 || b < 0) fail(PASTA_E_ARG, "chunk %d has no pixels", i);
+    c->cstart[i] = (int)a;
+    c->cstop[i] = (int)(b + 1);
+  }
+  c->cstart[0] = 0;
+  c->cstop[n_chunks - 1] = (int)n;
+  const int nc = n_chunks, p1 = c->p1;
+  for (int i = 0; i < nc; i++)
+    if (c->cstop[i] - c->cstart[i] < 2) fail(PASTA_E_ARG, "chunk %d is empty", i);
+  c->xa.assign(n, 0.0f);
+  c->xb.assign(n, 0.0f);
+  c->fac.assign(n, 0.0f);
+  for (int ch = 0; ch < nc; ch++) {
+    const int s = c->cstart[ch], e = c->cstop[ch];
+    for (int i = s; i < e; i++) {
+      float x = (float)map_range(wl[i], wl[s], wl[e - 1], -1.0, 1.0, false);
+      if (ch > 0 && i < c->cstop[ch - 1]) c->xb[i] = x;  // overlap with the previous chunk
+      else c->xa[i] = x;
+    }
+  }
+  for (int ch = 0; ch + 1 < nc; ch++) {  // factor_arrays (continuum_fitting.rs:184-200)
+    const int e = c->cstop[ch], sn = c->cstart[ch + 1];
+    for (int i = sn; i < e; i++)
+      c->fac[i] = poly_blend(map_range((float)wl[i], (float)wl[sn], (float)wl[e - 1], 1.0f, 0.0f, false));
+  }
+  // Legendre Gram per chunk, FP64 Cholesky
+  c->chol.assign((size_t)nc * p1 * p1, 0.0);
+  std::vector<double> G((size_t)p1 * p1), P(p1);
+  for (int ch = 0; ch < nc && !c->bad; ch++) {
+    std::fill(G.begin(), G.end(), 0.0);
+    for (int i = c->cstart[ch]; i < c->cstop[ch]; i++) {
+      const float xf = (ch > 0 && i < c->cstop[ch - 1]) ? c->xb[i] : c->xa[i];
+      legendre_host((double)xf, p1, P.data());
+      for (int a = 0; a < p1; a++)
+        for (int b = 0; b <= a; b++) G[(size_t)a * p1 + b] += P[a] * P[b];
+    }
+    double *L = &c->chol[(size_t)ch * p1 * p1];
+    for (int a = 0; a < p1; a++) {
+      for (int b = 0; b <= a; b++) {
+        double s = G[(size_t)a * p1 + b];
+        for (int k = 0; k < b; k++) s -= L[a * p1 + k] * L[b * p1 + k];
+        if (a == b) {
+          if (!(s > 1e-12 * std::max(1.0, G[(size_t)a * p1 + a]))) {
+            c->bad = 1;
+            c->bad_msg = "chunk polynomial basis is rank deficient";
+            s = 1.0;
+          }
+          L[a * p1 + a] = std::sqrt(s);
+        } else {
+          L[a * p1 + b] = s / L[b * p1 + b];
+        }
+      }
+    }
+  }
+  // the reference's chi2 loops panic on these layouts (continuum_fitting.rs:301-357)
+  if (!c->bad) {
+    if (nc < 2) { c->bad = 1; c->bad_msg = "chunk fitter needs at least 2 chunks"; }
+    else if (n < 100) { c->bad = 1; c->bad_msg = "spectrum shorter than 100 pixels"; }
+    else if (c->cstart[1] < 50) { c->bad = 1; c->bad_msg = "second chunk starts before pixel 50"; }
+    else {
+      for (int ch = 1; ch < nc; ch++) {
+        const int nx = ch == nc - 1 ? (int)n - 50 : c->cstart[ch + 1];
+        if (c->cstop[ch - 1] < c->cstart[ch] || nx < c->cstop[ch - 1]) {
+          c->bad = 1;
+          c->bad_msg = "chunk overlaps are inconsistent";
+          break;
+        }
+      }
+    }
+  }
+}
+
+// LinearModelFitter::new (continuum_fitting.rs:53-56): thin Householder QR
+// in double of the design matrix; Q (f32) spans the same column space.
+void linear_setup(pasta_continuum *c, const float *design, int k) {
+  const int64_t n = c->n;
+  if (k < 1 || k > MAX_LIN_K) fail(PASTA_E_UNSUPPORTED, "design matrix must have 1..%d columns", MAX_LIN_K);
+  if (n < k) fail(PASTA_E_ARG, "design matrix has fewer rows than columns");
+  c->k = k;
+  std::vector<double> A((size_t)n * k);  // column-major
+  for (int64_t i = 0; i < n; i++)
+    for (int j = 0; j < k; j++) A[(size_t)j * n + i] = design[(size_t)i * k + j];
+  std::vector<double> beta(k, 0.0);
+  c->R.assign((size_t)k * k, 0.0);
+  for (int j = 0; j < k; j++) {
+    double *cj = &A[(size_t)j * n];
+    double nrm = 0.0;
+    for (int64_t i = j; i < n; i++) nrm += cj[i] * cj[i];
+    nrm = std::sqrt(nrm);
+    double alpha = cj[j] > 0 ? -nrm : nrm;
+    if (nrm == 0.0) { beta[j] = 0.0; c->R[(size_t)j * k + j] = 0.0; continue; }
+    cj[j] -= alpha;
+    double vv = 0.0;
+    for (int64_t i = j; i < n; i++) vv += cj[i] * cj[i];
+    beta[j] = 2.0 / vv;
+    for (int l = j + 1; l < k; l++) {
+      double *cl = &A[(size_t)l * n];
+      double s = 0.0;
+      for (int64_t i = j; i < n; i++) s += cj[i] * cl[i];
+      s *= beta[j];
+      for (int64_t i = j; i < n; i++) cl[i] -= s * cj[i];
+    }
+    c->R[(size_t)j * k + j] = alpha;
+    for (int l = j + 1; l < k; l++) c->R[(size_t)j * k + l] = A[(size_t)l * n + j];
+  }
+  double rmax = 0.0;
+  for (int j = 0; j < k; j++) rmax = std::max(rmax, std::fabs(c->R[(size_t)j * k + j]));
+  for (int j = 0; j < k; j++)
+    if (!(std::fabs(c->R[(size_t)j * k + j]) > 1e-10 * rmax)) {
+      c->bad = 1;
+      c->bad_msg = "design matrix is rank deficient";
+    }
+  // explicit Q: apply the reflectors to the first k unit vectors
+  c->qcol.assign((size_t)k * n, 0.0f);
+  std::vector<double> q(n);
+  for (int col = 0; col < k; col++) {
+    std::fill(q.begin(), q.end(), 0.0);
+    q[col] = 1.0;
+    for (int j = k - 1; j >= 0; j--) {
+      if (beta[j] == 0.0) continue;
+      const double *v = &A[(size_t)j * n];
+      double s = 0.0;
+      for (int64_t i = j; i < n; i++) s += v[i] * q[i];
+      s *= beta[j];
+      for (int64_t i = j; i < n; i++) q[i] -= s * v[i];
+    }
+    for (int64_t i = 0; i < n; i++) c->qcol[(size_t)col * n + i] = (float)q[i];
+  }
+}
+
+// Host result of a continuum solve -> the reference's parameter vector.
+std::vector<float> params_from_device(const pasta_continuum *c, const double *p) {
+  std::vector<float> out;
+  if (c->kind == PASTA_CONT_CHUNK) {
+    const int p1 = c->p1;
+    auto T = legendre_to_monomial(p1);
+    for (int ch = 0; ch < c->nc; ch++)
+      for (int j = 0; j < p1; j++) {
+        double s = 0.0;
+        for (int k = 0; k < p1; k++) s += p[ch * p1 + k] * T[(size_t)k * p1 + j];
+        out.push_back((float)s);
+      }
+  } else if (c->kind == PASTA_CONT_LINEAR) {
+    const int k = c->k;
+    std::vector<double> x(k);
+    for (int j = k - 1; j >= 0; j--) {
+      double s = p[j];
+      for (int l = j + 1; l < k; l++) s -= c->R[(size_t)j * k + l] * x[l];
+      x[j] = s / c->R[(size_t)j * k + j];
+    }
+    for (double v : x) out.push_back((float)v);
+  } else {
+    out.push_back((float)p[0]);
+  }
+  return out;
+}
+
+int cont_nparams(const pasta_continuum *c) {
+  if (c->kind == PASTA_CONT_CHUNK) return c->nc * c->p1;
+  if (c->kind == PASTA_CONT_LINEAR) return c->k;
+  return 1;
+}
+int device_param_stride(const pasta_continuum *c) {
+  if (c->kind == PASTA_CONT_CHUNK) return c->nc * c->p1;
+  if (c->kind == PASTA_CONT_LINEAR) return c->k;
+  return 1;
+}
+
+// Assemble a device star from its dispersion, continuum and observed data.
+DevStar make_star(const pasta_dispersion *d, const pasta_continuum *c, const float *dflux, const float *dvar,
+                  int64_t n) {
+  DevStar s{};
+  s.n_obs = (int)n;
+  s.disp_kind = d ? d->dev_kind : DISP_NONE;
+  s.gw = d ? d->gw : 0;
+  s.flux = dflux;
+  s.var = dvar;
+  if (d) {
+    s.fidx = d->dfidx.p;
+    s.wl_obs = d->dwl.p;
+    s.wl_first = d->wl_first; s.wl_last = d->wl_last;
+    s.wl_min = d->wl_min; s.wl_max = d->wl_max;
+    s.fidx_min = d->fidx_min; s.fidx_max = d->fidx_max;
+    s.gk = d->dgk.p;
+  }
+  if (c) {
+    s.cont_kind = c->kind;
+    s.cont_bad = c->bad;
+    s.n_chunks = c->nc;
+    s.p1 = c->p1;
+    s.k_lin = c->k;
+    s.ignore = c->ignore;
+    s.cstart = c->dcs.p;
+    s.cstop = c->dce.p;
+    s.xa = c->dxa.p; s.xb = c->dxb.p; s.fac = c->dfac.p;
+    s.chol = c->dchol.p;
+    s.q = c->dq.p;
+    s.cont = c->dcont.p;
+  } else {
+    s.cont_kind = CONT_CONSTANT;
+  }
+  return s;
+}
+
+void check_disp_grid(const pasta_grid *g, const pasta_dispersion *d) {
+  if (!d) return;
+  if (d->synth_n != g->npx)
+    fail(PASTA_E_ARG, "Length of model and wavelength grid don't match. model: %lld, synth_wl: %lld",
+         (long long)g->npx, (long long)d->synth_n);
+}
+
+// ============================================================ pipeline
+struct EvalArgs {
+  const DevStar *stars = nullptr;
+  const double *labels = nullptr;
+  const int *eval_star = nullptr;
+  const int *eval_active = nullptr;
+  int64_t E = 0;
+  double *cost = nullptr;
+  int *status = nullptr;
+  double *params = nullptr;
+  int param_stride = 0;
+  int need_chi2 = 0;
+  int full_window = 0;
+  int max_m = 1;
+  float *out_obs = nullptr;
+  int64_t out_stride = 0;
+  float *out_synth = nullptr;
+  const float *given = nullptr;  // model given at observed pixels
+};
+
+int max_pairs_for(const pasta_grid *g, int max_m) {
+  if (max_m <= 1) return 0;
+  const int V = FFTN - (max_m - 1);
+  const int64_t nblk = (g->npx + V - 1) / V;
+  return (int)((nblk + 1) / 2);
+}
+
+int width_upper_bound(const pasta_grid *g, double vsini_hi) {
+  if (g->d.dvelo <= 0.0 || !(vsini_hi > 0.0)) return 1;
+  int w = rotation_width(vsini_hi, g->d.dvelo);
+  return std::min(w, FFTN);
+}
+
+// Launch the evaluation pipeline for a.E evaluations, in workspace-sized
+// sub-batches.  Capturable in a CUDA graph (no allocation, no sync).
+void run_evals(pasta_grid *g, const EvalArgs &a, cudaStream_t s) {
+  Ctx &C = ctx();
+  const int64_t cap = g->ws.cap;
+  const int max_pairs = max_pairs_for(g, a.max_m);
+  for (int64_t off = 0; off < a.E; off += cap) {
+    const int64_t cnt = std::min(cap, a.E - off);
+    EvalBatch b{};
+    b.E = (int)cnt;
+    b.labels = a.labels + 5 * off;
+    b.eval_star = a.eval_star + off;
+    b.eval_active = a.eval_active ? a.eval_active + off : nullptr;
+    b.stars = a.stars;
+    b.prep = g->ws.prep.p;
+    b.H = g->ws.H.p;
+    b.bufA = g->ws.A.p;
+    b.bufB = g->ws.B.p;
+    b.stride = g->ws.stride;
+    b.cost = a.cost ? a.cost + off : nullptr;
+    b.status = a.status ? a.status + off : nullptr;
+    b.params = a.params ? a.params + (size_t)off * a.param_stride : nullptr;
+    b.param_stride = a.param_stride;
+    b.max_pairs = max_pairs;
+    b.need_chi2 = a.need_chi2;
+    if (a.given) {
+      launch_chi2_given(g->d, b, a.given, s);
+      continue;
+    }
+    if (a.full_window) launch_prep_full(g->d, b, s);
+    else launch_prep(g->d, b, s);
+    if (a.max_m > 1) launch_rotker(g->d, b, C.tw.p, s);
+    launch_interp(g->d, b, s);
+    if (a.max_m > 1) launch_rot(g->d, b, C.tw.p, s);
+    launch_gauss(g->d, b, s);
+    if (a.need_chi2) launch_chi2(g->d, b, s);
+    else if (b.status) launch_prep_status(b, s);
+    if (a.out_obs) launch_resample_out(g->d, b, a.out_obs + (size_t)off * a.out_stride, a.out_stride, s);
+    if (a.out_synth) launch_copy_broadened(g->d, b, a.out_synth + (size_t)off * g->npx, s);
+  }
+  CK(cudaGetLastError());
+}
+
+void ensure_workspace(pasta_grid *g, int64_t E) {
+  const int64_t want = workspace_cap(g, E);
+  if (g->ws.cap < want || g->ws.stride != g->stride) g->ws.ensure(want, g->stride);
+}
+
+// ================================================================= swarm
+PsoParams make_pso_params(const pasta_grid *g, const pasta_pso_settings &st) {
+  if (st.num_particles < 1 || st.num_particles > MAX_PARTICLES)
+    fail(PASTA_E_ARG, "num_particles must be in 1..%d", MAX_PARTICLES);
+  if (st.max_iters < 0) fail(PASTA_E_ARG, "max_iters must be >= 0");
+  if (st.social_factor < 0.0) fail(PASTA_E_ARG, "`ParticleSwarm`: social factor must be >=0.");
+  if (st.delta < 0.0) fail(PASTA_E_ARG, "`ParticleSwarm`: delta must be >=0.");
+  PsoParams P{};
+  P.P = st.num_particles;
+  P.max_iters = st.max_iters;
+  P.inertia = st.inertia_factor;
+  P.cognitive = st.cognitive_factor;
+  P.social = st.social_factor;
+  P.vs_lo = st.vsini_lo; P.vs_hi = st.vsini_hi;
+  P.rv_lo = st.rv_lo; P.rv_hi = st.rv_hi;
+  double mn[5] = {g->tv.front(), g->mv.front(), g->lv.front(), st.vsini_lo, st.rv_lo};
+  double mx[5] = {g->tv.back(), g->mv.back(), g->lv.back(), st.vsini_hi, st.rv_hi};
+  for (int i = 0; i < 5; i++) {
+    P.ckind[i] = st.ckind[i];
+    P.ca[i] = st.ca[i];
+    P.cb[i] = st.cb[i];
+    if (st.ckind[i] == 1) { mn[i] = st.ca[i]; mx[i] = st.ca[i]; }
+    else if (st.ckind[i] == 2) { mn[i] = std::max(mn[i], st.ca[i]); mx[i] = std::min(mx[i], st.cb[i]); }
+    P.mn[i] = mn[i];
+    P.mx[i] = mx[i];
+  }
+  return P;
+}
+
+// bounds.rs:21-35 + particleswarm.rs:137-150 on the shared draw stream.
+int init_swarm_host(const pasta_grid *g, const PsoParams &S, uint64_t seed, double *x, double *v) {
+  uint64_t cand = 0;
+  for (int p = 0; p < S.P;) {
+    if (cand > 20000000ull) return S_BOUNDS;
+    double t[5];
+    for (int d = 0; d < 5; d++)
+      t[d] = S.mn[d] == S.mx[d] ? S.mn[d] : uniform_between(S.mn[d], S.mx[d], draw_u01(seed, PH_INIT_POS, cand, 0, d));
+    cand++;
+    if (pso_within(g->hg, S, t)) {
+      for (int d = 0; d < 5; d++) x[p * 5 + d] = t[d];
+      p++;
+    }
+  }
+  for (int p = 0; p < S.P; p++)
+    for (int d = 0; d < 5; d++) {
+      const double w = S.mx[d] - S.mn[d];
+      v[p * 5 + d] = (-w == w) ? -w : uniform_between(-w, w, draw_u01(seed, PH_INIT_VEL, p, 0, d));
+    }
+  return S_OK;
+}
+
+struct StarInput {
+  const pasta_dispersion *d;
+  const pasta_continuum *c;
+  const pasta_pso_settings *st;
+  const float *flux, *var;
+  int64_t n;
+  uint64_t seed;
+};
+
+// Upload the observed data of S stars (concatenated) and build DevStars.
+struct StarSet {
+  DBuf<float> flux, var;
+  DBuf<DevStar> dstars;
+  std::vector<DevStar> h;
+  void build(const std::vector<StarInput> &in) {
+    int64_t tot = 0;
+    for (auto &s : in) tot += s.n;
+    std::vector<float> f(tot), v(tot);
+    std::vector<int64_t> off(in.size());
+    int64_t o = 0;
+    for (size_t i = 0; i < in.size(); i++) {
+      off[i] = o;
+      std::memcpy(&f[o], in[i].flux, in[i].n * sizeof(float));
+      std::memcpy(&v[o], in[i].var, in[i].n * sizeof(float));
+      o += in[i].n;
+    }
+    flux.upload(f);
+    var.upload(v);
+    h.resize(in.size());
+    for (size_t i = 0; i < in.size(); i++) h[i] = make_star(in[i].d, in[i].c, flux.p + off[i], var.p + off[i], in[i].n);
+    dstars.upload(h);
+  }
+};
+
+void validate_star(const pasta_grid *g, const StarInput &s) {
+  check_disp_grid(g, s.d);
+  if (s.n != (int64_t)s.d->wl.size()) fail(PASTA_E_ARG, "Observed spectrum and target dispersion must have the same length");
+  if (s.c && s.c->kind != PASTA_CONT_CONSTANT && s.c->n != s.n)
+    fail(PASTA_E_ARG, "Length of observed and continuum spectrum are different %lld, %lld", (long long)s.n, (long long)s.c->n);
+}
+
+struct SwarmBuffers {
+  int S = 0, Pmax = 0;
+  DBuf<double> x, v, bx, cost, bcost, gx, gcost, labels, ecost;
+  DBuf<int> iter, status, done, active, eval_active, eval_star, estatus;
+  DBuf<uint64_t> seed;
+  DBuf<PsoParams> params;
+  Swarm view() {
+    Swarm w;
+    w.S = S; w.Pmax = Pmax;
+    w.x = x.p; w.v = v.p; w.bx = bx.p; w.cost = cost.p; w.bcost = bcost.p;
+    w.gx = gx.p; w.gcost = gcost.p; w.iter = iter.p; w.status = status.p; w.done = done.p;
+    w.active = active.p; w.seed = seed.p; w.params = params.p; w.labels = labels.p;
+    w.eval_active = eval_active.p;
+    return w;
+  }
+  void alloc(int S_, int Pmax_) {
+    S = S_; Pmax = Pmax_;
+    const size_t E = (size_t)S * Pmax;
+    x.alloc(E * 5); v.alloc(E * 5); bx.alloc(E * 5); cost.alloc(E); bcost.alloc(E);
+    gx.alloc((size_t)S * 5); gcost.alloc(S); labels.alloc(E * 5); ecost.alloc(E);
+    iter.alloc(S); status.alloc(S); done.alloc(S); active.alloc(S);
+    eval_active.alloc(E); eval_star.alloc(E); estatus.alloc(E);
+    seed.alloc(S); params.alloc(S);
+    std::vector<int> es(E);
+    for (size_t e = 0; e < E; e++) es[e] = (int)(e / Pmax);
+    CK(cudaMemcpy(eval_star.p, es.data(), E * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemset(eval_active.p, 0, E * sizeof(int)));
+    CK(cudaMemset(x.p, 0, E * 5 * sizeof(double)));
+    CK(cudaMemset(v.p, 0, E * 5 * sizeof(double)));
+    CK(cudaMemset(labels.p, 0, E * 5 * sizeof(double)));
+  }
+};
+
+// Final refit at the best labels (fitting.rs:436-440) -> continuum params.
+void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, const std::vector<double> &best,
+                 const std::vector<int> &ok, std::vector<std::vector<float>> &params, cudaStream_t s) {
+  const int S = (int)in.size();
+  int pstride = 1, max_m = 1;
+  for (auto &x : in) {
+    pstride = std::max(pstride, device_param_stride(x.c));
+    double vhi = x.st->vsini_hi;
+    if (x.st->ckind[3] == 1) vhi = x.st->ca[3];
+    max_m = std::max(max_m, width_upper_bound(g, vhi));
+  }
+  DBuf<double> lab, cost, par;
+  DBuf<int> es, ea, st;
+  lab.upload(best);
+  std::vector<int> star(S);
+  for (int i = 0; i < S; i++) star[i] = i;
+  es.upload(star);
+  ea.upload(ok);
+  cost.alloc(S);
+  st.alloc(S);
+  par.alloc((size_t)S * pstride);
+  EvalArgs a;
+  a.stars = ss.dstars.p;
+  a.labels = lab.p;
+  a.eval_star = es.p;
+  a.eval_active = ea.p;
+  a.E = S;
+  a.cost = cost.p;
+  a.status = st.p;
+  a.params = par.p;
+  a.param_stride = pstride;
+  a.need_chi2 = 1;
+  a.max_m = max_m;
+  ensure_workspace(g, S);
+  run_evals(g, a, s);
+  std::vector<double> hp((size_t)S * pstride);
+  CK(cudaMemcpyAsync(hp.data(), par.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  params.assign(S, {});
+  for (int i = 0; i < S; i++)
+    if (ok[i]) params[i] = params_from_device(in[i].c, &hp[(size_t)i * pstride]);
+}
+
+// Batched form: all stars' swarms on the device, one CUDA graph per step.
+void fit_batched(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result *res,
+                 std::vector<std::vector<float>> &params, double *trace) {
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
+  const double t0 = now_s();
+  const int S = (int)in.size();
+  int Pmax = 0, iters = 0, max_m = 1;
+  std::vector<PsoParams> pp(S);
+  for (int i = 0; i < S; i++) {
+    pp[i] = make_pso_params(g, *in[i].st);
+    Pmax = std::max(Pmax, pp[i].P);
+    iters = std::max(iters, pp[i].max_iters);
+    max_m = std::max(max_m, width_upper_bound(g, pp[i].mx[3]));
+  }
+  StarSet ss;
+  ss.build(in);
+  SwarmBuffers W;
+  W.alloc(S, Pmax);
+  const size_t E = (size_t)S * Pmax;
+  std::vector<double> hx(E * 5, 0.0), hv(E * 5, 0.0);
+  std::vector<int> status(S, 0), done(S, 0), active(S, 1), iter(S, -1);
+  std::vector<uint64_t> seeds(S);
+  for (int i = 0; i < S; i++) {
+    seeds[i] = in[i].seed;
+    int st = init_swarm_host(g, pp[i], in[i].seed, &hx[(size_t)i * Pmax * 5], &hv[(size_t)i * Pmax * 5]);
+    if (st) { status[i] = st; done[i] = 1; }
+  }
+  CK(cudaMemcpy(W.x.p, hx.data(), E * 5 * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(W.v.p, hv.data(), E * 5 * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(W.status.p, status.data(), S * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(W.done.p, done.data(), S * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(W.active.p, active.data(), S * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(W.iter.p, iter.data(), S * sizeof(int), cudaMemcpyHostToDevice));
+  W.seed.upload(seeds);
+  W.params.upload(pp);
+  ensure_workspace(g, (int64_t)E);
+  Swarm sw = W.view();
+  EvalArgs a;
+  a.stars = ss.dstars.p;
+  a.labels = W.labels.p;
+  a.eval_star = W.eval_star.p;
+  a.eval_active = W.eval_active.p;
+  a.E = (int64_t)E;
+  a.cost = W.ecost.p;
+  a.status = W.estatus.p;
+  a.need_chi2 = 1;
+  a.max_m = max_m;
+  // capture one PSO step: positions -> evaluations -> bests
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const bool use_graph = !getenv("PASTA_NO_GRAPH");
+  auto step = [&]() {
+    launch_pso_update(g->d, sw, s);
+    run_evals(g, a, s);
+    launch_pso_best(sw, W.ecost.p, W.estatus.p, s);
+  };
+  if (use_graph) {
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    step();
+    CK(cudaStreamEndCapture(s, &graph));
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+  }
+  std::vector<double> tx, tc;
+  const int Ptr = pp.empty() ? 0 : pp[0].P;
+  for (int it = 0; it <= iters; it++) {
+    if (use_graph) CK(cudaGraphLaunch(exec, s));
+    else step();
+    if (trace) {
+      tx.resize((size_t)Pmax * 5);
+      tc.resize(Pmax);
+      CK(cudaMemcpyAsync(tx.data(), W.x.p, tx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(tc.data(), W.cost.p, tc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (it <= pp[0].max_iters)
+        for (int p = 0; p < Ptr; p++) {
+          double *t = trace + ((size_t)it * Ptr + p) * 6;
+          for (int d = 0; d < 5; d++) t[d] = tx[(size_t)p * 5 + d];
+          t[5] = tc[p];
+        }
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  std::vector<double> gx((size_t)S * 5), gc(S);
+  CK(cudaMemcpyAsync(gx.data(), W.gx.p, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(gc.data(), W.gcost.p, gc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(status.data(), W.status.p, S * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(iter.data(), W.iter.p, S * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::vector<int> ok(S);
+  for (int i = 0; i < S; i++) ok[i] = status[i] == 0 ? 1 : 0;
+  final_refit(g, ss, in, gx, ok, params, s);
+  const double dt = now_s() - t0;
+  for (int i = 0; i < S; i++) {
+    pasta_fit_result &r = res[i];
+    std::memset(&r, 0, sizeof r);
+    for (int d = 0; d < 5; d++) r.label[d] = gx[(size_t)i * 5 + d];
+    r.chi2 = gc[i];
+    r.iterations = pp[i].max_iters;
+    r.status = status[i];
+    r.time = dt;
+    r.n_params = (int)params[i].size();
+  }
+}
+
+// Plain form: one star at a time, the swarm on the host, one launch per
+// stage per iteration with a device->host round trip of the costs.
+void fit_plain(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result *res,
+               std::vector<std::vector<float>> &params, double *trace) {
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
+  const int S = (int)in.size();
+  params.assign(S, {});
+  for (int si = 0; si < S; si++) {
+    const double t0 = now_s();
+    const StarInput &X = in[si];
+    PsoParams pp = make_pso_params(g, *X.st);
+    const int P = pp.P;
+    StarSet ss;
+    ss.build({X});
+    std::vector<double> x((size_t)P * 5), v((size_t)P * 5), bx, cost(P), bcost(P), gxv(5);
+    double gcost = 0;
+    int status = init_swarm_host(g, pp, X.seed, x.data(), v.data());
+    DBuf<double> dl, dc;
+    DBuf<int> de, ds;
+    dl.alloc((size_t)P * 5);
+    dc.alloc(P);
+    ds.alloc(P);
+    de.upload(std::vector<int>(P, 0));
+    ensure_workspace(g, P);
+    EvalArgs a;
+    a.stars = ss.dstars.p;
+    a.labels = dl.p;
+    a.eval_star = de.p;
+    a.E = P;
+    a.cost = dc.p;
+    a.status = ds.p;
+    a.need_chi2 = 1;
+    a.max_m = width_upper_bound(g, pp.mx[3]);
+    std::vector<int> est(P);
+    auto evaluate = [&]() -> int {
+      CK(cudaMemcpyAsync(dl.p, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      run_evals(g, a, s);
+      CK(cudaMemcpyAsync(cost.data(), dc.p, P * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(est.data(), ds.p, P * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int p = 0; p < P; p++)
+        if (est[p]) return est[p];
+      return 0;
+    };
+    auto dump = [&](int it) {
+      if (!trace || si != 0) return;
+      for (int p = 0; p < P; p++) {
+        double *t = trace + ((size_t)it * P + p) * 6;
+        for (int d = 0; d < 5; d++) t[d] = x[(size_t)p * 5 + d];
+        t[5] = cost[p];
+      }
+    };
+    if (!status) status = evaluate();
+    if (!status) {  // sort by cost (stable), NaN last
+      std::vector<int> idx(P);
+      for (int p = 0; p < P; p++) idx[p] = p;
+      auto key = [&](int p) { return cost[p] != cost[p] ? INFINITY : cost[p]; };
+      std::stable_sort(idx.begin(), idx.end(), [&](int a_, int b_) { return key(a_) < key(b_); });
+      std::vector<double> x2(x.size()), v2(v.size()), c2(P);
+      for (int r = 0; r < P; r++) {
+        for (int d = 0; d < 5; d++) { x2[(size_t)r * 5 + d] = x[(size_t)idx[r] * 5 + d]; v2[(size_t)r * 5 + d] = v[(size_t)idx[r] * 5 + d]; }
+        c2[r] = cost[idx[r]];
+      }
+      x = x2; v = v2; cost = c2;
+      bx = x; bcost = cost;
+      for (int d = 0; d < 5; d++) gxv[d] = x[d];
+      gcost = cost[0];
+      dump(0);
+    }
+    for (int it = 0; it < pp.max_iters && !status; it++) {
+      for (int p = 0; p < P && !status; p++) {
+        for (int d = 0; d < 5; d++) {
+          const double momentum = v[p * 5 + d] * pp.inertia;
+          const double to_opt = bx[p * 5 + d] - x[p * 5 + d];
+          const double pull = (to_opt == 0.0 ? 0.0 : uniform_between(0.0, to_opt, draw_u01(X.seed, PH_ITER, it, p, 2 * d))) * pp.cognitive;
+          const double to_g = gxv[d] - x[p * 5 + d];
+          const double pullg = (to_g == 0.0 ? 0.0 : uniform_between(0.0, to_g, draw_u01(X.seed, PH_ITER, it, p, 2 * d + 1))) * pp.social;
+          v[p * 5 + d] = momentum + pull + pullg;
+          double nx[5];
+          for (int k = 0; k < 5; k++) nx[k] = x[p * 5 + k];
+          nx[d] += v[p * 5 + d];
+          double c;
+          int st = pso_clamp_1d(g->hg, pp, nx, d, c);
+          if (st) { status = st; break; }
+          x[p * 5 + d] = c;
+          if (!pso_within(g->hg, pp, &x[p * 5])) { status = S_BOUNDS; break; }
+        }
+      }
+      if (status) break;
+      status = evaluate();
+      if (status) break;
+      for (int p = 0; p < P; p++) {
+        if (cost[p] < bcost[p]) {
+          for (int d = 0; d < 5; d++) bx[p * 5 + d] = x[p * 5 + d];
+          bcost[p] = cost[p];
+          if (cost[p] < gcost) {
+            for (int d = 0; d < 5; d++) gxv[d] = x[p * 5 + d];
+            gcost = cost[p];
+          }
+        }
+      }
+      dump(it + 1);
+    }
+    std::vector<std::vector<float>> pr;
+    final_refit(g, ss, {X}, gxv, {status == 0 ? 1 : 0}, pr, s);
+    params[si] = pr[0];
+    pasta_fit_result &r = res[si];
+    std::memset(&r, 0, sizeof r);
+    for (int d = 0; d < 5; d++) r.label[d] = gxv[d];
+    r.chi2 = gcost;
+    r.iterations = pp.max_iters;
+    r.status = status;
+    r.time = now_s() - t0;
+    r.n_params = (int)params[si].size();
+  }
+}
+
+}  // namespace
+
+// ================================================================ serving
+struct pasta_server {
+  pasta_grid *g = nullptr;
+  int slots = 0, Pmax = 0;
+  int64_t budget = 0, used = 0;
+  struct Req {
+    int64_t id;
+    const pasta_dispersion *d;
+    const pasta_continuum *c;
+    pasta_pso_settings st;
+    std::vector<float> flux, var;
+    double t_submit;
+    uint64_t seed;
+    int64_t bytes;
+  };
+  std::deque<Req> queue;
+  std::vector<std::unique_ptr<Req>> slot_req;
+  std::vector<std::unique_ptr<DBuf<float>>> slot_flux, slot_var;
+  std::vector<DevStar> hstars;
+  DBuf<DevStar> dstars;
+  SwarmBuffers W;
+  std::vector<PsoParams> pp;
+  struct Done {
+    int64_t id;
+    pasta_fit_result r;
+    std::vector<float> params;
+  };
+  std::deque<Done> done;
+  int64_t next_id = 1;
+  int max_m = 1, graph_max_m = 0;
+  int64_t graph_gen = -1;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  std::mutex mu;
+  ~pasta_server() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+// ================================================================= C ABI
+extern "C" {
+
+int pasta_abi_version(void) { return PASTA_B200_ABI_VERSION; }
+const char *pasta_last_error(void) { return g_last_error.c_str(); }
+int64_t pasta_kernel_launch_count(void) { return kernel_launches(); }
+
+int pasta_set_device(int device) {
+  return guard([&] {
+    CK(cudaSetDevice(device));
+    g_dev = device;
+    ctx();
+  });
+}
+
+// interpolate.rs:267-331 (Grid::new) + model_fetchers.rs:136-166 (column order)
+int pasta_grid_create(const double *labels, const uint16_t *spectra, const float *maxima, int64_t n_models,
+                      int64_t n_px, int wl_kind, double wl_a, double wl_b, const double *wl_values,
+                      pasta_grid **out) {
+  return guard([&] {
+    if (!labels || !spectra || !out || n_models < 1 || n_px < 2) fail(PASTA_E_ARG, "invalid grid arguments");
+    if (wl_kind < 0 || wl_kind > 2) fail(PASTA_E_ARG, "invalid wavelength grid kind");
+    Ctx &C = ctx();
+    std::unique_ptr<pasta_grid> g(new pasta_grid());
+    g->dev = C.dev;
+    auto ins = [](std::vector<double> &v, double x) {
+      if (std::find(v.begin(), v.end(), x) == v.end()) v.insert(std::lower_bound(v.begin(), v.end(), x), x);
+    };
+    for (int64_t i = 0; i < n_models; i++) {
+      for (int k = 0; k < 3; k++)
+        if (labels[3 * i + k] != labels[3 * i + k]) fail(PASTA_E_ARG, "NaN grid label");
+      ins(g->tv, labels[3 * i]);
+      ins(g->mv, labels[3 * i + 1]);
+      ins(g->lv, labels[3 * i + 2]);
+    }
+    const int nt = (int)g->tv.size(), nm = (int)g->mv.size(), nl = (int)g->lv.size();
+    g->llo.assign(nt, nl - 1);
+    g->lhi.assign(nt, 0);
+    auto idx = [](const std::vector<double> &v, double x) {
+      return (int)(std::lower_bound(v.begin(), v.end(), x) - v.begin());
+    };
+    for (int64_t i = 0; i < n_models; i++) {
+      int ti = idx(g->tv, labels[3 * i]), li = idx(g->lv, labels[3 * i + 2]);
+      g->llo[ti] = std::min(g->llo[ti], li);
+      g->lhi[ti] = std::max(g->lhi[ti], li);
+    }
+    for (int i = 0; i < nt; i++)
+      if (g->llo[i] > g->lhi[i]) fail(PASTA_E_ARG, "Invalid logg limits");
+    g->cum.resize(nt);
+    int64_t acc = 0;
+    for (int i = 0; i < nt; i++) { g->cum[i] = acc; acc += g->lhi[i] - g->llo[i] + 1; }
+    g->n_cols = acc * nm;
+    if (g->n_cols != n_models)
+      fail(PASTA_E_ARG, "grid is incomplete: %lld models given, %lld gridpoints expected", (long long)n_models,
+           (long long)g->n_cols);
+    g->npx = n_px;
+    g->stride = (n_px + 63) / 64 * 64;
+    g->hg = GridGeom{g->tv.data(), g->mv.data(), g->lv.data(), g->llo.data(), g->lhi.data(), g->cum.data(), nt, nm, nl};
+    // place each model at its column; rows padded to `stride` with zeros
+    std::vector<int64_t> col(n_models);
+    std::vector<char> seen(g->n_cols, 0);
+    std::vector<float> fac(g->n_cols, 1.0f / 65535.0f);
+    for (int64_t i = 0; i < n_models; i++) {
+      int ti = idx(g->tv, labels[3 * i]), mi = idx(g->mv, labels[3 * i + 1]), li = idx(g->lv, labels[3 * i + 2]);
+      int64_t c = (g->cum[ti] + li - g->llo[ti]) * (int64_t)nm + mi;
+      if (seen[c]) fail(PASTA_E_ARG, "duplicate grid model (%g, %g, %g)", labels[3 * i], labels[3 * i + 1], labels[3 * i + 2]);
+      seen[c] = 1;
+      col[i] = c;
+      if (maxima) {
+        if (maxima[i] < 0.0f) fail(PASTA_E_ARG, "Negative factor: %g", (double)maxima[i]);
+        fac[c] = maxima[i] / 65535.0f;
+      }
+    }
+    g->spectra.alloc((size_t)g->n_cols * g->stride);
+    CK(cudaMemset(g->spectra.p, 0, (size_t)g->n_cols * g->stride * sizeof(uint16_t)));
+    bool in_order = true;
+    for (int64_t i = 0; i < n_models; i++) in_order &= col[i] == i;
+    if (in_order) {
+      CK(cudaMemcpy2D(g->spectra.p, g->stride * sizeof(uint16_t), spectra, n_px * sizeof(uint16_t),
+                      n_px * sizeof(uint16_t), n_models, cudaMemcpyHostToDevice));
+    } else {
+      for (int64_t i = 0; i < n_models; i++)
+        CK(cudaMemcpy(g->spectra.p + (size_t)col[i] * g->stride, spectra + (size_t)i * n_px, n_px * sizeof(uint16_t),
+                      cudaMemcpyHostToDevice));
+    }
+    g->factor.upload(fac);
+    g->dtv.upload(g->tv); g->dmv.upload(g->mv); g->dlv.upload(g->lv);
+    g->dllo.upload(g->llo); g->dlhi.upload(g->lhi); g->dcum.upload(g->cum);
+    g->wl_kind = wl_kind;
+    g->wl_a = wl_a;
+    g->wl_b = wl_b;
+    if (wl_kind == WL_NONUNI) {
+      if (!wl_values) fail(PASTA_E_ARG, "non-uniform grid needs wavelength values");
+      g->wl_vals.assign(wl_values, wl_values + n_px);
+      g->dwl.upload(g->wl_vals);
+    }
+    DevGrid &d = g->d;
+    d.g = GridGeom{g->dtv.p, g->dmv.p, g->dlv.p, g->dllo.p, g->dlhi.p, g->dcum.p, nt, nm, nl};
+    d.spectra = g->spectra.p;
+    d.factor = g->factor.p;
+    d.stride = g->stride;
+    d.npx = (int)n_px;
+    d.tail_start = (int)(n_px - n_px % 128);
+    d.wl_kind = wl_kind;
+    d.wl_a = wl_a;
+    d.wl_b = wl_b;
+    d.wl_vals = g->dwl.p;
+    if (wl_kind == WL_LIN) { d.synth_first = wl_a; d.synth_last = wl_a + wl_b * (double)n_px; }
+    else if (wl_kind == WL_LOG) { d.synth_first = std::pow(10.0, wl_a); d.synth_last = std::pow(10.0, wl_a + wl_b * (double)n_px); }
+    else { d.synth_first = wl_values[0]; d.synth_last = wl_values[n_px - 1]; }
+    if (wl_kind == WL_LIN) d.dvelo = wl_b / ((wl_a + wl_a + wl_b * (double)n_px) / 2.0);
+    else if (wl_kind == WL_LOG) d.dvelo = M_LN10 * wl_b;
+    else d.dvelo = 0.0;
+    *out = g.release();
+  });
+}
+
+int pasta_grid_destroy(pasta_grid *g) {
+  return guard([&] {
+    if (!g) return;
+    CK(cudaSetDevice(g->dev));
+    CK(cudaDeviceSynchronize());
+    delete g;
+  });
+}
+
+int pasta_grid_shape(const pasta_grid *g, int64_t *o) {
+  return guard([&] {
+    o[0] = (int64_t)g->tv.size(); o[1] = (int64_t)g->mv.size(); o[2] = (int64_t)g->lv.size();
+    o[3] = g->npx; o[4] = g->n_cols;
+  });
+}
+int pasta_grid_axis(const pasta_grid *g, int axis, double *out) {
+  return guard([&] {
+    const auto &v = axis == 0 ? g->tv : axis == 1 ? g->mv : g->lv;
+    std::copy(v.begin(), v.end(), out);
+  });
+}
+int pasta_grid_logg_limits(const pasta_grid *g, int64_t *lo, int64_t *hi) {
+  return guard([&] {
+    for (size_t i = 0; i < g->llo.size(); i++) { lo[i] = g->llo[i]; hi[i] = g->lhi[i]; }
+  });
+}
+int pasta_grid_cumulative_size(const pasta_grid *g, int64_t *out) {
+  return guard([&] { std::copy(g->cum.begin(), g->cum.end(), out); });
+}
+int pasta_grid_clamp_1d(const pasta_grid *g, double t, double m, double lg, int index, double *out) {
+  return guard([&] {
+    if (index < 0 || index > 2) fail(PASTA_E_ARG, "Index out of bounds %d", index);
+    double p[3] = {t, m, lg}, lo, hi;
+    int st = grid_limits_at(g->hg, p, index, lo, hi);
+    if (st) fail(PASTA_E_OUT_OF_GRID, index == 0 ? "Cannot clamp teff at logg=%g" : "Cannot clamp logg at Teff=%g",
+                 index == 0 ? lg : t);
+    if (!(lo <= hi)) fail(PASTA_E_CLAMP, "clamp limits invalid");
+    double x = p[index];
+    *out = x < lo ? lo : (x > hi ? hi : x);
+  });
+}
+int pasta_grid_is_teff_logg_between_bounds(const pasta_grid *g, double t, double lg, int *out) {
+  return guard([&] { *out = teff_logg_ok(g->hg, t, lg) ? 1 : 0; });
+}
+int pasta_grid_coefficients(const pasta_grid *g, double t, double m, double lg, int64_t *cols64, float *w64,
+                            double *t16, double *l16, double *m4) {
+  return guard([&] {
+    int cols[64];
+    float w[64];
+    double ft[16], fl[16], fm[4];
+    int st = local_grid(g->hg, t, m, lg, cols, w, ft, fl, fm);
+    if (st) fail(st == S_NAN ? PASTA_E_NAN : st == S_OUT_OF_GRID ? PASTA_E_OUT_OF_GRID : PASTA_E_NEIGHBORS,
+                 "%s (%g, %g, %g)", status_message(st), t, m, lg);
+    for (int i = 0; i < 64; i++) {
+      if (cols64) cols64[i] = cols[i];
+      if (w64) w64[i] = w[i];
+    }
+    if (t16) std::copy(ft, ft + 16, t16);
+    if (l16) std::copy(fl, fl + 16, l16);
+    if (m4) std::copy(fm, fm + 4, m4);
+  });
+}
+
+// -------------------------------------------------------- dispersions
+int pasta_dispersion_create(int synth_kind, double synth_a, double synth_b, int64_t synth_n,
+                            const double *synth_values, int kind, const double *wl_obs, int64_t n_obs,
+                            double resolution, const float *disp, pasta_dispersion **out) {
+  return guard([&] {
+    if (!wl_obs || n_obs < 1 || !out) fail(PASTA_E_ARG, "invalid dispersion arguments");
+    ctx();
+    std::unique_ptr<pasta_dispersion> d(new pasta_dispersion());
+    d->kind = kind;
+    d->synth_kind = synth_kind;
+    d->synth_a = synth_a;
+    d->synth_b = synth_b;
+    d->synth_n = synth_n;
+    if (synth_kind == WL_NONUNI) d->synth_vals.assign(synth_values, synth_values + synth_n);
+    d->wl.assign(wl_obs, wl_obs + n_obs);
+    d->fidx.resize(n_obs);
+    for (int64_t i = 0; i < n_obs; i++)
+      d->fidx[i] = wl_float_index(synth_kind, synth_a, synth_b, d->synth_vals, wl_obs[i]);
+    d->wl_first = d->wl.front();
+    d->wl_last = d->wl.back();
+    d->wl_min = *std::min_element(d->wl.begin(), d->wl.end());
+    d->wl_max = *std::max_element(d->wl.begin(), d->wl.end());
+    d->fidx_min = *std::min_element(d->fidx.begin(), d->fidx.end());
+    d->fidx_max = *std::max_element(d->fidx.begin(), d->fidx.end());
+    const auto &vals = d->synth_vals;
+    if (kind == PASTA_DISP_NONE) {
+      d->dev_kind = DISP_NONE;
+    } else if (kind == PASTA_DISP_FIXED) {
+      if (resolution <= 0.0) fail(PASTA_E_ARG, "Resolution must be positive");
+      if (synth_kind == WL_LOG) {  // convolve_rv.rs:169-196
+        double sigma = 1.0 / (M_LN10 * 2.355 * resolution * synth_b);
+        int n = odd_width(6.0 * sigma);
+        if (n > 2 * 255 + 1) fail(PASTA_E_UNSUPPORTED, "instrument kernel of %d taps exceeds the supported 511", n);
+        d->gk.assign(n, 0.0f);
+        make_gaussian(d->gk.data(), n, (float)sigma);
+        d->gw = n;
+        d->dev_kind = DISP_FIXED;
+      } else {  // convolve_rv.rs:244-287
+        std::vector<float> sig(synth_n);
+        for (int64_t i = 0; i < synth_n; i++) {
+          if (synth_kind == WL_LIN) sig[i] = (float)(wl_at(synth_kind, synth_a, synth_b, vals, i) / (resolution * synth_b * 2.355));
+          else if (i == 0 || i == synth_n - 1) sig[i] = 2.0f;
+          else sig[i] = (float)(vals[i] / (resolution * ((vals[i + 1] - vals[i - 1]) / 2.0) * 2.355));
+        }
+        disp_per_pixel(d.get(), sig);
+      }
+    } else if (kind == PASTA_DISP_VARIABLE) {  // convolve_rv.rs:350-402
+      if (!disp) fail(PASTA_E_ARG, "variable dispersion needs disp values");
+      const size_t L = d->wl.size();
+      std::vector<float> dr(synth_n);
+      size_t j = 0;
+      for (int64_t i = 0; i < synth_n; i++) {  // resample_observed_to_synth (convolve_rv.rs:303-331)
+        double x = wl_at(synth_kind, synth_a, synth_b, vals, i);
+        while (j < L - 1 && d->wl[j + 1] < x) j++;
+        if (j == L - 1) dr[i] = disp[j];
+        else {
+          float w = (float)((x - d->wl[j]) / (d->wl[j + 1] - d->wl[j]));
+          dr[i] = (1.0f - w) * disp[j] + w * disp[j + 1];
+        }
+      }
+      std::vector<float> sig(synth_n);
+      for (int64_t i = 0; i < synth_n; i++) {
+        if (synth_kind == WL_LOG) sig[i] = dr[i] / (float)(synth_b * M_LN10 * wl_at(synth_kind, synth_a, synth_b, vals, i));
+        else if (synth_kind == WL_LIN) sig[i] = dr[i] / (float)synth_b;
+        else if (i == 0 || i == synth_n - 1) sig[i] = 2.0f;
+        else sig[i] = dr[i] / (float)((vals[i + 1] - vals[i - 1]) / 2.0);
+      }
+      disp_per_pixel(d.get(), sig);
+    } else {
+      fail(PASTA_E_ARG, "invalid dispersion kind %d", kind);
+    }
+    d->dfidx.upload(d->fidx);
+    d->dwl.upload(d->wl);
+    if (!d->gk.empty()) d->dgk.upload(d->gk);
+    *out = d.release();
+  });
+}
+int pasta_dispersion_destroy(pasta_dispersion *d) {
+  return guard([&] { delete d; });
+}
+int pasta_dispersion_kernels(const pasta_dispersion *d, int64_t *width, float *out) {
+  return guard([&] {
+    *width = d->gw;
+    if (out && d->dev_kind == DISP_PIXEL) {  // width x n_synth row-major
+      for (int64_t i = 0; i < d->synth_n; i++)
+        for (int t = 0; t < d->gw; t++) out[(size_t)t * d->synth_n + i] = d->gk[(size_t)i * d->gw + t];
+    } else if (out && d->dev_kind == DISP_FIXED) {
+      std::copy(d->gk.begin(), d->gk.end(), out);
+    }
+  });
+}
+
+// --------------------------------------------------------- continuum
+int pasta_continuum_create(int kind, const double *wl, int64_t n, int n_chunks, int p_order, double overlap,
+                           const float *design, int k, const float *continuum, int ignore,
+                           pasta_continuum **out) {
+  return guard([&] {
+    if (!out) fail(PASTA_E_ARG, "null output");
+    ctx();
+    std::unique_ptr<pasta_continuum> c(new pasta_continuum());
+    c->kind = kind;
+    c->n = n;
+    if (kind == PASTA_CONT_CHUNK) {
+      if (!wl) fail(PASTA_E_ARG, "chunk fitter needs wavelengths");
+      chunk_setup(c.get(), wl, n_chunks, p_order, overlap);
+      c->dcs.upload(c->cstart);
+      c->dce.upload(c->cstop);
+      c->dxa.upload(c->xa);
+      c->dxb.upload(c->xb);
+      c->dfac.upload(c->fac);
+      c->dchol.upload(c->chol);
+    } else if (kind == PASTA_CONT_LINEAR) {
+      if (!design) fail(PASTA_E_ARG, "linear fitter needs a design matrix");
+      linear_setup(c.get(), design, k);
+      c->dq.upload(c->qcol);
+    } else if (kind == PASTA_CONT_FIXED) {
+      if (!continuum) fail(PASTA_E_ARG, "fixed continuum needs values");
+      c->cont.assign(continuum, continuum + n);
+      c->ignore = ignore;
+      if (n - 2 * (int64_t)ignore <= 0) { c->bad = 1; c->bad_msg = "ignore_first_and_last too large"; }
+      c->dcont.upload(c->cont);
+    } else if (kind != PASTA_CONT_CONSTANT) {
+      fail(PASTA_E_ARG, "invalid continuum kind %d", kind);
+    }
+    *out = c.release();
+  });
+}
+int pasta_continuum_destroy(pasta_continuum *c) {
+  return guard([&] { delete c; });
+}
+int pasta_continuum_nparams(const pasta_continuum *c) { return cont_nparams(c); }
+
+// ContinuumFitter::fit_continuum on a given model (lib.rs:862-874)
+int pasta_continuum_fit(const pasta_continuum *c, const float *model, const float *flux, const float *var, int64_t n,
+                        float *params, double *chi2) {
+  return guard([&] {
+    if (c->kind != PASTA_CONT_CONSTANT && n != c->n)
+      fail(PASTA_E_ARG, "Length of observed and synthetic spectrum are different %lld, %lld", (long long)n, (long long)c->n);
+    if (c->bad) fail(PASTA_E_CONTINUUM, "%s", c->bad_msg.c_str());
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    DBuf<float> dm, df, dv;
+    dm.upload(model, n);
+    df.upload(flux, n);
+    dv.upload(var, n);
+    DevStar st = make_star(nullptr, c, df.p, dv.p, n);
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    EvalPrep ep{};
+    DBuf<EvalPrep> dp;
+    dp.upload(&ep, 1);
+    DBuf<double> dc, dpar;
+    DBuf<int> dst;
+    dc.alloc(1);
+    dst.alloc(1);
+    const int ps = device_param_stride(c);
+    dpar.alloc(ps);
+    EvalBatch b{};
+    b.E = 1;
+    b.stars = ds.p;
+    b.prep = dp.p;
+    b.cost = dc.p;
+    b.status = dst.p;
+    b.params = dpar.p;
+    b.param_stride = ps;
+    DevGrid G{};
+    launch_chi2_given(G, b, dm.p, s);
+    CK(cudaGetLastError());
+    double hc;
+    int hs;
+    std::vector<double> hp(ps);
+    CK(cudaMemcpyAsync(&hc, dc.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&hs, dst.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hp.data(), dpar.p, ps * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hs) fail(PASTA_E_CONTINUUM, "%s", status_message(hs));
+    auto pv = params_from_device(c, hp.data());
+    if (params) std::copy(pv.begin(), pv.end(), params);
+    *chi2 = hc;
+  });
+}
+
+// ContinuumFitter::build_continuum (lib.rs:927-939)
+int pasta_continuum_build(const pasta_continuum *c, const float *params, int64_t np, float *out) {
+  return guard([&] {
+    if (np != cont_nparams(c))
+      fail(PASTA_E_ARG, "Incorrect number of continuum parameters: %lld, expected: %d", (long long)np, cont_nparams(c));
+    if (c->kind == PASTA_CONT_CONSTANT) { out[0] = params[0]; return; }
+    if (c->kind == PASTA_CONT_FIXED) { std::copy(c->cont.begin(), c->cont.end(), out); return; }
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    if (c->kind == PASTA_CONT_LINEAR) {  // D * params with D = Q R
+      const int k = c->k;
+      std::vector<double> z(k, 0.0);
+      for (int j = 0; j < k; j++)
+        for (int l = j; l < k; l++) z[j] += c->R[(size_t)j * k + l] * (double)params[l];
+      for (int64_t i = 0; i < c->n; i++) {
+        double s2 = 0.0;
+        for (int j = 0; j < k; j++) s2 += (double)c->qcol[(size_t)j * c->n + i] * z[j];
+        out[i] = (float)s2;
+      }
+      return;
+    }
+    // chunk: monomial -> Legendre coefficients, then the device blend
+    const int p1 = c->p1;
+    auto T = legendre_to_monomial(p1);
+    std::vector<double> coef((size_t)c->nc * MAX_P1, 0.0);
+    for (int ch = 0; ch < c->nc; ch++) {
+      // solve T^T l = a (upper triangular in the column index)
+      std::vector<double> a(p1), l(p1);
+      for (int j = 0; j < p1; j++) a[j] = params[ch * p1 + j];
+      for (int k = p1 - 1; k >= 0; k--) {
+        double s2 = a[k];
+        for (int kk = k + 1; kk < p1; kk++) s2 -= T[(size_t)kk * p1 + k] * l[kk];
+        l[k] = s2 / T[(size_t)k * p1 + k];
+      }
+      for (int k = 0; k < p1; k++) coef[(size_t)ch * MAX_P1 + k] = l[k];
+    }
+    DevStar st = make_star(nullptr, c, nullptr, nullptr, c->n);
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    DBuf<double> dcoef;
+    dcoef.upload(coef);
+    DBuf<float> dout;
+    dout.alloc(c->n);
+    launch_build_chunk(ds.p, dcoef.p, (int)c->n, dout.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout.p, c->n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  });
+}
+
+// ----------------------------------------------------- model / chi2
+static int run_label_batch(const pasta_grid *gc, const pasta_dispersion *d, const pasta_continuum *c,
+                           const float *flux, const float *var, int64_t n, const double *labels, int ncols,
+                           int64_t L, float *out_obs, float *out_synth, double *out_chi2, int32_t *status,
+                           int full_window, int no_rotation) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(gc);
+    if (L < 0) fail(PASTA_E_ARG, "negative label count");
+    if (L == 0) return;
+    check_disp_grid(g, d);
+    if (d && c && c->kind != PASTA_CONT_CONSTANT && c->n != (int64_t)d->wl.size())
+      fail(PASTA_E_ARG, "continuum fitter and dispersion have different lengths");
+    if (c && flux && n != (int64_t)d->wl.size())
+      fail(PASTA_E_ARG, "Observed spectrum and target dispersion must have the same length");
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    std::lock_guard<std::mutex> lk(g->mu);
+    std::vector<double> lab((size_t)L * 5, 0.0);
+    double vmax = 0.0;
+    for (int64_t i = 0; i < L; i++) {
+      for (int k = 0; k < ncols; k++) lab[(size_t)i * 5 + k] = labels[(size_t)i * ncols + k];
+      if (no_rotation) lab[(size_t)i * 5 + 3] = 0.0;
+      double v = lab[(size_t)i * 5 + 3];
+      if (v > vmax) vmax = v;
+    }
+    DBuf<float> df, dv;
+    const int64_t nobs = d ? (int64_t)d->wl.size() : 0;
+    if (flux) { df.upload(flux, n); dv.upload(var, n); }
+    DevStar st = make_star(d, c, df.p, dv.p, nobs);
+    if (!d) { st.disp_kind = DISP_NONE; }
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    DBuf<double> dl, dc;
+    DBuf<int> de, dst;
+    dl.upload(lab);
+    de.upload(std::vector<int>(L, 0));
+    dc.alloc(L);
+    dst.alloc(L);
+    DBuf<float> dout;
+    EvalArgs a;
+    a.stars = ds.p;
+    a.labels = dl.p;
+    a.eval_star = de.p;
+    a.E = L;
+    a.cost = dc.p;
+    a.status = dst.p;
+    a.need_chi2 = out_chi2 ? 1 : 0;
+    a.full_window = full_window;
+    a.max_m = width_upper_bound(g, vmax);
+    if (out_obs) { dout.alloc((size_t)L * nobs); a.out_obs = dout.p; a.out_stride = nobs; }
+    if (out_synth) { dout.alloc((size_t)L * g->npx); a.out_synth = dout.p; }
+    ensure_workspace(g, L);
+    run_evals(g, a, s);
+    std::vector<int> hst(L, 0);
+    CK(cudaMemcpyAsync(hst.data(), dst.p, L * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (out_chi2) {
+      std::vector<double> hc(L);
+      CK(cudaMemcpyAsync(hc.data(), dc.p, L * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int64_t i = 0; i < L; i++) out_chi2[i] = hst[i] ? NAN : hc[i];
+    }
+    CK(cudaStreamSynchronize(s));
+    if (status)
+      for (int64_t i = 0; i < L; i++) status[i] = hst[i];
+    if (out_obs) {
+      CK(cudaMemcpyAsync(out_obs, dout.p, (size_t)L * nobs * sizeof(float), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int64_t i = 0; i < L; i++)
+        if (hst[i]) std::fill(out_obs + i * nobs, out_obs + (i + 1) * nobs, NAN);
+    }
+    if (out_synth) {
+      CK(cudaMemcpyAsync(out_synth, dout.p, (size_t)L * g->npx * sizeof(float), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int64_t i = 0; i < L; i++)
+        if (hst[i]) std::fill(out_synth + i * g->npx, out_synth + (i + 1) * g->npx, NAN);
+    }
+  });
+}
+
+int pasta_interpolate(const pasta_grid *g, const double *tml, int64_t L, float *out, int32_t *status) {
+  return run_label_batch(g, nullptr, nullptr, nullptr, nullptr, 0, tml, 3, L, nullptr, out, nullptr, status, 1, 1);
+}
+int pasta_interpolate_and_convolve(const pasta_grid *g, const pasta_dispersion *d, const double *labels, int64_t L,
+                                   float *out, int32_t *status) {
+  return run_label_batch(g, d, nullptr, nullptr, nullptr, 0, labels, 4, L, nullptr, out, nullptr, status, 1, 0);
+}
+int pasta_produce_model(const pasta_grid *g, const pasta_dispersion *d, const double *labels, int64_t L, float *out,
+                        int32_t *status) {
+  if (!d) { g_last_error = "dispersion required"; return PASTA_E_ARG; }
+  return run_label_batch(g, d, nullptr, nullptr, nullptr, 0, labels, 5, L, out, nullptr, nullptr, status, 0, 0);
+}
+int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c, const float *flux,
+               const float *var, int64_t n, const double *labels, int64_t L, double *out, int32_t *status) {
+  if (!d || !c || !flux || !var) { g_last_error = "dispersion, continuum and data required"; return PASTA_E_ARG; }
+  return run_label_batch(g, d, c, flux, var, n, labels, 5, L, nullptr, nullptr, out, status, 0, 0);
+}
+
+int pasta_dispersion_convolve(const pasta_dispersion *d, const float *in, int64_t n, float *out) {
+  return guard([&] {
+    if (n != d->synth_n)
+      fail(PASTA_E_ARG, "flux_arr and wavelength grid don't match. flux_arr: %lld, synth_wl: %lld", (long long)n,
+           (long long)d->synth_n);
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    DBuf<float> di, dout;
+    di.upload(in, n);
+    dout.alloc(n);
+    DevStar st = make_star(d, nullptr, nullptr, nullptr, 0);
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    DevGrid G{};
+    G.npx = (int)n;
+    launch_gauss_standalone(G, ds.p, di.p, dout.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  });
+}
+
+// ------------------------------------------------------------- fit
+static int fit_common(const pasta_grid *gc, std::vector<StarInput> &in, int mode, pasta_fit_result *results,
+                      float *const *params, double *trace) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(gc);
+    if (in.empty()) return;
+    for (auto &s : in) validate_star(g, s);
+    std::lock_guard<std::mutex> lk(g->mu);
+    std::vector<std::vector<float>> pv;
+    if (mode == PASTA_FIT_PLAIN) fit_plain(g, in, results, pv, trace);
+    else fit_batched(g, in, results, pv, trace);
+    for (size_t i = 0; i < in.size(); i++)
+      if (params && params[i]) std::copy(pv[i].begin(), pv[i].end(), params[i]);
+  });
+}
+
+int pasta_fit(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c,
+              const pasta_pso_settings *settings, const float *flux, const float *var, int64_t n, int64_t S,
+              const uint64_t *seeds, int mode, pasta_fit_result *results, float *params, double *trace) {
+  std::vector<StarInput> in(S);
+  std::vector<float *> pp(S);
+  const int np = c ? cont_nparams(c) : 1;
+  for (int64_t i = 0; i < S; i++) {
+    in[i] = StarInput{d, c, settings, flux + (size_t)i * n, var + (size_t)i * n, n, seeds[i]};
+    pp[i] = params ? params + (size_t)i * np : nullptr;
+  }
+  return fit_common(g, in, mode, results, pp.data(), trace);
+}
+
+int pasta_fit_many(const pasta_grid *g, int64_t S, const pasta_dispersion *const *d, const pasta_continuum *const *c,
+                   const pasta_pso_settings *settings, const float *const *flux, const float *const *var,
+                   const int64_t *n, const uint64_t *seeds, int mode, pasta_fit_result *results,
+                   float *const *params) {
+  std::vector<StarInput> in(S);
+  for (int64_t i = 0; i < S; i++) in[i] = StarInput{d[i], c[i], &settings[i], flux[i], var[i], n[i], seeds[i]};
+  return fit_common(g, in, mode, results, params, nullptr);
+}
+
+// ------------------------------------------------------------ serving
+int pasta_server_create(const pasta_grid *gc, int max_slots, int64_t hbm_budget_bytes, pasta_server **out) {
+  return guard([&] {
+    if (max_slots < 1) fail(PASTA_E_ARG, "max_slots must be >= 1");
+    ctx();
+    std::unique_ptr<pasta_server> sv(new pasta_server());
+    sv->g = const_cast<pasta_grid *>(gc);
+    sv->slots = max_slots;
+    sv->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t)1 << 40;
+    sv->slot_req.resize(max_slots);
+    sv->slot_flux.resize(max_slots);
+    sv->slot_var.resize(max_slots);
+    sv->hstars.assign(max_slots, DevStar{});
+    sv->pp.assign(max_slots, PsoParams{});
+    *out = sv.release();
+  });
+}
+
+int pasta_server_submit(pasta_server *sv, const pasta_dispersion *d, const pasta_continuum *c,
+                        const pasta_pso_settings *settings, const float *flux, const float *var, int64_t n,
+                        uint64_t seed, int64_t *request_id) {
+  return guard([&] {
+    StarInput si{d, c, settings, flux, var, n, seed};
+    validate_star(sv->g, si);
+    make_pso_params(sv->g, *settings);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    pasta_server::Req r;
+    r.id = sv->next_id++;
+    r.d = d;
+    r.c = c;
+    r.st = *settings;
+    r.flux.assign(flux, flux + n);
+    r.var.assign(var, var + n);
+    r.t_submit = now_s();
+    r.seed = seed;
+    r.bytes = n * 8 + (int64_t)settings->num_particles * 200;
+    sv->queue.push_back(std::move(r));
+    if (request_id) *request_id = sv->queue.back().id;
+  });
+}
+
+namespace {
+
+void server_rebuild(pasta_server *sv, int Pmax) {
+  // (re)allocate slot swarm arrays for a larger particle count; only when empty
+  sv->Pmax = Pmax;
+  sv->W.alloc(sv->slots, Pmax);
+  std::vector<int> z(sv->slots, 0), done1(sv->slots, 1), im(sv->slots, -1);
+  CK(cudaMemcpy(sv->W.active.p, z.data(), z.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sv->W.done.p, done1.data(), z.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sv->W.status.p, z.data(), z.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sv->W.iter.p, im.data(), z.size() * sizeof(int), cudaMemcpyHostToDevice));
+  sv->pp.assign(sv->slots, PsoParams{});
+  sv->W.params.upload(sv->pp);
+  sv->dstars.upload(sv->hstars);
+  if (sv->exec) { cudaGraphExecDestroy(sv->exec); sv->exec = nullptr; }
+  if (sv->graph) { cudaGraphDestroy(sv->graph); sv->graph = nullptr; }
+}
+
+}  // namespace
+
+int pasta_server_step(pasta_server *sv) {
+  int active_after = 0;
+  int rc = guard([&] {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    pasta_grid *g = sv->g;
+    std::lock_guard<std::mutex> lg(g->mu);
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    bool any_active = false;
+    for (int i = 0; i < sv->slots; i++) any_active |= (bool)sv->slot_req[i];
+    // grow the particle capacity when the device loop is idle
+    int needP = sv->Pmax;
+    for (auto &r : sv->queue) needP = std::max(needP, r.st.num_particles);
+    if (needP != sv->Pmax && !any_active) server_rebuild(sv, needP);
+    // admit queued requests into free slots within the HBM budget
+    std::vector<int> admitted;
+    for (int i = 0; i < sv->slots && !sv->queue.empty(); i++) {
+      if (sv->slot_req[i]) continue;
+      auto &r = sv->queue.front();
+      if (r.st.num_particles > sv->Pmax) break;
+      if (sv->used + r.bytes > sv->budget && any_active) break;
+      std::unique_ptr<pasta_server::Req> rp(new pasta_server::Req(std::move(r)));
+      sv->queue.pop_front();
+      sv->used += rp->bytes;
+      sv->slot_flux[i].reset(new DBuf<float>());
+      sv->slot_var[i].reset(new DBuf<float>());
+      sv->slot_flux[i]->upload(rp->flux);
+      sv->slot_var[i]->upload(rp->var);
+      sv->hstars[i] = make_star(rp->d, rp->c, sv->slot_flux[i]->p, sv->slot_var[i]->p, (int64_t)rp->flux.size());
+      PsoParams P = make_pso_params(g, rp->st);
+      sv->pp[i] = P;
+      sv->max_m = std::max(sv->max_m, width_upper_bound(g, P.mx[3]));
+      std::vector<double> x((size_t)sv->Pmax * 5, 0.0), v((size_t)sv->Pmax * 5, 0.0);
+      int st = init_swarm_host(g, P, rp->seed, x.data(), v.data());
+      const size_t base = (size_t)i * sv->Pmax * 5;
+      CK(cudaMemcpyAsync(sv->W.x.p + base, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->W.v.p + base, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      int one = 1, zero = 0, m1 = -1, done0 = st ? 1 : 0;
+      uint64_t sd = rp->seed;
+      CK(cudaMemcpyAsync(sv->W.active.p + i, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->W.done.p + i, &done0, sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->W.status.p + i, st ? &st : &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->W.iter.p + i, &m1, sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->W.seed.p + i, &sd, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->W.params.p + i, &P, sizeof(PsoParams), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->dstars.p + i, &sv->hstars[i], sizeof(DevStar), cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+      sv->slot_req[i] = std::move(rp);
+      admitted.push_back(i);
+    }
+    bool any = false;
+    for (int i = 0; i < sv->slots; i++) any |= (bool)sv->slot_req[i];
+    if (!any) return;
+    const int64_t E = (int64_t)sv->slots * sv->Pmax;
+    ensure_workspace(g, E);
+    Swarm sw = sv->W.view();
+    EvalArgs a;
+    a.stars = sv->dstars.p;
+    a.labels = sv->W.labels.p;
+    a.eval_star = sv->W.eval_star.p;
+    a.eval_active = sv->W.eval_active.p;
+    a.E = E;
+    a.cost = sv->W.ecost.p;
+    a.status = sv->W.estatus.p;
+    a.need_chi2 = 1;
+    a.max_m = sv->max_m;
+    if (sv->exec && (sv->graph_max_m < sv->max_m || sv->graph_gen != g->ws.gen)) {
+      // a wider rotation kernel was admitted, or the workspace moved
+      cudaGraphExecDestroy(sv->exec);
+      cudaGraphDestroy(sv->graph);
+      sv->exec = nullptr;
+      sv->graph = nullptr;
+    }
+    if (!sv->exec) {
+      sv->graph_max_m = sv->max_m;
+      sv->graph_gen = g->ws.gen;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      launch_pso_update(g->d, sw, s);
+      run_evals(g, a, s);
+      launch_pso_best(sw, sv->W.ecost.p, sv->W.estatus.p, s);
+      CK(cudaStreamEndCapture(s, &sv->graph));
+      CK(cudaGraphInstantiate(&sv->exec, sv->graph, 0));
+    }
+    CK(cudaGraphLaunch(sv->exec, s));
+    std::vector<int> done(sv->slots), status(sv->slots);
+    CK(cudaMemcpyAsync(done.data(), sv->W.done.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(status.data(), sv->W.status.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // retire finished requests: final refit for their params, free the slot
+    std::vector<int> fin;
+    for (int i = 0; i < sv->slots; i++)
+      if (sv->slot_req[i] && done[i]) fin.push_back(i);
+    if (!fin.empty()) {
+      std::vector<double> gx((size_t)sv->slots * 5), gc(sv->slots);
+      CK(cudaMemcpyAsync(gx.data(), sv->W.gx.p, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(gc.data(), sv->W.gcost.p, gc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      std::vector<StarInput> in;
+      std::vector<double> best;
+      std::vector<int> ok;
+      StarSet ss;
+      ss.h.clear();
+      std::vector<DevStar> hs;
+      for (int i : fin) {
+        auto &r = *sv->slot_req[i];
+        in.push_back(StarInput{r.d, r.c, &r.st, r.flux.data(), r.var.data(), (int64_t)r.flux.size(), r.seed});
+        hs.push_back(sv->hstars[i]);
+        for (int d = 0; d < 5; d++) best.push_back(gx[(size_t)i * 5 + d]);
+        ok.push_back(status[i] == 0 ? 1 : 0);
+      }
+      ss.dstars.upload(hs);
+      std::vector<std::vector<float>> params;
+      final_refit(g, ss, in, best, ok, params, s);
+      const double tnow = now_s();
+      for (size_t q = 0; q < fin.size(); q++) {
+        const int i = fin[q];
+        auto &r = *sv->slot_req[i];
+        pasta_server::Done dn;
+        dn.id = r.id;
+        std::memset(&dn.r, 0, sizeof dn.r);
+        for (int d = 0; d < 5; d++) dn.r.label[d] = gx[(size_t)i * 5 + d];
+        dn.r.chi2 = gc[i];
+        dn.r.iterations = r.st.max_iters;
+        dn.r.status = status[i];
+        dn.r.time = tnow - r.t_submit;
+        dn.params = params[q];
+        dn.r.n_params = (int)dn.params.size();
+        sv->done.push_back(std::move(dn));
+        sv->used -= r.bytes;
+        sv->slot_req[i].reset();
+        int zero = 0;
+        CK(cudaMemcpyAsync(sv->W.active.p + i, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+      }
+      CK(cudaStreamSynchronize(s));
+      for (int i : fin) { sv->slot_flux[i].reset(); sv->slot_var[i].reset(); }
+    }
+    for (int i = 0; i < sv->slots; i++) active_after += sv->slot_req[i] ? 1 : 0;
+  });
+  return rc ? rc : active_after;
+}
+
+int pasta_server_poll(pasta_server *sv, int64_t *ids, pasta_fit_result *results, float *params, int64_t pstride,
+                      int max, int *n_out) {
+  return guard([&] {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    int k = 0;
+    while (k < max && !sv->done.empty()) {
+      auto &d = sv->done.front();
+      if (ids) ids[k] = d.id;
+      if (results) results[k] = d.r;
+      if (params) std::copy(d.params.begin(), d.params.begin() + std::min<int64_t>(pstride, d.params.size()),
+                            params + (size_t)k * pstride);
+      sv->done.pop_front();
+      k++;
+    }
+    *n_out = k;
+  });
+}
+
+int pasta_server_pending(const pasta_server *sv, int64_t *queued, int64_t *active, int64_t *done) {
+  return guard([&] {
+    pasta_server *s = const_cast<pasta_server *>(sv);
+    std::lock_guard<std::mutex> lk(s->mu);
+    int64_t a = 0;
+    for (auto &r : s->slot_req) a += r ? 1 : 0;
+    if (queued) *queued = (int64_t)s->queue.size();
+    if (active) *active = a;
+    if (done) *done = (int64_t)s->done.size();
+  });
+}
+
+int pasta_server_destroy(pasta_server *sv) {
+  return guard([&] {
+    if (!sv) return;
+    ctx();
+    CK(cudaDeviceSynchronize());
+    delete sv;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// fft.cuh -- shared-memory complex FFT of 2048 points for one 256-thread CTA.
+//
+// Stockham autosort (Govindaraju et al., "High performance discrete Fourier
+// transforms on graphics processors", SC 2008) with radices 8, 8, 8, 4.
+// Data live in shared memory as separate real/imaginary float arrays with
+// one pad word every 32 entries, which keeps the strided stage reads and
+// the first stages' scattered writes off a single bank.  Twiddles
+// W_2048^k = exp(-2 pi i k / 2048) come from a table the host computed in
+// double.  Forward is unnormalised; the inverse is unnormalised too
+// (caller scales by 1/2048, like convolve_rv.rs:153-154).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace pb {
+
+constexpr int FFT_T = 256;
+constexpr int FFT_SM = 2048 + 64;
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 5); }
+
+struct cf {
+  float x, y;
+};
+__device__ __forceinline__ cf cmul(cf a, cf b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+__device__ __forceinline__ cf cadd(cf a, cf b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ cf csub(cf a, cf b) { return {a.x - b.x, a.y - b.y}; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ cf rot90(cf a) {
+  return INV ? cf{-a.y, a.x} : cf{a.y, -a.x};
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(cf &v0, cf &v1, cf &v2, cf &v3) {
+  cf t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = rot90<INV>(csub(v1, v3));
+  v0 = cadd(t0, t2);
+  v2 = csub(t0, t2);
+  v1 = cadd(t1, t3);
+  v3 = csub(t1, t3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(cf v[8]) {
+  cf e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  cf o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<INV>(e0, e1, e2, e3);
+  dft4<INV>(o0, o1, o2, o3);
+  const float c = 0.70710678118654752f;
+  o1 = cmul(o1, cf{c, INV ? c : -c});
+  o2 = rot90<INV>(o2);
+  o3 = cmul(o3, cf{-c, INV ? c : -c});
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+// One Stockham stage of radix R at sub-transform length Ns.  All reads of
+// the stage happen before a barrier, all writes after it, so the transform
+// runs in place.  The caller must __syncthreads() after filling the input.
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const float2 *__restrict__ tw) {
+  constexpr int N = 2048, J = N / R, PER = J / FFT_T;
+  cf v[PER][R];
+  const int step = N / (Ns * R);
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int j = threadIdx.x + q * FFT_T;
+    const int jm = j & (Ns - 1);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int a = pidx(j + r * J);
+      cf x = {re[a], im[a]};
+      if (r > 0 && jm != 0) {
+        float2 w = __ldg(&tw[(jm * r * step) & (N - 1)]);
+        x = cmul(x, cf{w.x, INV ? -w.y : w.y});
+      }
+      v[q][r] = x;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int j = threadIdx.x + q * FFT_T;
+    const int jm = j & (Ns - 1);
+    if constexpr (R == 8) dft8<INV>(v[q]);
+    else dft4<INV>(v[q][0], v[q][1], v[q][2], v[q][3]);
+    const int idxD = (j / Ns) * Ns * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int a = pidx(idxD + r * Ns);
+      re[a] = v[q][r].x;
+      im[a] = v[q][r].y;
+    }
+  }
+  __syncthreads();
+}
+
+template <bool INV>
+__device__ __forceinline__ void fft2048(float *re, float *im, const float2 *__restrict__ tw) {
+  fft_stage<8, INV>(re, im, 1, tw);
+  fft_stage<8, INV>(re, im, 8, tw);
+  fft_stage<8, INV>(re, im, 64, tw);
+  fft_stage<4, INV>(re, im, 512, tw);
+}
+
+}  // namespace pb

@@ -1,0 +1,70 @@
+// kernels.h -- launch wrappers of the pasta_b200 sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pb {
+
+// Per-launch description of one batch of evaluations.
+struct EvalBatch {
+  int E;                     // evaluations in this batch
+  const double *labels;      // [E][5]
+  const int *eval_star;      // [E] index into stars
+  const int *eval_active;    // [E] or null: 0 = skip
+  const DevStar *stars;
+  EvalPrep *prep;            // [E]
+  float2 *H;                 // [E][1025] rotation kernel half-spectra
+  float *bufA, *bufB;        // [E][stride] spectra workspaces
+  int64_t stride;            // floats per evaluation row
+  double *cost;              // [E]
+  int *status;               // [E]
+  double *params;            // [E][param_stride] or null
+  int param_stride;
+  int max_pairs;             // max ceil(nblk/2) over the batch
+  int need_chi2;
+};
+
+void launch_prep(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// same, for entry points that need every synthetic pixel and no resampling
+void launch_prep_full(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+void launch_rotker(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
+void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+void launch_rot(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
+void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// copy the preparation status to b.status (batches without chi2)
+void launch_prep_status(const EvalBatch &b, cudaStream_t s);
+// model at the observed pixels: out [E][out_stride]
+void launch_resample_out(const DevGrid &G, const EvalBatch &b, float *out, int64_t out_stride,
+                         cudaStream_t s);
+// broadened synth spectrum (before resampling): out [E][npx]
+void launch_copy_broadened(const DevGrid &G, const EvalBatch &b, float *out, cudaStream_t s);
+// chi2 of a model given at the observed pixels (continuum utility entry points)
+void launch_chi2_given(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s);
+void launch_build_chunk(const DevStar *star, const double *coef, int n, float *out, cudaStream_t s);
+void launch_gauss_standalone(const DevGrid &G, const DevStar *star, const float *in, float *out,
+                             cudaStream_t s);
+
+// swarm state of S stars x Pmax particles (structure of arrays)
+struct Swarm {
+  int S, Pmax;
+  double *x, *v, *bx;        // [S][Pmax][5]
+  double *cost, *bcost;      // [S][Pmax]
+  double *gx, *gcost;        // [S][5], [S]
+  int *iter, *status, *done; // [S]
+  int *active;               // [S] slot in use
+  uint64_t *seed;            // [S]
+  PsoParams *params;         // [S]
+  double *labels;            // [S*Pmax][5] evaluation labels
+  int *eval_active;          // [S*Pmax]
+};
+// positions for this step (update, or publish host-placed initial positions)
+void launch_pso_update(const DevGrid &G, const Swarm &w, cudaStream_t s);
+// after evaluation: initial sort or best update, iteration counter, done flags
+void launch_pso_best(const Swarm &w, const double *cost, const int *status, cudaStream_t s);
+
+int64_t kernel_launches();
+void count_launch(int n = 1);
+
+}  // namespace pb

@@ -1,0 +1,234 @@
+"""GPU parity: the CUDA path (through the C ABI / drop-in module) against the
+CPU oracle on the same seeded inputs.
+
+Tolerances (stated per test):
+* model flux (interpolate, produce_model): vs the oracle's FP32 mirror,
+  max |gpu - ref| <= 1e-5 * max |ref| over the spectrum.
+* chi2: vs the oracle's FP64 mode, relative 1e-5.
+* seeded PSO replay: vs the oracle on the same draw stream, dTeff <= 1 K,
+  d[M/H], dlogg <= 1e-3, dvsini, dRV <= 0.01 km/s.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FLUX_TOL = 1e-5
+CHI2_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def env():
+    import oracle as O
+    from pasta_b200 import pasta as P
+    from pasta_b200 import synth as S
+
+    spec = S.config0_grid(n_px=20000)
+    labels, spectra, factors = S.make_grid(spec)
+    wl = P.WlGrid(spec.log_first, spec.log_step, spec.n_px, log=True)
+    interp = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+    og = O.Grid(labels, spectra, factors, O.WL_LOGSPACE, spec.log_first, spec.log_step)
+    star = S.make_star(spec, [7130.0, 0.07, 4.02, 50.0, 20.0], 15000, 100.0, 85000.0, seed=11)
+    return dict(O=O, P=P, S=S, spec=spec, labels=labels, spectra=spectra, interp=interp, og=og, star=star, wl=wl)
+
+
+def relmax(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+LABELS3 = [(7130.0, 0.07, 4.02), (6000.0, -0.5, 3.5), (8000.0, 0.5, 4.5), (6250.0, 0.0, 3.75),
+           (6010.0, -0.49, 4.49), (7999.0, 0.41, 3.61), (7000.0, 0.1, 4.0)]
+
+
+@pytest.mark.parametrize("tml", LABELS3)
+def test_interpolate_matches_oracle(env, tml):
+    gpu = env["interp"].interpolate(*tml)
+    ref = env["og"].interpolate(*tml, env["O"].F32)
+    assert gpu.shape == ref.shape
+    assert relmax(gpu, ref) <= FLUX_TOL
+
+
+def test_interpolate_at_node_is_the_model(env):
+    i = 200
+    t, m, g = env["labels"][i]
+    gpu = env["interp"].interpolate(t, m, g)
+    n = len(gpu) - len(gpu) % 128
+    assert np.abs(gpu[:n] - env["spectra"][i][:n] / 65535.0).max() < 1e-6
+
+
+@pytest.mark.parametrize("disp_kind", ["fixed", "none", "variable"])
+@pytest.mark.parametrize("vsini,rv", [(0.0, 0.0), (3.0, -40.0), (50.0, 20.0), (180.0, 120.0), (300.0, -149.0)])
+def test_produce_model_matches_oracle(env, disp_kind, vsini, rv):
+    O, P, star = env["O"], env["P"], env["star"]
+    if disp_kind == "fixed":
+        d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+        od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    elif disp_kind == "none":
+        d = P.NoConvolutionDispersion(star.wl, env["wl"])
+        od = O.Disp(env["og"], O.DISP_NONE, star.wl)
+    else:
+        sig = (star.wl / np.linspace(60000.0, 90000.0, len(star.wl)) / 2.355).astype(np.float32)
+        d = P.VariableResolutionDispersion(star.wl, sig, env["wl"])
+        od = O.Disp(env["og"], O.DISP_VARIABLE, star.wl, disp=sig)
+    lab = [7130.0, 0.07, 4.02, vsini, rv]
+    gpu = env["interp"].produce_model(d, *lab)
+    ref = od.produce_model(lab, O.F32)
+    assert relmax(gpu, ref) <= FLUX_TOL
+
+
+def _fitters(env, kind):
+    O, P, star, S = env["O"], env["P"], env["star"], env["S"]
+    n = len(star.wl)
+    if kind == "chunk":
+        return P.ChunkContinuumFitter(star.wl, 5, 8, 0.2), O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    if kind == "chunk12":
+        return P.ChunkContinuumFitter(star.wl, 12, 3, 0.25), O.Cont(O.CONT_CHUNK, star.wl, 12, 3, 0.25)
+    if kind == "linear":
+        D = S.legendre_design(star.wl, 40)
+        return P.LinearModelContinuumFitter(D), O.Cont(O.CONT_LINEAR, design=D)
+    if kind == "fixed":
+        c = (1.0 + 0.1 * np.linspace(-1, 1, n)).astype(np.float32)
+        return P.FixedContinuum(c, 10), O.Cont(O.CONT_FIXED, continuum=c, ignore=10)
+    return P.ConstantContinuum(), O.Cont(O.CONT_CONSTANT, n=n)
+
+
+@pytest.mark.parametrize("kind", ["chunk", "chunk12", "linear", "fixed", "constant"])
+def test_chi2_matches_oracle_f64(env, kind):
+    O, P, star = env["O"], env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    cont, oc = _fitters(env, kind)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(8, 2), (0, 300), (-150, 150))
+    labs = np.array([list(star.label), [7100.0, 0.0, 4.1, 40.0, 15.0], [6600.0, -0.3, 3.8, 120.0, -60.0],
+                     [7900.0, 0.45, 4.45, 0.0, 0.0]])
+    gpu = np.array(fitter.chi2(env["interp"], star.flux, star.var, labs))
+    ref, st = O.chi2(env["og"], od, oc, star.flux, star.var, labs, O.F64)
+    assert (st == 0).all()
+    np.testing.assert_allclose(gpu, ref, rtol=CHI2_TOL)
+
+
+def test_chi2_errors_are_nan(env):
+    O, P, star = env["O"], env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(8, 2), (0, 300), (-150, 150))
+    labs = [[9000.0, 0.0, 4.0, 10.0, 0.0],   # outside the grid
+            [7000.0, 0.0, 4.0, -1.0, 0.0],   # vsini < 0
+            [7000.0, 0.0, 4.0, 10.0, 900.0],  # RV leaves the synthetic grid
+            [7000.0, 0.0, 4.0, 10.0, 0.0]]
+    out = fitter.chi2(env["interp"], star.flux, star.var, labs)
+    assert np.isnan(out[:3]).all() and np.isfinite(out[3])
+    with pytest.raises(P.PastaError):
+        fitter.chi2(env["interp"], star.flux, star.var, labs, allow_nan=False)
+
+
+def test_fit_replay_matches_oracle(env):
+    """Seeded PSO on the shared draw stream: GPU batched vs oracle (FP64 and FP32 mirror)."""
+    O, P, star = env["O"], env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    settings = P.PSOSettings(40, 60)
+    fitter = env["interp"].get_fitter(d, cont, settings, (0.0, 300.0), (-150.0, 150.0))
+    r = fitter.fit(env["interp"], star.flux, star.var, seed=1234)
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    oc = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    st = O.settings(40, 60, (0.0, 300.0), (-150.0, 150.0))
+    ref, rc = O.fit(env["og"], od, oc, st, star.flux[None], star.var[None], [1234], O.F64, over_stars=False)
+    assert rc == 0
+    lab = np.array(r.label.as_list())
+    rl = ref[0]["label"]
+    tol = np.array([1.0, 1e-3, 1e-3, 0.01, 0.01])
+    assert (np.abs(lab - rl) <= tol).all(), (lab, rl)
+    assert abs(r.chi2 - ref[0]["chi2"]) <= 1e-5 * ref[0]["chi2"]
+    assert r.iterations == 60 and len(r.continuum_params) == 45
+
+
+def test_plain_and_batched_agree(env):
+    P, star = env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(24, 15), (0.0, 300.0), (-150.0, 150.0))
+    a = fitter.fit(env["interp"], star.flux, star.var, seed=99, mode=0)
+    b = fitter.fit(env["interp"], star.flux, star.var, seed=99, mode=1)
+    assert a.label.as_list() == b.label.as_list()
+    assert a.chi2 == b.chi2
+
+
+def test_fit_bulk_is_each_star_alone(env):
+    P, S, spec = env["P"], env["S"], env["spec"]
+    star = env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(16, 8), (0.0, 300.0), (-150.0, 150.0))
+    labs = S.random_labels(spec, 3, seed=5, vsini=(0, 100), rv=(-50, 50))
+    stars = [S.make_star(spec, l, len(star.wl), 80.0, 85000.0, seed=20 + i) for i, l in enumerate(labs)]
+    # same wavelengths for all (fit_bulk shares the fitter)
+    fl = np.stack([s.flux for s in stars])
+    vr = np.stack([s.var for s in stars])
+    bulk = fitter.fit_bulk(env["interp"], fl, vr, seeds=[1, 2, 3])
+    for i in range(3):
+        one = fitter.fit(env["interp"], fl[i], vr[i], seed=i + 1)
+        assert bulk[i].label.as_list() == one.label.as_list()
+        assert bulk[i].chi2 == one.chi2
+
+
+def test_server_result_same_alone_and_in_mix(env):
+    P, S, spec = env["P"], env["S"], env["spec"]
+    interp = env["interp"]
+    labs = S.random_labels(spec, 5, seed=8, vsini=(0, 150), rv=(-80, 80))
+    reqs = []
+    for i, l in enumerate(labs):
+        n = 6000 + 1500 * i
+        st = S.make_star(spec, l, n, 60.0, 85000.0, seed=40 + i)
+        d = P.FixedResolutionDispersion(st.wl, 85000.0, env["wl"])
+        c = P.ChunkContinuumFitter(st.wl, 4 + i, 3 + i % 4, 0.2)
+        reqs.append((d, c, st))
+    settings = P.PSOSettings(16, 10)
+    # alone
+    alone = []
+    for (d, c, st) in reqs:
+        fitter = interp.get_fitter(d, c, settings, (0.0, 300.0), (-150.0, 150.0))
+        alone.append(fitter.fit(interp, st.flux, st.var, seed=77))
+    # in the mix, staggered arrivals
+    srv = P.Server(interp, max_slots=3)
+    ids = []
+    done = {}
+    pending = list(range(len(reqs)))
+    step = 0
+    while len(done) < len(reqs):
+        if pending and step % 3 == 0:
+            i = pending.pop(0)
+            d, c, st = reqs[i]
+            ids.append(srv.submit(d, c, settings, st.flux, st.var, (0.0, 300.0), (-150.0, 150.0), seed=77))
+        srv.step()
+        for rid, status, res in srv.poll():
+            assert status == 0
+            done[rid] = res
+        step += 1
+        assert step < 1000
+    for i, rid in enumerate(ids):
+        assert done[rid].label.as_list() == alone[i].label.as_list()
+        assert done[rid].chi2 == alone[i].chi2
+
+
+def test_continuum_utilities(env):
+    O, P, star = env["O"], env["P"], env["star"]
+    og = env["og"]
+    od = O.Disp(og, O.DISP_FIXED, star.wl, 85000.0)
+    model = od.produce_model(star.label, O.F32).astype(np.float32)
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    oc = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    params, chi2 = cont.fit_continuum(model, star.flux, star.var)
+    rp, rchi2 = oc.fit(star.flux, star.var, model, O.F64)
+    assert abs(chi2 - rchi2) <= CHI2_TOL * rchi2
+    c_gpu = cont.build_continuum(params)
+    c_ref = oc.build(rp, O.F64)
+    assert relmax(c_gpu, c_ref) < 1e-4
+
+
+def test_dispersion_convolve_matches_oracle(env):
+    O, P, star = env["O"], env["P"], env["star"]
+    x = env["og"].interpolate(7130.0, 0.07, 4.02, O.F32)
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    assert relmax(d.convolve(x), od.convolve(x, O.F32)) <= FLUX_TOL
