@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark: batched PSO fits of synthetic stars on B200 (one process per GPU).
+
+Workload (the reference's batched configuration): a 60 x 21 x 11 grid of
+80,000-pixel uint16 models (13,860 models, 2.2 GB resident in HBM); 1,024
+synthetic stars per GPU with labels uniform in the grid, vsini 0-300 km/s, RV
+-150..150 km/s, 10k-60k observed pixels and SNR 20-200; R = 85,000 Gaussian
+instrument profile; 8-chunk degree-5 continuum with 0.2 overlap; PSO with 64
+particles x 200 iterations.  Data are synthetic and seeded (there is no
+public dataset for this path).
+
+A step is one PSO iteration over the whole batch: every star's 64
+particles are evaluated (interpolate -> rotation -> instrument ->
+shift/resample -> continuum -> chi2) and every swarm is updated.
+value = star fits/s = chi2 evals/s / evals per fit (64 x 201).  e2e =
+the same metric for a complete fit of the batch through the public API
+(host arrays in, results out).
+
+--impl reference times the CPU restatement of the reference's path (the
+oracle, FP32 mirror, all host threads, stars in parallel like fit_bulk) on
+a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "star fits/s & χ² evals/s vs plain GPU path at equal label error; p99 latency"
+PARTICLES, ITERS = 64, 200
+EVALS_PER_FIT = PARTICLES * (ITERS + 1)
+RESOLUTION = 85000.0
+# bytes per interpolated pixel of the interpolation kernel: 64 neighbours x 2 B read + 4 B written
+INTERP_BYTES_PER_PX = 64 * 2 + 4
+# DRAM bytes per interpolated pixel measured by ncu on the interpolation kernel
+# (profiles/interp_config1.md); None until measured
+INTERP_DRAM_BYTES_PER_PX = None
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ workload
+def make_grid(spec, use_gpu):
+    """Config-1 grid; the matrix product runs on the GPU when present (same model as synth.make_grid)."""
+    from pasta_b200 import synth as S
+    if not use_gpu:
+        return S.make_grid(spec)
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    labels = S.gridpoints(spec)
+    lm = S.LineModel(spec)
+    prof = torch.from_numpy(lm.profiles(spec.wl(), dtype=np.float32)).cuda()
+    spectra = np.empty((len(labels), spec.n_px), np.uint16)
+    for s in range(0, len(labels), 2048):
+        d = torch.from_numpy(lm.depths(labels[s:s + 2048]).astype(np.float32)).cuda()
+        f = (1.0 - d @ prof).clamp_(min=0.0)
+        spectra[s:s + 2048] = torch.clamp(torch.round(f * 65535.0), 0, 65535).to(torch.int32).cpu().numpy().astype(np.uint16)
+    del prof
+    torch.cuda.empty_cache()
+    return labels, spectra, None
+
+
+def make_workload(n_stars, seed, spec):
+    from pasta_b200 import synth as S
+    rng = np.random.default_rng(seed)
+    labels = S.random_labels(spec, n_stars, seed=seed, vsini=(0.0, 300.0), rv=(-150.0, 150.0))
+    n_obs = rng.integers(10000, 60001, n_stars)
+    snr = rng.uniform(20.0, 200.0, n_stars)
+    return S.make_stars(spec, labels, n_obs, snr, RESOLUTION, seed=seed)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from pasta_b200 import pasta as P
+    from pasta_b200 import synth as S
+    from pasta_b200.dist import gather_to_rank0, max_over_ranks, sum_over_ranks
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    from pasta_b200 import _ffi
+    _ffi.check(_ffi.lib().pasta_set_device(local))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    n_stars = args.stars
+    spec = S.config1_grid(n_px=args.npx)
+    t = time.time()
+    labels, spectra, factors = make_grid(spec, use_gpu=True)
+    wl = P.WlGrid(spec.log_first, spec.log_step, spec.n_px, log=True)
+    interp = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+    log(f"[rank {rank}] grid {spectra.shape} in {time.time() - t:.1f}s")
+    t = time.time()
+    stars = make_workload(n_stars, 1000 + rank, spec)
+    disps = [P.FixedResolutionDispersion(s.wl, RESOLUTION, wl) for s in stars]
+    conts = [P.ChunkContinuumFitter(s.wl, 8, 5, 0.2) for s in stars]
+    settings = P.PSOSettings(PARTICLES, ITERS)
+    seeds = [int(7 + 100003 * rank + i) for i in range(n_stars)]
+    log(f"[rank {rank}] {n_stars} stars in {time.time() - t:.1f}s")
+
+    # -------- device-timed steps (kernel throughput)
+    b = P.BatchFit(interp, disps, conts, settings, [s.flux for s in stars], [s.var for s in stars],
+                   (0.0, 300.0), (-150.0, 150.0), seeds=seeds)
+    info = b.info()
+    if args.warmup + args.steps + 3 > ITERS + 1:
+        raise SystemExit("steps + warmup exceed the fit's PSO steps")
+    b.step(args.warmup)
+    barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = _ffi.lib().pasta_kernel_launch_count()
+    with ClockSampler(local) as clk:
+        dev_ms = b.step(args.steps)
+    torch.cuda.synchronize(dev)
+    barrier()
+    launches = info["kernels_per_step"] * args.steps + (_ffi.lib().pasta_kernel_launch_count() - launches0)
+    t_max = max_over_ranks(dev_ms / 1000.0, dev)
+    evals_step = info["evals_per_step"]
+    evals_total = sum_over_ranks(evals_step * args.steps, dev)
+    evals_per_s = evals_total / t_max
+    fits_per_s = evals_per_s / EVALS_PER_FIT
+
+    # -------- per-stage breakdown (CUDA events between the stages, live)
+    prof = [b.profile_step() for _ in range(3)]
+    stage = {k: float(np.mean([p[k] for p in prof])) for k in prof[0]}
+    b.finish()
+    del b
+
+    # -------- end to end: one complete fit of the batch through the public API
+    fl = [s.flux for s in stars]
+    vr = [s.var for s in stars]
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    res = P.fit_many(interp, disps, conts, settings, fl, vr, (0.0, 300.0), (-150.0, 150.0), seeds=seeds)
+    torch.cuda.synchronize(dev)
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dev)
+    barrier()
+    e2e_fits = sum_over_ranks(len(res), dev) / t_e2e
+    h2d = int(sum(x.nbytes + y.nbytes for x, y in zip(fl, vr)))
+    d2h = int(sum(8 * 8 + 4 * len(r.continuum_params) for r in res))
+    err = np.array([np.abs(np.array(r.label.as_list()) - s.label) for r, s in zip(res, stars)])
+
+    # -------- plain one-star-at-a-time GPU path on a sample
+    n_plain = min(args.plain_stars, n_stars)
+    t0 = time.perf_counter()
+    plain = P.fit_many(interp, disps[:n_plain], conts[:n_plain], settings, fl[:n_plain], vr[:n_plain],
+                       (0.0, 300.0), (-150.0, 150.0), seeds=seeds[:n_plain], mode=1)
+    torch.cuda.synchronize(dev)
+    t_plain = time.perf_counter() - t0
+    same = all(a.label.as_list() == r.label.as_list() and a.chi2 == r.chi2 for a, r in zip(plain, res[:n_plain]))
+    plain_fits = n_plain / t_plain
+
+    # -------- CPU baseline (oracle, rank 0 at N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(labels, spectra, factors, spec, stars, seeds, budget_s=args.cpu_seconds)
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    interp_s = stage["interp_ms"] / 1000.0
+    interp_bytes = stage["interp_px"] * INTERP_BYTES_PER_PX
+    achieved = interp_bytes / interp_s / 1e9
+    traffic = None if INTERP_DRAM_BYTES_PER_PX is None else stage["interp_px"] * INTERP_DRAM_BYTES_PER_PX
+    step_ms = dev_ms / args.steps
+    line = {
+        "metric": METRIC, "value": fits_per_s, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (u16 grid, f64 continuum solves)", "data": "synthetic (seeded)",
+        "config": {"workload": "batched fits: %d stars/GPU, grid 60x21x11 x %d px uint16 (%.1f GB), "
+                               "N_obs 10k-60k, vsini 0-300, RV +-150, R=85000, 8 chunks deg 5, PSO %dx%d"
+                               % (n_stars, spec.n_px, spectra.nbytes / 1e9, PARTICLES, ITERS),
+                   "stars_per_gpu": n_stars, "particles": PARTICLES, "iterations": ITERS,
+                   "evals_per_step": evals_step, "parallelism": "replicas x%d (stars sharded, no collective)" % world,
+                   "l2": "inputs larger than L2 (%.1f GB grid, ~%.0f GB read per step)"
+                         % (spectra.nbytes / 1e9, interp_bytes / 1e9)},
+        "evals_per_s": evals_per_s,
+        "e2e": {"value": e2e_fits, "unit": "fits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "seconds": t_e2e, "what": "fit_many of the whole batch (201 PSO steps + final refit), host arrays"},
+        "latency_s": {"p50": t_e2e, "p99": t_e2e, "note": "batched form: every star completes with the batch"},
+        "plain_gpu": {"fits_per_s": plain_fits, "stars": n_plain, "identical_results": same,
+                      "batched_e2e_over_plain": e2e_fits / (plain_fits * world)},
+        "label_error_vs_truth": {"median_abs": np.median(err, axis=0).tolist(),
+                                 "order": ["teff", "m", "logg", "vsini", "rv"]},
+        "stage_ms": {k: v for k, v in stage.items() if k.endswith("_ms")},
+        "roofline": {"bound": "hbm", "kernel": "k_interp", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": interp_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+# ------------------------------------------------------------ CPU baseline
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    return O
+
+
+def cpu_setup(O, labels, spectra, factors, spec):
+    return O.Grid(labels, spectra, factors, O.WL_LOGSPACE, spec.log_first, spec.log_step)
+
+
+def cpu_sample(O, og, stars, seeds, n_stars, iters, nthreads):
+    """Fit n_stars stars (threads over stars) with `iters` PSO iterations; returns (seconds, evals)."""
+    st = O.settings(PARTICLES, iters, (0.0, 300.0), (-150.0, 150.0))
+    t0 = time.perf_counter()
+    evals = 0
+    # stars with different wavelength grids: one oracle call per group of nthreads stars
+    import concurrent.futures as cf
+
+    def one(i):
+        s = stars[i]
+        od = O.Disp(og, O.DISP_FIXED, s.wl, RESOLUTION)
+        oc = O.Cont(O.CONT_CHUNK, s.wl, 8, 5, 0.2)
+        res, rc = O.fit(og, od, oc, st, s.flux[None], s.var[None], [seeds[i]], O.F32, nthreads=1, over_stars=True)
+        return PARTICLES * (iters + 1)
+
+    with cf.ThreadPoolExecutor(nthreads) as ex:
+        for e in ex.map(one, range(n_stars)):
+            evals += e
+    return time.perf_counter() - t0, evals
+
+
+def cpu_baseline(labels, spectra, factors, spec, stars, seeds, budget_s=20.0):
+    O = _oracle()
+    og = cpu_setup(O, labels, spectra, factors, spec)
+    nthreads = os.cpu_count() or 1
+    t1, e1 = cpu_sample(O, og, stars, seeds, 1, 0, 1)  # calibration: one star, initial swarm only
+    per_eval = t1 / e1
+    n = max(nthreads, int(budget_s * nthreads / (per_eval * PARTICLES)))
+    n = min(n, len(stars))
+    t, e = cpu_sample(O, og, stars, seeds, n, 0, nthreads)
+    evals_s = e / t
+    return {"value": evals_s / EVALS_PER_FIT, "unit": "fits/s", "cores": nthreads, "kind": "port",
+            "evals_per_s": evals_s,
+            "sample": "%d stars x %d particles (initial swarm evaluation, %d chi2 evals) in %.1fs on %d threads; "
+                      "fits/s = evals/s / %d" % (n, PARTICLES, e, t, nthreads, EVALS_PER_FIT)}
+
+
+def run_reference(args):
+    rank, world, local = env_rank()
+    if rank != 0:
+        return None
+    from pasta_b200 import synth as S
+    O = _oracle()
+    spec = S.config1_grid(n_px=args.npx)
+    t = time.time()
+    labels, spectra, factors = S.make_grid(spec)
+    log(f"[reference] grid in {time.time() - t:.1f}s")
+    stars = make_workload(args.stars, 1000, spec)
+    seeds = [int(7 + i) for i in range(args.stars)]
+    og = cpu_setup(O, labels, spectra, factors, spec)
+    nthreads = os.cpu_count() or 1
+    per_step = nthreads  # one star per thread per step, initial swarm evaluated
+    times, evals = [], []
+    cursor = 0
+    for k in range(args.warmup + args.steps):
+        idx = [(cursor + j) % len(stars) for j in range(per_step)]
+        cursor += per_step
+        sub = [stars[i] for i in idx]
+        sd = [seeds[i] for i in idx]
+        t, e = cpu_sample(O, og, sub, sd, len(sub), 0, nthreads)
+        if k >= args.warmup:
+            times.append(t)
+            evals.append(e)
+    tot_t, tot_e = float(np.sum(times)), float(np.sum(evals))
+    evals_s = tot_e / tot_t
+    value = evals_s / EVALS_PER_FIT
+    sample = ("per step %d stars x %d particles (initial swarm, %d chi2 evals) on %d threads; fits/s = evals/s / %d"
+              % (per_step, PARTICLES, per_step * PARTICLES, nthreads, EVALS_PER_FIT))
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "batched fits: grid 60x21x11 x %d px uint16, N_obs 10k-60k, PSO %dx%d, "
+                                   "8 chunks deg 5" % (spec.n_px, PARTICLES, ITERS),
+                       "implementation": "C++ restatement of the reference CPU path (oracle FP32 mirror); the "
+                                         "Rust reference cannot be built here"},
+            "evals_per_s": evals_s,
+            "cpu_baseline": {"value": value, "unit": "fits/s", "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--stars", type=int, default=1024)
+    ap.add_argument("--npx", type=int, default=80000)
+    ap.add_argument("--plain-stars", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    if args.impl == "ours":
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -204,6 +204,32 @@ int pasta_fit_many(const pasta_grid *g, int64_t S,
                    const int64_t *n, const uint64_t *seeds, int mode,
                    pasta_fit_result *results, float *const *params);
 
+/* Step-wise batched fit (what pasta_fit_many runs): create uploads the
+ * stars and places the swarms, step advances every swarm by `steps` PSO
+ * steps (the first step evaluates the initial swarm) and reports the device
+ * time between CUDA events on the library's stream, finish runs the final
+ * refit and returns results.  profile_step runs one step stage by stage and
+ * writes 12 doubles: stage times in ms (swarm update, prep, rotation
+ * spectra, interpolation, rotation FFT, instrument profile, chi2, best
+ * update), then the step's interpolated pixels, evaluations, observed
+ * pixels and rotation FFT blocks.  info: stars, particles, evaluations per
+ * step, iterations, steps done, kernels per captured step.  No counterpart
+ * in the reference (its fit runs to completion inside argmin's Executor). */
+typedef struct pasta_batch pasta_batch;
+int pasta_batch_create(const pasta_grid *g, int64_t S,
+                       const pasta_dispersion *const *d,
+                       const pasta_continuum *const *c,
+                       const pasta_pso_settings *settings,
+                       const float *const *flux, const float *const *var,
+                       const int64_t *n, const uint64_t *seeds,
+                       pasta_batch **out);
+int pasta_batch_step(pasta_batch *b, int steps, double *device_ms);
+int pasta_batch_profile_step(pasta_batch *b, double *out12);
+int pasta_batch_info(const pasta_batch *b, int64_t *out6);
+int pasta_batch_finish(pasta_batch *b, pasta_fit_result *results,
+                       float *const *params);
+int pasta_batch_destroy(pasta_batch *b);
+
 /* ------------------------------------------------------- serving
  * Continuous batching: requests are admitted into device slots as slots and
  * HBM budget free up, every admitted star advances one PSO iteration per

@@ -62,6 +62,12 @@ SIGNATURES = {
     "pasta_chi2": (I, [P, P, P, P, P, I64, P, I64, P, P]),
     "pasta_fit": (I, [P, P, P, P, P, P, I64, I64, P, I, P, P, P]),
     "pasta_fit_many": (I, [P, I64, P, P, P, P, P, P, P, I, P, P]),
+    "pasta_batch_create": (I, [P, I64, P, P, P, P, P, P, P, P]),
+    "pasta_batch_step": (I, [P, I, P]),
+    "pasta_batch_profile_step": (I, [P, P]),
+    "pasta_batch_info": (I, [P, P]),
+    "pasta_batch_finish": (I, [P, P, P]),
+    "pasta_batch_destroy": (I, [P]),
     "pasta_server_create": (I, [P, I, I64, P]),
     "pasta_server_submit": (I, [P, P, P, P, P, P, I64, C.c_uint64, P]),
     "pasta_server_step": (I, [P]),

@@ -202,10 +202,13 @@ namespace {
 int64_t workspace_cap(const pasta_grid *g, int64_t want) {
   // per evaluation: two spectrum rows + rotation half spectrum + prep record
   const int64_t per = g->stride * 8 + 1025 * 8 + (int64_t)sizeof(EvalPrep);
+  // default: up to 40% of the device's memory for evaluation workspaces
   int64_t budget = 24ll << 30;
-  if (const char *e = getenv("PASTA_WORKSPACE_BYTES")) budget = atoll(e);
   size_t fr = 0, tot = 0;
-  if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+  const bool have = cudaMemGetInfo(&fr, &tot) == cudaSuccess;
+  if (have) budget = (int64_t)(0.4 * (double)tot);
+  if (const char *e = getenv("PASTA_WORKSPACE_BYTES")) budget = atoll(e);
+  if (have) {
     const int64_t avail = (int64_t)fr - (2ll << 30) + (int64_t)g->ws.cap * per;
     if (avail < budget) budget = avail;
   }
@@ -816,24 +819,58 @@ void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, c
     if (ok[i]) params[i] = params_from_device(in[i].c, &hp[(size_t)i * pstride]);
 }
 
-// Batched form: all stars' swarms on the device, one CUDA graph per step.
-void fit_batched(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result *res,
-                 std::vector<std::vector<float>> &params, double *trace) {
+// Batched form: all stars' swarms on the device, one CUDA graph per PSO
+// step (position update -> evaluation pipeline -> best update).
+struct Batch {
+  pasta_grid *g = nullptr;
+  std::vector<StarInput> in;
+  std::vector<pasta_pso_settings> settings;
+  std::vector<PsoParams> pp;
+  StarSet ss;
+  SwarmBuffers W;
+  EvalArgs a;
+  Swarm sw{};
+  int S = 0, Pmax = 0, iters = 0, max_m = 1, steps_done = 0;
+  int kernels_per_step = 0;
+  double t0 = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[12] = {};
+  ~Batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+  void step_eager(cudaStream_t s) {
+    launch_pso_update(g->d, sw, s);
+    run_evals(g, a, s);
+    launch_pso_best(sw, W.ecost.p, W.estatus.p, s);
+  }
+};
+
+void batch_init(Batch &B, pasta_grid *g, const std::vector<StarInput> &in) {
   Ctx &C = ctx();
   cudaStream_t s = C.stream;
-  const double t0 = now_s();
-  const int S = (int)in.size();
-  int Pmax = 0, iters = 0, max_m = 1;
-  std::vector<PsoParams> pp(S);
-  for (int i = 0; i < S; i++) {
-    pp[i] = make_pso_params(g, *in[i].st);
-    Pmax = std::max(Pmax, pp[i].P);
-    iters = std::max(iters, pp[i].max_iters);
-    max_m = std::max(max_m, width_upper_bound(g, pp[i].mx[3]));
+  B.t0 = now_s();
+  B.g = g;
+  B.in = in;
+  B.S = (int)in.size();
+  B.settings.resize(B.S);
+  for (int i = 0; i < B.S; i++) {
+    B.settings[i] = *in[i].st;
+    B.in[i].st = &B.settings[i];
   }
-  StarSet ss;
-  ss.build(in);
-  SwarmBuffers W;
+  B.pp.resize(B.S);
+  for (int i = 0; i < B.S; i++) {
+    B.pp[i] = make_pso_params(g, B.settings[i]);
+    B.Pmax = std::max(B.Pmax, B.pp[i].P);
+    B.iters = std::max(B.iters, B.pp[i].max_iters);
+    B.max_m = std::max(B.max_m, width_upper_bound(g, B.pp[i].mx[3]));
+  }
+  const int S = B.S, Pmax = B.Pmax;
+  B.ss.build(in);
+  SwarmBuffers &W = B.W;
   W.alloc(S, Pmax);
   const size_t E = (size_t)S * Pmax;
   std::vector<double> hx(E * 5, 0.0), hv(E * 5, 0.0);
@@ -841,7 +878,7 @@ void fit_batched(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_resu
   std::vector<uint64_t> seeds(S);
   for (int i = 0; i < S; i++) {
     seeds[i] = in[i].seed;
-    int st = init_swarm_host(g, pp[i], in[i].seed, &hx[(size_t)i * Pmax * 5], &hv[(size_t)i * Pmax * 5]);
+    int st = init_swarm_host(g, B.pp[i], in[i].seed, &hx[(size_t)i * Pmax * 5], &hv[(size_t)i * Pmax * 5]);
     if (st) { status[i] = st; done[i] = 1; }
   }
   CK(cudaMemcpy(W.x.p, hx.data(), E * 5 * sizeof(double), cudaMemcpyHostToDevice));
@@ -851,11 +888,11 @@ void fit_batched(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_resu
   CK(cudaMemcpy(W.active.p, active.data(), S * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(W.iter.p, iter.data(), S * sizeof(int), cudaMemcpyHostToDevice));
   W.seed.upload(seeds);
-  W.params.upload(pp);
+  W.params.upload(B.pp);
   ensure_workspace(g, (int64_t)E);
-  Swarm sw = W.view();
-  EvalArgs a;
-  a.stars = ss.dstars.p;
+  B.sw = W.view();
+  EvalArgs &a = B.a;
+  a.stars = B.ss.dstars.p;
   a.labels = W.labels.p;
   a.eval_star = W.eval_star.p;
   a.eval_active = W.eval_active.p;
@@ -863,63 +900,150 @@ void fit_batched(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_resu
   a.cost = W.ecost.p;
   a.status = W.estatus.p;
   a.need_chi2 = 1;
-  a.max_m = max_m;
-  // capture one PSO step: positions -> evaluations -> bests
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  const bool use_graph = !getenv("PASTA_NO_GRAPH");
-  auto step = [&]() {
-    launch_pso_update(g->d, sw, s);
-    run_evals(g, a, s);
-    launch_pso_best(sw, W.ecost.p, W.estatus.p, s);
-  };
-  if (use_graph) {
+  a.max_m = B.max_m;
+  for (auto &e : B.ev) CK(cudaEventCreate(&e));
+  if (!getenv("PASTA_NO_GRAPH")) {
+    const int64_t k0 = kernel_launches();
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    step();
-    CK(cudaStreamEndCapture(s, &graph));
-    CK(cudaGraphInstantiate(&exec, graph, 0));
+    B.step_eager(s);
+    CK(cudaStreamEndCapture(s, &B.graph));
+    CK(cudaGraphInstantiate(&B.exec, B.graph, 0));
+    B.kernels_per_step = (int)(kernel_launches() - k0);
   }
+}
+
+// Launch n PSO steps; returns the device time between CUDA events recorded
+// on the launching stream around them.
+double batch_steps(Batch &B, int n, double *trace) {
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
   std::vector<double> tx, tc;
-  const int Ptr = pp.empty() ? 0 : pp[0].P;
-  for (int it = 0; it <= iters; it++) {
-    if (use_graph) CK(cudaGraphLaunch(exec, s));
-    else step();
-    if (trace) {
-      tx.resize((size_t)Pmax * 5);
-      tc.resize(Pmax);
-      CK(cudaMemcpyAsync(tx.data(), W.x.p, tx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(tc.data(), W.cost.p, tc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  const int Ptr = B.pp.empty() ? 0 : B.pp[0].P;
+  CK(cudaEventRecord(B.ev[0], s));
+  for (int k = 0; k < n; k++) {
+    if (B.exec) CK(cudaGraphLaunch(B.exec, s));
+    else B.step_eager(s);
+    const int it = B.steps_done++;
+    if (trace && it <= B.pp[0].max_iters) {
+      tx.resize((size_t)B.Pmax * 5);
+      tc.resize(B.Pmax);
+      CK(cudaMemcpyAsync(tx.data(), B.W.x.p, tx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(tc.data(), B.W.cost.p, tc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      if (it <= pp[0].max_iters)
-        for (int p = 0; p < Ptr; p++) {
-          double *t = trace + ((size_t)it * Ptr + p) * 6;
-          for (int d = 0; d < 5; d++) t[d] = tx[(size_t)p * 5 + d];
-          t[5] = tc[p];
-        }
+      for (int p = 0; p < Ptr; p++) {
+        double *t = trace + ((size_t)it * Ptr + p) * 6;
+        for (int d = 0; d < 5; d++) t[d] = tx[(size_t)p * 5 + d];
+        t[5] = tc[p];
+      }
     }
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
+  CK(cudaEventRecord(B.ev[1], s));
+  CK(cudaEventSynchronize(B.ev[1]));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, B.ev[0], B.ev[1]));
+  return ms;
+}
+
+// One step launched stage by stage with events between the stages:
+// out[0] swarm update, [1] prep, [2] rotation spectra, [3] interpolation,
+// [4] rotation FFT, [5] instrument profile, [6] chi2, [7] best update,
+// [8] interpolated pixels (sum of windows), [9] evaluations, [10] sum of
+// observed pixels, [11] rotation blocks.
+void batch_profile_step(Batch &B, double *out) {
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
+  pasta_grid *g = B.g;
+  const EvalArgs &a = B.a;
+  if (a.E > g->ws.cap) fail(PASTA_E_UNSUPPORTED, "profiled step needs the batch in one workspace");
+  EvalBatch b{};
+  b.E = (int)a.E;
+  b.labels = a.labels;
+  b.eval_star = a.eval_star;
+  b.eval_active = a.eval_active;
+  b.stars = a.stars;
+  b.prep = g->ws.prep.p;
+  b.H = g->ws.H.p;
+  b.bufA = g->ws.A.p;
+  b.bufB = g->ws.B.p;
+  b.stride = g->ws.stride;
+  b.cost = a.cost;
+  b.status = a.status;
+  b.max_pairs = max_pairs_for(g, a.max_m);
+  b.need_chi2 = 1;
+  CK(cudaEventRecord(B.ev[0], s));
+  launch_pso_update(g->d, B.sw, s);
+  CK(cudaEventRecord(B.ev[1], s));
+  launch_prep(g->d, b, s);
+  CK(cudaEventRecord(B.ev[2], s));
+  if (a.max_m > 1) launch_rotker(g->d, b, C.tw.p, s);
+  CK(cudaEventRecord(B.ev[3], s));
+  launch_interp(g->d, b, s);
+  CK(cudaEventRecord(B.ev[4], s));
+  if (a.max_m > 1) launch_rot(g->d, b, C.tw.p, s);
+  CK(cudaEventRecord(B.ev[5], s));
+  launch_gauss(g->d, b, s);
+  CK(cudaEventRecord(B.ev[6], s));
+  launch_chi2(g->d, b, s);
+  CK(cudaEventRecord(B.ev[7], s));
+  launch_pso_best(B.sw, B.W.ecost.p, B.W.estatus.p, s);
+  CK(cudaEventRecord(B.ev[8], s));
+  CK(cudaGetLastError());
+  CK(cudaEventSynchronize(B.ev[8]));
+  for (int i = 0; i < 8; i++) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, B.ev[i], B.ev[i + 1]));
+    out[i] = ms;
+  }
+  B.steps_done++;
+  std::vector<EvalPrep> hp(a.E);
+  CK(cudaMemcpy(hp.data(), g->ws.prep.p, a.E * sizeof(EvalPrep), cudaMemcpyDeviceToHost));
+  double px = 0, ev = 0, obs = 0, blk = 0;
+  std::vector<DevStar> hs = B.ss.h;
+  for (const auto &P : hp) {
+    if (P.status) continue;
+    px += P.i_hi - P.i_lo;
+    ev += 1;
+    obs += hs[P.star].n_obs;
+    blk += P.nblk;
+  }
+  out[8] = px;
+  out[9] = ev;
+  out[10] = obs;
+  out[11] = blk;
+}
+
+void batch_finish(Batch &B, pasta_fit_result *res, std::vector<std::vector<float>> &params) {
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
+  const int S = B.S;
   std::vector<double> gx((size_t)S * 5), gc(S);
-  CK(cudaMemcpyAsync(gx.data(), W.gx.p, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(gc.data(), W.gcost.p, gc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(status.data(), W.status.p, S * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(iter.data(), W.iter.p, S * sizeof(int), cudaMemcpyDeviceToHost, s));
+  std::vector<int> status(S);
+  CK(cudaMemcpyAsync(gx.data(), B.W.gx.p, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(gc.data(), B.W.gcost.p, gc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(status.data(), B.W.status.p, S * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   std::vector<int> ok(S);
   for (int i = 0; i < S; i++) ok[i] = status[i] == 0 ? 1 : 0;
-  final_refit(g, ss, in, gx, ok, params, s);
-  const double dt = now_s() - t0;
+  final_refit(B.g, B.ss, B.in, gx, ok, params, s);
+  const double dt = now_s() - B.t0;
   for (int i = 0; i < S; i++) {
     pasta_fit_result &r = res[i];
     std::memset(&r, 0, sizeof r);
     for (int d = 0; d < 5; d++) r.label[d] = gx[(size_t)i * 5 + d];
     r.chi2 = gc[i];
-    r.iterations = pp[i].max_iters;
+    r.iterations = B.pp[i].max_iters;
     r.status = status[i];
     r.time = dt;
     r.n_params = (int)params[i].size();
   }
+}
+
+void fit_batched(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result *res,
+                 std::vector<std::vector<float>> &params, double *trace) {
+  Batch B;
+  batch_init(B, g, in);
+  batch_steps(B, B.iters + 1, trace);
+  batch_finish(B, res, params);
 }
 
 // Plain form: one star at a time, the swarm on the host, one launch per
@@ -1649,6 +1773,68 @@ int pasta_fit_many(const pasta_grid *g, int64_t S, const pasta_dispersion *const
   std::vector<StarInput> in(S);
   for (int64_t i = 0; i < S; i++) in[i] = StarInput{d[i], c[i], &settings[i], flux[i], var[i], n[i], seeds[i]};
   return fit_common(g, in, mode, results, params, nullptr);
+}
+
+// ----------------------------------------------------- batch sessions
+struct pasta_batch {
+  Batch B;
+};
+
+int pasta_batch_create(const pasta_grid *gc, int64_t S, const pasta_dispersion *const *d,
+                       const pasta_continuum *const *c, const pasta_pso_settings *settings, const float *const *flux,
+                       const float *const *var, const int64_t *n, const uint64_t *seeds, pasta_batch **out) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(gc);
+    if (S < 1 || !out) fail(PASTA_E_ARG, "invalid batch arguments");
+    std::vector<StarInput> in(S);
+    for (int64_t i = 0; i < S; i++) in[i] = StarInput{d[i], c[i], &settings[i], flux[i], var[i], n[i], seeds[i]};
+    for (auto &s : in) validate_star(g, s);
+    std::lock_guard<std::mutex> lk(g->mu);
+    std::unique_ptr<pasta_batch> b(new pasta_batch());
+    batch_init(b->B, g, in);
+    *out = b.release();
+  });
+}
+
+int pasta_batch_step(pasta_batch *b, int steps, double *device_ms) {
+  return guard([&] {
+    std::lock_guard<std::mutex> lk(b->B.g->mu);
+    double ms = batch_steps(b->B, steps, nullptr);
+    if (device_ms) *device_ms = ms;
+  });
+}
+
+int pasta_batch_profile_step(pasta_batch *b, double *out12) {
+  return guard([&] {
+    std::lock_guard<std::mutex> lk(b->B.g->mu);
+    batch_profile_step(b->B, out12);
+  });
+}
+
+int pasta_batch_info(const pasta_batch *b, int64_t *out6) {
+  return guard([&] {
+    const Batch &B = b->B;
+    out6[0] = B.S;
+    out6[1] = B.Pmax;
+    out6[2] = (int64_t)B.S * B.Pmax;
+    out6[3] = B.iters;
+    out6[4] = B.steps_done;
+    out6[5] = B.kernels_per_step;
+  });
+}
+
+int pasta_batch_finish(pasta_batch *b, pasta_fit_result *results, float *const *params) {
+  return guard([&] {
+    std::lock_guard<std::mutex> lk(b->B.g->mu);
+    std::vector<std::vector<float>> pv;
+    batch_finish(b->B, results, pv);
+    for (int i = 0; i < b->B.S; i++)
+      if (params && params[i]) std::copy(pv[i].begin(), pv[i].end(), params[i]);
+  });
+}
+
+int pasta_batch_destroy(pasta_batch *b) {
+  return guard([&] { delete b; });
 }
 
 // ------------------------------------------------------------ serving

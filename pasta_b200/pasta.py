@@ -855,3 +855,65 @@ class Server:
         q, a, d = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().pasta_server_pending(self._h, C.byref(q), C.byref(a), C.byref(d)))
         return q.value, a.value, d.value
+
+
+class BatchFit:
+    """Step-wise batched fit of many stars (pasta_batch_*): the object the
+    benchmark times.  ``step(n)`` advances every swarm n PSO steps (the first
+    step evaluates the initial swarm) and returns the device milliseconds."""
+
+    def __init__(self, interpolator, dispersions, continuum_fitters, settings, fluxes, vars_, vsini_range, rv_range,
+                 seeds=None, constraints=None):
+        S = len(fluxes)
+        self.S = S
+        self._st = (_ffi.PsoSettingsC * S)()
+        for i in range(S):
+            s = settings[i] if isinstance(settings, (list, tuple)) else settings
+            self._st[i] = _settings_c(s, vsini_range, rv_range, constraints)
+        self._fl = [f32(x) for x in fluxes]
+        self._vr = [f32(x) for x in vars_]
+        n = np.array([len(x) for x in self._fl], np.int64)
+        seeds = np.asarray([_seed(None) for _ in range(S)] if seeds is None else seeds, np.uint64)
+        P = C.c_void_p
+        self._keep = (dispersions, continuum_fitters, interpolator)
+        dh = (P * S)(*[d._h.value for d in dispersions])
+        ch = (P * S)(*[c._h.value for c in continuum_fitters])
+        fp = (P * S)(*[x.ctypes.data for x in self._fl])
+        vp = (P * S)(*[x.ctypes.data for x in self._vr])
+        h = C.c_void_p()
+        check(lib().pasta_batch_create(interpolator._grid._h, S, dh, ch, self._st, fp, vp, ptr(n), ptr(seeds),
+                                       C.byref(h)))
+        self._h = h
+        self._nparams = [max(c.nparams(), 1) for c in continuum_fitters]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and h.value and _ffi._lib is not None:
+            lib().pasta_batch_destroy(h)
+
+    def step(self, n: int = 1) -> float:
+        ms = C.c_double()
+        check(lib().pasta_batch_step(self._h, int(n), C.byref(ms)))
+        return ms.value
+
+    def profile_step(self) -> dict:
+        out = np.zeros(12)
+        check(lib().pasta_batch_profile_step(self._h, ptr(out)))
+        names = ["update_ms", "prep_ms", "rotker_ms", "interp_ms", "rot_ms", "gauss_ms", "chi2_ms", "best_ms",
+                 "interp_px", "evals", "obs_px", "rot_blocks"]
+        return dict(zip(names, out.tolist()))
+
+    def info(self) -> dict:
+        out = np.zeros(6, np.int64)
+        check(lib().pasta_batch_info(self._h, ptr(out)))
+        return dict(zip(["stars", "particles", "evals_per_step", "iterations", "steps_done", "kernels_per_step"],
+                        out.tolist()))
+
+    def finish(self) -> list:
+        res = (_ffi.FitResultC * self.S)()
+        params = [np.zeros(k, np.float32) for k in self._nparams]
+        pp = (C.c_void_p * self.S)(*[p.ctypes.data for p in params])
+        check(lib().pasta_batch_finish(self._h, res, pp))
+        return [(int(res[i].status), OptimizationResult(Label(*res[i].label), params[i][:res[i].n_params],
+                                                         res[i].chi2, res[i].iterations, res[i].time))
+                for i in range(self.S)]

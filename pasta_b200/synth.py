@@ -286,3 +286,61 @@ def legendre_design(wl: np.ndarray, k: int) -> np.ndarray:
     """n x k Legendre design matrix on wl mapped to [-1, 1] (config-4 linear continuum model)."""
     x = (wl - wl[0]) / (wl[-1] - wl[0]) * 2.0 - 1.0
     return np.polynomial.legendre.legvander(x, k - 1).astype(np.float32)
+
+
+def make_stars(spec: GridSpec, labels: np.ndarray, n_obs, snr, resolution: float, seed: int,
+               rv_max: float = 150.0, vsini_max: float = 300.0, chunk: int = 32) -> list:
+    """Vectorised make_star for many stars (same physics, batched FFTs)."""
+    labels = np.asarray(labels, dtype=np.float64)
+    n_stars = len(labels)
+    n_obs = np.broadcast_to(np.asarray(n_obs), (n_stars,))
+    snr = np.broadcast_to(np.asarray(snr, dtype=np.float64), (n_stars,))
+    lm = LineModel(spec)
+    wl = spec.wl()
+    prof = lm.profiles(wl, dtype=np.float32)
+    dvelo = np.log(10.0) * spec.log_step
+    lo, hi = observed_window(spec, rv_max, vsini_max, resolution)
+    npx = spec.n_px
+    nf = 1 << int(np.ceil(np.log2(npx + 4096)))
+    if resolution > 0:
+        sig = 1.0 / (np.log(10.0) * 2.355 * resolution * spec.log_step)
+        n = int(np.ceil(6 * sig))
+        n = n + 1 - n % 2
+        x = np.arange(n) - (n - 1) / 2
+        g = np.exp(-0.5 * (x / sig) ** 2)
+        g /= g.sum()
+        G = np.fft.rfft(np.roll(np.pad(g, (0, nf - n)), -((n - 1) // 2)))
+    else:
+        G = None
+    out = []
+    for s0 in range(0, n_stars, chunk):
+        lab = labels[s0:s0 + chunk]
+        f = 1.0 - (lm.depths(lab[:, :3]).astype(np.float32) @ prof).astype(np.float64)
+        np.clip(f, 0.0, None, out=f)
+        if spec.includes_factor:
+            bb = np.stack([blackbody(wl, t) for t in lab[:, 0]])
+            f = f * bb
+            f = f / f.max(axis=1, keepdims=True)
+        F = np.fft.rfft(f, nf, axis=1)
+        for k in range(len(lab)):
+            if lab[k, 3] > 0:
+                kk = rotation_profile(lab[k, 3], dvelo)
+                m = len(kk)
+                F[k] *= np.fft.rfft(np.roll(np.pad(kk, (0, nf - m)), -((m - 1) // 2)))
+        if G is not None:
+            F *= G[None, :]
+        conv = np.fft.irfft(F, nf, axis=1)[:, :npx]
+        for k in range(len(lab)):
+            i = s0 + k
+            rng = np.random.default_rng([seed, i])
+            wl_obs = np.geomspace(lo, hi, int(n_obs[i]))
+            src = wl_obs * (1.0 - lab[k, 4] / C_KMS)
+            model = np.interp(np.log10(src), np.log10(wl), conv[k])
+            xx = np.linspace(-1.0, 1.0, len(wl_obs))
+            a1, a2 = rng.uniform(-0.2, 0.2, 2)
+            signal = model * (1.0 + a1 * xx + a2 * xx * xx)
+            sigma = np.abs(signal) / snr[i] + 1e-6
+            flux = signal + sigma * rng.standard_normal(len(wl_obs))
+            out.append(Star(wl_obs, flux.astype(np.float32), (sigma ** 2).astype(np.float32), lab[k].copy(),
+                            float(snr[i])))
+    return out

@@ -114,7 +114,7 @@ def test_chi2_errors_are_nan(env):
     fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(8, 2), (0, 300), (-150, 150))
     labs = [[9000.0, 0.0, 4.0, 10.0, 0.0],   # outside the grid
             [7000.0, 0.0, 4.0, -1.0, 0.0],   # vsini < 0
-            [7000.0, 0.0, 4.0, 10.0, 900.0],  # RV leaves the synthetic grid
+            [7000.0, 0.0, 4.0, 10.0, 9000.0],  # RV leaves the synthetic grid
             [7000.0, 0.0, 4.0, 10.0, 0.0]]
     out = fitter.chi2(env["interp"], star.flux, star.var, labs)
     assert np.isnan(out[:3]).all() and np.isfinite(out[3])

@@ -1,0 +1,169 @@
+"""CPU known-answer tests of the oracle (no GPU).
+
+The reference ships no tests or golden vectors and cannot be built here, so
+the oracle is pinned by properties that the reference's algorithm has by
+construction (cubic.rs Lagrange weights, convolve_rv.rs kernels and
+resampling, continuum_fitting.rs least squares), plus regression against the
+committed fixtures in tests/golden/.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from pasta_b200 import synth as S
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def small():
+    spec = S.config0_grid(n_px=4000)
+    labels, spectra, factors = S.make_grid(spec)
+    g = O.Grid(labels, spectra, factors, O.WL_LOGSPACE, spec.log_first, spec.log_step)
+    return spec, labels, spectra, g
+
+
+def test_grid_axes_and_order(small):
+    spec, labels, spectra, g = small
+    t, m, lg = g.axes()
+    np.testing.assert_array_equal(t, spec.teffs)
+    np.testing.assert_array_equal(m, np.sort(spec.ms))
+    np.testing.assert_array_equal(lg, spec.loggs)
+
+
+def test_interpolation_at_nodes_reproduces_models(small):
+    """Lagrange property (cubic.rs:29-60): weights are one-hot at a grid node."""
+    spec, labels, spectra, g = small
+    n = spec.n_px - spec.n_px % 128
+    for i in (0, 57, 211, 494):
+        out = g.interpolate(*labels[i], O.F32)
+        assert np.abs(out[:n] - spectra[i][:n] / np.float32(65535.0)).max() < 1e-6
+        # tail pixels carry the extra 1/65535 (interpolate.rs:978)
+        np.testing.assert_allclose(out[n:], spectra[i][n:] / 65535.0 / 65535.0, rtol=1e-6, atol=1e-12)
+
+
+def _poly_grid(deg):
+    """Grid whose spectra are a polynomial of total degree `deg` in the labels."""
+    t = np.arange(6000.0, 8001.0, 250.0)
+    m = np.round(np.arange(-0.5, 0.501, 0.1), 2)
+    lg = np.arange(3.5, 4.501, 0.25)
+    pts = np.array([(a, b, c) for a in t for c in lg for b in m])
+    rng = np.random.default_rng(0)
+    npx = 256
+    coef = rng.uniform(0.0, 1.0, (npx, 3))
+    x = np.stack([(pts[:, 0] - 6000) / 2000, (pts[:, 1] + 0.5), (pts[:, 2] - 3.5)], axis=1)
+    vals = 0.1 + 0.25 * (x[:, 0][:, None] ** deg * coef[:, 0] + x[:, 1][:, None] ** deg * coef[:, 1]
+                         + x[:, 2][:, None] ** deg * coef[:, 2])
+    spectra = np.clip(np.rint(vals * 65535.0), 0, 65535).astype(np.uint16)
+    return pts, spectra, coef
+
+
+def test_cubic_spectra_are_reproduced_inside_the_grid():
+    """cubic Lagrange interpolation is exact for cubic dependence on the labels."""
+    pts, spectra, coef = _poly_grid(3)
+    g = O.Grid(pts, spectra, None, O.WL_LOGSPACE, 3.6, 1e-5)
+    # exact reference: interpolate the quantized node values with the f64 weights
+    for lab in [(6700.0, 0.03, 3.9), (7333.0, -0.27, 4.11)]:
+        cols, w = g.local_grid(*lab)
+        data = spectra.astype(np.float64)
+        # column order is list_gridpoints (teff, logg, m inner) = pts order here
+        exact = sum(w[j] * data[cols[j]] for j in range(64) if cols[j] >= 0) / 65535.0
+        out = g.interpolate(*lab, O.F64)
+        np.testing.assert_allclose(out[:128], exact[:128], rtol=1e-12)
+        # and the polynomial itself (up to the uint16 quantisation)
+        x = np.array([(lab[0] - 6000) / 2000, lab[1] + 0.5, lab[2] - 3.5])
+        poly = 0.1 + 0.25 * (x[0] ** 3 * coef[:, 0] + x[1] ** 3 * coef[:, 1] + x[2] ** 3 * coef[:, 2])
+        assert np.abs(out[:128] - poly[:128]).max() < 3e-5
+
+
+def test_weights_sum_to_one(small):
+    spec, labels, spectra, g = small
+    rng = np.random.default_rng(1)
+    for _ in range(20):
+        lab = (rng.uniform(6000, 8000), rng.uniform(-0.5, 0.5), rng.uniform(3.5, 4.5))
+        cols, w = g.local_grid(*lab)
+        assert abs(w.sum() - 1.0) < 1e-12
+        assert (w[cols < 0] == 0).all()
+
+
+def test_outside_grid_is_an_error(small):
+    g = small[3]
+    with pytest.raises(O.OracleError):
+        g.interpolate(9000.0, 0.0, 4.0)
+    with pytest.raises(O.OracleError):
+        g.interpolate(7000.0, 0.7, 4.0)
+
+
+@pytest.mark.parametrize("vsini", [1.0, 10.0, 50.0, 300.0])
+def test_rotation_kernel(vsini):
+    """convolve_rv.rs:438-475: odd width from the formula, normalised, symmetric."""
+    dvelo = np.log(10.0) * 1.2e-6
+    k = O.rotation_kernel(vsini, dvelo)
+    vrot = vsini / 299792.0
+    n = max(1, int(np.ceil(2 * vrot / dvelo * np.sqrt(1 + (4 * (0.6 - 1) / (np.pi * 0.6)) ** 2))) + 2)
+    n = n + 1 - n % 2
+    assert len(k) == n
+    assert abs(k.sum() - 1.0) < 1e-6
+    np.testing.assert_allclose(k, k[::-1], atol=1e-6)
+
+
+def test_identity_resampling_and_exact_shift(small):
+    """rv = 0 on the synthetic pixels is the identity (convolve_rv.rs:586-594)."""
+    spec, labels, spectra, g = small
+    wl = spec.wl()[300:3500]
+    d = O.Disp(g, O.DISP_NONE, wl)
+    lab = [7000.0, 0.0, 4.0, 0.0, 0.0]
+    m = d.produce_model(lab, O.F64)
+    ref = g.interpolate(7000.0, 0.0, 4.0, O.F64)[300:3500]
+    assert np.abs(m - ref).max() < 1e-6
+
+
+def test_chunk_fitter_recovers_polynomial_continuum(small):
+    """observed = model * polynomial of degree <= p: chi2 -> 0 and the continuum is recovered."""
+    spec, labels, spectra, g = small
+    wl = spec.wl()[200:3800]
+    model = np.linspace(0.5, 1.0, len(wl))
+    x = (wl - wl[0]) / (wl[-1] - wl[0])
+    cont = 1.0 + 0.3 * x - 0.2 * x ** 2 + 0.05 * x ** 3
+    flux = (model * cont).astype(np.float32)
+    var = np.full(len(wl), 1e-4, np.float32)
+    c = O.Cont(O.CONT_CHUNK, wl, 5, 8, 0.2)
+    params, chi2 = c.fit(flux, var, model, O.F64)
+    assert chi2 < 1e-6
+    built = c.build(params, O.F64)
+    np.testing.assert_allclose(built, cont, rtol=1e-5)
+
+
+def test_f32_mirror_vs_f64(small):
+    spec, labels, spectra, g = small
+    star = S.make_star(spec, [7130.0, 0.07, 4.02, 50.0, 20.0], 3000, 100.0, 85000.0, seed=2)
+    d = O.Disp(g, O.DISP_FIXED, star.wl, 85000.0)
+    m32, m64 = d.produce_model(star.label, O.F32), d.produce_model(star.label, O.F64)
+    assert np.abs(m32 - m64).max() / np.abs(m64).max() < 2e-6
+    c = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    x32, _ = O.chi2(g, d, c, star.flux, star.var, star.label[None], O.F32)
+    x64, _ = O.chi2(g, d, c, star.flux, star.var, star.label[None], O.F64)
+    assert abs(x32[0] - x64[0]) / x64[0] < 1e-4
+
+
+def test_draw_stream():
+    a = [O.draw_u01(7, 3, i, 2, 1) for i in range(2000)]
+    assert min(a) >= 0.0 and max(a) < 1.0
+    assert abs(np.mean(a) - 0.5) < 0.03
+    assert O.draw_u01(7, 3, 5, 2, 1) == O.draw_u01(7, 3, 5, 2, 1)
+    assert O.draw_u01(7, 3, 5, 2, 1) != O.draw_u01(8, 3, 5, 2, 1)
+
+
+def test_seeded_fit_is_deterministic(small):
+    spec, labels, spectra, g = small
+    star = S.make_star(spec, [7130.0, 0.07, 4.02, 50.0, 20.0], 3000, 100.0, 85000.0, seed=2)
+    d = O.Disp(g, O.DISP_FIXED, star.wl, 85000.0)
+    c = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    st = O.settings(12, 6, (0.0, 300.0), (-150.0, 150.0))
+    r1, rc1 = O.fit(g, d, c, st, star.flux[None], star.var[None], [5], O.F32, nthreads=4, over_stars=False)
+    r2, rc2 = O.fit(g, d, c, st, star.flux[None], star.var[None], [5], O.F32, nthreads=1, over_stars=True)
+    assert rc1 == 0 and rc2 == 0
+    np.testing.assert_array_equal(r1[0]["label"], r2[0]["label"])
+    assert r1[0]["chi2"] == r2[0]["chi2"]
