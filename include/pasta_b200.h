@@ -176,6 +176,26 @@ int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d,
                int64_t n, const double *labels, int64_t L, double *out,
                int32_t *status);
 
+/* pasta_chi2 for callers that cannot allocate device memory: a host
+ * framework that gives the GPU's whole memory to its own pool, a real-time
+ * loop that may not call cudaMalloc (which can synchronise the device), a
+ * service whose footprint is fixed after start-up.  No counterpart in the
+ * reference.  flux, var (n floats), labels (L x 5 doubles), out (L doubles)
+ * and status (L int32) are DEVICE buffers the caller owns; the work is
+ * queued on `stream` (a cudaStream_t; NULL = the legacy default stream) and
+ * is complete when that stream reaches it.  The evaluation workspace is a
+ * 32 MiB static device array inside the library, held by every GPU that
+ * loads it until exit and shared by all calls: L is limited to what fits
+ * (about 200 labels for a 20,000-pixel grid, 51 for 80,000 pixels) and larger
+ * L is rejected with PASTA_E_ARG; calls whose work overlaps on the GPU race
+ * on the array.  The first call on a device sets up the array's address and
+ * should come before any stream capture.  Nothing is allocated: no
+ * cudaMalloc, cudaFree or allocating library routine. */
+int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d,
+                       const pasta_continuum *c, const float *flux,
+                       const float *var, int64_t n, const double *labels,
+                       int64_t L, double *out, int32_t *status, void *stream);
+
 /* ------------------------------------------------------------- fit
  * SingleFitter::fit / fit_bulk (fitting.rs:399-458; lib.rs:1478-1540) with
  * the particle swarm of particleswarm.rs:111-307.  S stars share the

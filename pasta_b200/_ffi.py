@@ -60,6 +60,7 @@ SIGNATURES = {
     "pasta_produce_model": (I, [P, P, P, I64, P, P]),
     "pasta_interpolate_and_convolve": (I, [P, P, P, I64, P, P]),
     "pasta_chi2": (I, [P, P, P, P, P, I64, P, I64, P, P]),
+    "pasta_chi2_noalloc": (I, [P, P, P, P, P, I64, P, I64, P, P, P]),
     "pasta_fit": (I, [P, P, P, P, P, P, I64, I64, P, I, P, P, P]),
     "pasta_fit_many": (I, [P, I64, P, P, P, P, P, P, P, I, P, P]),
     "pasta_batch_create": (I, [P, I64, P, P, P, P, P, P, P, P]),

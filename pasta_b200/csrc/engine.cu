@@ -2079,3 +2079,32 @@ int pasta_server_destroy(pasta_server *sv) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Read-only views of the handles for the allocation-free entry point
+// (noalloc.cu): the grid's device description and one assembled star.
+// Nothing is allocated or copied.
+namespace pb {
+int internal_eval_view(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c, const float *flux,
+                       const float *var, int64_t n, DevGrid *grid, int64_t *stride, DevStar *star, int *device,
+                       std::string *err) {
+  try {
+    if (!g || !d || !c) fail(PASTA_E_ARG, "grid, dispersion and continuum handles are required");
+    StarInput si{d, c, nullptr, flux, var, n, 0};
+    validate_star(g, si);
+    *grid = g->d;
+    *stride = g->stride;
+    *star = make_star(d, c, flux, var, n);
+    *device = g->dev;
+    return PASTA_OK;
+  } catch (const PErr &e) {
+    *err = e.what();
+    return e.code;
+  }
+}
+}  // namespace pb
+
+namespace pb {
+// lets noalloc.cu report through pasta_last_error()
+void internal_set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace pb

@@ -1,0 +1,211 @@
+// noalloc.cu -- chi2 of a batch of labels without allocating device memory.
+//
+// Some callers of this library cannot call cudaMalloc.  A host framework may
+// hand the whole of the GPU's memory to its own pool allocator at start-up.
+// A real-time loop may not take the driver's allocation path (cudaMalloc can
+// synchronise the device) between frames.  A multi-tenant service may have
+// its footprint fixed once the process is up.  For them pasta_chi2_noalloc
+// evaluates chi2 exactly like pasta_chi2.  The inputs and outputs are device
+// buffers the caller already owns.  The evaluation workspace lives in the
+// file-scope array g_noalloc_scratch below.
+//
+// The array is NOALLOC_SCRATCH_BYTES (32 MiB).  Every GPU that loads the
+// library holds it until the process exits.  All calls share it and it keeps
+// the last call's contents.  No part of it has to start at zero: every stage
+// writes the rows it later reads.  Calls whose work overlaps on the GPU race
+// on the array, so a caller serialises its calls (one stream, or
+// synchronisation between streams).
+//
+// Set-up: the first call on a device, with that device current, resolves
+// the array's device address with cudaGetSymbolAddress and copies the FFT
+// twiddle table into g_noalloc_twiddle.  That first call should therefore
+// come before any stream capture.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pasta_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pb {
+int internal_eval_view(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c, const float *flux,
+                       const float *var, int64_t n, DevGrid *grid, int64_t *stride, DevStar *star, int *device,
+                       std::string *err);
+void internal_set_last_error(const std::string &msg);
+}
+
+using namespace pb;
+
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = 32u << 20;
+constexpr int MAX_DEVICES = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(256) float2 g_noalloc_twiddle[FFTN];
+
+struct DeviceSetup {
+  bool ready = false;
+  unsigned char *scratch = nullptr;
+  float2 *twiddle = nullptr;
+};
+std::mutex g_setup_mu;
+DeviceSetup g_setup[MAX_DEVICES];
+
+// errors are reported through pasta_last_error()
+struct ErrSink {
+  ErrSink &operator=(const std::string &m) {
+    internal_set_last_error(m);
+    return *this;
+  }
+  ErrSink &operator=(const char *m) { return *this = std::string(m); }
+} g_noalloc_err;
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// bytes of scratch one label needs: prep record, rotation half spectrum,
+// eval->star index and the two spectrum rows
+size_t per_label_bytes(int64_t stride) {
+  return align256(sizeof(EvalPrep)) + align256(1025 * sizeof(float2)) + align256(sizeof(int)) +
+         2 * align256((size_t)stride * sizeof(float));
+}
+
+int setup_device(int dev, DeviceSetup **out) {
+  std::lock_guard<std::mutex> lk(g_setup_mu);
+  if (dev < 0 || dev >= MAX_DEVICES) {
+    g_noalloc_err = "device index out of range";
+    return PASTA_E_ARG;
+  }
+  DeviceSetup &s = g_setup[dev];
+  if (!s.ready) {
+    cudaError_t e = cudaGetSymbolAddress((void **)&s.scratch, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      g_noalloc_err = std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") + cudaGetErrorString(e);
+      return PASTA_E_CUDA;
+    }
+    e = cudaGetSymbolAddress((void **)&s.twiddle, g_noalloc_twiddle);
+    if (e != cudaSuccess) {
+      g_noalloc_err = std::string("cudaGetSymbolAddress(g_noalloc_twiddle) failed: ") + cudaGetErrorString(e);
+      return PASTA_E_CUDA;
+    }
+    float2 tw[FFTN];
+    for (int k = 0; k < FFTN; k++) {
+      const double a = -2.0 * M_PI * (double)k / (double)FFTN;
+      tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    e = cudaMemcpyToSymbol(g_noalloc_twiddle, tw, sizeof tw);
+    if (e != cudaSuccess) {
+      g_noalloc_err = std::string("twiddle upload failed: ") + cudaGetErrorString(e);
+      return PASTA_E_CUDA;
+    }
+    s.ready = true;
+  }
+  *out = &s;
+  return PASTA_OK;
+}
+
+// writes the star descriptor and the all-zero eval->star map into scratch
+__global__ void k_noalloc_init(DevStar st, DevStar *dst, int *eval_star, int L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *dst = st;
+  if (i < L) eval_star[i] = 0;
+}
+
+}  // namespace
+
+// chi2 of L labels (like pasta_chi2) with every buffer supplied by the caller:
+// flux, var [n] f32, labels [L x 5] f64, out [L] f64, status [L] int32 are
+// device pointers; stream is a cudaStream_t (NULL: the legacy default stream).
+// Asynchronous: results are valid once the stream has reached this work.
+extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c,
+                                  const float *flux, const float *var, int64_t n, const double *labels, int64_t L,
+                                  double *out, int32_t *status, void *stream) {
+  DevGrid G;
+  DevStar star;
+  int64_t stride = 0;
+  int dev = 0;
+  std::string err;
+  int rc = internal_eval_view(g, d, c, flux, var, n, &G, &stride, &star, &dev, &err);
+  if (rc) {
+    g_noalloc_err = err;
+    return rc;
+  }
+  if (!flux || !var || !labels || !out || !status) {
+    g_noalloc_err = "flux, var, labels, out and status must be device pointers";
+    return PASTA_E_ARG;
+  }
+  if (L < 1) {
+    g_noalloc_err = "at least one label is required";
+    return PASTA_E_ARG;
+  }
+  const size_t fixed = align256(sizeof(DevStar));
+  const size_t per = per_label_bytes(stride);
+  const int64_t max_labels = NOALLOC_SCRATCH_BYTES > fixed ? (int64_t)((NOALLOC_SCRATCH_BYTES - fixed) / per) : 0;
+  if (L > max_labels) {
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "%lld labels exceed the allocation-free scratch (%zu bytes): at most %lld labels for a grid of %lld "
+             "pixels",
+             (long long)L, NOALLOC_SCRATCH_BYTES, (long long)max_labels, (long long)G.npx);
+    g_noalloc_err = buf;
+    return PASTA_E_ARG;
+  }
+  cudaError_t e = cudaSetDevice(dev);
+  if (e != cudaSuccess) {
+    g_noalloc_err = std::string("cudaSetDevice failed: ") + cudaGetErrorString(e);
+    return PASTA_E_CUDA;
+  }
+  DeviceSetup *S = nullptr;
+  rc = setup_device(dev, &S);
+  if (rc) return rc;
+  // carve the scratch
+  unsigned char *p = S->scratch;
+  DevStar *dstar = (DevStar *)p;
+  p += fixed;
+  EvalPrep *prep = (EvalPrep *)p;
+  p += align256(sizeof(EvalPrep) * (size_t)L);
+  float2 *H = (float2 *)p;
+  p += align256(1025 * sizeof(float2) * (size_t)L);
+  int *eval_star = (int *)p;
+  p += align256(sizeof(int) * (size_t)L);
+  float *A = (float *)p;
+  p += align256((size_t)stride * sizeof(float) * (size_t)L);
+  float *B = (float *)p;
+  cudaStream_t s = (cudaStream_t)stream;
+  k_noalloc_init<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(star, dstar, eval_star, (int)L);
+  EvalBatch b{};
+  b.E = (int)L;
+  b.labels = labels;
+  b.eval_star = eval_star;
+  b.stars = dstar;
+  b.prep = prep;
+  b.H = H;
+  b.bufA = A;
+  b.bufB = B;
+  b.stride = stride;
+  b.cost = out;
+  b.status = status;
+  // labels live on the device, so the rotation blocks are sized for the
+  // widest kernel the reference accepts (2048 taps); work items beyond an
+  // evaluation's own blocks return at once
+  const int V = 1;  // FFTN - (2048 - 1)
+  b.max_pairs = (int)(((int64_t)(G.npx + V - 1) / V + 1) / 2);
+  b.need_chi2 = 1;
+  launch_prep(G, b, s);
+  launch_rotker(G, b, S->twiddle, s);
+  launch_interp(G, b, s);
+  launch_rot(G, b, S->twiddle, s);
+  launch_gauss(G, b, s);
+  launch_chi2(G, b, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_noalloc_err = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+    return PASTA_E_CUDA;
+  }
+  return PASTA_OK;
+}
