@@ -24,6 +24,22 @@ constexpr int MAX_CHUNKS = 32;
 constexpr int MAX_P1 = 16;          // polynomial order + 1
 constexpr int MAX_LIN_K = 128;      // linear-model columns
 constexpr int MAX_PARTICLES = 1024;
+// the fused broadening kernel needs this many outputs per 2048-point block
+constexpr int MIN_FUSED_OUTPUTS = 128;
+
+// Legendre recurrence in f32 with explicit rounding, evaluated identically
+// by the host (Gram matrices) and the device (moments, continuum):
+// P0 = 1, P1 = x, P(k+1) = fma(A_k x, P_k, -(C_k P(k-1))), A_k = (2k+1)/(k+1),
+// C_k = k/(k+1) rounded to f32.
+PB_HD float leg_a(int k) { return (float)((double)(2 * k + 1) / (double)(k + 1)); }
+PB_HD float leg_c(int k) { return (float)((double)k / (double)(k + 1)); }
+PB_HD float leg_step(float a, float c, float x, float pk, float pkm1) {
+#ifdef __CUDA_ARCH__
+  return __fmaf_rn(__fmul_rn(a, x), pk, -__fmul_rn(c, pkm1));
+#else
+  return std::fmaf(a * x, pk, -(c * pkm1));
+#endif
+}
 
 // status codes (mirror include/pasta_b200.h)
 enum : int {
@@ -97,7 +113,10 @@ struct EvalPrep {
   int status;
   int star;
   int m;          // rotation kernel width (odd); 1 = identity
-  int nblk;       // overlap-save blocks of the rotation FFT
+  int nblk;       // blocks of the broadening kernel (fused) or of the rotation FFT (unfused)
+  int hg;         // instrument-profile half width (0: no instrument profile)
+  int fused;      // 1: rotation and instrument profile in one kernel (k_broaden)
+  int final_in_b; // 1: the broadened spectrum ends in buffer B, else in A
   int o_lo, o_hi; // synth pixels the resampler reads [o_lo, o_hi)
   int g_lo, g_hi; // rotation outputs the Gaussian reads [g_lo, g_hi)
   int i_lo, i_hi; // interpolated pixels needed [i_lo, i_hi) (multiples of 8)

@@ -317,13 +317,14 @@ float poly_blend(float x) {  // continuum_fitting.rs:119-123
   float s = std::sin(xc * (float)M_PI / 2.0f);
   return s * s;
 }
-void legendre_host(double x, int p1, double *P) {
-  P[0] = 1.0;
-  if (p1 > 1) P[1] = x;
-  for (int k = 1; k + 1 < p1; k++) {
-    const double a = (double)(2 * k + 1) / (double)(k + 1), c = (double)k / (double)(k + 1);
-    P[k + 1] = a * x * P[k] - c * P[k - 1];
-  }
+// Legendre values at x exactly as the device evaluates them (f32 recurrence
+// with explicit rounding, common.cuh), widened to double for the Gram.
+void legendre_host(float x, int p1, double *P) {
+  float p[MAX_P1];
+  p[0] = 1.0f;
+  if (p1 > 1) p[1] = x;
+  for (int k = 1; k + 1 < p1; k++) p[k + 1] = leg_step(leg_a(k), leg_c(k), x, p[k], p[k - 1]);
+  for (int k = 0; k < p1; k++) P[k] = (double)p[k];
 }
 // monomial coefficients of P_0..P_{p1-1}: T[k][j]
 std::vector<double> legendre_to_monomial(int p1) {
@@ -391,7 +392,7 @@ void chunk_setup(pasta_continuum *c, const double *wl, int n_chunks, int p_order
     std::fill(G.begin(), G.end(), 0.0);
     for (int i = c->cstart[ch]; i < c->cstop[ch]; i++) {
       const float xf = (ch > 0 && i < c->cstop[ch - 1]) ? c->xb[i] : c->xa[i];
-      legendre_host((double)xf, p1, P.data());
+      legendre_host(xf, p1, P.data());
       for (int a = 0; a < p1; a++)
         for (int b = 0; b <= a; b++) G[(size_t)a * p1 + b] += P[a] * P[b];
     }
@@ -584,17 +585,22 @@ struct EvalArgs {
   int need_chi2 = 0;
   int full_window = 0;
   int max_m = 1;
+  int max_hg = 0;                // widest instrument half width among the stars
+  uint32_t chunk_p1_mask = 0;    // chunk continua present, by coefficient count
+  int other_cont = 0;            // linear / fixed / constant continua present
   float *out_obs = nullptr;
   int64_t out_stride = 0;
   float *out_synth = nullptr;
   const float *given = nullptr;  // model given at observed pixels
 };
 
-int max_pairs_for(const pasta_grid *g, int max_m) {
-  if (max_m <= 1) return 0;
-  const int V = FFTN - (max_m - 1);
-  const int64_t nblk = (g->npx + V - 1) / V;
-  return (int)((nblk + 1) / 2);
+// continuum kinds and instrument widths of the stars a batch can touch
+void star_kinds(const std::vector<DevStar> &h, EvalArgs &a) {
+  for (const auto &st : h) {
+    if (st.cont_kind == CONT_CHUNK) a.chunk_p1_mask |= 1u << st.p1;
+    else a.other_cont = 1;
+    if (st.disp_kind != DISP_NONE) a.max_hg = std::max(a.max_hg, (st.gw - 1) / 2);
+  }
 }
 
 int width_upper_bound(const pasta_grid *g, double vsini_hi) {
@@ -608,7 +614,12 @@ int width_upper_bound(const pasta_grid *g, double vsini_hi) {
 void run_evals(pasta_grid *g, const EvalArgs &a, cudaStream_t s) {
   Ctx &C = ctx();
   const int64_t cap = g->ws.cap;
-  const int max_pairs = max_pairs_for(g, a.max_m);
+  int max_pairs, max_pairs_unfused, may_unfuse;
+  pipeline_pairs((int)g->npx, a.max_m, a.max_hg, &max_pairs, &max_pairs_unfused, &may_unfuse);
+  PipelineOpts o;
+  o.full_window = a.full_window;
+  o.rot = a.max_m > 1;
+  o.may_unfuse = may_unfuse;
   for (int64_t off = 0; off < a.E; off += cap) {
     const int64_t cnt = std::min(cap, a.E - off);
     EvalBatch b{};
@@ -627,19 +638,15 @@ void run_evals(pasta_grid *g, const EvalArgs &a, cudaStream_t s) {
     b.params = a.params ? a.params + (size_t)off * a.param_stride : nullptr;
     b.param_stride = a.param_stride;
     b.max_pairs = max_pairs;
+    b.max_pairs_unfused = max_pairs_unfused;
     b.need_chi2 = a.need_chi2;
+    b.chunk_p1_mask = a.chunk_p1_mask;
+    b.other_cont = a.other_cont;
     if (a.given) {
       launch_chi2_given(g->d, b, a.given, s);
       continue;
     }
-    if (a.full_window) launch_prep_full(g->d, b, s);
-    else launch_prep(g->d, b, s);
-    if (a.max_m > 1) launch_rotker(g->d, b, C.tw.p, s);
-    launch_interp(g->d, b, s);
-    if (a.max_m > 1) launch_rot(g->d, b, C.tw.p, s);
-    launch_gauss(g->d, b, s);
-    if (a.need_chi2) launch_chi2(g->d, b, s);
-    else if (b.status) launch_prep_status(b, s);
+    launch_pipeline(g->d, b, C.tw.p, o, s);
     if (a.out_obs) launch_resample_out(g->d, b, a.out_obs + (size_t)off * a.out_stride, a.out_stride, s);
     if (a.out_synth) launch_copy_broadened(g->d, b, a.out_synth + (size_t)off * g->npx, s);
   }
@@ -809,6 +816,7 @@ void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, c
   a.param_stride = pstride;
   a.need_chi2 = 1;
   a.max_m = max_m;
+  star_kinds(ss.h, a);
   ensure_workspace(g, S);
   run_evals(g, a, s);
   std::vector<double> hp((size_t)S * pstride);
@@ -901,6 +909,7 @@ void batch_init(Batch &B, pasta_grid *g, const std::vector<StarInput> &in) {
   a.status = W.estatus.p;
   a.need_chi2 = 1;
   a.max_m = B.max_m;
+  star_kinds(B.ss.h, a);
   for (auto &e : B.ev) CK(cudaEventCreate(&e));
   if (!getenv("PASTA_NO_GRAPH")) {
     const int64_t k0 = kernel_launches();
@@ -968,8 +977,11 @@ void batch_profile_step(Batch &B, double *out) {
   b.stride = g->ws.stride;
   b.cost = a.cost;
   b.status = a.status;
-  b.max_pairs = max_pairs_for(g, a.max_m);
+  int may_unfuse;
+  pipeline_pairs((int)g->npx, a.max_m, a.max_hg, &b.max_pairs, &b.max_pairs_unfused, &may_unfuse);
   b.need_chi2 = 1;
+  b.chunk_p1_mask = a.chunk_p1_mask;
+  b.other_cont = a.other_cont;
   CK(cudaEventRecord(B.ev[0], s));
   launch_pso_update(g->d, B.sw, s);
   CK(cudaEventRecord(B.ev[1], s));
@@ -979,9 +991,12 @@ void batch_profile_step(Batch &B, double *out) {
   CK(cudaEventRecord(B.ev[3], s));
   launch_interp(g->d, b, s);
   CK(cudaEventRecord(B.ev[4], s));
-  if (a.max_m > 1) launch_rot(g->d, b, C.tw.p, s);
+  launch_broaden(g->d, b, C.tw.p, s);
   CK(cudaEventRecord(B.ev[5], s));
-  launch_gauss(g->d, b, s);
+  if (may_unfuse) {
+    launch_rot(g->d, b, C.tw.p, s);
+    launch_gauss(g->d, b, s);
+  }
   CK(cudaEventRecord(B.ev[6], s));
   launch_chi2(g->d, b, s);
   CK(cudaEventRecord(B.ev[7], s));
@@ -1080,6 +1095,7 @@ void fit_plain(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result
     a.status = ds.p;
     a.need_chi2 = 1;
     a.max_m = width_upper_bound(g, pp.mx[3]);
+    star_kinds(ss.h, a);
     std::vector<int> est(P);
     auto evaluate = [&]() -> int {
       CK(cudaMemcpyAsync(dl.p, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -1197,6 +1213,8 @@ struct pasta_server {
   int64_t next_id = 1;
   int max_m = 1, graph_max_m = 0;
   int64_t graph_gen = -1;
+  uint32_t graph_mask = 0;  // continuum kinds / instrument width the captured step covers
+  int graph_other = 0, graph_hg = 0;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   std::mutex mu;
@@ -1551,6 +1569,8 @@ int pasta_continuum_fit(const pasta_continuum *c, const float *model, const floa
     b.status = dst.p;
     b.params = dpar.p;
     b.param_stride = ps;
+    b.chunk_p1_mask = st.cont_kind == CONT_CHUNK ? 1u << st.p1 : 0u;
+    b.other_cont = st.cont_kind == CONT_CHUNK ? 0 : 1;
     DevGrid G{};
     launch_chi2_given(G, b, dm.p, s);
     CK(cudaGetLastError());
@@ -1667,6 +1687,7 @@ static int run_label_batch(const pasta_grid *gc, const pasta_dispersion *d, cons
     a.need_chi2 = out_chi2 ? 1 : 0;
     a.full_window = full_window;
     a.max_m = width_upper_bound(g, vmax);
+    star_kinds({st}, a);
     if (out_obs) { dout.alloc((size_t)L * nobs); a.out_obs = dout.p; a.out_stride = nobs; }
     if (out_synth) { dout.alloc((size_t)L * g->npx); a.out_synth = dout.p; }
     ensure_workspace(g, L);
@@ -1964,8 +1985,19 @@ int pasta_server_step(pasta_server *sv) {
     a.status = sv->W.estatus.p;
     a.need_chi2 = 1;
     a.max_m = sv->max_m;
-    if (sv->exec && (sv->graph_max_m < sv->max_m || sv->graph_gen != g->ws.gen)) {
-      // a wider rotation kernel was admitted, or the workspace moved
+    {
+      std::vector<DevStar> occ;
+      for (int i = 0; i < sv->slots; i++)
+        if (sv->slot_req[i]) occ.push_back(sv->hstars[i]);
+      star_kinds(occ, a);
+      a.chunk_p1_mask |= sv->graph_mask;  // keep what the captured graph already covers
+      if (sv->graph_other) a.other_cont = 1;
+      a.max_hg = std::max(a.max_hg, sv->graph_hg);
+    }
+    const bool grown = sv->graph_max_m < sv->max_m || (a.chunk_p1_mask & ~sv->graph_mask) ||
+                       (a.other_cont && !sv->graph_other) || a.max_hg > sv->graph_hg;
+    if (sv->exec && (grown || sv->graph_gen != g->ws.gen)) {
+      // a wider kernel or a new continuum kind was admitted, or the workspace moved
       cudaGraphExecDestroy(sv->exec);
       cudaGraphDestroy(sv->graph);
       sv->exec = nullptr;
@@ -1974,6 +2006,9 @@ int pasta_server_step(pasta_server *sv) {
     if (!sv->exec) {
       sv->graph_max_m = sv->max_m;
       sv->graph_gen = g->ws.gen;
+      sv->graph_mask = a.chunk_p1_mask;
+      sv->graph_other = a.other_cont;
+      sv->graph_hg = a.max_hg;
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       launch_pso_update(g->d, sw, s);
       run_evals(g, a, s);
@@ -2009,6 +2044,7 @@ int pasta_server_step(pasta_server *sv) {
         ok.push_back(status[i] == 0 ? 1 : 0);
       }
       ss.dstars.upload(hs);
+      ss.h = hs;
       std::vector<std::vector<float>> params;
       final_refit(g, ss, in, best, ok, params, s);
       const double tnow = now_s();

@@ -1,11 +1,12 @@
-// kernels.cu -- the bandwidth and FFT kernels of the per-particle hot path.
+// kernels.cu -- the bandwidth, FFT and reduction kernels of the hot path.
 //
 // Buffer protocol per evaluation e (rows of `stride` floats):
 //   k_interp writes the interpolated spectrum to A.
-//   k_rot writes the rotation-broadened spectrum to B (skipped when the
-//     rotation is the identity; then A holds it).
-//   k_gauss writes the instrument-broadened spectrum to the other buffer.
-//   k_chi2 / k_resample_out read the final buffer (final_row()).
+//   k_broaden (rotation FFT + instrument profile, fused) reads A, writes B.
+//   Very wide kernels (m - 1 + 2 hg > 2048 - 128) take the unfused pair
+//   k_rot (A -> B) and k_gauss (B -> A, or A -> B when the rotation is the
+//   identity).  EvalPrep::final_in_b says where the result is.
+//   k_chi2_* / k_resample_out read the final row.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -14,21 +15,31 @@
 
 namespace pb {
 
-__device__ __forceinline__ const float *rot_row(const EvalBatch &b, const EvalPrep &P, int e) {
-  return (P.m > 1 ? b.bufB : b.bufA) + (size_t)e * b.stride;
+__device__ __forceinline__ const float *final_row(const EvalBatch &b, const EvalPrep &P, int e) {
+  return (P.final_in_b ? b.bufB : b.bufA) + (size_t)e * b.stride;
 }
-__device__ __forceinline__ const float *final_row(const EvalBatch &b, const EvalPrep &P, int disp_kind, int e) {
-  const bool rot_in_b = P.m > 1;
-  const bool in_b = disp_kind == DISP_NONE ? rot_in_b : !rot_in_b;
-  return (in_b ? b.bufB : b.bufA) + (size_t)e * b.stride;
+
+static int g_num_sms = 0;
+static int num_sms() {
+  if (!g_num_sms) {
+    int dev;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
 }
 
 // ---------------------------------------------------------------- interp
-// flux[px] = sum_n w_n * (u16_n[px] * factor_n) over the 64 neighbours
+// flux[px] = sum_n w_n * u16_n[px] * factor_n over the 64 neighbours
 // (interpolate.rs:954-981), 8 pixels per thread from one 128-bit load per
 // neighbour.  Grid: x = evaluation, y = 2048-pixel tile, so CTAs that run
-// together read the same tile of the resident grid (particles of one star
-// share neighbours, which then hit in L2).
+// together read the same 57 MB tile slab of the resident grid, which stays
+// in L2 across evaluations.  The weight and the dequantisation factor are
+// folded into one f32 (w * factor); the u16 -> f32 conversion is exact
+// (PRMT under the exponent of 2^23, one packed add), and the accumulation is
+// one packed f32x2 FMA per two pixels.  Neighbours with weight 0 (absent or
+// exactly at a node) contribute exactly 0 and are skipped.
 constexpr int IT_T = 256, IT_TILE = IT_T * 8;
 
 __global__ void __launch_bounds__(IT_T) k_interp(DevGrid G, EvalBatch b) {
@@ -39,44 +50,60 @@ __global__ void __launch_bounds__(IT_T) k_interp(DevGrid G, EvalBatch b) {
   const int ilo = P.i_lo, ihi = P.i_hi;
   if (t0 >= ihi || t0 + IT_TILE <= ilo) return;
   __shared__ const uint16_t *rows[64];
-  __shared__ float ws[64], fs[64];
+  __shared__ float ws[64], fs[64], wf[64];
   if (threadIdx.x < 64) {
     const int c = P.cols[threadIdx.x];
-    rows[threadIdx.x] = c >= 0 ? G.spectra + (size_t)c * G.stride : nullptr;
-    ws[threadIdx.x] = P.w[threadIdx.x];
-    fs[threadIdx.x] = c >= 0 ? G.factor[c] : 0.0f;
+    const float f = c >= 0 ? G.factor[c] : 0.0f;
+    const float w = c >= 0 ? P.w[threadIdx.x] : 0.0f;
+    ws[threadIdx.x] = w;
+    fs[threadIdx.x] = f;
+    wf[threadIdx.x] = w * f;
+    rows[threadIdx.x] = c >= 0 ? G.spectra + (size_t)c * G.stride : G.spectra;
   }
   __syncthreads();
   const int px = t0 + threadIdx.x * 8;
   if (px < ilo || px >= ihi) return;
+  float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e * b.stride + px);
+  if (px + 8 <= G.tail_start) {
+    float2 acc[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) acc[k] = make_float2(0.0f, 0.0f);
+    const float2 bias = make_float2(-8388608.0f, -8388608.0f);
+#pragma unroll 16
+    for (int n = 0; n < 64; n++) {
+      const float w = wf[n];
+      if (w == 0.0f) continue;
+      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rows[n] + px));
+      const float2 w2 = make_float2(w, w);
+      const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        float2 v = make_float2(__int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7410)),
+                               __int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7432)));
+        v = __fadd2_rn(v, bias);
+        acc[k] = __ffma2_rn(w2, v, acc[k]);
+      }
+    }
+    out[0] = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
+    out[1] = make_float4(acc[2].x, acc[2].y, acc[3].x, acc[3].y);
+    return;
+  }
+  // last tile: the final npx % 128 pixels carry an extra 1/65535 (interpolate.rs:978)
   float acc[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) acc[k] = 0.0f;
-  const bool tail = px + 8 > G.tail_start;
-#pragma unroll 8
   for (int n = 0; n < 64; n++) {
-    const uint16_t *r = rows[n];
-    if (r == nullptr) continue;
-    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(r + px));
+    if (ws[n] == 0.0f) continue;
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rows[n] + px));
     const float wn = ws[n], fn = fs[n];
     const uint32_t u[4] = {q.x, q.y, q.z, q.w};
-    if (!tail) {
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        acc[2 * k] = fmaf(wn, __fmul_rn((float)(u[k] & 0xFFFFu), fn), acc[2 * k]);
-        acc[2 * k + 1] = fmaf(wn, __fmul_rn((float)(u[k] >> 16), fn), acc[2 * k + 1]);
-      }
-    } else {
-      // the last npx % 128 pixels carry an extra 1/65535 (interpolate.rs:978)
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const float x = (float)((u[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
-        const float v = px + k >= G.tail_start ? __fmul_rn(__fdiv_rn(x, 65535.0f), fn) : __fmul_rn(x, fn);
-        acc[k] = fmaf(wn, v, acc[k]);
-      }
+    for (int k = 0; k < 8; k++) {
+      const float x = (float)((u[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
+      const float v = px + k >= G.tail_start ? __fmul_rn(__fdiv_rn(x, 65535.0f), fn) : __fmul_rn(x, fn);
+      acc[k] = fmaf(wn, v, acc[k]);
     }
   }
-  float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e * b.stride + px);
   out[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
   out[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
 }
@@ -88,22 +115,122 @@ void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   count_launch();
 }
 
-// ------------------------------------------------------------ rotation
-// Overlap-save convolution with the rotation kernel (the reference uses
-// overlap-add, convolve_rv.rs:121-157; both are the same linear
-// convolution).  Two real blocks of one evaluation ride in the real and
-// imaginary parts of one complex 2048-point FFT; the kernel is real, so the
-// two products separate again after the inverse transform.  Block b of an
-// evaluation produces rotation outputs [g_lo + b V, g_lo + (b+1) V) with
-// V = 2048 - (m - 1).  Persistent CTAs walk (evaluation, block pair) items.
-__global__ void __launch_bounds__(FFT_T) k_rot(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+// ------------------------------------------------ instrument profile (tile)
+// FixedTargetDispersionLogSpace: g[i] = sum_k gk[k] r[i + h - k], r zero
+// outside the grid (convolve_rv.rs:207-210).  Per-pixel kernels
+// (VariableTargetDispersion / FixedTargetDispersionNonLog):
+// g[i] = kernel_i . r[i-h .. i+h], pixels within h of either end pass
+// through (convolve_rv.rs:213-233, 414-430).  r(t) reads the rotation
+// output for synth pixel t from wherever the caller staged it.
+template <class RF>
+__device__ __forceinline__ float instrument(const DevStar &st, int N, int i, int h, const RF &r) {
+  const int w = 2 * h + 1;
+  float acc = 0.0f;
+  if (st.disp_kind == DISP_FIXED) {
+    const float *g = st.gk;
+    for (int k = 0; k < w; k++) acc = fmaf(__ldg(&g[k]), r(i + h - k), acc);
+  } else {
+    if (i < h || i >= N - h) return r(i);
+    const float *kk = st.gk + (size_t)i * w;
+    for (int t = 0; t < w; t++) acc = fmaf(__ldg(&kk[t]), r(i - h + t), acc);
+  }
+  return acc;
+}
+
+// ------------------------------------------------------ fused broadening
+// One work item = two blocks of one evaluation.  Block b yields the final
+// outputs [o_lo + b V, o_lo + (b+1) V) with V = 2048 - (m - 1) - 2 hg: the
+// rotation outputs [s - hg, s + V + hg) come from one overlap-save block of
+// 2048 inputs (the reference uses overlap-add, convolve_rv.rs:121-157; both
+// are the same linear convolution), and the instrument profile is then
+// applied from shared memory.  The two real blocks ride in the real and
+// imaginary parts of one complex FFT (the kernel is real, so the two
+// products separate after the inverse).  Rotation outputs outside [0, N)
+// are zero, like the reference's cropped segment.  With the identity
+// rotation the FFT is skipped.
+__global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   __shared__ float re[FFT_SM], im[FFT_SM];
   const long long total = (long long)b.E * b.max_pairs;
+  const int N = G.npx;
   for (long long item = blockIdx.x; item < total; item += gridDim.x) {
     const int e = (int)(item / b.max_pairs), pair = (int)(item % b.max_pairs);
     const EvalPrep &P = b.prep[e];
+    const int m = P.m, nblk = P.nblk, hg = P.hg;
+    if (P.status || !P.fused || 2 * pair >= nblk) continue;
+    const DevStar &st = b.stars[P.star];
+    const int hw = (m - 1) / 2;
+    const int V = FFTN - (m - 1) - 2 * hg;
+    const int s0 = P.o_lo + 2 * pair * V, s1 = s0 + V;
+    const bool has1 = 2 * pair + 1 < nblk;
+    const int ilo = P.i_lo, ihi = P.i_hi, ohi = P.o_hi;
+    const float *x = b.bufA + (size_t)e * b.stride;
+    // input t of a block is synth pixel (s - hg - hw + t) for the rotation,
+    // (s - hg + t) for the identity
+    const int shift = m > 1 ? hg + hw : hg;
+    for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
+      const int j0 = s0 - shift + t, j1 = s1 - shift + t;
+      re[pidx(t)] = (j0 >= ilo && j0 < ihi) ? x[j0] : 0.0f;
+      im[pidx(t)] = (has1 && j1 >= ilo && j1 < ihi) ? x[j1] : 0.0f;
+    }
+    __syncthreads();
+    int base = 0;  // data index of rotation output (s - hg)
+    if (m > 1) {
+      fft2048<false>(re, im, tw);
+      const float2 *H = b.H + (size_t)e * 1025;
+      for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
+        float2 h = k <= 1024 ? H[k] : H[FFTN - k];
+        if (k > 1024) h.y = -h.y;
+        const int a = pidx(k);
+        const cf z = cmul(cf{re[a], im[a]}, cf{h.x, h.y});
+        re[a] = z.x;
+        im[a] = z.y;
+      }
+      __syncthreads();
+      fft2048<true>(re, im, tw);
+      base = m - 1;
+      const float sc = 1.0f / 2048.0f;
+      for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
+        const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
+        re[pidx(t)] = (i0 >= 0 && i0 < N) ? re[pidx(t)] * sc : 0.0f;
+        im[pidx(t)] = (i1 >= 0 && i1 < N) ? im[pidx(t)] * sc : 0.0f;
+      }
+      __syncthreads();
+    }
+    float *y = b.bufB + (size_t)e * b.stride;
+    for (int u = threadIdx.x; u < V; u += FFT_T) {
+      const int i0 = s0 + u;
+      if (i0 < ohi)
+        y[i0] = hg > 0 ? instrument(st, N, i0, hg, [&](int i) { return re[pidx(base + i - (s0 - hg))]; })
+                       : re[pidx(base + u)];
+      const int i1 = s1 + u;
+      if (has1 && i1 < ohi)
+        y[i1] = hg > 0 ? instrument(st, N, i1, hg, [&](int i) { return im[pidx(base + i - (s1 - hg))]; })
+                       : im[pidx(base + u)];
+    }
+    __syncthreads();
+  }
+}
+
+void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cudaStream_t s) {
+  if (b.E <= 0 || b.max_pairs <= 0) return;
+  const long long total = (long long)b.E * b.max_pairs;
+  long long grid = (long long)num_sms() * 6;
+  if (grid > total) grid = total;
+  k_broaden<<<(unsigned)grid, FFT_T, 0, s>>>(G, b, tw);
+  count_launch();
+}
+
+// ------------------------------------------- unfused rotation (wide kernels)
+// Overlap-save with the rotation kernel alone: block b produces rotation
+// outputs [g_lo + b V, g_lo + (b+1) V), V = 2048 - (m - 1), into B.
+__global__ void __launch_bounds__(FFT_T, 3) k_rot(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+  __shared__ float re[FFT_SM], im[FFT_SM];
+  const long long total = (long long)b.E * b.max_pairs_unfused;
+  for (long long item = blockIdx.x; item < total; item += gridDim.x) {
+    const int e = (int)(item / b.max_pairs_unfused), pair = (int)(item % b.max_pairs_unfused);
+    const EvalPrep &P = b.prep[e];
     const int m = P.m, nblk = P.nblk;
-    if (P.status || m <= 1 || 2 * pair >= nblk) continue;
+    if (P.status || P.fused || m <= 1 || 2 * pair >= nblk) continue;
     const int V = FFTN - (m - 1), hw = (m - 1) / 2;
     const int s0 = P.g_lo + 2 * pair * V, s1 = s0 + V;
     const bool has1 = 2 * pair + 1 < nblk;
@@ -141,73 +268,37 @@ __global__ void __launch_bounds__(FFT_T) k_rot(DevGrid G, EvalBatch b, const flo
   }
 }
 
-static int g_num_sms = 0;
-static int num_sms() {
-  if (!g_num_sms) {
-    int dev;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
-  }
-  return g_num_sms;
-}
-
 void launch_rot(const DevGrid &G, const EvalBatch &b, const float2 *tw, cudaStream_t s) {
-  if (b.E <= 0 || b.max_pairs <= 0) return;
-  long long total = (long long)b.E * b.max_pairs;
-  long long grid = (long long)num_sms() * 8;
+  if (b.E <= 0 || b.max_pairs_unfused <= 0) return;
+  const long long total = (long long)b.E * b.max_pairs_unfused;
+  long long grid = (long long)num_sms() * 6;
   if (grid > total) grid = total;
   k_rot<<<(unsigned)grid, FFT_T, 0, s>>>(G, b, tw);
   count_launch();
 }
 
-// ----------------------------------------------------- instrument profile
-// FixedTargetDispersionLogSpace: one Gaussian, output i = sum_k g[k]
-// r[i + h - k] with r zero outside the grid (convolve_rv.rs:207-210).
-// Per-pixel kernels (VariableTargetDispersion / FixedTargetDispersionNonLog):
-// output i = kernel_i . r[i-h .. i+h], pixels within h of either end pass
-// through (convolve_rv.rs:213-233, 414-430).
-constexpr int GT = 256, G_TILE = 1024, G_HMAX = 256;
-
-__device__ __forceinline__ void gauss_tile(const DevStar &st, const float *src, float *dst, int N, int t0, int t1,
-                                           int glo, int ghi, float *sbuf) {
-  const int w = st.gw, h = (w - 1) / 2;
-  const int base = t0 - h;
-  for (int j = threadIdx.x; j < (t1 - t0) + 2 * h; j += blockDim.x) {
-    const int g = base + j;
-    sbuf[j] = (g >= glo && g < ghi) ? src[g] : 0.0f;
-  }
-  __syncthreads();
-  for (int i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
-    float acc = 0.0f;
-    if (st.disp_kind == DISP_FIXED) {
-      const float *g = st.gk;
-      for (int k = 0; k < w; k++) acc = fmaf(__ldg(&g[k]), sbuf[i + h - k - base], acc);
-    } else {
-      if (i < h || i >= N - h) {
-        acc = sbuf[i - base];
-      } else {
-        const float *kk = st.gk + (size_t)i * w;
-        for (int t = 0; t < w; t++) acc = fmaf(__ldg(&kk[t]), sbuf[i - h + t - base], acc);
-      }
-    }
-    dst[i] = acc;
-  }
-}
+// unfused instrument profile: src = rotation output, dst = the other buffer
+constexpr int GT = 256, G_TILE = 4096, G_HMAX = 256;
 
 __global__ void __launch_bounds__(GT) k_gauss(DevGrid G, EvalBatch b) {
   __shared__ float sbuf[G_TILE + 2 * G_HMAX];
   const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
-  if (P.status) return;
+  if (P.status || P.fused || P.hg == 0) return;
   const DevStar &st = b.stars[P.star];
-  if (st.disp_kind == DISP_NONE) return;
-  const int t0 = max(blockIdx.y * G_TILE, P.o_lo), t1 = min((int)(blockIdx.y + 1) * G_TILE, P.o_hi);
+  const int t0 = max((int)blockIdx.y * G_TILE, P.o_lo), t1 = min((int)(blockIdx.y + 1) * G_TILE, P.o_hi);
   if (t0 >= t1) return;
   const bool rot_in_b = P.m > 1;
   const float *src = (rot_in_b ? b.bufB : b.bufA) + (size_t)e * b.stride;
   float *dst = (rot_in_b ? b.bufA : b.bufB) + (size_t)e * b.stride;
-  gauss_tile(st, src, dst, G.npx, t0, t1, P.g_lo, P.g_hi, sbuf);
+  const int h = P.hg, base = t0 - h;
+  for (int j = threadIdx.x; j < (t1 - t0) + 2 * h; j += blockDim.x) {
+    const int g = base + j;
+    sbuf[j] = (g >= P.g_lo && g < P.g_hi) ? src[g] : 0.0f;
+  }
+  __syncthreads();
+  for (int i = t0 + threadIdx.x; i < t1; i += blockDim.x)
+    dst[i] = instrument(st, G.npx, i, h, [&](int t) { return sbuf[t - base]; });
 }
 
 void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
@@ -226,7 +317,14 @@ __global__ void __launch_bounds__(GT) k_gauss_alone(int N, const DevStar *stp, c
     for (int i = t0 + threadIdx.x; i < t1; i += blockDim.x) out[i] = in[i];
     return;
   }
-  gauss_tile(st, in, out, N, t0, t1, 0, N, sbuf);
+  const int h = (st.gw - 1) / 2, base = t0 - h;
+  for (int j = threadIdx.x; j < (t1 - t0) + 2 * h; j += blockDim.x) {
+    const int g = base + j;
+    sbuf[j] = (g >= 0 && g < N) ? in[g] : 0.0f;
+  }
+  __syncthreads();
+  for (int i = t0 + threadIdx.x; i < t1; i += blockDim.x)
+    out[i] = instrument(st, N, i, h, [&](int t) { return sbuf[t - base]; });
 }
 void launch_gauss_standalone(const DevGrid &G, const DevStar *star, const float *in, float *out, cudaStream_t s) {
   k_gauss_alone<<<(G.npx + G_TILE - 1) / G_TILE, GT, 0, s>>>(G.npx, star, in, out);
@@ -285,7 +383,7 @@ __global__ void k_resample_out(DevGrid G, EvalBatch b, float *out, int64_t out_s
   const EvalPrep &P = b.prep[e];
   if (P.status) return;
   const DevStar &st = b.stars[P.star];
-  const Resampler R = make_resampler(G, st, P, final_row(b, P, st.disp_kind, e), nullptr);
+  const Resampler R = make_resampler(G, st, P, final_row(b, P, e), nullptr);
   for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < st.n_obs; i += gridDim.y * blockDim.x)
     out[(size_t)e * out_stride + i] = R(i);
 }
@@ -300,8 +398,7 @@ __global__ void k_copy_broadened(DevGrid G, EvalBatch b, float *out) {
   const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
   if (P.status) return;
-  const DevStar &st = b.stars[P.star];
-  const float *row = final_row(b, P, st.disp_kind, e);
+  const float *row = final_row(b, P, e);
   for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < G.npx; i += gridDim.y * blockDim.x)
     out[(size_t)e * G.npx + i] = row[i];
 }
@@ -312,8 +409,8 @@ void launch_copy_broadened(const DevGrid &G, const EvalBatch &b, float *out, cud
   count_launch();
 }
 
-// ------------------------------------------------------------ chi2
-constexpr int CT = 512, CW = CT / 32;
+// ------------------------------------------------------------------ chi2
+constexpr int CT = 256, CW = CT / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -321,20 +418,19 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// block sum of n <= MAX_P1 per-thread doubles into out[0..n)
-__device__ __forceinline__ void block_sum_vec(const double (&v)[MAX_P1], int n, double (*ws)[MAX_P1],
-                                              double *out) {
+// block sum of K per-thread doubles into out[0..K)
+template <int K>
+__device__ __forceinline__ void block_sum_vec(const double (&v)[K], double (*ws)[MAX_P1], double *out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < MAX_P1; k++) {
-    if (k < n) {
-      const double s = warp_sum(v[k]);
-      if (lane == 0) ws[warp][k] = s;
-    }
+  for (int k = 0; k < K; k++) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) ws[warp][k] = s;
   }
   __syncthreads();
   if (warp == 0) {
-    for (int k = 0; k < n; k++) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
       double s = lane < CW ? ws[lane][k] : 0.0;
       s = warp_sum(s);
       if (lane == 0) out[k] = s;
@@ -360,134 +456,153 @@ __device__ __forceinline__ double block_sum(double v, double (*ws)[MAX_P1]) {
   return r;
 }
 
-// Legendre P_0..P_{p1-1} at x (double recurrence; the host Gram uses the
-// identical recurrence and coefficients).
-__device__ __forceinline__ void legendre(double x, int p1, double (&P)[MAX_P1]) {
-  P[0] = 1.0;
-  P[1] = x;
+// Legendre P_0..P_{K-1} at x (f32, the host Gram uses the same recurrence)
+template <int K>
+__device__ __forceinline__ void legendre(float x, float (&P)[K]) {
+  P[0] = 1.0f;
+  if (K > 1) P[1] = x;
 #pragma unroll
-  for (int k = 1; k < MAX_P1 - 1; k++) {
-    if (k + 1 < p1) {
-      const double a = (double)(2 * k + 1) / (double)(k + 1), c = (double)k / (double)(k + 1);
-      P[k + 1] = a * x * P[k] - c * P[k - 1];
-    }
+  for (int k = 1; k + 1 < K; k++) P[k + 1] = leg_step(leg_a(k), leg_c(k), x, P[k], P[k - 1]);
+}
+
+template <int K>
+__device__ __forceinline__ float poly_eval(const float *coef, float x) {
+  float P[K];
+  legendre<K>(x, P);
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < K; k++) s = fmaf(coef[k], P[k], s);
+  return s;
+}
+
+__device__ __forceinline__ void write_result(const EvalBatch &b, int e, double chi2, int status) {
+  if (threadIdx.x == 0) {
+    b.cost[e] = status ? __longlong_as_double(0x7FF8000000000000ll) : chi2;
+    b.status[e] = status;
   }
 }
 
-__device__ __forceinline__ float poly_eval(const double *coef, int p1, float xf) {
-  double P[MAX_P1];
-  legendre((double)xf, p1, P);
-  double s = 0.0;
-#pragma unroll
-  for (int k = 0; k < MAX_P1; k++)
-    if (k < p1) s += coef[k] * P[k];
-  return (float)s;
-}
-
-// CostFunction::cost after produce_model (fitting.rs:322-325): the
-// continuum fit of observed/model and the variance-weighted chi2, one CTA
-// per evaluation.
-//  chunk   (continuum_fitting.rs:216-226, 280-360): per chunk the unweighted
-//          least-squares polynomial of flux/model is the projection onto
-//          the chunk's polynomial space; it is solved here in a Legendre
-//          basis with the FP64 Cholesky factor of its Gram matrix (same
-//          space as the reference's monomial SVD, far better conditioned),
-//          then chi2 is summed over [50, N-50) with the sin^2 blend in the
-//          overlaps and divided by N - 100.
-//  linear  (continuum_fitting.rs:68-95): projection onto the design
-//          matrix's column space through its orthonormal basis Q; chi2 of
-//          the ratio-space residual over [50, N-50) divided by N.
-//  fixed   (continuum_fitting.rs:441-474), constant (484-500).
-// Moments and chi2 accumulate in FP64.
-__global__ void __launch_bounds__(CT) k_chi2(DevGrid G, EvalBatch b, const float *given) {
+// ChunkFitter::fit_continuum (continuum_fitting.rs:382-396): per chunk the
+// unweighted least-squares polynomial of flux/model (216-226) is the
+// projection onto the chunk's polynomial space; it is solved here in a
+// Legendre basis with the FP64 Cholesky factor of its Gram matrix (the same
+// space as the reference's monomial SVD, far better conditioned).  chi2 is
+// summed over [50, N-50) with the sin^2 blend in the overlaps and divided
+// by N - 100 (280-360).  Moments and chi2 accumulate in FP64.  One CTA per
+// evaluation; K = polynomial order + 1 (one instantiation per order present).
+template <int K>
+__global__ void __launch_bounds__(CT, 4) k_chi2_chunk(DevGrid G, EvalBatch b, const float *given) {
   __shared__ double ws[CW][MAX_P1];
-  __shared__ double zs[MAX_CHUNKS * MAX_P1 > MAX_LIN_K ? MAX_CHUNKS * MAX_P1 : MAX_LIN_K];
+  __shared__ double zs[MAX_CHUNKS * K];
+  __shared__ float cf32[MAX_CHUNKS * K];
   const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
+  const DevStar &st = b.stars[P.star];
+  if (st.cont_kind != CONT_CHUNK || st.p1 != K) return;
   if (P.status) {
-    if (threadIdx.x == 0) {
-      b.cost[e] = __longlong_as_double(0x7FF8000000000000ll);
-      b.status[e] = P.status;
-    }
+    write_result(b, e, 0.0, P.status);
     return;
   }
+  if (st.cont_bad) {
+    write_result(b, e, 0.0, S_CONTINUUM);
+    return;
+  }
+  const int N = st.n_obs, nc = st.n_chunks;
+  const Resampler R = make_resampler(G, st, P, given ? nullptr : final_row(b, P, e), given);
+  const float *flux = st.flux, *var = st.var;
+  for (int c = 0; c < nc; c++) {
+    const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
+    double z[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) z[k] = 0.0;
+    for (int i = lo + threadIdx.x; i < hi; i += CT) {
+      const double y = (double)(flux[i] / R(i));
+      const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
+      float Pk[K];
+      legendre<K>(xf, Pk);
+#pragma unroll
+      for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
+    }
+    block_sum_vec<K>(z, ws, zs + c * K);
+  }
+  // per-chunk FP64 Cholesky solve G c = z
+  if (threadIdx.x < nc) {
+    const int c = threadIdx.x;
+    const double *L = st.chol + (size_t)c * K * K;
+    double *z = zs + c * K;
+    double u[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double s = z[k];
+#pragma unroll
+      for (int j = 0; j < k; j++) s -= L[k * K + j] * u[j];
+      u[k] = s / L[k * K + k];
+    }
+#pragma unroll
+    for (int k = K - 1; k >= 0; k--) {
+      double s = u[k];
+#pragma unroll
+      for (int j = k + 1; j < K; j++) s -= L[j * K + k] * z[j];
+      z[k] = s / L[k * K + k];
+      cf32[c * K + k] = (float)z[k];
+    }
+    if (b.params)
+      for (int k = 0; k < K; k++) b.params[(size_t)e * b.param_stride + c * K + k] = z[k];
+  }
+  __syncthreads();
+  double acc = 0.0;
+  for (int i = 50 + threadIdx.x; i < st.cstart[1]; i += CT) {  // [50, start_1): chunk 0 alone
+    const float p = poly_eval<K>(cf32, st.xa[i]);
+    const float r = flux[i] - p * R(i);
+    acc += (double)(r * r / var[i]);
+  }
+  for (int c = 1; c < nc; c++) {
+    const int s0 = st.cstart[c], sp = st.cstop[c - 1];
+    const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
+    const float *cp = cf32 + (c - 1) * K, *cc = cf32 + c * K;
+    for (int i = s0 + threadIdx.x; i < sp; i += CT) {  // overlap: blend previous and current
+      const float pv = poly_eval<K>(cp, st.xa[i]);
+      const float cu = poly_eval<K>(cc, st.xb[i]);
+      const float f = st.fac[i];
+      const float p = pv * f + cu * (1.0f - f);
+      const float r = flux[i] - p * R(i);
+      acc += (double)(r * r / var[i]);
+    }
+    for (int i = sp + threadIdx.x; i < nx; i += CT) {
+      const float p = poly_eval<K>(cc, st.xa[i]);
+      const float r = flux[i] - p * R(i);
+      acc += (double)(r * r / var[i]);
+    }
+  }
+  const double chi2 = block_sum(acc, ws) / (double)(N - 100);
+  write_result(b, e, chi2, 0);
+}
+
+// LinearModelFitter (continuum_fitting.rs:68-95): projection onto the design
+// matrix's column space through its orthonormal basis Q; chi2 of the
+// ratio-space residual over [50, N-50) divided by N.  FixedContinuum
+// (441-474) and ConstantContinuum (484-500) too.
+__global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const float *given) {
+  __shared__ double ws[CW][MAX_P1];
+  __shared__ double zs[MAX_LIN_K];
+  const int e = blockIdx.x;
+  const EvalPrep &P = b.prep[e];
   const DevStar &st = b.stars[P.star];
+  if (st.cont_kind == CONT_CHUNK) return;
+  if (P.status) {
+    write_result(b, e, 0.0, P.status);
+    return;
+  }
+  if (st.cont_bad) {
+    write_result(b, e, 0.0, S_CONTINUUM);
+    return;
+  }
   const int N = st.n_obs;
-  const Resampler R = make_resampler(G, st, P, given ? nullptr : final_row(b, P, st.disp_kind, e), given);
+  const Resampler R = make_resampler(G, st, P, given ? nullptr : final_row(b, P, e), given);
   const float *flux = st.flux, *var = st.var;
   double chi2 = 0.0;
-  int status = 0;
   double *par = b.params ? b.params + (size_t)e * b.param_stride : nullptr;
-
-  if (st.cont_kind == CONT_CHUNK) {
-    const int nc = st.n_chunks, p1 = st.p1;
-    if (st.cont_bad) status = S_CONTINUUM;
-    else {
-      for (int c = 0; c < nc; c++) {
-        const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
-        double z[MAX_P1];
-#pragma unroll
-        for (int k = 0; k < MAX_P1; k++) z[k] = 0.0;
-        for (int i = lo + threadIdx.x; i < hi; i += CT) {
-          const float y = flux[i] / R(i);
-          const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
-          double Pk[MAX_P1];
-          legendre((double)xf, p1, Pk);
-          const double yd = (double)y;
-#pragma unroll
-          for (int k = 0; k < MAX_P1; k++)
-            if (k < p1) z[k] += Pk[k] * yd;
-        }
-        block_sum_vec(z, p1, ws, zs + c * MAX_P1);
-      }
-      // per-chunk FP64 Cholesky solve G c = z
-      if (threadIdx.x < nc) {
-        const int c = threadIdx.x;
-        const double *L = st.chol + (size_t)c * p1 * p1;
-        double *z = zs + c * MAX_P1;
-        double u[MAX_P1];
-        for (int k = 0; k < p1; k++) {
-          double s = z[k];
-          for (int j = 0; j < k; j++) s -= L[k * p1 + j] * u[j];
-          u[k] = s / L[k * p1 + k];
-        }
-        for (int k = p1 - 1; k >= 0; k--) {
-          double s = u[k];
-          for (int j = k + 1; j < p1; j++) s -= L[j * p1 + k] * z[j];
-          z[k] = s / L[k * p1 + k];
-        }
-        if (par)
-          for (int k = 0; k < p1; k++) par[c * p1 + k] = z[k];
-      }
-      __syncthreads();
-      double acc = 0.0;
-      // [50, start_1): chunk 0 alone
-      for (int i = 50 + threadIdx.x; i < st.cstart[1]; i += CT) {
-        const float p = poly_eval(zs, p1, st.xa[i]);
-        const float r = flux[i] - p * R(i);
-        acc += (double)(r * r / var[i]);
-      }
-      for (int c = 1; c < nc; c++) {
-        const int s0 = st.cstart[c], sp = st.cstop[c - 1];
-        const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
-        const double *cp = zs + (c - 1) * MAX_P1, *cc = zs + c * MAX_P1;
-        for (int i = s0 + threadIdx.x; i < sp; i += CT) {  // overlap: blend previous and current
-          const float pv = poly_eval(cp, p1, st.xa[i]);
-          const float cu = poly_eval(cc, p1, st.xb[i]);
-          const float f = st.fac[i];
-          const float p = pv * f + cu * (1.0f - f);
-          const float r = flux[i] - p * R(i);
-          acc += (double)(r * r / var[i]);
-        }
-        for (int i = sp + threadIdx.x; i < nx; i += CT) {
-          const float p = poly_eval(cc, p1, st.xa[i]);
-          const float r = flux[i] - p * R(i);
-          acc += (double)(r * r / var[i]);
-        }
-      }
-      chi2 = block_sum(acc, ws) / (double)(N - 100);
-    }
-  } else if (st.cont_kind == CONT_LINEAR) {
+  if (st.cont_kind == CONT_LINEAR) {
     const int K = st.k_lin;
     for (int g0 = 0; g0 < K; g0 += MAX_P1) {
       const int nk = min(MAX_P1, K - g0);
@@ -498,17 +613,17 @@ __global__ void __launch_bounds__(CT) k_chi2(DevGrid G, EvalBatch b, const float
         const double bd = (double)(flux[i] / R(i));
 #pragma unroll
         for (int k = 0; k < MAX_P1; k++)
-          if (k < nk) z[k] += (double)__ldg(&st.q[(size_t)(g0 + k) * N + i]) * bd;
+          if (k < nk) z[k] = fma((double)__ldg(&st.q[(size_t)(g0 + k) * N + i]), bd, z[k]);
       }
-      block_sum_vec(z, nk, ws, zs + g0);
+      block_sum_vec<MAX_P1>(z, ws, zs + g0);
     }
-    if (par && threadIdx.x < K)
+    if (par)
       for (int k = threadIdx.x; k < K; k += CT) par[k] = zs[k];
     double acc = 0.0;
     for (int i = 50 + threadIdx.x; i < N - 50; i += CT) {
       const float bb = flux[i] / R(i);
       double fit = 0.0;
-      for (int k = 0; k < K; k++) fit += (double)__ldg(&st.q[(size_t)k * N + i]) * zs[k];
+      for (int k = 0; k < K; k++) fit = fma((double)__ldg(&st.q[(size_t)k * N + i]), zs[k], fit);
       const float r = (float)fit - bb;
       acc += (double)(r / var[i] * r);
     }
@@ -534,10 +649,46 @@ __global__ void __launch_bounds__(CT) k_chi2(DevGrid G, EvalBatch b, const float
     chi2 = block_sum(acc, ws) / (double)N;
     if (par && threadIdx.x == 0) par[0] = (double)mean;
   }
-  if (threadIdx.x == 0) {
-    b.cost[e] = status ? __longlong_as_double(0x7FF8000000000000ll) : chi2;
-    b.status[e] = status;
+  write_result(b, e, chi2, 0);
+}
+
+template <int K>
+static void launch_chunk(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
+  k_chi2_chunk<K><<<b.E, CT, 0, s>>>(G, b, given);
+  count_launch();
+}
+
+static void launch_chi2_impl(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
+  if (b.E <= 0) return;
+  const uint32_t m = b.chunk_p1_mask;
+  if (m & (1u << 1)) launch_chunk<1>(G, b, given, s);
+  if (m & (1u << 2)) launch_chunk<2>(G, b, given, s);
+  if (m & (1u << 3)) launch_chunk<3>(G, b, given, s);
+  if (m & (1u << 4)) launch_chunk<4>(G, b, given, s);
+  if (m & (1u << 5)) launch_chunk<5>(G, b, given, s);
+  if (m & (1u << 6)) launch_chunk<6>(G, b, given, s);
+  if (m & (1u << 7)) launch_chunk<7>(G, b, given, s);
+  if (m & (1u << 8)) launch_chunk<8>(G, b, given, s);
+  if (m & (1u << 9)) launch_chunk<9>(G, b, given, s);
+  if (m & (1u << 10)) launch_chunk<10>(G, b, given, s);
+  if (m & (1u << 11)) launch_chunk<11>(G, b, given, s);
+  if (m & (1u << 12)) launch_chunk<12>(G, b, given, s);
+  if (m & (1u << 13)) launch_chunk<13>(G, b, given, s);
+  if (m & (1u << 14)) launch_chunk<14>(G, b, given, s);
+  if (m & (1u << 15)) launch_chunk<15>(G, b, given, s);
+  if (m & (1u << 16)) launch_chunk<16>(G, b, given, s);
+  if (b.other_cont) {
+    k_chi2_other<<<b.E, CT, 0, s>>>(G, b, given);
+    count_launch();
   }
+}
+
+void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) { launch_chi2_impl(G, b, nullptr, s); }
+
+// ContinuumFitter::fit_continuum on a given model (lib.rs:862-874): the
+// evaluations' resampled model is `given` (observed pixels).
+void launch_chi2_given(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
+  launch_chi2_impl(G, b, given, s);
 }
 
 // per-evaluation status when no chi2 is computed (model / spectrum outputs)
@@ -550,36 +701,46 @@ void launch_prep_status(const EvalBatch &b, cudaStream_t s) {
   count_launch();
 }
 
-void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
-  if (b.E <= 0) return;
-  k_chi2<<<b.E, CT, 0, s>>>(G, b, nullptr);
-  count_launch();
-}
-
-// ContinuumFitter::fit_continuum on a given model (lib.rs:862-874): the
-// evaluations' resampled model is `given` (observed pixels).
-void launch_chi2_given(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
-  if (b.E <= 0) return;
-  k_chi2<<<b.E, CT, 0, s>>>(G, b, given);
-  count_launch();
-}
-
 // ChunkFitter::build_continuum_from_chunks (continuum_fitting.rs:228-278)
 // from Legendre coefficients: continuum = blend of the chunk polynomials.
+template <int K>
+__device__ float build_one(const DevStar &st, const double *coef, int i) {
+  const int nc = st.n_chunks;
+  int c = 0;
+  while (c + 1 < nc && i >= st.cstart[c + 1]) c++;
+  float cp[K], cc[K];
+  for (int k = 0; k < K; k++) cc[k] = (float)coef[c * MAX_P1 + k];
+  if (c > 0 && i < st.cstop[c - 1]) {
+    for (int k = 0; k < K; k++) cp[k] = (float)coef[(c - 1) * MAX_P1 + k];
+    const float pv = poly_eval<K>(cp, st.xa[i]);
+    const float cu = poly_eval<K>(cc, st.xb[i]);
+    const float f = st.fac[i];
+    return pv * f + cu * (1.0f - f);
+  }
+  return poly_eval<K>(cc, st.xa[i]);
+}
+
 __global__ void k_build_chunk(const DevStar *stp, const double *coef, int n, float *out) {
   const DevStar &st = *stp;
-  const int nc = st.n_chunks, p1 = st.p1;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int c = 0;
-    while (c + 1 < nc && i >= st.cstart[c + 1]) c++;
     float v;
-    if (c > 0 && i < st.cstop[c - 1]) {
-      const float pv = poly_eval(coef + (c - 1) * MAX_P1, p1, st.xa[i]);
-      const float cu = poly_eval(coef + c * MAX_P1, p1, st.xb[i]);
-      const float f = st.fac[i];
-      v = pv * f + cu * (1.0f - f);
-    } else {
-      v = poly_eval(coef + c * MAX_P1, p1, st.xa[i]);
+    switch (st.p1) {
+      case 1: v = build_one<1>(st, coef, i); break;
+      case 2: v = build_one<2>(st, coef, i); break;
+      case 3: v = build_one<3>(st, coef, i); break;
+      case 4: v = build_one<4>(st, coef, i); break;
+      case 5: v = build_one<5>(st, coef, i); break;
+      case 6: v = build_one<6>(st, coef, i); break;
+      case 7: v = build_one<7>(st, coef, i); break;
+      case 8: v = build_one<8>(st, coef, i); break;
+      case 9: v = build_one<9>(st, coef, i); break;
+      case 10: v = build_one<10>(st, coef, i); break;
+      case 11: v = build_one<11>(st, coef, i); break;
+      case 12: v = build_one<12>(st, coef, i); break;
+      case 13: v = build_one<13>(st, coef, i); break;
+      case 14: v = build_one<14>(st, coef, i); break;
+      case 15: v = build_one<15>(st, coef, i); break;
+      default: v = build_one<16>(st, coef, i); break;
     }
     out[i] = v;
   }
@@ -587,6 +748,39 @@ __global__ void k_build_chunk(const DevStar *stp, const double *coef, int n, flo
 void launch_build_chunk(const DevStar *star, const double *coef, int n, float *out, cudaStream_t s) {
   k_build_chunk<<<(n + 255) / 256, 256, 0, s>>>(star, coef, n, out);
   count_launch();
+}
+
+void pipeline_pairs(int npx, int max_m, int max_hg, int *max_pairs, int *max_pairs_unfused, int *may_unfuse) {
+  const int wide = (max_m - 1) + 2 * max_hg;
+  *may_unfuse = wide > FFTN - MIN_FUSED_OUTPUTS ? 1 : 0;
+  if (max_m <= 1 && max_hg == 0) {
+    *max_pairs = 0;
+  } else {
+    const int V = *may_unfuse ? MIN_FUSED_OUTPUTS : FFTN - wide;
+    const int nblk = (npx + V - 1) / V;
+    *max_pairs = (nblk + 1) / 2;
+  }
+  if (*may_unfuse && max_m > 1) {
+    const int V = FFTN - (max_m - 1);
+    const int nblk = (npx + V - 1) / V;
+    *max_pairs_unfused = (nblk + 1) / 2;
+  } else {
+    *max_pairs_unfused = 0;
+  }
+}
+
+void launch_pipeline(const DevGrid &G, const EvalBatch &b, const float2 *tw, const PipelineOpts &o, cudaStream_t s) {
+  if (o.full_window) launch_prep_full(G, b, s);
+  else launch_prep(G, b, s);
+  if (o.rot) launch_rotker(G, b, tw, s);
+  launch_interp(G, b, s);
+  launch_broaden(G, b, tw, s);
+  if (o.may_unfuse) {
+    launch_rot(G, b, tw, s);
+    launch_gauss(G, b, s);
+  }
+  if (b.need_chi2) launch_chi2(G, b, s);
+  else if (b.status) launch_prep_status(b, s);
 }
 
 }  // namespace pb

@@ -21,15 +21,31 @@ struct EvalBatch {
   int *status;               // [E]
   double *params;            // [E][param_stride] or null
   int param_stride;
-  int max_pairs;             // max ceil(nblk/2) over the batch
+  int max_pairs;             // fused broadening: max ceil(nblk/2) over the batch
+  int max_pairs_unfused;     // unfused rotation FFT: max ceil(nblk/2) (0: none can occur)
   int need_chi2;
+  uint32_t chunk_p1_mask;    // bit p1 set: a chunk continuum with p1 coefficients is present
+  int other_cont;            // a linear / fixed / constant continuum is present
 };
+
+// Everything from the preparation to chi2 (or to the outputs) for one batch.
+struct PipelineOpts {
+  int full_window = 0;       // every synthetic pixel, no resampling (interpolate entry points)
+  int rot = 1;               // some evaluation may rotate (launch the rotation spectra)
+  int may_unfuse = 0;        // some evaluation may need the unfused path
+};
+void launch_pipeline(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, const PipelineOpts &o,
+                     cudaStream_t s);
+// pair counts for a batch whose widest rotation is max_m taps and widest
+// instrument half width max_hg
+void pipeline_pairs(int npx, int max_m, int max_hg, int *max_pairs, int *max_pairs_unfused, int *may_unfuse);
 
 void launch_prep(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // same, for entry points that need every synthetic pixel and no resampling
 void launch_prep_full(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_rotker(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_rot(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s);

@@ -190,18 +190,16 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   b.stride = stride;
   b.cost = out;
   b.status = status;
-  // labels live on the device, so the rotation blocks are sized for the
-  // widest kernel the reference accepts (2048 taps); work items beyond an
+  // labels live on the device, so the blocks are sized for the widest
+  // rotation kernel the reference accepts (2048 taps); work items beyond an
   // evaluation's own blocks return at once
-  const int V = 1;  // FFTN - (2048 - 1)
-  b.max_pairs = (int)(((int64_t)(G.npx + V - 1) / V + 1) / 2);
+  const int hg = star.disp_kind == DISP_NONE ? 0 : (star.gw - 1) / 2;
+  PipelineOpts o;
+  pipeline_pairs(G.npx, FFTN, hg, &b.max_pairs, &b.max_pairs_unfused, &o.may_unfuse);
   b.need_chi2 = 1;
-  launch_prep(G, b, s);
-  launch_rotker(G, b, S->twiddle, s);
-  launch_interp(G, b, s);
-  launch_rot(G, b, S->twiddle, s);
-  launch_gauss(G, b, s);
-  launch_chi2(G, b, s);
+  b.chunk_p1_mask = star.cont_kind == CONT_CHUNK ? 1u << star.p1 : 0u;
+  b.other_cont = star.cont_kind == CONT_CHUNK ? 0 : 1;
+  launch_pipeline(G, b, S->twiddle, o, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     g_noalloc_err = std::string("kernel launch failed: ") + cudaGetErrorString(e);

@@ -105,8 +105,21 @@ __global__ void k_prep(DevGrid G, EvalBatch b, int full_window) {
   P.o_lo = o_lo; P.o_hi = o_hi;
   P.g_lo = g_lo; P.g_hi = g_hi;
   P.i_lo = i_lo; P.i_hi = i_hi;
-  const int V = FFTN - (m - 1);
-  P.nblk = m > 1 ? (g_hi - g_lo + V - 1) / V : 0;
+  P.hg = hg;
+  // fused: each 2048-point block yields Vf final outputs; the rotation halo
+  // (m - 1) and the instrument halo (2 hg) both come out of the block
+  const int Vf = FFTN - (m - 1) - 2 * hg;
+  const bool work = m > 1 || hg > 0;
+  if (Vf >= MIN_FUSED_OUTPUTS) {
+    P.fused = 1;
+    P.nblk = work ? (o_hi - o_lo + Vf - 1) / Vf : 0;
+    P.final_in_b = work ? 1 : 0;
+  } else {  // very wide kernels: rotation FFT into B, instrument profile into A
+    P.fused = 0;
+    const int V = FFTN - (m - 1);
+    P.nblk = m > 1 ? (g_hi - g_lo + V - 1) / V : 0;
+    P.final_in_b = hg > 0 ? (m > 1 ? 0 : 1) : (m > 1 ? 1 : 0);
+  }
   P.status = status;
 }
 

@@ -899,8 +899,8 @@ class BatchFit:
     def profile_step(self) -> dict:
         out = np.zeros(12)
         check(lib().pasta_batch_profile_step(self._h, ptr(out)))
-        names = ["update_ms", "prep_ms", "rotker_ms", "interp_ms", "rot_ms", "gauss_ms", "chi2_ms", "best_ms",
-                 "interp_px", "evals", "obs_px", "rot_blocks"]
+        names = ["update_ms", "prep_ms", "rotker_ms", "interp_ms", "broaden_ms", "unfused_ms", "chi2_ms", "best_ms",
+                 "interp_px", "evals", "obs_px", "broaden_blocks"]
         return dict(zip(names, out.tolist()))
 
     def info(self) -> dict:
