@@ -101,6 +101,7 @@ struct DevStar {
   double wl_min, wl_max;      // extreme observed wavelengths (windows on NonUniform grids)
   double fidx_min, fidx_max;  // extreme float indices (windows on uniform grids)
   const float *gk;      // DISP_FIXED: [gw]; DISP_PIXEL: [npx][gw]
+  const float2 *gspec;  // DISP_FIXED: 2048-point spectrum of gk (1025 bins), else null
   const int *cstart, *cstop;  // chunk bounds
   const float *xa, *xb, *fac; // per observed pixel: coordinate in lower/upper chunk, blend factor
   const double *chol;   // per chunk: p1 x p1 lower Cholesky factor of the Legendre Gram (row-major)

@@ -230,7 +230,40 @@ struct pasta_dispersion {
   std::vector<float> gk;  // fixed: [gw]; per pixel: [synth_n][gw]
   DBuf<double> dfidx, dwl;
   DBuf<float> dgk;
+  DBuf<float2> dgspec;  // fixed kernel: 2048-point spectrum (1025 bins)
 };
+
+namespace {
+// Spectrum of a short real kernel zero-padded to 2048 points, in double
+// (radix-2, iterative), returned as 1025 f32 bins.
+std::vector<float2> kernel_spectrum(const std::vector<float> &k) {
+  const int n = FFTN;
+  std::vector<double> re(n, 0.0), im(n, 0.0);
+  for (size_t i = 0; i < k.size() && i < (size_t)n; i++) re[i] = k[i];
+  for (int i = 1, j = 0; i < n; i++) {  // bit reversal
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) { std::swap(re[i], re[j]); std::swap(im[i], im[j]); }
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    const double ang = -2.0 * M_PI / len;
+    for (int i = 0; i < n; i += len)
+      for (int j = 0; j < len / 2; j++) {
+        const double wr = std::cos(ang * j), wi = std::sin(ang * j);
+        const double ar = re[i + j + len / 2], ai = im[i + j + len / 2];
+        const double vr = ar * wr - ai * wi, vi = ar * wi + ai * wr;
+        re[i + j + len / 2] = re[i + j] - vr;
+        im[i + j + len / 2] = im[i + j] - vi;
+        re[i + j] += vr;
+        im[i + j] += vi;
+      }
+  }
+  std::vector<float2> out(n / 2 + 1);
+  for (int i = 0; i <= n / 2; i++) out[i] = make_float2((float)re[i], (float)im[i]);
+  return out;
+}
+}  // namespace
 
 namespace {
 
@@ -544,6 +577,7 @@ DevStar make_star(const pasta_dispersion *d, const pasta_continuum *c, const flo
     s.wl_min = d->wl_min; s.wl_max = d->wl_max;
     s.fidx_min = d->fidx_min; s.fidx_max = d->fidx_max;
     s.gk = d->dgk.p;
+    s.gspec = d->dgspec.p;
   }
   if (c) {
     s.cont_kind = c->kind;
@@ -1478,6 +1512,7 @@ int pasta_dispersion_create(int synth_kind, double synth_a, double synth_b, int6
     d->dfidx.upload(d->fidx);
     d->dwl.upload(d->wl);
     if (!d->gk.empty()) d->dgk.upload(d->gk);
+    if (d->dev_kind == DISP_FIXED) d->dgspec.upload(kernel_spectrum(d->gk));
     *out = d.release();
   });
 }

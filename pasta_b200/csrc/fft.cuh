@@ -2,9 +2,10 @@
 //
 // Stockham autosort (Govindaraju et al., "High performance discrete Fourier
 // transforms on graphics processors", SC 2008) with radices 8, 8, 8, 4.
-// Data live in shared memory as separate real/imaginary float arrays with
-// one pad word every 32 entries, which keeps the strided stage reads and
-// the first stages' scattered writes off a single bank.  Twiddles
+// Data live in shared memory as separate real/imaginary float arrays whose
+// index is XOR-swizzled within each 32-word row (bits 0-4 ^= bits 3-7):
+// every stage's strided reads and scattered writes, and the linear
+// accesses, then touch 32 distinct banks per warp.  Twiddles
 // W_2048^k = exp(-2 pi i k / 2048) come from a table the host computed in
 // double.  Forward is unnormalised; the inverse is unnormalised too
 // (caller scales by 1/2048, like convolve_rv.rs:153-154).
@@ -14,8 +15,8 @@
 namespace pb {
 
 constexpr int FFT_T = 256;
-constexpr int FFT_SM = 2048 + 64;
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 5); }
+constexpr int FFT_SM = 2048;
+__device__ __forceinline__ int pidx(int i) { return (i & ~31) | ((i ^ (i >> 3)) & 31); }
 
 struct cf {
   float x, y;
@@ -69,12 +70,26 @@ __device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const fl
 #pragma unroll
     for (int r = 0; r < R; r++) {
       const int a = pidx(j + r * J);
-      cf x = {re[a], im[a]};
-      if (r > 0 && jm != 0) {
-        float2 w = __ldg(&tw[(jm * r * step) & (N - 1)]);
-        x = cmul(x, cf{w.x, INV ? -w.y : w.y});
+      v[q][r] = cf{re[a], im[a]};
+    }
+    if (jm != 0) {
+      // twiddles W^(jm r step): W^1, W^2, W^4 from the table, the others by
+      // at most two multiplications
+      const int k1 = jm * step;
+      const float2 t1 = __ldg(&tw[k1 & (N - 1)]), t2 = __ldg(&tw[(2 * k1) & (N - 1)]);
+      const cf w1{t1.x, INV ? -t1.y : t1.y}, w2{t2.x, INV ? -t2.y : t2.y};
+      v[q][1] = cmul(v[q][1], w1);
+      v[q][2] = cmul(v[q][2], w2);
+      const cf w3 = cmul(w1, w2);
+      v[q][3] = cmul(v[q][3], w3);
+      if constexpr (R == 8) {
+        const float2 t4 = __ldg(&tw[(4 * k1) & (N - 1)]);
+        const cf w4{t4.x, INV ? -t4.y : t4.y};
+        v[q][4] = cmul(v[q][4], w4);
+        v[q][5] = cmul(v[q][5], cmul(w4, w1));
+        v[q][6] = cmul(v[q][6], cmul(w4, w2));
+        v[q][7] = cmul(v[q][7], cmul(w4, w3));
       }
-      v[q][r] = x;
     }
   }
   __syncthreads();

@@ -49,30 +49,53 @@ __global__ void __launch_bounds__(IT_T) k_interp(DevGrid G, EvalBatch b) {
   const int t0 = blockIdx.y * IT_TILE;
   const int ilo = P.i_lo, ihi = P.i_hi;
   if (t0 >= ihi || t0 + IT_TILE <= ilo) return;
+  // the neighbours with a non-zero weight, compacted and padded to a
+  // multiple of 8 with zero-weight entries (which add exactly 0), so the
+  // main loop issues its loads in branch-free groups of 8
   __shared__ const uint16_t *rows[64];
   __shared__ float ws[64], fs[64], wf[64];
-  if (threadIdx.x < 64) {
-    const int c = P.cols[threadIdx.x];
-    const float f = c >= 0 ? G.factor[c] : 0.0f;
-    const float w = c >= 0 ? P.w[threadIdx.x] : 0.0f;
-    ws[threadIdx.x] = w;
-    fs[threadIdx.x] = f;
-    wf[threadIdx.x] = w * f;
-    rows[threadIdx.x] = c >= 0 ? G.spectra + (size_t)c * G.stride : G.spectra;
+  __shared__ int nnz;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int base = 0;
+    for (int h = 0; h < 2; h++) {
+      const int n = h * 32 + lane;
+      const int c = P.cols[n];
+      const float f = c >= 0 ? G.factor[c] : 0.0f;
+      const float w = c >= 0 ? P.w[n] : 0.0f;
+      const bool keep = w * f != 0.0f;
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int pos = base + __popc(bal & ((1u << lane) - 1u));
+        ws[pos] = w;
+        fs[pos] = f;
+        wf[pos] = w * f;
+        rows[pos] = G.spectra + (size_t)c * G.stride;
+      }
+      base += __popc(bal);
+    }
+    const int padded = (base + 7) & ~7;
+    for (int pos = base + lane; pos < padded; pos += 32) {
+      ws[pos] = 0.0f;
+      fs[pos] = 0.0f;
+      wf[pos] = 0.0f;
+      rows[pos] = G.spectra;
+    }
+    if (lane == 0) nnz = padded;
   }
   __syncthreads();
   const int px = t0 + threadIdx.x * 8;
   if (px < ilo || px >= ihi) return;
   float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e * b.stride + px);
+  const int nn = nnz;
   if (px + 8 <= G.tail_start) {
     float2 acc[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) acc[k] = make_float2(0.0f, 0.0f);
     const float2 bias = make_float2(-8388608.0f, -8388608.0f);
-#pragma unroll 16
-    for (int n = 0; n < 64; n++) {
+#pragma unroll 8
+    for (int n = 0; n < nn; n++) {
       const float w = wf[n];
-      if (w == 0.0f) continue;
       const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rows[n] + px));
       const float2 w2 = make_float2(w, w);
       const uint32_t u[4] = {q.x, q.y, q.z, q.w};
@@ -92,8 +115,7 @@ __global__ void __launch_bounds__(IT_T) k_interp(DevGrid G, EvalBatch b) {
   float acc[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) acc[k] = 0.0f;
-  for (int n = 0; n < 64; n++) {
-    if (ws[n] == 0.0f) continue;
+  for (int n = 0; n < nn; n++) {
     const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rows[n] + px));
     const float wn = ws[n], fn = fs[n];
     const uint32_t u[4] = {q.x, q.y, q.z, q.w};
@@ -148,8 +170,9 @@ __device__ __forceinline__ float instrument(const DevStar &st, int N, int i, int
 // products separate after the inverse).  Rotation outputs outside [0, N)
 // are zero, like the reference's cropped segment.  With the identity
 // rotation the FFT is skipped.
-__global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   __shared__ float re[FFT_SM], im[FFT_SM];
+  __shared__ float gks[2 * 255 + 1];  // the fixed instrument kernel of the current item
   const long long total = (long long)b.E * b.max_pairs;
   const int N = G.npx;
   for (long long item = blockIdx.x; item < total; item += gridDim.x) {
@@ -172,16 +195,31 @@ __global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, co
       re[pidx(t)] = (j0 >= ilo && j0 < ihi) ? x[j0] : 0.0f;
       im[pidx(t)] = (has1 && j1 >= ilo && j1 < ihi) ? x[j1] : 0.0f;
     }
+    const bool fixedk = hg > 0 && st.disp_kind == DISP_FIXED;
+    const int gw = 2 * hg + 1;
+    if (fixedk)
+      for (int t = threadIdx.x; t < gw; t += FFT_T) gks[t] = st.gk[t];
     __syncthreads();
     int base = 0;  // data index of rotation output (s - hg)
+    // Away from the grid ends the Gaussian acts on rotation outputs that are
+    // all inside [0, N), where rotation-then-Gaussian equals one convolution
+    // with the combined kernel: multiply the spectra and skip the taps.
+    const int e_last = min((has1 ? s1 : s0) + V, ohi);
+    const bool fold = fixedk && m > 1 && st.gspec != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     if (m > 1) {
       fft2048<false>(re, im, tw);
       const float2 *H = b.H + (size_t)e * 1025;
       for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
         float2 h = k <= 1024 ? H[k] : H[FFTN - k];
         if (k > 1024) h.y = -h.y;
+        cf hk{h.x, h.y};
+        if (fold) {
+          float2 g = k <= 1024 ? st.gspec[k] : st.gspec[FFTN - k];
+          if (k > 1024) g.y = -g.y;
+          hk = cmul(hk, cf{g.x, g.y});
+        }
         const int a = pidx(k);
-        const cf z = cmul(cf{re[a], im[a]}, cf{h.x, h.y});
+        const cf z = cmul(cf{re[a], im[a]}, hk);
         re[a] = z.x;
         im[a] = z.y;
       }
@@ -189,6 +227,16 @@ __global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, co
       fft2048<true>(re, im, tw);
       base = m - 1;
       const float sc = 1.0f / 2048.0f;
+      if (fold) {  // output i sits at base + 2 hg + (i - s)
+        float *y = b.bufB + (size_t)e * b.stride;
+        for (int u = threadIdx.x; u < V; u += FFT_T) {
+          const int i0 = s0 + u, i1 = s1 + u;
+          if (i0 < ohi) y[i0] = re[pidx(base + 2 * hg + u)] * sc;
+          if (has1 && i1 < ohi) y[i1] = im[pidx(base + 2 * hg + u)] * sc;
+        }
+        __syncthreads();
+        continue;
+      }
       for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
         const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
         re[pidx(t)] = (i0 >= 0 && i0 < N) ? re[pidx(t)] * sc : 0.0f;
@@ -198,14 +246,27 @@ __global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, co
     }
     float *y = b.bufB + (size_t)e * b.stride;
     for (int u = threadIdx.x; u < V; u += FFT_T) {
-      const int i0 = s0 + u;
-      if (i0 < ohi)
-        y[i0] = hg > 0 ? instrument(st, N, i0, hg, [&](int i) { return re[pidx(base + i - (s0 - hg))]; })
-                       : re[pidx(base + u)];
-      const int i1 = s1 + u;
-      if (has1 && i1 < ohi)
-        y[i1] = hg > 0 ? instrument(st, N, i1, hg, [&](int i) { return im[pidx(base + i - (s1 - hg))]; })
-                       : im[pidx(base + u)];
+      const int i0 = s0 + u, i1 = s1 + u;
+      float v0, v1;
+      if (hg == 0) {
+        v0 = re[pidx(base + u)];
+        v1 = im[pidx(base + u)];
+      } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at base + (i - s + hg)
+        float a0 = 0.0f, a1 = 0.0f;
+        for (int k = 0; k < gw; k++) {
+          const float g = gks[k];
+          const int t = pidx(base + u + 2 * hg - k);
+          a0 = fmaf(g, re[t], a0);
+          a1 = fmaf(g, im[t], a1);
+        }
+        v0 = a0;
+        v1 = a1;
+      } else {
+        v0 = instrument(st, N, i0, hg, [&](int i) { return re[pidx(base + i - (s0 - hg))]; });
+        v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return im[pidx(base + i - (s1 - hg))]; }) : 0.0f;
+      }
+      if (i0 < ohi) y[i0] = v0;
+      if (has1 && i1 < ohi) y[i1] = v1;
     }
     __syncthreads();
   }
@@ -214,7 +275,7 @@ __global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, co
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cudaStream_t s) {
   if (b.E <= 0 || b.max_pairs <= 0) return;
   const long long total = (long long)b.E * b.max_pairs;
-  long long grid = (long long)num_sms() * 6;
+  long long grid = (long long)num_sms() * 4;  // persistent: the CTAs that fit at once (64 regs x 256)
   if (grid > total) grid = total;
   k_broaden<<<(unsigned)grid, FFT_T, 0, s>>>(G, b, tw);
   count_launch();
@@ -515,6 +576,7 @@ __global__ void __launch_bounds__(CT, 4) k_chi2_chunk(DevGrid G, EvalBatch b, co
     double z[K];
 #pragma unroll
     for (int k = 0; k < K; k++) z[k] = 0.0;
+#pragma unroll 4
     for (int i = lo + threadIdx.x; i < hi; i += CT) {
       const double y = (double)(flux[i] / R(i));
       const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
@@ -560,6 +622,7 @@ __global__ void __launch_bounds__(CT, 4) k_chi2_chunk(DevGrid G, EvalBatch b, co
     const int s0 = st.cstart[c], sp = st.cstop[c - 1];
     const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
     const float *cp = cf32 + (c - 1) * K, *cc = cf32 + c * K;
+#pragma unroll 2
     for (int i = s0 + threadIdx.x; i < sp; i += CT) {  // overlap: blend previous and current
       const float pv = poly_eval<K>(cp, st.xa[i]);
       const float cu = poly_eval<K>(cc, st.xb[i]);
@@ -568,6 +631,7 @@ __global__ void __launch_bounds__(CT, 4) k_chi2_chunk(DevGrid G, EvalBatch b, co
       const float r = flux[i] - p * R(i);
       acc += (double)(r * r / var[i]);
     }
+#pragma unroll 4
     for (int i = sp + threadIdx.x; i < nx; i += CT) {
       const float p = poly_eval<K>(cc, st.xa[i]);
       const float r = flux[i] - p * R(i);
