@@ -230,9 +230,9 @@ int pasta_fit_many(const pasta_grid *g, int64_t S,
  * time between CUDA events on the library's stream, finish runs the final
  * refit and returns results.  profile_step runs one step stage by stage and
  * writes 12 doubles: stage times in ms (swarm update, prep, rotation
- * spectra, interpolation, rotation FFT, instrument profile, chi2, best
- * update), then the step's interpolated pixels, evaluations, observed
- * pixels and rotation FFT blocks.  info: stars, particles, evaluations per
+ * spectra, interpolation, fused broadening, unfused rotation + instrument
+ * profile, resampling + chi2, best update), then the step's interpolated
+ * pixels, evaluations, observed pixels and broadening blocks.  info: stars, particles, evaluations per
  * step, iterations, steps done, kernels per captured step.  No counterpart
  * in the reference (its fit runs to completion inside argmin's Executor). */
 typedef struct pasta_batch pasta_batch;

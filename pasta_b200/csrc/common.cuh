@@ -94,6 +94,7 @@ struct DevStar {
   int k_lin;         // linear model columns
   int ignore;        // fixed continuum ignore_first_and_last
   int cont_bad;      // continuum fitter cannot evaluate chi2 on this spectrum
+  int obs_sorted;    // observed float indices never decrease (the resampling index is monotone)
   const float *flux, *var;
   const double *fidx;   // float index of every observed pixel in the synth grid
   const double *wl_obs; // observed wavelengths (NonUniform synth grids)
@@ -118,6 +119,8 @@ struct EvalPrep {
   int hg;         // instrument-profile half width (0: no instrument profile)
   int fused;      // 1: rotation and instrument profile in one kernel (k_broaden)
   int final_in_b; // 1: the broadened spectrum ends in buffer B, else in A
+  int epi;        // 1: k_broaden resamples to the observed pixels itself (no synth row)
+  int mobs_in_b;  // model at the observed pixels: 1 = row of B, 0 = row of A
   int o_lo, o_hi; // synth pixels the resampler reads [o_lo, o_hi)
   int g_lo, g_hi; // rotation outputs the Gaussian reads [g_lo, g_hi)
   int i_lo, i_hi; // interpolated pixels needed [i_lo, i_hi) (multiples of 8)

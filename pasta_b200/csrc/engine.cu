@@ -160,23 +160,38 @@ double now_s() {
 // =================================================================== grid
 struct Workspace {
   int64_t cap = 0, stride = 0;
+  int bnd_stride = 0;
   int64_t gen = 0;  // bumped on every reallocation (captured graphs compare it)
   DBuf<float> A, B;
   DBuf<float2> H;
   DBuf<EvalPrep> prep;
-  void ensure(int64_t want, int64_t str) {
-    if (want <= cap && str == stride) return;
+  DBuf<int> bnd;       // first observed pixel per broadening block
+  DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
+  DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
+  void ensure(int64_t want, int64_t str, int bstr) {
+    if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); prep.release();
+    bnd.release(); ccoef.release(); cpart.release();
     cap = 0;
     A.alloc((size_t)want * str);
     B.alloc((size_t)want * str);
     H.alloc((size_t)want * 1025);
     prep.alloc((size_t)want);
+    bnd.alloc((size_t)want * bstr);
+    ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
+    cpart.alloc((size_t)want * MAX_CHUNKS);
     cap = want;
     stride = str;
+    bnd_stride = bstr;
     gen++;
   }
 };
+
+// bytes of workspace one evaluation takes with rows of `stride` floats
+int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
+  return stride * 8 + 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)bnd_stride * 4 +
+         (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8);
+}
 
 struct pasta_grid {
   int dev = 0;
@@ -199,9 +214,10 @@ struct pasta_grid {
 
 namespace {
 
-int64_t workspace_cap(const pasta_grid *g, int64_t want) {
+int64_t workspace_cap(const pasta_grid *g, int64_t want, int64_t stride) {
   // per evaluation: two spectrum rows + rotation half spectrum + prep record
-  const int64_t per = g->stride * 8 + 1025 * 8 + (int64_t)sizeof(EvalPrep);
+  // + block bounds + chunk coefficients and partial sums
+  const int64_t per = workspace_bytes_per_eval(stride, bnd_stride_for((int)g->npx));
   // default: up to 40% of the device's memory for evaluation workspaces
   int64_t budget = 24ll << 30;
   size_t fr = 0, tot = 0;
@@ -209,7 +225,8 @@ int64_t workspace_cap(const pasta_grid *g, int64_t want) {
   if (have) budget = (int64_t)(0.4 * (double)tot);
   if (const char *e = getenv("PASTA_WORKSPACE_BYTES")) budget = atoll(e);
   if (have) {
-    const int64_t avail = (int64_t)fr - (2ll << 30) + (int64_t)g->ws.cap * per;
+    const int64_t avail = (int64_t)fr - (2ll << 30) +
+                          (int64_t)g->ws.cap * workspace_bytes_per_eval(g->ws.stride, g->ws.bnd_stride);
     if (avail < budget) budget = avail;
   }
   int64_t cap = std::max<int64_t>(1, budget / per);
@@ -226,6 +243,7 @@ struct pasta_dispersion {
   int64_t synth_n = 0;
   std::vector<double> synth_vals, wl, fidx;
   double wl_first = 0, wl_last = 0, wl_min = 0, wl_max = 0, fidx_min = 0, fidx_max = 0;
+  int sorted = 0;  // observed wavelengths and float indices never decrease
   int gw = 0;
   std::vector<float> gk;  // fixed: [gw]; per pixel: [synth_n][gw]
   DBuf<double> dfidx, dwl;
@@ -576,6 +594,7 @@ DevStar make_star(const pasta_dispersion *d, const pasta_continuum *c, const flo
     s.wl_first = d->wl_first; s.wl_last = d->wl_last;
     s.wl_min = d->wl_min; s.wl_max = d->wl_max;
     s.fidx_min = d->fidx_min; s.fidx_max = d->fidx_max;
+    s.obs_sorted = d->sorted;
     s.gk = d->dgk.p;
     s.gspec = d->dgspec.p;
   }
@@ -621,18 +640,26 @@ struct EvalArgs {
   int max_m = 1;
   int max_hg = 0;                // widest instrument half width among the stars
   uint32_t chunk_p1_mask = 0;    // chunk continua present, by coefficient count
+  int max_chunks = 0;            // most chunks of those continua
   int other_cont = 0;            // linear / fixed / constant continua present
+  int64_t max_nobs = 0;          // longest observed spectrum
   float *out_obs = nullptr;
   int64_t out_stride = 0;
   float *out_synth = nullptr;
   const float *given = nullptr;  // model given at observed pixels
+  int64_t given_stride = 0;      // floats between the given rows of consecutive evaluations
 };
 
 // continuum kinds and instrument widths of the stars a batch can touch
 void star_kinds(const std::vector<DevStar> &h, EvalArgs &a) {
   for (const auto &st : h) {
-    if (st.cont_kind == CONT_CHUNK) a.chunk_p1_mask |= 1u << st.p1;
-    else a.other_cont = 1;
+    if (st.cont_kind == CONT_CHUNK) {
+      a.chunk_p1_mask |= 1u << st.p1;
+      a.max_chunks = std::max(a.max_chunks, st.n_chunks);
+    } else {
+      a.other_cont = 1;
+    }
+    a.max_nobs = std::max<int64_t>(a.max_nobs, st.n_obs);
     if (st.disp_kind != DISP_NONE) a.max_hg = std::max(a.max_hg, (st.gw - 1) / 2);
   }
 }
@@ -641,6 +668,39 @@ int width_upper_bound(const pasta_grid *g, double vsini_hi) {
   if (g->d.dvelo <= 0.0 || !(vsini_hi > 0.0)) return 1;
   int w = rotation_width(vsini_hi, g->d.dvelo);
   return std::min(w, FFTN);
+}
+
+// The batch of evaluations [off, off + cnt) of a in the grid's workspace.
+EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt) {
+  if (a.max_nobs > g->ws.stride) fail(PASTA_E_INTERNAL, "workspace rows are shorter than the observed spectrum");
+  EvalBatch b{};
+  b.E = (int)cnt;
+  b.labels = a.labels ? a.labels + 5 * off : nullptr;
+  b.eval_star = a.eval_star + off;
+  b.eval_active = a.eval_active ? a.eval_active + off : nullptr;
+  b.stars = a.stars;
+  b.prep = g->ws.prep.p;
+  b.H = g->ws.H.p;
+  b.bufA = g->ws.A.p;
+  b.bufB = g->ws.B.p;
+  b.stride = g->ws.stride;
+  b.cost = a.cost ? a.cost + off : nullptr;
+  b.status = a.status ? a.status + off : nullptr;
+  b.params = a.params ? a.params + (size_t)off * a.param_stride : nullptr;
+  b.param_stride = a.param_stride;
+  b.need_chi2 = a.need_chi2;
+  b.chunk_p1_mask = a.chunk_p1_mask;
+  b.max_chunks = a.max_chunks;
+  b.other_cont = a.other_cont;
+  // chi2 batches resample inside the broadening kernel unless a synth row is wanted
+  b.obs_epi = a.need_chi2 && !a.out_obs && !a.out_synth && !a.full_window ? 1 : 0;
+  b.bnd = g->ws.bnd.p;
+  b.bnd_stride = g->ws.bnd_stride;
+  b.ccoef = g->ws.ccoef.p;
+  b.cpart = g->ws.cpart.p;
+  b.given = a.given ? a.given + (size_t)off * a.given_stride : nullptr;
+  b.given_stride = a.given_stride;
+  return b;
 }
 
 // Launch the evaluation pipeline for a.E evaluations, in workspace-sized
@@ -656,28 +716,11 @@ void run_evals(pasta_grid *g, const EvalArgs &a, cudaStream_t s) {
   o.may_unfuse = may_unfuse;
   for (int64_t off = 0; off < a.E; off += cap) {
     const int64_t cnt = std::min(cap, a.E - off);
-    EvalBatch b{};
-    b.E = (int)cnt;
-    b.labels = a.labels + 5 * off;
-    b.eval_star = a.eval_star + off;
-    b.eval_active = a.eval_active ? a.eval_active + off : nullptr;
-    b.stars = a.stars;
-    b.prep = g->ws.prep.p;
-    b.H = g->ws.H.p;
-    b.bufA = g->ws.A.p;
-    b.bufB = g->ws.B.p;
-    b.stride = g->ws.stride;
-    b.cost = a.cost ? a.cost + off : nullptr;
-    b.status = a.status ? a.status + off : nullptr;
-    b.params = a.params ? a.params + (size_t)off * a.param_stride : nullptr;
-    b.param_stride = a.param_stride;
+    EvalBatch b = make_batch(g, a, off, cnt);
     b.max_pairs = max_pairs;
     b.max_pairs_unfused = max_pairs_unfused;
-    b.need_chi2 = a.need_chi2;
-    b.chunk_p1_mask = a.chunk_p1_mask;
-    b.other_cont = a.other_cont;
     if (a.given) {
-      launch_chi2_given(g->d, b, a.given, s);
+      launch_chi2(g->d, b, s);
       continue;
     }
     launch_pipeline(g->d, b, C.tw.p, o, s);
@@ -687,9 +730,15 @@ void run_evals(pasta_grid *g, const EvalArgs &a, cudaStream_t s) {
   CK(cudaGetLastError());
 }
 
-void ensure_workspace(pasta_grid *g, int64_t E) {
-  const int64_t want = workspace_cap(g, E);
-  if (g->ws.cap < want || g->ws.stride != g->stride) g->ws.ensure(want, g->stride);
+// Workspace for E evaluations (or as many as fit) whose rows hold both a
+// synth spectrum and an observed spectrum of max_nobs pixels.
+void ensure_workspace(pasta_grid *g, int64_t E, int64_t max_nobs) {
+  const int64_t need = std::max<int64_t>(g->stride, (max_nobs + 63) / 64 * 64);
+  const int64_t stride = std::max(need, g->ws.stride);  // rows never shrink
+  const int bstr = bnd_stride_for((int)g->npx);
+  const int64_t want = workspace_cap(g, E, stride);
+  if (g->ws.cap >= want && g->ws.stride == stride && g->ws.bnd_stride == bstr) return;
+  g->ws.ensure(want, stride, bstr);
 }
 
 // ================================================================= swarm
@@ -851,7 +900,7 @@ void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, c
   a.need_chi2 = 1;
   a.max_m = max_m;
   star_kinds(ss.h, a);
-  ensure_workspace(g, S);
+  ensure_workspace(g, S, a.max_nobs);
   run_evals(g, a, s);
   std::vector<double> hp((size_t)S * pstride);
   CK(cudaMemcpyAsync(hp.data(), par.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -931,7 +980,6 @@ void batch_init(Batch &B, pasta_grid *g, const std::vector<StarInput> &in) {
   CK(cudaMemcpy(W.iter.p, iter.data(), S * sizeof(int), cudaMemcpyHostToDevice));
   W.seed.upload(seeds);
   W.params.upload(B.pp);
-  ensure_workspace(g, (int64_t)E);
   B.sw = W.view();
   EvalArgs &a = B.a;
   a.stars = B.ss.dstars.p;
@@ -944,6 +992,7 @@ void batch_init(Batch &B, pasta_grid *g, const std::vector<StarInput> &in) {
   a.need_chi2 = 1;
   a.max_m = B.max_m;
   star_kinds(B.ss.h, a);
+  ensure_workspace(g, (int64_t)E, a.max_nobs);
   for (auto &e : B.ev) CK(cudaEventCreate(&e));
   if (!getenv("PASTA_NO_GRAPH")) {
     const int64_t k0 = kernel_launches();
@@ -989,33 +1038,19 @@ double batch_steps(Batch &B, int n, double *trace) {
 
 // One step launched stage by stage with events between the stages:
 // out[0] swarm update, [1] prep, [2] rotation spectra, [3] interpolation,
-// [4] rotation FFT, [5] instrument profile, [6] chi2, [7] best update,
+// [4] fused broadening (block bounds + k_broaden), [5] unfused rotation and
+// instrument profile, [6] resampling left over + chi2, [7] best update,
 // [8] interpolated pixels (sum of windows), [9] evaluations, [10] sum of
-// observed pixels, [11] rotation blocks.
+// observed pixels, [11] broadening blocks.
 void batch_profile_step(Batch &B, double *out) {
   Ctx &C = ctx();
   cudaStream_t s = C.stream;
   pasta_grid *g = B.g;
   const EvalArgs &a = B.a;
   if (a.E > g->ws.cap) fail(PASTA_E_UNSUPPORTED, "profiled step needs the batch in one workspace");
-  EvalBatch b{};
-  b.E = (int)a.E;
-  b.labels = a.labels;
-  b.eval_star = a.eval_star;
-  b.eval_active = a.eval_active;
-  b.stars = a.stars;
-  b.prep = g->ws.prep.p;
-  b.H = g->ws.H.p;
-  b.bufA = g->ws.A.p;
-  b.bufB = g->ws.B.p;
-  b.stride = g->ws.stride;
-  b.cost = a.cost;
-  b.status = a.status;
+  EvalBatch b = make_batch(g, a, 0, a.E);
   int may_unfuse;
   pipeline_pairs((int)g->npx, a.max_m, a.max_hg, &b.max_pairs, &b.max_pairs_unfused, &may_unfuse);
-  b.need_chi2 = 1;
-  b.chunk_p1_mask = a.chunk_p1_mask;
-  b.other_cont = a.other_cont;
   CK(cudaEventRecord(B.ev[0], s));
   launch_pso_update(g->d, B.sw, s);
   CK(cudaEventRecord(B.ev[1], s));
@@ -1025,6 +1060,7 @@ void batch_profile_step(Batch &B, double *out) {
   CK(cudaEventRecord(B.ev[3], s));
   launch_interp(g->d, b, s);
   CK(cudaEventRecord(B.ev[4], s));
+  launch_obs_bounds(g->d, b, s);
   launch_broaden(g->d, b, C.tw.p, s);
   CK(cudaEventRecord(B.ev[5], s));
   if (may_unfuse) {
@@ -1032,6 +1068,7 @@ void batch_profile_step(Batch &B, double *out) {
     launch_gauss(g->d, b, s);
   }
   CK(cudaEventRecord(B.ev[6], s));
+  launch_resample_obs(g->d, b, s);
   launch_chi2(g->d, b, s);
   CK(cudaEventRecord(B.ev[7], s));
   launch_pso_best(B.sw, B.W.ecost.p, B.W.estatus.p, s);
@@ -1119,7 +1156,6 @@ void fit_plain(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result
     dc.alloc(P);
     ds.alloc(P);
     de.upload(std::vector<int>(P, 0));
-    ensure_workspace(g, P);
     EvalArgs a;
     a.stars = ss.dstars.p;
     a.labels = dl.p;
@@ -1130,6 +1166,7 @@ void fit_plain(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result
     a.need_chi2 = 1;
     a.max_m = width_upper_bound(g, pp.mx[3]);
     star_kinds(ss.h, a);
+    ensure_workspace(g, P, a.max_nobs);
     std::vector<int> est(P);
     auto evaluate = [&]() -> int {
       CK(cudaMemcpyAsync(dl.p, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -1248,7 +1285,7 @@ struct pasta_server {
   int max_m = 1, graph_max_m = 0;
   int64_t graph_gen = -1;
   uint32_t graph_mask = 0;  // continuum kinds / instrument width the captured step covers
-  int graph_other = 0, graph_hg = 0;
+  int graph_other = 0, graph_hg = 0, graph_chunks = 0;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   std::mutex mu;
@@ -1462,6 +1499,7 @@ int pasta_dispersion_create(int synth_kind, double synth_a, double synth_b, int6
     d->wl_max = *std::max_element(d->wl.begin(), d->wl.end());
     d->fidx_min = *std::min_element(d->fidx.begin(), d->fidx.end());
     d->fidx_max = *std::max_element(d->fidx.begin(), d->fidx.end());
+    d->sorted = std::is_sorted(d->fidx.begin(), d->fidx.end()) && std::is_sorted(d->wl.begin(), d->wl.end());
     const auto &vals = d->synth_vals;
     if (kind == PASTA_DISP_NONE) {
       d->dev_kind = DISP_NONE;
@@ -1605,9 +1643,17 @@ int pasta_continuum_fit(const pasta_continuum *c, const float *model, const floa
     b.params = dpar.p;
     b.param_stride = ps;
     b.chunk_p1_mask = st.cont_kind == CONT_CHUNK ? 1u << st.p1 : 0u;
+    b.max_chunks = st.cont_kind == CONT_CHUNK ? st.n_chunks : 0;
     b.other_cont = st.cont_kind == CONT_CHUNK ? 0 : 1;
+    DBuf<float> dcoef;
+    DBuf<double> dpart;
+    dcoef.alloc((size_t)MAX_CHUNKS * MAX_P1);
+    dpart.alloc(MAX_CHUNKS);
+    b.ccoef = dcoef.p;
+    b.cpart = dpart.p;
+    b.given = dm.p;
     DevGrid G{};
-    launch_chi2_given(G, b, dm.p, s);
+    launch_chi2(G, b, s);
     CK(cudaGetLastError());
     double hc;
     int hs;
@@ -1725,7 +1771,7 @@ static int run_label_batch(const pasta_grid *gc, const pasta_dispersion *d, cons
     star_kinds({st}, a);
     if (out_obs) { dout.alloc((size_t)L * nobs); a.out_obs = dout.p; a.out_stride = nobs; }
     if (out_synth) { dout.alloc((size_t)L * g->npx); a.out_synth = dout.p; }
-    ensure_workspace(g, L);
+    ensure_workspace(g, L, a.max_nobs);
     run_evals(g, a, s);
     std::vector<int> hst(L, 0);
     CK(cudaMemcpyAsync(hst.data(), dst.p, L * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -2008,7 +2054,6 @@ int pasta_server_step(pasta_server *sv) {
     for (int i = 0; i < sv->slots; i++) any |= (bool)sv->slot_req[i];
     if (!any) return;
     const int64_t E = (int64_t)sv->slots * sv->Pmax;
-    ensure_workspace(g, E);
     Swarm sw = sv->W.view();
     EvalArgs a;
     a.stars = sv->dstars.p;
@@ -2028,9 +2073,12 @@ int pasta_server_step(pasta_server *sv) {
       a.chunk_p1_mask |= sv->graph_mask;  // keep what the captured graph already covers
       if (sv->graph_other) a.other_cont = 1;
       a.max_hg = std::max(a.max_hg, sv->graph_hg);
+      a.max_chunks = std::max(a.max_chunks, sv->graph_chunks);
     }
+    ensure_workspace(g, E, a.max_nobs);
     const bool grown = sv->graph_max_m < sv->max_m || (a.chunk_p1_mask & ~sv->graph_mask) ||
-                       (a.other_cont && !sv->graph_other) || a.max_hg > sv->graph_hg;
+                       (a.other_cont && !sv->graph_other) || a.max_hg > sv->graph_hg ||
+                       a.max_chunks > sv->graph_chunks;
     if (sv->exec && (grown || sv->graph_gen != g->ws.gen)) {
       // a wider kernel or a new continuum kind was admitted, or the workspace moved
       cudaGraphExecDestroy(sv->exec);
@@ -2044,6 +2092,7 @@ int pasta_server_step(pasta_server *sv) {
       sv->graph_mask = a.chunk_p1_mask;
       sv->graph_other = a.other_cont;
       sv->graph_hg = a.max_hg;
+      sv->graph_chunks = a.max_chunks;
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       launch_pso_update(g->d, sw, s);
       run_evals(g, a, s);

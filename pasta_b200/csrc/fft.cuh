@@ -58,8 +58,11 @@ __device__ __forceinline__ void dft8(cf v[8]) {
 // One Stockham stage of radix R at sub-transform length Ns.  All reads of
 // the stage happen before a barrier, all writes after it, so the transform
 // runs in place.  The caller must __syncthreads() after filling the input.
-template <int R, bool INV>
-__device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const float2 *__restrict__ tw) {
+// ld(i) returns input element i, st(i, v) stores output element i; the
+// defaults use the swizzled re/im arrays (the first stage may read from a
+// staging buffer, the last may write elsewhere).
+template <int R, bool INV, class LD, class ST>
+__device__ __forceinline__ void fft_stage_io(int Ns, const float2 *__restrict__ tw, const LD &ld, const ST &st) {
   constexpr int N = 2048, J = N / R, PER = J / FFT_T;
   cf v[PER][R];
   const int step = N / (Ns * R);
@@ -68,10 +71,7 @@ __device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const fl
     const int j = threadIdx.x + q * FFT_T;
     const int jm = j & (Ns - 1);
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int a = pidx(j + r * J);
-      v[q][r] = cf{re[a], im[a]};
-    }
+    for (int r = 0; r < R; r++) v[q][r] = ld(j + r * J);
     if (jm != 0) {
       // twiddles W^(jm r step): W^1, W^2, W^4 from the table, the others by
       // at most two multiplications
@@ -101,13 +101,30 @@ __device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const fl
     else dft4<INV>(v[q][0], v[q][1], v[q][2], v[q][3]);
     const int idxD = (j / Ns) * Ns * R + jm;
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int a = pidx(idxD + r * Ns);
-      re[a] = v[q][r].x;
-      im[a] = v[q][r].y;
-    }
+    for (int r = 0; r < R; r++) st(idxD + r * Ns, v[q][r]);
   }
   __syncthreads();
+}
+
+struct SmemLoad {
+  const float *re, *im;
+  __device__ __forceinline__ cf operator()(int i) const {
+    const int a = pidx(i);
+    return cf{re[a], im[a]};
+  }
+};
+struct SmemStore {
+  float *re, *im;
+  __device__ __forceinline__ void operator()(int i, cf v) const {
+    const int a = pidx(i);
+    re[a] = v.x;
+    im[a] = v.y;
+  }
+};
+
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const float2 *__restrict__ tw) {
+  fft_stage_io<R, INV>(Ns, tw, SmemLoad{re, im}, SmemStore{re, im});
 }
 
 template <bool INV>

@@ -2,11 +2,15 @@
 //
 // Buffer protocol per evaluation e (rows of `stride` floats):
 //   k_interp writes the interpolated spectrum to A.
-//   k_broaden (rotation FFT + instrument profile, fused) reads A, writes B.
+//   k_broaden (rotation FFT + instrument profile, fused) reads A and writes
+//   the broadened synth row to B, or in chi2 batches the model resampled
+//   to the observed pixels (EvalPrep::epi).
 //   Very wide kernels (m - 1 + 2 hg > 2048 - 128) take the unfused pair
 //   k_rot (A -> B) and k_gauss (B -> A, or A -> B when the rotation is the
-//   identity).  EvalPrep::final_in_b says where the result is.
-//   k_chi2_* / k_resample_out read the final row.
+//   identity).  EvalPrep::final_in_b says where the synth row is.
+//   k_resample_obs resamples the synth rows k_broaden did not, into the
+//   other buffer (EvalPrep::mobs_in_b); the chi2 kernels read that model.
+//   k_resample_out / k_copy_broadened serve the model entry points.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -137,6 +141,64 @@ void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   count_launch();
 }
 
+// ------------------------------------------------------------ resampling
+// shift_and_resample (convolve_rv.rs:569-603): index in double, weight from
+// the f32-rounded index minus the f32 floor, linear interpolation in f32.
+struct ResPos {
+  int j;    // left synth pixel
+  float w;  // weight of pixel j + 1
+};
+__device__ __forceinline__ float resample_value(float w, float sj, float sj1) {
+  return __fadd_rn(__fmul_rn(1.0f - w, sj), __fmul_rn(w, sj1));
+}
+struct Resampler {
+  const float *s;
+  int N, kind;
+  double shift_log, shift_factor, lin_offset;
+  const double *fidx, *wl_obs, *wl_vals;
+  const float *given;  // model given directly at the observed pixels
+  // j never decreases with i when the float indices do not
+  __device__ __forceinline__ ResPos pos(int i) const {
+    double idx;
+    if (kind == WL_LOG) idx = fidx[i] + shift_log;
+    else if (kind == WL_LIN) idx = __dadd_rn(__dmul_rn(shift_factor, fidx[i]), lin_offset);
+    else {
+      const double wl = __dmul_rn(wl_obs[i], shift_factor);
+      bool f;
+      int k = lower_bound(wl_vals, N, wl, f);
+      if (f) idx = (double)k;
+      else if (k == 0) idx = 0.0;
+      else if (k == N) idx = (double)N - 1.0;
+      else idx = __dadd_rn(__dadd_rn(__ddiv_rn(wl - wl_vals[k - 1], wl_vals[k] - wl_vals[k - 1]), (double)k), -1.0);
+    }
+    const double fl = floor(idx);
+    int j = fl > 0 ? (int)fl : 0;
+    if (j > N - 2) j = N - 2;  // the preparation kernel rejected j + 1 >= N already
+    return ResPos{j, (float)idx - (float)j};
+  }
+  __device__ __forceinline__ float operator()(int i) const {
+    if (given) return given[i];
+    const ResPos q = pos(i);
+    return resample_value(q.w, s[q.j], s[q.j + 1]);
+  }
+};
+
+__device__ __forceinline__ Resampler make_resampler(const DevGrid &G, const DevStar &st, const EvalPrep &P,
+                                                    const float *row, const float *given) {
+  Resampler r;
+  r.s = row;
+  r.N = G.npx;
+  r.kind = G.wl_kind;
+  r.shift_log = P.shift_log;
+  r.shift_factor = P.shift_factor;
+  r.lin_offset = P.lin_offset;
+  r.fidx = st.fidx;
+  r.wl_obs = st.wl_obs;
+  r.wl_vals = G.wl_vals;
+  r.given = given;
+  return r;
+}
+
 // ------------------------------------------------ instrument profile (tile)
 // FixedTargetDispersionLogSpace: g[i] = sum_k gk[k] r[i + h - k], r zero
 // outside the grid (convolve_rv.rs:207-210).  Per-pixel kernels
@@ -160,46 +222,141 @@ __device__ __forceinline__ float instrument(const DevStar &st, int N, int i, int
 }
 
 // ------------------------------------------------------ fused broadening
-// One work item = two blocks of one evaluation.  Block b yields the final
-// outputs [o_lo + b V, o_lo + (b+1) V) with V = 2048 - (m - 1) - 2 hg: the
+// One work item = two blocks of one evaluation.  Block k yields V = 2048 -
+// (m - 1) - 2 hg final outputs starting at s_k = o_lo + k (V - 1): the
 // rotation outputs [s - hg, s + V + hg) come from one overlap-save block of
 // 2048 inputs (the reference uses overlap-add, convolve_rv.rs:121-157; both
 // are the same linear convolution), and the instrument profile is then
-// applied from shared memory.  The two real blocks ride in the real and
-// imaginary parts of one complex FFT (the kernel is real, so the two
-// products separate after the inverse).  Rotation outputs outside [0, N)
-// are zero, like the reference's cropped segment.  With the identity
-// rotation the FFT is skipped.
+// applied from shared memory.  Block k owns synth pixels [s_k, s_k + V - 1);
+// its last output is the partner j + 1 of its last owned pixel j.  The two
+// real blocks ride in the real and imaginary parts of one complex FFT (the
+// kernel is real, so the two products separate after the inverse).
+// Rotation outputs outside [0, N) are zero, like the reference's cropped
+// segment.  With the identity rotation the FFT is skipped.
+//
+// Epilogue: either the owned synth pixels go to row B, or (chi2 batches,
+// EvalPrep::epi) the block resamples the observed pixels whose left synth
+// pixel it owns (EvalBatch::bnd lists them per block) straight from shared
+// memory and writes the model at the observed pixels to row B; the synth
+// row never reaches memory.
+// Asynchronous 16-byte global -> shared copies (cp.async): the next work
+// item's input streams in while the current one is transformed.  A copy
+// with ok == false reads nothing and fills zeros.
+__device__ __forceinline__ void cp_async16(float *smem, const float *gmem, bool ok) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = ok ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// staging row: synth pixels [a0, a0 + BR_STG) with a0 = j0 rounded down to
+// 4, so a block's 2048 inputs start at offset j0 - a0 in 0..3
+constexpr int BR_STG = 2064;
+// dynamic shared memory of k_broaden (floats): two staging rows, the
+// swizzled FFT arrays, the two blocks' outputs, the instrument taps
+constexpr int BR_SMEM_FLOATS = 2 * BR_STG + 2 * FFT_SM + 2 * FFT_SM + 512;
+
+// pixels outside [ilo, ihi) are zero; ilo and ihi are multiples of 8, so
+// every 16-byte chunk is wholly inside or outside
+__device__ __forceinline__ void stage_row(float *stg, const float *row, int j0, int ilo, int ihi) {
+  const int a0 = j0 & ~3;
+  for (int c = threadIdx.x; c < BR_STG / 4; c += FFT_T) {
+    const int g = a0 + 4 * c;
+    const bool ok = g >= ilo && g + 4 <= ihi;
+    cp_async16(stg + 4 * c, ok ? row + g : row + ilo, ok);
+  }
+}
+
+struct BroadenItem {
+  int e, pair, m, hg, V, s0, s1, j0, j1;
+  bool has1;
+};
+
+// the work item `item` of this batch, or false when it has nothing to do
+__device__ __forceinline__ bool broaden_item(const EvalBatch &b, long long item, BroadenItem &w) {
+  w.e = (int)(item / b.max_pairs);
+  w.pair = (int)(item % b.max_pairs);
+  const EvalPrep &P = b.prep[w.e];
+  if (P.status || !P.fused || 2 * w.pair >= P.nblk) return false;
+  w.m = P.m;
+  w.hg = P.hg;
+  w.V = FFTN - (w.m - 1) - 2 * w.hg;
+  w.s0 = P.o_lo + 2 * w.pair * (w.V - 1);
+  w.s1 = w.s0 + (w.V - 1);
+  w.has1 = 2 * w.pair + 1 < P.nblk;
+  // input t of a block is synth pixel (s - hg - hw + t) for the rotation,
+  // (s - hg + t) for the identity
+  const int shift = w.m > 1 ? w.hg + (w.m - 1) / 2 : w.hg;
+  w.j0 = w.s0 - shift;
+  w.j1 = w.s1 - shift;
+  return true;
+}
+
+// this CTA's first item at or after `item` that has work (total: none)
+__device__ __forceinline__ long long next_item(const EvalBatch &b, long long item, long long total) {
+  BroadenItem w;
+  for (; item < total; item += gridDim.x)
+    if (broaden_item(b, item, w)) return item;
+  return total;
+}
+
+// start the copies of an item's input into the staging rows
+__device__ __forceinline__ void stage_item(const EvalBatch &b, long long item, float *stg0, float *stg1) {
+  BroadenItem w;
+  broaden_item(b, item, w);
+  const EvalPrep &P = b.prep[w.e];
+  const float *row = b.bufA + (size_t)w.e * b.stride;
+  stage_row(stg0, row, w.j0, P.i_lo, P.i_hi);
+  if (w.has1) stage_row(stg1, row, w.j1, P.i_lo, P.i_hi);
+}
+
+struct StageLoad {
+  const float *s0, *s1;
+  bool has1;
+  __device__ __forceinline__ cf operator()(int i) const { return cf{s0[i], has1 ? s1[i] : 0.0f}; }
+};
+// last inverse stage of the folded path: FFT index i is output i - lo
+struct FoldStore {
+  float *o0, *o1;
+  int lo, V;
+  float sc;
+  __device__ __forceinline__ void operator()(int i, cf v) const {
+    const int u = i - lo;
+    if ((unsigned)u < (unsigned)V) {
+      o0[u] = v.x * sc;
+      o1[u] = v.y * sc;
+    }
+  }
+};
+
 __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
-  __shared__ float re[FFT_SM], im[FFT_SM];
-  __shared__ float gks[2 * 255 + 1];  // the fixed instrument kernel of the current item
+  extern __shared__ __align__(16) float br_smem[];
+  float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
+  float *re = stg1 + BR_STG, *im = re + FFT_SM;
+  float *ob0 = im + FFT_SM, *ob1 = ob0 + FFT_SM;
+  float *gks = ob1 + FFT_SM;  // the fixed instrument kernel of the current item
   const long long total = (long long)b.E * b.max_pairs;
   const int N = G.npx;
-  for (long long item = blockIdx.x; item < total; item += gridDim.x) {
-    const int e = (int)(item / b.max_pairs), pair = (int)(item % b.max_pairs);
+  long long item = next_item(b, blockIdx.x, total);
+  if (item < total) stage_item(b, item, stg0, stg1);
+  cp_async_commit();
+  while (item < total) {
+    const long long nxt = next_item(b, item + gridDim.x, total);
+    BroadenItem w;
+    broaden_item(b, item, w);
+    cp_async_wait_all();
+    __syncthreads();  // the item's input is staged
+    const int e = w.e, pair = w.pair, m = w.m, hg = w.hg, V = w.V, s0 = w.s0, s1 = w.s1;
+    const bool has1 = w.has1;
     const EvalPrep &P = b.prep[e];
-    const int m = P.m, nblk = P.nblk, hg = P.hg;
-    if (P.status || !P.fused || 2 * pair >= nblk) continue;
+    const int nblk = P.nblk, ohi = P.o_hi;
     const DevStar &st = b.stars[P.star];
-    const int hw = (m - 1) / 2;
-    const int V = FFTN - (m - 1) - 2 * hg;
-    const int s0 = P.o_lo + 2 * pair * V, s1 = s0 + V;
-    const bool has1 = 2 * pair + 1 < nblk;
-    const int ilo = P.i_lo, ihi = P.i_hi, ohi = P.o_hi;
-    const float *x = b.bufA + (size_t)e * b.stride;
-    // input t of a block is synth pixel (s - hg - hw + t) for the rotation,
-    // (s - hg + t) for the identity
-    const int shift = m > 1 ? hg + hw : hg;
-    for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
-      const int j0 = s0 - shift + t, j1 = s1 - shift + t;
-      re[pidx(t)] = (j0 >= ilo && j0 < ihi) ? x[j0] : 0.0f;
-      im[pidx(t)] = (has1 && j1 >= ilo && j1 < ihi) ? x[j1] : 0.0f;
-    }
     const bool fixedk = hg > 0 && st.disp_kind == DISP_FIXED;
     const int gw = 2 * hg + 1;
     if (fixedk)
       for (int t = threadIdx.x; t < gw; t += FFT_T) gks[t] = st.gk[t];
-    __syncthreads();
+    const StageLoad ld{stg0 + (w.j0 & 3), stg1 + (w.j1 & 3), has1};
     int base = 0;  // data index of rotation output (s - hg)
     // Away from the grid ends the Gaussian acts on rotation outputs that are
     // all inside [0, N), where rotation-then-Gaussian equals one convolution
@@ -207,7 +364,12 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     if (m > 1) {
-      fft2048<false>(re, im, tw);
+      fft_stage_io<8, false>(1, tw, ld, SmemStore{re, im});  // first stage straight from the staging rows
+      if (nxt < total) stage_item(b, nxt, stg0, stg1);
+      cp_async_commit();
+      fft_stage<8, false>(re, im, 8, tw);
+      fft_stage<8, false>(re, im, 64, tw);
+      fft_stage<4, false>(re, im, 512, tw);
       const float2 *H = b.H + (size_t)e * 1025;
       for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
         float2 h = k <= 1024 ? H[k] : H[FFTN - k];
@@ -224,60 +386,133 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
         im[a] = z.y;
       }
       __syncthreads();
-      fft2048<true>(re, im, tw);
+      fft_stage<8, true>(re, im, 1, tw);
+      fft_stage<8, true>(re, im, 8, tw);
+      fft_stage<8, true>(re, im, 64, tw);
       base = m - 1;
       const float sc = 1.0f / 2048.0f;
-      if (fold) {  // output i sits at base + 2 hg + (i - s)
-        float *y = b.bufB + (size_t)e * b.stride;
-        for (int u = threadIdx.x; u < V; u += FFT_T) {
-          const int i0 = s0 + u, i1 = s1 + u;
-          if (i0 < ohi) y[i0] = re[pidx(base + 2 * hg + u)] * sc;
-          if (has1 && i1 < ohi) y[i1] = im[pidx(base + 2 * hg + u)] * sc;
+      if (fold) {  // output u sits at base + 2 hg + u
+        fft_stage_io<4, true>(512, tw, SmemLoad{re, im}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
+      } else {
+        fft_stage<4, true>(re, im, 512, tw);
+        for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
+          const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
+          re[pidx(t)] = (i0 >= 0 && i0 < N) ? re[pidx(t)] * sc : 0.0f;
+          im[pidx(t)] = (i1 >= 0 && i1 < N) ? im[pidx(t)] * sc : 0.0f;
         }
         __syncthreads();
-        continue;
       }
-      for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
-        const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
-        re[pidx(t)] = (i0 >= 0 && i0 < N) ? re[pidx(t)] * sc : 0.0f;
-        im[pidx(t)] = (i1 >= 0 && i1 < N) ? im[pidx(t)] * sc : 0.0f;
+    } else {  // identity rotation: the staged input is the rotation output
+      for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
+        const cf v = ld(t);
+        re[pidx(t)] = v.x;
+        im[pidx(t)] = v.y;
       }
       __syncthreads();
+      if (nxt < total) stage_item(b, nxt, stg0, stg1);
+      cp_async_commit();
     }
-    float *y = b.bufB + (size_t)e * b.stride;
-    for (int u = threadIdx.x; u < V; u += FFT_T) {
-      const int i0 = s0 + u, i1 = s1 + u;
-      float v0, v1;
-      if (hg == 0) {
-        v0 = re[pidx(base + u)];
-        v1 = im[pidx(base + u)];
-      } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at base + (i - s + hg)
-        float a0 = 0.0f, a1 = 0.0f;
-        for (int k = 0; k < gw; k++) {
-          const float g = gks[k];
-          const int t = pidx(base + u + 2 * hg - k);
-          a0 = fmaf(g, re[t], a0);
-          a1 = fmaf(g, im[t], a1);
+    if (!fold) {
+      for (int u = threadIdx.x; u < V; u += FFT_T) {
+        const int i0 = s0 + u, i1 = s1 + u;
+        float v0, v1;
+        if (hg == 0) {
+          v0 = re[pidx(base + u)];
+          v1 = im[pidx(base + u)];
+        } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at base + (i - s + hg)
+          float a0 = 0.0f, a1 = 0.0f;
+          for (int k = 0; k < gw; k++) {
+            const float g = gks[k];
+            const int t = pidx(base + u + 2 * hg - k);
+            a0 = fmaf(g, re[t], a0);
+            a1 = fmaf(g, im[t], a1);
+          }
+          v0 = a0;
+          v1 = a1;
+        } else {
+          v0 = instrument(st, N, i0, hg, [&](int i) { return re[pidx(base + i - (s0 - hg))]; });
+          v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return im[pidx(base + i - (s1 - hg))]; }) : 0.0f;
         }
-        v0 = a0;
-        v1 = a1;
-      } else {
-        v0 = instrument(st, N, i0, hg, [&](int i) { return re[pidx(base + i - (s0 - hg))]; });
-        v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return im[pidx(base + i - (s1 - hg))]; }) : 0.0f;
+        ob0[u] = v0;
+        ob1[u] = v1;
       }
-      if (i0 < ohi) y[i0] = v0;
-      if (has1 && i1 < ohi) y[i1] = v1;
     }
     __syncthreads();
+    float *y = b.bufB + (size_t)e * b.stride;
+    if (P.epi) {
+      // observed pixels [bnd[2 pair], bnd[2 pair + 2]) have their left synth
+      // pixel in this item's blocks; the boundary between them is bnd[2 pair + 1]
+      const int *bd = b.bnd + (size_t)e * b.bnd_stride + 2 * pair;
+      const int q0 = bd[0], q1 = bd[1], q2 = has1 ? bd[2] : q1;
+      const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
+      for (int i = q0 + threadIdx.x; i < q2; i += FFT_T) {
+        const ResPos q = R.pos(i);
+        const bool k1 = i >= q1;
+        const float *o = k1 ? ob1 : ob0;
+        const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
+        y[i] = resample_value(q.w, o[u], o[u + 1]);
+      }
+    } else {
+      // owned pixels; the last block also writes its final output
+      const int n0 = 2 * pair + 1 == nblk ? V : V - 1, n1 = 2 * pair + 2 == nblk ? V : V - 1;
+      for (int u = threadIdx.x; u < V; u += FFT_T) {
+        const int i0 = s0 + u, i1 = s1 + u;
+        if (u < n0 && i0 < ohi) y[i0] = ob0[u];
+        if (has1 && u < n1 && i1 < ohi) y[i1] = ob1[u];
+      }
+    }
+    item = nxt;
   }
+  cp_async_wait_all();
 }
 
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cudaStream_t s) {
   if (b.E <= 0 || b.max_pairs <= 0) return;
+  const size_t smem = BR_SMEM_FLOATS * sizeof(float);
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !attr[dev]) {
+    cudaFuncSetAttribute(k_broaden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr[dev] = true;
+  }
   const long long total = (long long)b.E * b.max_pairs;
   long long grid = (long long)num_sms() * 4;  // persistent: the CTAs that fit at once (64 regs x 256)
   if (grid > total) grid = total;
-  k_broaden<<<(unsigned)grid, FFT_T, 0, s>>>(G, b, tw);
+  k_broaden<<<(unsigned)grid, FFT_T, smem, s>>>(G, b, tw);
+  count_launch();
+}
+
+// First observed pixel of every fused broadening block: bnd[k] = the
+// smallest i whose left synth pixel is >= s_k (binary search on the
+// monotone resampling index); bnd[0] = 0, bnd[nblk] = n_obs.
+__global__ void k_obs_bounds(DevGrid G, EvalBatch b) {
+  const int e = blockIdx.x;
+  const EvalPrep &P = b.prep[e];
+  if (P.status || !P.epi) return;
+  const int k = blockIdx.y * blockDim.x + threadIdx.x, nblk = P.nblk;
+  if (k > nblk) return;
+  const DevStar &st = b.stars[P.star];
+  int *bd = b.bnd + (size_t)e * b.bnd_stride;
+  if (k == 0 || k == nblk) {
+    bd[k] = k == 0 ? 0 : st.n_obs;
+    return;
+  }
+  const int target = P.o_lo + k * (FFTN - (P.m - 1) - 2 * P.hg - 1);
+  const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
+  int lo = 0, hi = st.n_obs;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (R.pos(mid).j < target) lo = mid + 1;
+    else hi = mid;
+  }
+  bd[k] = lo;
+}
+
+void launch_obs_bounds(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
+  if (b.E <= 0 || b.max_pairs <= 0 || !b.obs_epi) return;
+  dim3 grid(b.E, (2 * b.max_pairs + 1 + 63) / 64);
+  k_obs_bounds<<<grid, 64, 0, s>>>(G, b);
   count_launch();
 }
 
@@ -392,53 +627,6 @@ void launch_gauss_standalone(const DevGrid &G, const DevStar *star, const float 
   count_launch();
 }
 
-// ------------------------------------------------------------ resampling
-// shift_and_resample (convolve_rv.rs:569-603): index in double, weight from
-// the f32-rounded index minus the f32 floor, linear interpolation in f32.
-struct Resampler {
-  const float *s;
-  int N, kind;
-  double shift_log, shift_factor, lin_offset;
-  const double *fidx, *wl_obs, *wl_vals;
-  const float *given;  // model given directly at the observed pixels
-  __device__ __forceinline__ float operator()(int i) const {
-    if (given) return given[i];
-    double idx;
-    if (kind == WL_LOG) idx = fidx[i] + shift_log;
-    else if (kind == WL_LIN) idx = __dadd_rn(__dmul_rn(shift_factor, fidx[i]), lin_offset);
-    else {
-      const double wl = __dmul_rn(wl_obs[i], shift_factor);
-      bool f;
-      int k = lower_bound(wl_vals, N, wl, f);
-      if (f) idx = (double)k;
-      else if (k == 0) idx = 0.0;
-      else if (k == N) idx = (double)N - 1.0;
-      else idx = __dadd_rn(__dadd_rn(__ddiv_rn(wl - wl_vals[k - 1], wl_vals[k] - wl_vals[k - 1]), (double)k), -1.0);
-    }
-    const double fl = floor(idx);
-    int j = fl > 0 ? (int)fl : 0;
-    if (j > N - 2) j = N - 2;  // the preparation kernel rejected j + 1 >= N already
-    const float w = (float)idx - (float)j;
-    return __fadd_rn(__fmul_rn(1.0f - w, s[j]), __fmul_rn(w, s[j + 1]));
-  }
-};
-
-__device__ __forceinline__ Resampler make_resampler(const DevGrid &G, const DevStar &st, const EvalPrep &P,
-                                                    const float *row, const float *given) {
-  Resampler r;
-  r.s = row;
-  r.N = G.npx;
-  r.kind = G.wl_kind;
-  r.shift_log = P.shift_log;
-  r.shift_factor = P.shift_factor;
-  r.lin_offset = P.lin_offset;
-  r.fidx = st.fidx;
-  r.wl_obs = st.wl_obs;
-  r.wl_vals = G.wl_vals;
-  r.given = given;
-  return r;
-}
-
 __global__ void k_resample_out(DevGrid G, EvalBatch b, float *out, int64_t out_stride) {
   const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
@@ -543,110 +731,159 @@ __device__ __forceinline__ void write_result(const EvalBatch &b, int e, double c
   }
 }
 
-// ChunkFitter::fit_continuum (continuum_fitting.rs:382-396): per chunk the
-// unweighted least-squares polynomial of flux/model (216-226) is the
-// projection onto the chunk's polynomial space; it is solved here in a
-// Legendre basis with the FP64 Cholesky factor of its Gram matrix (the same
-// space as the reference's monomial SVD, far better conditioned).  chi2 is
-// summed over [50, N-50) with the sin^2 blend in the overlaps and divided
-// by N - 100 (280-360).  Moments and chi2 accumulate in FP64.  One CTA per
-// evaluation; K = polynomial order + 1 (one instantiation per order present).
-template <int K>
-__global__ void __launch_bounds__(CT, 4) k_chi2_chunk(DevGrid G, EvalBatch b, const float *given) {
-  __shared__ double ws[CW][MAX_P1];
-  __shared__ double zs[MAX_CHUNKS * K];
-  __shared__ float cf32[MAX_CHUNKS * K];
+// model at the observed pixels of evaluation e
+__device__ __forceinline__ const float *model_row(const EvalBatch &b, const EvalPrep &P, int e) {
+  if (b.given) return b.given + (size_t)e * b.given_stride;
+  return (P.mobs_in_b ? b.bufB : b.bufA) + (size_t)e * b.stride;
+}
+
+// Evaluations that k_broaden did not resample: the model at the observed
+// pixels from the final synth row, into the buffer the synth row is not in.
+__global__ void k_resample_obs(DevGrid G, EvalBatch b) {
   const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
+  if (P.status || P.epi) return;
   const DevStar &st = b.stars[P.star];
-  if (st.cont_kind != CONT_CHUNK || st.p1 != K) return;
-  if (P.status) {
-    write_result(b, e, 0.0, P.status);
-    return;
-  }
-  if (st.cont_bad) {
-    write_result(b, e, 0.0, S_CONTINUUM);
-    return;
-  }
-  const int N = st.n_obs, nc = st.n_chunks;
-  const Resampler R = make_resampler(G, st, P, given ? nullptr : final_row(b, P, e), given);
-  const float *flux = st.flux, *var = st.var;
-  for (int c = 0; c < nc; c++) {
-    const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
-    double z[K];
+  const Resampler R = make_resampler(G, st, P, final_row(b, P, e), nullptr);
+  float *out = (P.mobs_in_b ? b.bufB : b.bufA) + (size_t)e * b.stride;
+  for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < st.n_obs; i += gridDim.y * blockDim.x) out[i] = R(i);
+}
+void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
+  if (b.E <= 0) return;
+  dim3 grid(b.E, 8);
+  k_resample_obs<<<grid, 256, 0, s>>>(G, b);
+  count_launch();
+}
+
+// ChunkFitter::fit_continuum (continuum_fitting.rs:382-396), one CTA per
+// (evaluation, chunk): the unweighted least-squares polynomial of
+// flux/model over the chunk (216-226) is the projection onto the chunk's
+// polynomial space; it is solved here in a Legendre basis with the FP64
+// Cholesky factor of its Gram matrix (the same space as the reference's
+// monomial SVD, far better conditioned).  Moments accumulate in FP64.
+// K = polynomial order + 1 (one instantiation per order present).
+template <int K>
+__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch b) {
+  __shared__ double ws[CW][MAX_P1];
+  __shared__ double zs[K];
+  const int e = blockIdx.x, c = blockIdx.y;
+  const EvalPrep &P = b.prep[e];
+  if (P.status) return;
+  const DevStar &st = b.stars[P.star];
+  if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
+  const float *mod = model_row(b, P, e), *flux = st.flux;
+  const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
+  double z[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) z[k] = 0.0;
+  for (int k = 0; k < K; k++) z[k] = 0.0;
 #pragma unroll 4
-    for (int i = lo + threadIdx.x; i < hi; i += CT) {
-      const double y = (double)(flux[i] / R(i));
-      const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
-      float Pk[K];
-      legendre<K>(xf, Pk);
+  for (int i = lo + threadIdx.x; i < hi; i += CT) {
+    const double y = (double)(flux[i] / mod[i]);
+    const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
+    float Pk[K];
+    legendre<K>(xf, Pk);
 #pragma unroll
-      for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
-    }
-    block_sum_vec<K>(z, ws, zs + c * K);
+    for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
   }
-  // per-chunk FP64 Cholesky solve G c = z
-  if (threadIdx.x < nc) {
-    const int c = threadIdx.x;
+  block_sum_vec<K>(z, ws, zs);
+  if (threadIdx.x == 0) {  // FP64 Cholesky solve G a = z, in place in zs
     const double *L = st.chol + (size_t)c * K * K;
-    double *z = zs + c * K;
-    double u[K];
-#pragma unroll
     for (int k = 0; k < K; k++) {
-      double s = z[k];
-#pragma unroll
-      for (int j = 0; j < k; j++) s -= L[k * K + j] * u[j];
-      u[k] = s / L[k * K + k];
+      double t = zs[k];
+      for (int j = 0; j < k; j++) t -= L[k * K + j] * zs[j];
+      zs[k] = t / L[k * K + k];
     }
-#pragma unroll
     for (int k = K - 1; k >= 0; k--) {
-      double s = u[k];
-#pragma unroll
-      for (int j = k + 1; j < K; j++) s -= L[j * K + k] * z[j];
-      z[k] = s / L[k * K + k];
-      cf32[c * K + k] = (float)z[k];
+      double t = zs[k];
+      for (int j = k + 1; j < K; j++) t -= L[j * K + k] * zs[j];
+      zs[k] = t / L[k * K + k];
     }
-    if (b.params)
-      for (int k = 0; k < K; k++) b.params[(size_t)e * b.param_stride + c * K + k] = z[k];
+    float *cf = b.ccoef + ((size_t)e * MAX_CHUNKS + c) * MAX_P1;
+    for (int k = 0; k < K; k++) cf[k] = (float)zs[k];
+    if (b.params) {
+      double *par = b.params + (size_t)e * b.param_stride + c * K;
+      for (int k = 0; k < K; k++) par[k] = zs[k];
+    }
+  }
+}
+
+// chi2 section of chunk c (continuum_fitting.rs:280-360): chunk 0 alone on
+// [50, start_1); chunk c >= 1 blended with chunk c - 1 (sin^2 factor) on
+// [start_c, stop_{c-1}), then alone up to start_{c+1} (N - 50 for the
+// last).  Partial sums per section in FP64, added in chunk order by
+// k_chunk_final.
+template <int K>
+__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b) {
+  __shared__ double ws[CW][MAX_P1];
+  __shared__ float cp[K], cc[K];
+  const int e = blockIdx.x, c = blockIdx.y;
+  const EvalPrep &P = b.prep[e];
+  if (P.status) return;
+  const DevStar &st = b.stars[P.star];
+  if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
+  const int N = st.n_obs, nc = st.n_chunks;
+  const float *mod = model_row(b, P, e), *flux = st.flux, *var = st.var;
+  const float *coef = b.ccoef + (size_t)e * MAX_CHUNKS * MAX_P1;
+  if (threadIdx.x < K) {
+    cc[threadIdx.x] = coef[c * MAX_P1 + threadIdx.x];
+    cp[threadIdx.x] = c > 0 ? coef[(c - 1) * MAX_P1 + threadIdx.x] : 0.0f;
   }
   __syncthreads();
   double acc = 0.0;
-  for (int i = 50 + threadIdx.x; i < st.cstart[1]; i += CT) {  // [50, start_1): chunk 0 alone
-    const float p = poly_eval<K>(cf32, st.xa[i]);
-    const float r = flux[i] - p * R(i);
-    acc += (double)(r * r / var[i]);
-  }
-  for (int c = 1; c < nc; c++) {
+  if (c == 0) {
+#pragma unroll 4
+    for (int i = 50 + threadIdx.x; i < st.cstart[1]; i += CT) {
+      const float p = poly_eval<K>(cc, st.xa[i]);
+      const float r = flux[i] - p * mod[i];
+      acc += (double)(r * r / var[i]);
+    }
+  } else {
     const int s0 = st.cstart[c], sp = st.cstop[c - 1];
     const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
-    const float *cp = cf32 + (c - 1) * K, *cc = cf32 + c * K;
 #pragma unroll 2
-    for (int i = s0 + threadIdx.x; i < sp; i += CT) {  // overlap: blend previous and current
+    for (int i = s0 + threadIdx.x; i < sp; i += CT) {
       const float pv = poly_eval<K>(cp, st.xa[i]);
       const float cu = poly_eval<K>(cc, st.xb[i]);
       const float f = st.fac[i];
       const float p = pv * f + cu * (1.0f - f);
-      const float r = flux[i] - p * R(i);
+      const float r = flux[i] - p * mod[i];
       acc += (double)(r * r / var[i]);
     }
 #pragma unroll 4
     for (int i = sp + threadIdx.x; i < nx; i += CT) {
       const float p = poly_eval<K>(cc, st.xa[i]);
-      const float r = flux[i] - p * R(i);
+      const float r = flux[i] - p * mod[i];
       acc += (double)(r * r / var[i]);
     }
   }
-  const double chi2 = block_sum(acc, ws) / (double)(N - 100);
-  write_result(b, e, chi2, 0);
+  const double t = block_sum(acc, ws);
+  if (threadIdx.x == 0) b.cpart[(size_t)e * MAX_CHUNKS + c] = t;
+}
+
+// chi2 = sum of the section partials in chunk order / (N - 100); errors as NaN
+__global__ void k_chunk_final(EvalBatch b) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= b.E) return;
+  const EvalPrep &P = b.prep[e];
+  const DevStar &st = b.stars[P.star];
+  if (st.cont_kind != CONT_CHUNK) return;
+  int status = P.status;
+  if (!status && st.cont_bad) status = S_CONTINUUM;
+  double chi2 = 0.0;
+  if (!status) {
+    const double *pt = b.cpart + (size_t)e * MAX_CHUNKS;
+    for (int c = 0; c < st.n_chunks; c++) chi2 += pt[c];
+    chi2 /= (double)(st.n_obs - 100);
+  }
+  b.cost[e] = status ? __longlong_as_double(0x7FF8000000000000ll) : chi2;
+  b.status[e] = status;
 }
 
 // LinearModelFitter (continuum_fitting.rs:68-95): projection onto the design
 // matrix's column space through its orthonormal basis Q; chi2 of the
 // ratio-space residual over [50, N-50) divided by N.  FixedContinuum
-// (441-474) and ConstantContinuum (484-500) too.
-__global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const float *given) {
+// (441-474) and ConstantContinuum (484-500) too.  One CTA per evaluation.
+__global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b) {
   __shared__ double ws[CW][MAX_P1];
   __shared__ double zs[MAX_LIN_K];
   const int e = blockIdx.x;
@@ -662,7 +899,7 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const
     return;
   }
   const int N = st.n_obs;
-  const Resampler R = make_resampler(G, st, P, given ? nullptr : final_row(b, P, e), given);
+  const float *mod = model_row(b, P, e);
   const float *flux = st.flux, *var = st.var;
   double chi2 = 0.0;
   double *par = b.params ? b.params + (size_t)e * b.param_stride : nullptr;
@@ -674,7 +911,7 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const
 #pragma unroll
       for (int k = 0; k < MAX_P1; k++) z[k] = 0.0;
       for (int i = threadIdx.x; i < N; i += CT) {
-        const double bd = (double)(flux[i] / R(i));
+        const double bd = (double)(flux[i] / mod[i]);
 #pragma unroll
         for (int k = 0; k < MAX_P1; k++)
           if (k < nk) z[k] = fma((double)__ldg(&st.q[(size_t)(g0 + k) * N + i]), bd, z[k]);
@@ -685,7 +922,7 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const
       for (int k = threadIdx.x; k < K; k += CT) par[k] = zs[k];
     double acc = 0.0;
     for (int i = 50 + threadIdx.x; i < N - 50; i += CT) {
-      const float bb = flux[i] / R(i);
+      const float bb = flux[i] / mod[i];
       double fit = 0.0;
       for (int k = 0; k < K; k++) fit = fma((double)__ldg(&st.q[(size_t)k * N + i]), zs[k], fit);
       const float r = (float)fit - bb;
@@ -696,18 +933,18 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const
     const int ig = st.ignore;
     double acc = 0.0;
     for (int i = ig + threadIdx.x; i < N - ig; i += CT) {
-      const float r = flux[i] - R(i) * st.cont[i];
+      const float r = flux[i] - mod[i] * st.cont[i];
       acc += (double)(r / var[i] * r);
     }
     chi2 = block_sum(acc, ws) / (double)(N - 2 * ig);
     if (par && threadIdx.x == 0) par[0] = 0.0;
   } else {
     double sum = 0.0;
-    for (int i = threadIdx.x; i < N; i += CT) sum += (double)(flux[i] / R(i));
+    for (int i = threadIdx.x; i < N; i += CT) sum += (double)(flux[i] / mod[i]);
     const float mean = (float)(block_sum(sum, ws) / (double)N);
     double acc = 0.0;
     for (int i = threadIdx.x; i < N; i += CT) {
-      const float r = flux[i] - R(i) * mean;
+      const float r = flux[i] - mod[i] * mean;
       acc += (double)(r / var[i] * r);
     }
     chi2 = block_sum(acc, ws) / (double)N;
@@ -717,42 +954,42 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b, const
 }
 
 template <int K>
-static void launch_chunk(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
-  k_chi2_chunk<K><<<b.E, CT, 0, s>>>(G, b, given);
-  count_launch();
+static void launch_chunk(const EvalBatch &b, cudaStream_t s) {
+  const dim3 grid(b.E, b.max_chunks);
+  k_chunk_moments<K><<<grid, CT, 0, s>>>(b);
+  k_chunk_resid<K><<<grid, CT, 0, s>>>(b);
+  count_launch(2);
 }
 
-static void launch_chi2_impl(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
+// chi2 of every evaluation from the model at its observed pixels
+// (model_row: resampled by k_broaden / k_resample_obs, or given)
+void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
   const uint32_t m = b.chunk_p1_mask;
-  if (m & (1u << 1)) launch_chunk<1>(G, b, given, s);
-  if (m & (1u << 2)) launch_chunk<2>(G, b, given, s);
-  if (m & (1u << 3)) launch_chunk<3>(G, b, given, s);
-  if (m & (1u << 4)) launch_chunk<4>(G, b, given, s);
-  if (m & (1u << 5)) launch_chunk<5>(G, b, given, s);
-  if (m & (1u << 6)) launch_chunk<6>(G, b, given, s);
-  if (m & (1u << 7)) launch_chunk<7>(G, b, given, s);
-  if (m & (1u << 8)) launch_chunk<8>(G, b, given, s);
-  if (m & (1u << 9)) launch_chunk<9>(G, b, given, s);
-  if (m & (1u << 10)) launch_chunk<10>(G, b, given, s);
-  if (m & (1u << 11)) launch_chunk<11>(G, b, given, s);
-  if (m & (1u << 12)) launch_chunk<12>(G, b, given, s);
-  if (m & (1u << 13)) launch_chunk<13>(G, b, given, s);
-  if (m & (1u << 14)) launch_chunk<14>(G, b, given, s);
-  if (m & (1u << 15)) launch_chunk<15>(G, b, given, s);
-  if (m & (1u << 16)) launch_chunk<16>(G, b, given, s);
-  if (b.other_cont) {
-    k_chi2_other<<<b.E, CT, 0, s>>>(G, b, given);
+  if (m && b.max_chunks > 0) {
+    if (m & (1u << 1)) launch_chunk<1>(b, s);
+    if (m & (1u << 2)) launch_chunk<2>(b, s);
+    if (m & (1u << 3)) launch_chunk<3>(b, s);
+    if (m & (1u << 4)) launch_chunk<4>(b, s);
+    if (m & (1u << 5)) launch_chunk<5>(b, s);
+    if (m & (1u << 6)) launch_chunk<6>(b, s);
+    if (m & (1u << 7)) launch_chunk<7>(b, s);
+    if (m & (1u << 8)) launch_chunk<8>(b, s);
+    if (m & (1u << 9)) launch_chunk<9>(b, s);
+    if (m & (1u << 10)) launch_chunk<10>(b, s);
+    if (m & (1u << 11)) launch_chunk<11>(b, s);
+    if (m & (1u << 12)) launch_chunk<12>(b, s);
+    if (m & (1u << 13)) launch_chunk<13>(b, s);
+    if (m & (1u << 14)) launch_chunk<14>(b, s);
+    if (m & (1u << 15)) launch_chunk<15>(b, s);
+    if (m & (1u << 16)) launch_chunk<16>(b, s);
+    k_chunk_final<<<(b.E + 255) / 256, 256, 0, s>>>(b);
     count_launch();
   }
-}
-
-void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) { launch_chi2_impl(G, b, nullptr, s); }
-
-// ContinuumFitter::fit_continuum on a given model (lib.rs:862-874): the
-// evaluations' resampled model is `given` (observed pixels).
-void launch_chi2_given(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s) {
-  launch_chi2_impl(G, b, given, s);
+  if (b.other_cont) {
+    k_chi2_other<<<b.E, CT, 0, s>>>(G, b);
+    count_launch();
+  }
 }
 
 // per-evaluation status when no chi2 is computed (model / spectrum outputs)
@@ -820,7 +1057,7 @@ void pipeline_pairs(int npx, int max_m, int max_hg, int *max_pairs, int *max_pai
   if (max_m <= 1 && max_hg == 0) {
     *max_pairs = 0;
   } else {
-    const int V = *may_unfuse ? MIN_FUSED_OUTPUTS : FFTN - wide;
+    const int V = (*may_unfuse ? MIN_FUSED_OUTPUTS : FFTN - wide) - 1;  // block advance
     const int nblk = (npx + V - 1) / V;
     *max_pairs = (nblk + 1) / 2;
   }
@@ -838,13 +1075,18 @@ void launch_pipeline(const DevGrid &G, const EvalBatch &b, const float2 *tw, con
   else launch_prep(G, b, s);
   if (o.rot) launch_rotker(G, b, tw, s);
   launch_interp(G, b, s);
+  launch_obs_bounds(G, b, s);
   launch_broaden(G, b, tw, s);
   if (o.may_unfuse) {
     launch_rot(G, b, tw, s);
     launch_gauss(G, b, s);
   }
-  if (b.need_chi2) launch_chi2(G, b, s);
-  else if (b.status) launch_prep_status(b, s);
+  if (b.need_chi2) {
+    launch_resample_obs(G, b, s);
+    launch_chi2(G, b, s);
+  } else if (b.status) {
+    launch_prep_status(b, s);
+  }
 }
 
 }  // namespace pb

@@ -26,7 +26,18 @@ struct EvalBatch {
   int need_chi2;
   uint32_t chunk_p1_mask;    // bit p1 set: a chunk continuum with p1 coefficients is present
   int other_cont;            // a linear / fixed / constant continuum is present
+  int max_chunks;            // most chunks of any chunk continuum in the batch
+  int obs_epi;               // chi2 batches: resample inside k_broaden, synth rows are not kept
+  int *bnd;                  // [E][bnd_stride] first observed pixel of every broadening block
+  int bnd_stride;
+  float *ccoef;              // [E][MAX_CHUNKS][MAX_P1] chunk polynomial coefficients (f32)
+  double *cpart;             // [E][MAX_CHUNKS] chi2 partial sums per chunk section
+  const float *given;        // model given at the observed pixels (continuum utilities) or null
+  int64_t given_stride;      // floats between the given rows of consecutive evaluations
 };
+
+// int entries per evaluation of EvalBatch::bnd for a grid of npx pixels
+inline int bnd_stride_for(int npx) { return npx / (MIN_FUSED_OUTPUTS - 1) + 3; }
 
 // Everything from the preparation to chi2 (or to the outputs) for one batch.
 struct PipelineOpts {
@@ -45,9 +56,14 @@ void launch_prep(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_prep_full(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_rotker(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// first observed pixel of every fused broadening block (chi2 batches)
+void launch_obs_bounds(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_rot(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// model at the observed pixels for the evaluations k_broaden did not resample
+void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// chi2 from the model at the observed pixels (b.given when set)
 void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // copy the preparation status to b.status (batches without chi2)
 void launch_prep_status(const EvalBatch &b, cudaStream_t s);
@@ -56,8 +72,6 @@ void launch_resample_out(const DevGrid &G, const EvalBatch &b, float *out, int64
                          cudaStream_t s);
 // broadened synth spectrum (before resampling): out [E][npx]
 void launch_copy_broadened(const DevGrid &G, const EvalBatch &b, float *out, cudaStream_t s);
-// chi2 of a model given at the observed pixels (continuum utility entry points)
-void launch_chi2_given(const DevGrid &G, const EvalBatch &b, const float *given, cudaStream_t s);
 void launch_build_chunk(const DevStar *star, const double *coef, int n, float *out, cudaStream_t s);
 void launch_gauss_standalone(const DevGrid &G, const DevStar *star, const float *in, float *out,
                              cudaStream_t s);

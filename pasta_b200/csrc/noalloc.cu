@@ -22,6 +22,7 @@
 // come before any stream capture.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -69,10 +70,12 @@ struct ErrSink {
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // bytes of scratch one label needs: prep record, rotation half spectrum,
-// eval->star index and the two spectrum rows
-size_t per_label_bytes(int64_t stride) {
+// eval->star index, the two spectrum rows, the broadening block bounds and
+// the chunk coefficients and partial sums
+size_t per_label_bytes(int64_t stride, int bnd_stride) {
   return align256(sizeof(EvalPrep)) + align256(1025 * sizeof(float2)) + align256(sizeof(int)) +
-         2 * align256((size_t)stride * sizeof(float));
+         2 * align256((size_t)stride * sizeof(float)) + align256((size_t)bnd_stride * sizeof(int)) +
+         align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float)) + align256((size_t)MAX_CHUNKS * sizeof(double));
 }
 
 int setup_device(int dev, DeviceSetup **out) {
@@ -143,8 +146,10 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
     g_noalloc_err = "at least one label is required";
     return PASTA_E_ARG;
   }
+  stride = std::max<int64_t>(stride, (n + 63) / 64 * 64);  // rows also hold the model at the observed pixels
+  const int bstr = bnd_stride_for(G.npx);
   const size_t fixed = align256(sizeof(DevStar));
-  const size_t per = per_label_bytes(stride);
+  const size_t per = per_label_bytes(stride, bstr);
   const int64_t max_labels = NOALLOC_SCRATCH_BYTES > fixed ? (int64_t)((NOALLOC_SCRATCH_BYTES - fixed) / per) : 0;
   if (L > max_labels) {
     char buf[256];
@@ -176,6 +181,12 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   float *A = (float *)p;
   p += align256((size_t)stride * sizeof(float) * (size_t)L);
   float *B = (float *)p;
+  p += align256((size_t)stride * sizeof(float) * (size_t)L);
+  int *bnd = (int *)p;
+  p += align256((size_t)bstr * sizeof(int) * (size_t)L);
+  float *ccoef = (float *)p;
+  p += align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float) * (size_t)L);
+  double *cpart = (double *)p;
   cudaStream_t s = (cudaStream_t)stream;
   k_noalloc_init<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(star, dstar, eval_star, (int)L);
   EvalBatch b{};
@@ -198,7 +209,13 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   pipeline_pairs(G.npx, FFTN, hg, &b.max_pairs, &b.max_pairs_unfused, &o.may_unfuse);
   b.need_chi2 = 1;
   b.chunk_p1_mask = star.cont_kind == CONT_CHUNK ? 1u << star.p1 : 0u;
+  b.max_chunks = star.cont_kind == CONT_CHUNK ? star.n_chunks : 0;
   b.other_cont = star.cont_kind == CONT_CHUNK ? 0 : 1;
+  b.obs_epi = 1;
+  b.bnd = bnd;
+  b.bnd_stride = bstr;
+  b.ccoef = ccoef;
+  b.cpart = cpart;
   launch_pipeline(G, b, S->twiddle, o, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) {

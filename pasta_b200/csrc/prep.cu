@@ -107,19 +107,27 @@ __global__ void k_prep(DevGrid G, EvalBatch b, int full_window) {
   P.i_lo = i_lo; P.i_hi = i_hi;
   P.hg = hg;
   // fused: each 2048-point block yields Vf final outputs; the rotation halo
-  // (m - 1) and the instrument halo (2 hg) both come out of the block
+  // (m - 1) and the instrument halo (2 hg) both come out of the block.
+  // Blocks advance by Vf - 1, so the block that owns synth pixel j (the
+  // first Vf - 1 of its outputs) also holds j + 1, the resampler's partner.
   const int Vf = FFTN - (m - 1) - 2 * hg;
   const bool work = m > 1 || hg > 0;
+  P.epi = 0;
   if (Vf >= MIN_FUSED_OUTPUTS) {
     P.fused = 1;
-    P.nblk = work ? (o_hi - o_lo + Vf - 1) / Vf : 0;
+    const int span = o_hi - 1 - o_lo > 1 ? o_hi - 1 - o_lo : 1;
+    P.nblk = work ? (span + Vf - 2) / (Vf - 1) : 0;
     P.final_in_b = work ? 1 : 0;
+    P.epi = work && b.obs_epi && st.obs_sorted && !full_window ? 1 : 0;
   } else {  // very wide kernels: rotation FFT into B, instrument profile into A
     P.fused = 0;
     const int V = FFTN - (m - 1);
     P.nblk = m > 1 ? (g_hi - g_lo + V - 1) / V : 0;
     P.final_in_b = hg > 0 ? (m > 1 ? 0 : 1) : (m > 1 ? 1 : 0);
   }
+  // the model at the observed pixels goes where no live data is: B when
+  // k_broaden resamples (it reads A), else the buffer without the synth row
+  P.mobs_in_b = P.epi ? 1 : (P.final_in_b ? 0 : 1);
   P.status = status;
 }
 
