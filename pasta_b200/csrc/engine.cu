@@ -163,19 +163,20 @@ struct Workspace {
   int bnd_stride = 0;
   int64_t gen = 0;  // bumped on every reallocation (captured graphs compare it)
   DBuf<float> A, B;
-  DBuf<float2> H;
+  DBuf<float2> H, HG;
   DBuf<EvalPrep> prep;
   DBuf<int> bnd;       // first observed pixel per broadening block
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   void ensure(int64_t want, int64_t str, int bstr) {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
-    A.release(); B.release(); H.release(); prep.release();
+    A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); ccoef.release(); cpart.release();
     cap = 0;
     A.alloc((size_t)want * str);
     B.alloc((size_t)want * str);
     H.alloc((size_t)want * 1025);
+    HG.alloc((size_t)want * 1025);
     prep.alloc((size_t)want);
     bnd.alloc((size_t)want * bstr);
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
@@ -189,7 +190,7 @@ struct Workspace {
 
 // bytes of workspace one evaluation takes with rows of `stride` floats
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
-  return stride * 8 + 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)bnd_stride * 4 +
+  return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)bnd_stride * 4 +
          (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8);
 }
 
@@ -681,6 +682,7 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.stars = a.stars;
   b.prep = g->ws.prep.p;
   b.H = g->ws.H.p;
+  b.HG = g->ws.HG.p;
   b.bufA = g->ws.A.p;
   b.bufB = g->ws.B.p;
   b.stride = g->ws.stride;

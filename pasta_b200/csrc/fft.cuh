@@ -55,35 +55,47 @@ __device__ __forceinline__ void dft8(cf v[8]) {
   v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 
-// One Stockham stage of radix R at sub-transform length Ns.  All reads of
+// One Stockham stage of radix R at sub-transform length NS.  All reads of
 // the stage happen before a barrier, all writes after it, so the transform
 // runs in place.  The caller must __syncthreads() after filling the input.
-// ld(i) returns input element i, st(i, v) stores output element i; the
-// defaults use the swizzled re/im arrays (the first stage may read from a
-// staging buffer, the last may write elsewhere).
-template <int R, bool INV, class LD, class ST>
-__device__ __forceinline__ void fft_stage_io(int Ns, const float2 *__restrict__ tw, const LD &ld, const ST &st) {
-  constexpr int N = 2048, J = N / R, PER = J / FFT_T;
+// ld(i, a) returns input element i (a = its swizzled shared-memory slot),
+// st(i, a, v) stores output element i; SmemLoad / SmemStore use the
+// swizzled re/im arrays, other functors may read a staging buffer or write
+// outputs elsewhere.
+//
+// Slot arithmetic: the swizzle only mixes bits 3-7 into bits 0-4, so
+// pidx(j + c) = pidx(j) + c for every multiple c of 256, and the writes of
+// the four stages of fft2048 reduce to one XOR with a per-thread base:
+//   NS = 1:   pidx(8j + r)           = (8j ^ (j & 31)) ^ r
+//   NS = 8:   pidx(d + 8r)           = (d ^ (j & 24)) ^ 9r
+//   NS = 64:  pidx(d + 64r)          = (d ^ ((j >> 3) & 7)) ^ (64r ^ 8(r & 3))
+//   NS = 512: pidx(j + 512r)         = pidx(j) + 512r
+// with d the first output index of the thread's butterfly.  The identities
+// hold for every thread and r of these stages (checked exhaustively).
+template <int R, int NS, bool INV, class LD, class ST>
+__device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD &ld, const ST &st) {
+  static_assert((R == 8 && (NS == 1 || NS == 8 || NS == 64)) || (R == 4 && NS == 512), "fft2048 stage");
+  constexpr int N = 2048, J = N / R, PER = J / FFT_T, STEP = N / (NS * R);
+  const int t = threadIdx.x;
+  const int p0 = pidx(t);
   cf v[PER][R];
-  const int step = N / (Ns * R);
 #pragma unroll
   for (int q = 0; q < PER; q++) {
-    const int j = threadIdx.x + q * FFT_T;
-    const int jm = j & (Ns - 1);
+    const int j = t + q * FFT_T;
 #pragma unroll
-    for (int r = 0; r < R; r++) v[q][r] = ld(j + r * J);
-    if (jm != 0) {
-      // twiddles W^(jm r step): W^1, W^2, W^4 from the table, the others by
-      // at most two multiplications
-      const int k1 = jm * step;
-      const float2 t1 = __ldg(&tw[k1 & (N - 1)]), t2 = __ldg(&tw[(2 * k1) & (N - 1)]);
+    for (int r = 0; r < R; r++) v[q][r] = ld(j + r * J, p0 + q * FFT_T + r * J);
+    if constexpr (NS > 1) {
+      // twiddles W^(jm r STEP): W^1, W^2, W^4 from the table, the others by
+      // at most two multiplications (jm = 0 multiplies by exactly 1)
+      const int k1 = (j & (NS - 1)) * STEP;
+      const float2 t1 = __ldg(&tw[k1]), t2 = __ldg(&tw[2 * k1]);
       const cf w1{t1.x, INV ? -t1.y : t1.y}, w2{t2.x, INV ? -t2.y : t2.y};
       v[q][1] = cmul(v[q][1], w1);
       v[q][2] = cmul(v[q][2], w2);
       const cf w3 = cmul(w1, w2);
       v[q][3] = cmul(v[q][3], w3);
       if constexpr (R == 8) {
-        const float2 t4 = __ldg(&tw[(4 * k1) & (N - 1)]);
+        const float2 t4 = __ldg(&tw[4 * k1]);
         const cf w4{t4.x, INV ? -t4.y : t4.y};
         v[q][4] = cmul(v[q][4], w4);
         v[q][5] = cmul(v[q][5], cmul(w4, w1));
@@ -95,44 +107,46 @@ __device__ __forceinline__ void fft_stage_io(int Ns, const float2 *__restrict__ 
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < PER; q++) {
-    const int j = threadIdx.x + q * FFT_T;
-    const int jm = j & (Ns - 1);
+    const int j = t + q * FFT_T;
     if constexpr (R == 8) dft8<INV>(v[q]);
     else dft4<INV>(v[q][0], v[q][1], v[q][2], v[q][3]);
-    const int idxD = (j / Ns) * Ns * R + jm;
+    const int d = (j / NS) * NS * R + (j & (NS - 1));
 #pragma unroll
-    for (int r = 0; r < R; r++) st(idxD + r * Ns, v[q][r]);
+    for (int r = 0; r < R; r++) {
+      int a;
+      if constexpr (NS == 1) a = (d ^ (j & 31)) ^ r;
+      else if constexpr (NS == 8) a = (d ^ (j & 24)) ^ (9 * r);
+      else if constexpr (NS == 64) a = (d ^ ((j >> 3) & 7)) ^ (64 * r ^ 8 * (r & 3));
+      else a = p0 + q * FFT_T + r * NS;
+      st(d + r * NS, a, v[q][r]);
+    }
   }
   __syncthreads();
 }
 
 struct SmemLoad {
   const float *re, *im;
-  __device__ __forceinline__ cf operator()(int i) const {
-    const int a = pidx(i);
-    return cf{re[a], im[a]};
-  }
+  __device__ __forceinline__ cf operator()(int, int a) const { return cf{re[a], im[a]}; }
 };
 struct SmemStore {
   float *re, *im;
-  __device__ __forceinline__ void operator()(int i, cf v) const {
-    const int a = pidx(i);
+  __device__ __forceinline__ void operator()(int, int a, cf v) const {
     re[a] = v.x;
     im[a] = v.y;
   }
 };
 
-template <int R, bool INV>
-__device__ __forceinline__ void fft_stage(float *re, float *im, int Ns, const float2 *__restrict__ tw) {
-  fft_stage_io<R, INV>(Ns, tw, SmemLoad{re, im}, SmemStore{re, im});
+template <int R, int NS, bool INV>
+__device__ __forceinline__ void fft_stage(float *re, float *im, const float2 *__restrict__ tw) {
+  fft_pass<R, NS, INV>(tw, SmemLoad{re, im}, SmemStore{re, im});
 }
 
 template <bool INV>
 __device__ __forceinline__ void fft2048(float *re, float *im, const float2 *__restrict__ tw) {
-  fft_stage<8, INV>(re, im, 1, tw);
-  fft_stage<8, INV>(re, im, 8, tw);
-  fft_stage<8, INV>(re, im, 64, tw);
-  fft_stage<4, INV>(re, im, 512, tw);
+  fft_stage<8, 1, INV>(re, im, tw);
+  fft_stage<8, 8, INV>(re, im, tw);
+  fft_stage<8, 64, INV>(re, im, tw);
+  fft_stage<4, 512, INV>(re, im, tw);
 }
 
 }  // namespace pb

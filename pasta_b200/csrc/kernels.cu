@@ -314,14 +314,14 @@ __device__ __forceinline__ void stage_item(const EvalBatch &b, long long item, f
 struct StageLoad {
   const float *s0, *s1;
   bool has1;
-  __device__ __forceinline__ cf operator()(int i) const { return cf{s0[i], has1 ? s1[i] : 0.0f}; }
+  __device__ __forceinline__ cf operator()(int i, int) const { return cf{s0[i], has1 ? s1[i] : 0.0f}; }
 };
 // last inverse stage of the folded path: FFT index i is output i - lo
 struct FoldStore {
   float *o0, *o1;
   int lo, V;
   float sc;
-  __device__ __forceinline__ void operator()(int i, cf v) const {
+  __device__ __forceinline__ void operator()(int i, int, cf v) const {
     const int u = i - lo;
     if ((unsigned)u < (unsigned)V) {
       o0[u] = v.x * sc;
@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
   float *gks = ob1 + FFT_SM;  // the fixed instrument kernel of the current item
   const long long total = (long long)b.E * b.max_pairs;
   const int N = G.npx;
+  const int p0 = pidx(threadIdx.x);
   long long item = next_item(b, blockIdx.x, total);
   if (item < total) stage_item(b, item, stg0, stg1);
   cp_async_commit();
@@ -362,39 +363,34 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
     // all inside [0, N), where rotation-then-Gaussian equals one convolution
     // with the combined kernel: multiply the spectra and skip the taps.
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
-    const bool fold = fixedk && m > 1 && st.gspec != nullptr && s0 - hg >= 0 && e_last + hg <= N;
+    const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     if (m > 1) {
-      fft_stage_io<8, false>(1, tw, ld, SmemStore{re, im});  // first stage straight from the staging rows
+      fft_pass<8, 1, false>(tw, ld, SmemStore{re, im});  // first stage straight from the staging rows
       if (nxt < total) stage_item(b, nxt, stg0, stg1);
       cp_async_commit();
-      fft_stage<8, false>(re, im, 8, tw);
-      fft_stage<8, false>(re, im, 64, tw);
-      fft_stage<4, false>(re, im, 512, tw);
-      const float2 *H = b.H + (size_t)e * 1025;
+      fft_stage<8, 8, false>(re, im, tw);
+      fft_stage<8, 64, false>(re, im, tw);
+      fft_stage<4, 512, false>(re, im, tw);
+      // the kernel spectrum (Hermitian: bins above 1024 are conjugates)
+      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
       for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
         float2 h = k <= 1024 ? H[k] : H[FFTN - k];
         if (k > 1024) h.y = -h.y;
-        cf hk{h.x, h.y};
-        if (fold) {
-          float2 g = k <= 1024 ? st.gspec[k] : st.gspec[FFTN - k];
-          if (k > 1024) g.y = -g.y;
-          hk = cmul(hk, cf{g.x, g.y});
-        }
-        const int a = pidx(k);
-        const cf z = cmul(cf{re[a], im[a]}, hk);
+        const int a = p0 + (k - threadIdx.x);  // pidx(k), k - threadIdx.x a multiple of 256
+        const cf z = cmul(cf{re[a], im[a]}, cf{h.x, h.y});
         re[a] = z.x;
         im[a] = z.y;
       }
       __syncthreads();
-      fft_stage<8, true>(re, im, 1, tw);
-      fft_stage<8, true>(re, im, 8, tw);
-      fft_stage<8, true>(re, im, 64, tw);
+      fft_stage<8, 1, true>(re, im, tw);
+      fft_stage<8, 8, true>(re, im, tw);
+      fft_stage<8, 64, true>(re, im, tw);
       base = m - 1;
       const float sc = 1.0f / 2048.0f;
       if (fold) {  // output u sits at base + 2 hg + u
-        fft_stage_io<4, true>(512, tw, SmemLoad{re, im}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
+        fft_pass<4, 512, true>(tw, SmemLoad{re, im}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
       } else {
-        fft_stage<4, true>(re, im, 512, tw);
+        fft_stage<4, 512, true>(re, im, tw);
         for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
           const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
           re[pidx(t)] = (i0 >= 0 && i0 < N) ? re[pidx(t)] * sc : 0.0f;
@@ -404,9 +400,9 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
       }
     } else {  // identity rotation: the staged input is the rotation output
       for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
-        const cf v = ld(t);
-        re[pidx(t)] = v.x;
-        im[pidx(t)] = v.y;
+        const cf v = ld(t, 0);
+        re[p0 + (t - threadIdx.x)] = v.x;
+        im[p0 + (t - threadIdx.x)] = v.y;
       }
       __syncthreads();
       if (nxt < total) stage_item(b, nxt, stg0, stg1);
@@ -445,6 +441,7 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
       const int *bd = b.bnd + (size_t)e * b.bnd_stride + 2 * pair;
       const int q0 = bd[0], q1 = bd[1], q2 = has1 ? bd[2] : q1;
       const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
+#pragma unroll 4
       for (int i = q0 + threadIdx.x; i < q2; i += FFT_T) {
         const ResPos q = R.pos(i);
         const bool k1 = i >= q1;
@@ -755,18 +752,22 @@ void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   count_launch();
 }
 
-// ChunkFitter::fit_continuum (continuum_fitting.rs:382-396), one CTA per
+// ChunkFitter::fit_continuum (continuum_fitting.rs:382-396), one warp per
 // (evaluation, chunk): the unweighted least-squares polynomial of
 // flux/model over the chunk (216-226) is the projection onto the chunk's
 // polynomial space; it is solved here in a Legendre basis with the FP64
 // Cholesky factor of its Gram matrix (the same space as the reference's
 // monomial SVD, far better conditioned).  Moments accumulate in FP64.
-// K = polynomial order + 1 (one instantiation per order present).
+// K = polynomial order + 1 (one instantiation per order present).  A warp
+// walks the whole chunk (no block barriers), so the loads of many chunks
+// are in flight per SM.
 template <int K>
 __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch b) {
-  __shared__ double ws[CW][MAX_P1];
-  __shared__ double zs[K];
-  const int e = blockIdx.x, c = blockIdx.y;
+  __shared__ double zs[CW][MAX_P1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long gw = (long long)blockIdx.x * CW + warp;
+  if (gw >= (long long)b.E * b.max_chunks) return;
+  const int e = (int)(gw / b.max_chunks), c = (int)(gw % b.max_chunks);
   const EvalPrep &P = b.prep[e];
   if (P.status) return;
   const DevStar &st = b.stars[P.star];
@@ -777,7 +778,7 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
 #pragma unroll
   for (int k = 0; k < K; k++) z[k] = 0.0;
 #pragma unroll 4
-  for (int i = lo + threadIdx.x; i < hi; i += CT) {
+  for (int i = lo + lane; i < hi; i += 32) {
     const double y = (double)(flux[i] / mod[i]);
     const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
     float Pk[K];
@@ -785,38 +786,54 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
 #pragma unroll
     for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
   }
-  block_sum_vec<K>(z, ws, zs);
-  if (threadIdx.x == 0) {  // FP64 Cholesky solve G a = z, in place in zs
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const double t = warp_sum(z[k]);
+    if (lane == 0) zs[warp][k] = t;
+  }
+  if (lane == 0) {  // FP64 Cholesky solve G a = z, in place
+    double *a = zs[warp];
     const double *L = st.chol + (size_t)c * K * K;
     for (int k = 0; k < K; k++) {
-      double t = zs[k];
-      for (int j = 0; j < k; j++) t -= L[k * K + j] * zs[j];
-      zs[k] = t / L[k * K + k];
+      double t = a[k];
+      for (int j = 0; j < k; j++) t -= L[k * K + j] * a[j];
+      a[k] = t / L[k * K + k];
     }
     for (int k = K - 1; k >= 0; k--) {
-      double t = zs[k];
-      for (int j = k + 1; j < K; j++) t -= L[j * K + k] * zs[j];
-      zs[k] = t / L[k * K + k];
+      double t = a[k];
+      for (int j = k + 1; j < K; j++) t -= L[j * K + k] * a[j];
+      a[k] = t / L[k * K + k];
     }
     float *cf = b.ccoef + ((size_t)e * MAX_CHUNKS + c) * MAX_P1;
-    for (int k = 0; k < K; k++) cf[k] = (float)zs[k];
+    for (int k = 0; k < K; k++) cf[k] = (float)a[k];
     if (b.params) {
       double *par = b.params + (size_t)e * b.param_stride + c * K;
-      for (int k = 0; k < K; k++) par[k] = zs[k];
+      for (int k = 0; k < K; k++) par[k] = a[k];
     }
   }
+}
+
+template <int K>
+__device__ __forceinline__ float poly_eval_r(const float (&coef)[K], float x) {
+  float P[K];
+  legendre<K>(x, P);
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < K; k++) s = fmaf(coef[k], P[k], s);
+  return s;
 }
 
 // chi2 section of chunk c (continuum_fitting.rs:280-360): chunk 0 alone on
 // [50, start_1); chunk c >= 1 blended with chunk c - 1 (sin^2 factor) on
 // [start_c, stop_{c-1}), then alone up to start_{c+1} (N - 50 for the
-// last).  Partial sums per section in FP64, added in chunk order by
-// k_chunk_final.
+// last).  One warp per section; partial sums in FP64, added in chunk order
+// by k_chunk_final.
 template <int K>
 __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b) {
-  __shared__ double ws[CW][MAX_P1];
-  __shared__ float cp[K], cc[K];
-  const int e = blockIdx.x, c = blockIdx.y;
+  const int lane = threadIdx.x & 31;
+  const long long gw = (long long)blockIdx.x * CW + (threadIdx.x >> 5);
+  if (gw >= (long long)b.E * b.max_chunks) return;
+  const int e = (int)(gw / b.max_chunks), c = (int)(gw % b.max_chunks);
   const EvalPrep &P = b.prep[e];
   if (P.status) return;
   const DevStar &st = b.stars[P.star];
@@ -824,16 +841,17 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
   const int N = st.n_obs, nc = st.n_chunks;
   const float *mod = model_row(b, P, e), *flux = st.flux, *var = st.var;
   const float *coef = b.ccoef + (size_t)e * MAX_CHUNKS * MAX_P1;
-  if (threadIdx.x < K) {
-    cc[threadIdx.x] = coef[c * MAX_P1 + threadIdx.x];
-    cp[threadIdx.x] = c > 0 ? coef[(c - 1) * MAX_P1 + threadIdx.x] : 0.0f;
+  float cc[K], cp[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    cc[k] = coef[c * MAX_P1 + k];
+    cp[k] = c > 0 ? coef[(c - 1) * MAX_P1 + k] : 0.0f;
   }
-  __syncthreads();
   double acc = 0.0;
   if (c == 0) {
 #pragma unroll 4
-    for (int i = 50 + threadIdx.x; i < st.cstart[1]; i += CT) {
-      const float p = poly_eval<K>(cc, st.xa[i]);
+    for (int i = 50 + lane; i < st.cstart[1]; i += 32) {
+      const float p = poly_eval_r<K>(cc, st.xa[i]);
       const float r = flux[i] - p * mod[i];
       acc += (double)(r * r / var[i]);
     }
@@ -841,23 +859,23 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
     const int s0 = st.cstart[c], sp = st.cstop[c - 1];
     const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
 #pragma unroll 2
-    for (int i = s0 + threadIdx.x; i < sp; i += CT) {
-      const float pv = poly_eval<K>(cp, st.xa[i]);
-      const float cu = poly_eval<K>(cc, st.xb[i]);
+    for (int i = s0 + lane; i < sp; i += 32) {
+      const float pv = poly_eval_r<K>(cp, st.xa[i]);
+      const float cu = poly_eval_r<K>(cc, st.xb[i]);
       const float f = st.fac[i];
       const float p = pv * f + cu * (1.0f - f);
       const float r = flux[i] - p * mod[i];
       acc += (double)(r * r / var[i]);
     }
 #pragma unroll 4
-    for (int i = sp + threadIdx.x; i < nx; i += CT) {
-      const float p = poly_eval<K>(cc, st.xa[i]);
+    for (int i = sp + lane; i < nx; i += 32) {
+      const float p = poly_eval_r<K>(cc, st.xa[i]);
       const float r = flux[i] - p * mod[i];
       acc += (double)(r * r / var[i]);
     }
   }
-  const double t = block_sum(acc, ws);
-  if (threadIdx.x == 0) b.cpart[(size_t)e * MAX_CHUNKS + c] = t;
+  acc = warp_sum(acc);
+  if (lane == 0) b.cpart[(size_t)e * MAX_CHUNKS + c] = acc;
 }
 
 // chi2 = sum of the section partials in chunk order / (N - 100); errors as NaN
@@ -955,7 +973,8 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b) {
 
 template <int K>
 static void launch_chunk(const EvalBatch &b, cudaStream_t s) {
-  const dim3 grid(b.E, b.max_chunks);
+  const long long warps = (long long)b.E * b.max_chunks;
+  const unsigned grid = (unsigned)((warps + CW - 1) / CW);
   k_chunk_moments<K><<<grid, CT, 0, s>>>(b);
   k_chunk_resid<K><<<grid, CT, 0, s>>>(b);
   count_launch(2);

@@ -15,6 +15,7 @@ struct EvalBatch {
   const DevStar *stars;
   EvalPrep *prep;            // [E]
   float2 *H;                 // [E][1025] rotation kernel half-spectra
+  float2 *HG;                // [E][1025] the same times the fixed instrument spectrum (or null)
   float *bufA, *bufB;        // [E][stride] spectra workspaces
   int64_t stride;            // floats per evaluation row
   double *cost;              // [E]

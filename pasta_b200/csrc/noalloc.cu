@@ -69,11 +69,12 @@ struct ErrSink {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// bytes of scratch one label needs: prep record, rotation half spectrum,
+// bytes of scratch one label needs: prep record, rotation half spectra
+// (alone and times the instrument spectrum),
 // eval->star index, the two spectrum rows, the broadening block bounds and
 // the chunk coefficients and partial sums
 size_t per_label_bytes(int64_t stride, int bnd_stride) {
-  return align256(sizeof(EvalPrep)) + align256(1025 * sizeof(float2)) + align256(sizeof(int)) +
+  return align256(sizeof(EvalPrep)) + 2 * align256(1025 * sizeof(float2)) + align256(sizeof(int)) +
          2 * align256((size_t)stride * sizeof(float)) + align256((size_t)bnd_stride * sizeof(int)) +
          align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float)) + align256((size_t)MAX_CHUNKS * sizeof(double));
 }
@@ -176,6 +177,8 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   p += align256(sizeof(EvalPrep) * (size_t)L);
   float2 *H = (float2 *)p;
   p += align256(1025 * sizeof(float2) * (size_t)L);
+  float2 *HG = (float2 *)p;
+  p += align256(1025 * sizeof(float2) * (size_t)L);
   int *eval_star = (int *)p;
   p += align256(sizeof(int) * (size_t)L);
   float *A = (float *)p;
@@ -196,6 +199,7 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   b.stars = dstar;
   b.prep = prep;
   b.H = H;
+  b.HG = HG;
   b.bufA = A;
   b.bufB = B;
   b.stride = stride;

@@ -171,6 +171,17 @@ __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const 
   fft2048<false>(re, im, tw);
   float2 *H = b.H + (size_t)e * 1025;
   for (int k = threadIdx.x; k <= 1024; k += FFT_T) H[k] = make_float2(re[pidx(k)], im[pidx(k)]);
+  // rotation x instrument spectrum for the blocks of the broadening kernel
+  // that apply both as one convolution
+  const DevStar &st = b.stars[P.star];
+  if (b.HG && st.gspec) {
+    float2 *HG = b.HG + (size_t)e * 1025;
+    for (int k = threadIdx.x; k <= 1024; k += FFT_T) {
+      const float2 g = st.gspec[k];
+      const cf z = cmul(cf{re[pidx(k)], im[pidx(k)]}, cf{g.x, g.y});
+      HG[k] = make_float2(z.x, z.y);
+    }
+  }
 }
 
 void launch_prep(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
