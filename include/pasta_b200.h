@@ -224,6 +224,26 @@ int pasta_fit_many(const pasta_grid *g, int64_t S,
                    const int64_t *n, const uint64_t *seeds, int mode,
                    pasta_fit_result *results, float *const *params);
 
+/* SingleFitter::compute_uncertainty / compute_uncertainty_bulk
+ * (fitting.rs:480-568, lib.rs:1545-1600): for each of S spectra (flux, var
+ * [S x n], one dispersion and continuum fitter) and its best-fit label
+ * (labels [S x 5]), the distances below and above each label where chi2
+ * reaches chi2_best * (1 + sqrt(2 / n_eff)), n_eff = 4 spec_res (l_last -
+ * l_first) / (l_first + l_last), found by Brent's method (tol 1e-3 in units
+ * of the search radius).  search_radius [5] or NULL for (2000, 0.3, 0.3,
+ * 40, 40); as in the reference the Teff radius is multiplied by Teff and the
+ * vsini radius is max(vsini * r, 100).  out [S x 5 x 2] (label-major,
+ * below then above) and bound_status [S x 5 x 2] (0 = found, else the
+ * PASTA_E_* that stopped the search, out = NaN); star_status [S] is the
+ * status of chi2 at the given label (non-zero fails all its bounds, where
+ * the reference returns an error). */
+int pasta_compute_uncertainty(const pasta_grid *g, const pasta_dispersion *d,
+                              const pasta_continuum *c, int64_t S,
+                              const float *flux, const float *var, int64_t n,
+                              double spec_res, const double *labels,
+                              const double *search_radius, double *out,
+                              int32_t *bound_status, int32_t *star_status);
+
 /* Step-wise batched fit (what pasta_fit_many runs): create uploads the
  * stars and places the swarms, step advances every swarm by `steps` PSO
  * steps (the first step evaluates the initial swarm) and reports the device

@@ -7,6 +7,7 @@ outputs (see pasta_oracle.h); pinned by analytic known-answer tests.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -278,3 +279,95 @@ def fit(grid, disp, cont, st, fluxes, vars_, seeds, prec=F32, nthreads=0, over_s
 
 def draw_u01(seed, phase, a, b, c):
     return lib().or_draw_u01(seed, phase, a, b, c)
+
+
+def limits_at(grid, tml, index):
+    """Grid::get_limits_at (interpolate.rs:645-663) for index 0..2."""
+    p = np.ascontiguousarray(tml[:3], dtype=np.float64)
+    lo, hi = C.c_double(), C.c_double()
+    if lib().or_limits_at(grid.h, _p(p), index, C.byref(lo), C.byref(hi)):
+        raise _err()
+    return lo.value, hi.value
+
+
+def _brent(f, a, b, tol=1e-3, max_iter=500):
+    """Brent's zero finder (Brent 1973, ch. 4; Numerical Recipes' zbrent) on
+    [a, b]; f raises on a failed evaluation.  Returns the root estimate."""
+    fa, fb = f(a), f(b)
+    if fa * fb > 0:
+        raise ValueError("f(min) and f(max) must have different signs")
+    c, fc = b, fb
+    d = e = b - a
+    eps = np.finfo(np.float64).eps
+    for _ in range(max_iter):
+        if (fb > 0 and fc > 0) or (fb < 0 and fc < 0):
+            c, fc = a, fa
+            d = e = b - a
+        if abs(fc) < abs(fb):
+            a, b, c = b, c, b
+            fa, fb, fc = fb, fc, fb
+        tol1 = 2.0 * eps * abs(b) + 0.5 * tol
+        xm = 0.5 * (c - b)
+        if abs(xm) <= tol1 or fb == 0.0:
+            return b
+        if abs(e) >= tol1 and abs(fa) > abs(fb):
+            s = fb / fa
+            if a == c:
+                p, q = 2.0 * xm * s, 1.0 - s
+            else:
+                qq, r = fa / fc, fb / fc
+                p = s * (2.0 * xm * qq * (qq - r) - (b - a) * (r - 1.0))
+                q = (qq - 1.0) * (r - 1.0) * (s - 1.0)
+            if p > 0:
+                q = -q
+            p = abs(p)
+            if 2.0 * p < min(3.0 * xm * q - abs(tol1 * q), abs(e * q)):
+                e, d = d, p / q
+            else:
+                d = e = xm
+        else:
+            d = e = xm
+        a, fa = b, fb
+        b += d if abs(d) > tol1 else math.copysign(tol1, xm)
+        fb = f(b)
+    raise ValueError("no convergence")
+
+
+def compute_uncertainty(grid, disp, cont, flux, var, spec_res, label, search_radius=None, prec=F64):
+    """SingleFitter::compute_uncertainty (fitting.rs:480-568) on the oracle's
+    chi2: {label index: (below, above)} with None for a failed search."""
+    sr = np.array(search_radius if search_radius is not None else [2000.0, 0.3, 0.3, 40.0, 40.0], float)
+    lab = np.asarray(label, dtype=np.float64)
+    sr[0] *= lab[0]
+    sr[3] = max(lab[3] * sr[3], 100.0)
+    c0, s0 = chi2(grid, disp, cont, flux, var, lab, prec)
+    if s0[0]:
+        raise OracleError("chi2 at the label failed")
+    n = 4.0 * spec_res * (disp.wl[-1] - disp.wl[0]) / (disp.wl[0] + disp.wl[-1])
+    target = c0[0] * (1.0 + math.sqrt(2.0 / n))
+    outer = {3: (0.0, 1e4), 4: (-1e3, 1e3)}
+    res = {}
+    for i in range(5):
+        pair = []
+        for right in (False, True):
+            try:
+                bl = lab.copy()
+                bl[i] += sr[i] if right else -sr[i]
+                lo, hi = outer[i] if i in outer else limits_at(grid, bl, i)
+                bound = min(max(bl[i], lo), hi)
+                resc = (bound - lab[i]) / sr[i]
+
+                def f(x, i=i):
+                    l2 = lab.copy()
+                    l2[i] += x * sr[i]
+                    c, s = chi2(grid, disp, cont, flux, var, l2, prec)
+                    if s[0]:
+                        raise ValueError("chi2 failed")
+                    return c[0] - target
+
+                sol = _brent(f, 0.0, min(resc, 1.0)) if right else _brent(f, resc, 0.0)
+                pair.append(sol * sr[i] if right else -sol * sr[i])
+            except (ValueError, OracleError):
+                pair.append(None)
+        res[i] = tuple(pair)
+    return res

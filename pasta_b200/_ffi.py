@@ -63,6 +63,7 @@ SIGNATURES = {
     "pasta_chi2_noalloc": (I, [P, P, P, P, P, I64, P, I64, P, P, P]),
     "pasta_fit": (I, [P, P, P, P, P, P, I64, I64, P, I, P, P, P]),
     "pasta_fit_many": (I, [P, I64, P, P, P, P, P, P, P, I, P, P]),
+    "pasta_compute_uncertainty": (I, [P, P, P, I64, P, P, I64, D, P, P, P, P, P]),
     "pasta_batch_create": (I, [P, I64, P, P, P, P, P, P, P, P]),
     "pasta_batch_step": (I, [P, I, P]),
     "pasta_batch_profile_step": (I, [P, P]),

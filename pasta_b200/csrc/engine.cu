@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <limits>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -1877,6 +1878,257 @@ int pasta_fit_many(const pasta_grid *g, int64_t S, const pasta_dispersion *const
   std::vector<StarInput> in(S);
   for (int64_t i = 0; i < S; i++) in[i] = StarInput{d[i], c[i], &settings[i], flux[i], var[i], n[i], seeds[i]};
   return fit_common(g, in, mode, results, params, nullptr);
+}
+
+// ---------------------------------------------------------- uncertainty
+namespace {
+
+// Brent's zero finder (R. P. Brent, "Algorithms for Minimization without
+// Derivatives", 1973, ch. 4; the same iteration as Numerical Recipes'
+// zbrent): bisection, secant and inverse quadratic interpolation with the
+// bracket [b, c] kept around the root.  SingleFitter::compute_uncertainty
+// runs it through argmin's BrentRoot with tol = 1e-3 (fitting.rs:536-541).
+// The search is a state machine so that one batched chi2 launch serves the
+// pending evaluation of every open search.
+struct BrentSearch {
+  double a = 0, b = 0, c = 0, d = 0, e = 0, fa = 0, fb = 0, fc = 0, tol = 1e-3;
+  int state = 0;  // 0: f(a), f(b) pending; 1: f(b) pending; 2: converged; 3: failed
+  int status = 0; // failure code
+  int iters = 0;
+  // after fb is known: either converge or move b and ask for f(b)
+  void advance() {
+    if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) {
+      c = a;
+      fc = fa;
+      d = b - a;
+      e = d;
+    }
+    if (std::fabs(fc) < std::fabs(fb)) {
+      a = b; b = c; c = a;
+      fa = fb; fb = fc; fc = fa;
+    }
+    const double tol1 = 2.0 * std::numeric_limits<double>::epsilon() * std::fabs(b) + 0.5 * tol;
+    const double xm = 0.5 * (c - b);
+    if (std::fabs(xm) <= tol1 || fb == 0.0) {
+      state = 2;
+      return;
+    }
+    if (++iters > 500) {
+      state = 3;
+      status = PASTA_E_INTERNAL;
+      return;
+    }
+    if (std::fabs(e) >= tol1 && std::fabs(fa) > std::fabs(fb)) {
+      const double s = fb / fa;
+      double p, q;
+      if (a == c) {
+        p = 2.0 * xm * s;
+        q = 1.0 - s;
+      } else {
+        const double qq = fa / fc, r = fb / fc;
+        p = s * (2.0 * xm * qq * (qq - r) - (b - a) * (r - 1.0));
+        q = (qq - 1.0) * (r - 1.0) * (s - 1.0);
+      }
+      if (p > 0.0) q = -q;
+      p = std::fabs(p);
+      const double min1 = 3.0 * xm * q - std::fabs(tol1 * q), min2 = std::fabs(e * q);
+      if (2.0 * p < std::min(min1, min2)) {
+        e = d;
+        d = p / q;
+      } else {
+        d = xm;
+        e = d;
+      }
+    } else {
+      d = xm;
+      e = d;
+    }
+    a = b;
+    fa = fb;
+    b += std::fabs(d) > tol1 ? d : std::copysign(tol1, xm);
+    state = 1;
+  }
+};
+
+}  // namespace
+
+// SingleFitter::compute_uncertainty (fitting.rs:480-568) for S spectra on
+// one dispersion and continuum fitter (compute_uncertainty_bulk,
+// lib.rs:1570-1600): per label i and side, the distance from `labels` to
+// where chi2 crosses chi2_best * (1 + sqrt(2 / n)), n = 4 R (l_last -
+// l_first) / (l_first + l_last), searched in units of the search radius
+// within the SingleBounds(grid, (0, 1e4), (-1e3, 1e3)) clamp.  All open
+// searches of all spectra evaluate together in one batched chi2 per round.
+int pasta_compute_uncertainty(const pasta_grid *gc, const pasta_dispersion *d, const pasta_continuum *c, int64_t S,
+                              const float *flux, const float *var, int64_t n, double spec_res, const double *labels,
+                              const double *search_radius, double *out, int32_t *bound_status,
+                              int32_t *star_status) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(gc);
+    if (!d || !c || !flux || !var || !labels || !out || !bound_status || !star_status)
+      fail(PASTA_E_ARG, "dispersion, continuum, data, labels and outputs are required");
+    if (S < 0) fail(PASTA_E_ARG, "negative spectrum count");
+    if (S == 0) return;
+    check_disp_grid(g, d);
+    if (n != (int64_t)d->wl.size()) fail(PASTA_E_ARG, "Observed spectrum and target dispersion must have the same length");
+    if (c->kind != PASTA_CONT_CONSTANT && c->n != n)
+      fail(PASTA_E_ARG, "Length of observed and continuum spectrum are different %lld, %lld", (long long)n,
+           (long long)c->n);
+    double sr0[5] = {2000.0, 0.3, 0.3, 40.0, 40.0};
+    if (search_radius) std::copy(search_radius, search_radius + 5, sr0);
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    std::lock_guard<std::mutex> lk(g->mu);
+    // one device star per spectrum
+    std::vector<StarInput> in(S);
+    for (int64_t i = 0; i < S; i++) in[i] = StarInput{d, c, nullptr, flux + (size_t)i * n, var + (size_t)i * n, n, 0};
+    StarSet ss;
+    ss.build(in);
+    EvalArgs a;
+    a.stars = ss.dstars.p;
+    a.need_chi2 = 1;
+    star_kinds(ss.h, a);
+    // the evaluation buffers hold the largest round: two points per search
+    const int64_t Emax = S * 20;
+    DBuf<double> dl, dc;
+    DBuf<int> de, dst;
+    dl.alloc((size_t)Emax * 5);
+    dc.alloc(Emax);
+    de.alloc(Emax);
+    dst.alloc(Emax);
+    ensure_workspace(g, std::min<int64_t>(Emax, 1 << 16), a.max_nobs);
+    std::vector<double> hl;
+    std::vector<int> hs;
+    std::vector<double> hc;
+    std::vector<int> hst;
+    // chi2 of the labels in hl (5 per point) for the stars in hs
+    auto evaluate = [&]() {
+      const int64_t E = (int64_t)hs.size();
+      hc.assign(E, 0.0);
+      hst.assign(E, 0);
+      if (E == 0) return;
+      double vmax = 0.0;
+      for (int64_t k = 0; k < E; k++) vmax = std::max(vmax, hl[(size_t)k * 5 + 3]);
+      CK(cudaMemcpyAsync(dl.p, hl.data(), (size_t)E * 5 * sizeof(double), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(de.p, hs.data(), (size_t)E * sizeof(int), cudaMemcpyHostToDevice, s));
+      a.labels = dl.p;
+      a.eval_star = de.p;
+      a.E = E;
+      a.cost = dc.p;
+      a.status = dst.p;
+      a.max_m = width_upper_bound(g, vmax);
+      run_evals(g, a, s);
+      CK(cudaMemcpyAsync(hc.data(), dc.p, (size_t)E * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hst.data(), dst.p, (size_t)E * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    };
+    // best chi2 at the given labels (an error there fails the whole spectrum)
+    hl.assign(labels, labels + (size_t)S * 5);
+    hs.resize(S);
+    for (int64_t i = 0; i < S; i++) hs[i] = (int)i;
+    evaluate();
+    const double l0 = d->wl.front(), l1 = d->wl.back();
+    const double neff = 4.0 * spec_res * (l1 - l0) / (l0 + l1);
+    std::vector<double> target(S), radius((size_t)S * 5);
+    for (int64_t i = 0; i < S; i++) {
+      star_status[i] = hst[i];
+      target[i] = hc[i] * (1.0 + std::sqrt(2.0 / neff));
+      const double *L = labels + (size_t)i * 5;
+      double *r = &radius[(size_t)i * 5];
+      for (int k = 0; k < 5; k++) r[k] = sr0[k];
+      r[0] *= L[0];
+      r[3] = std::max(L[3] * r[3], 100.0);
+    }
+    // bounds of every search; outer limits SingleBounds(grid, (0, 1e4), (-1e3, 1e3))
+    PsoParams lim{};
+    lim.vs_lo = 0.0; lim.vs_hi = 1e4;
+    lim.rv_lo = -1e3; lim.rv_hi = 1e3;
+    const int64_t NS = S * 10;  // search q = (spectrum, label, side): q = (i * 5 + k) * 2 + right
+    std::vector<BrentSearch> bs(NS);
+    for (int64_t q = 0; q < NS; q++) {
+      const int64_t i = q / 10;
+      const int k = (int)(q / 2 % 5), right = (int)(q % 2);
+      BrentSearch &B = bs[q];
+      if (star_status[i]) {
+        B.state = 3;
+        B.status = star_status[i];
+        continue;
+      }
+      double bl[5];
+      std::copy(labels + (size_t)i * 5, labels + (size_t)i * 5 + 5, bl);
+      const double r = radius[(size_t)i * 5 + k];
+      bl[k] += right ? r : -r;
+      double bound;
+      const int st = pso_clamp_1d(g->hg, lim, bl, k, bound);
+      if (st) {
+        B.state = 3;
+        B.status = st;
+        continue;
+      }
+      const double resc = (bound - labels[(size_t)i * 5 + k]) / r;
+      if (right) { B.a = 0.0; B.b = std::min(resc, 1.0); }
+      else { B.a = resc; B.b = 0.0; }
+    }
+    // rounds: every open search contributes its pending points
+    std::vector<int64_t> owner;
+    std::vector<int> which;
+    for (int round = 0; round < 1000; round++) {
+      hl.clear(); hs.clear(); owner.clear(); which.clear();
+      auto push = [&](int64_t q, double param, int w) {
+        const int64_t i = q / 10;
+        const int k = (int)(q / 2 % 5);
+        for (int t = 0; t < 5; t++) hl.push_back(labels[(size_t)i * 5 + t]);
+        hl[hl.size() - 5 + k] += param * radius[(size_t)i * 5 + k];
+        hs.push_back((int)i);
+        owner.push_back(q);
+        which.push_back(w);
+      };
+      for (int64_t q = 0; q < NS; q++) {
+        if (bs[q].state == 0) { push(q, bs[q].a, 0); push(q, bs[q].b, 1); }
+        else if (bs[q].state == 1) push(q, bs[q].b, 1);
+      }
+      if (hs.empty()) break;
+      evaluate();
+      for (size_t t = 0; t < owner.size(); t++) {
+        BrentSearch &B = bs[owner[t]];
+        if (B.state == 3) continue;
+        if (hst[t]) {
+          B.state = 3;
+          B.status = hst[t];
+          continue;
+        }
+        const double f = hc[t] - target[owner[t] / 10];
+        if (which[t] == 0) B.fa = f;
+        else B.fb = f;
+      }
+      for (int64_t q = 0; q < NS; q++) {
+        BrentSearch &B = bs[q];
+        if (B.state == 0) {
+          if (B.fa * B.fb > 0.0) {  // argmin: f(min) and f(max) must have different signs
+            B.state = 3;
+            B.status = PASTA_E_ARG;
+            continue;
+          }
+          B.c = B.b;
+          B.fc = B.fb;
+          B.d = B.b - B.a;
+          B.e = B.d;
+          B.advance();
+        } else if (B.state == 1) {
+          B.advance();
+        }
+      }
+    }
+    for (int64_t q = 0; q < NS; q++) {
+      const int64_t i = q / 10;
+      const int k = (int)(q / 2 % 5), right = (int)(q % 2);
+      const BrentSearch &B = bs[q];
+      const bool ok = B.state == 2;
+      const double r = radius[(size_t)i * 5 + k];
+      out[q] = ok ? (right ? B.b * r : -B.b * r) : NAN;
+      bound_status[q] = ok ? 0 : (B.status ? B.status : PASTA_E_INTERNAL);
+    }
+  });
 }
 
 // ----------------------------------------------------- batch sessions

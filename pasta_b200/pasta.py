@@ -38,7 +38,7 @@ __all__ = [
     "LinearModelContinuumFitter", "FixedContinuum", "ConstantContinuum", "FixConstraint",
     "RangeConstraint", "get_vsini_kernel", "InMemInterpolator", "OnDiskInterpolator",
     "CachedInterpolator", "PyWavelengthDispersion", "PyContinuumFitter", "SingleFitter",
-    "Server", "PastaError",
+    "Server", "PastaError", "LabelUncertainties",
 ]
 
 PastaError = _ffi.PastaError
@@ -107,6 +107,25 @@ class Label:
 
     def __repr__(self):
         return "Label(teff=%g, m=%g, logg=%g, vsini=%g, rv=%g)" % tuple(self.as_list())
+
+
+class LabelUncertainties:
+    """lib.rs:168-210: per label the (below, above) distances of the chi2
+    landscape crossing; None where the search failed."""
+
+    __slots__ = ("teff", "m", "logg", "vsini", "rv")
+
+    def __init__(self, teff, m, logg, vsini, rv):
+        self.teff, self.m, self.logg, self.vsini, self.rv = teff, m, logg, vsini, rv
+
+    def to_dict(self):
+        return dict(teff=self.teff, m=self.m, logg=self.logg, vsini=self.vsini, rv=self.rv)
+
+    def to_json(self):
+        return json.dumps({k: list(v) for k, v in self.to_dict().items()}, separators=(",", ":"))
+
+    def __repr__(self):
+        return "LabelUncertainties(%s)" % ", ".join("%s=%r" % kv for kv in self.to_dict().items())
 
 
 class OptimizationResult:
@@ -760,6 +779,39 @@ class SingleFitter:
         if allow_nan is False:
             _Interpolator._raise_status(st, "chi2")
         return [float(x) for x in out]
+
+
+    def compute_uncertainty(self, interpolator, observed_flux, observed_var, spec_res: float, label,
+                            search_radius=None) -> LabelUncertainties:
+        """Chi2-landscape uncertainties at a best-fit label (lib.rs:1545-1566,
+        fitting.rs:480-568); raises when chi2 at the label itself fails."""
+        return self.compute_uncertainty_bulk(interpolator, [observed_flux], [observed_var], spec_res, [label],
+                                             search_radius)[0]
+
+    def compute_uncertainty_bulk(self, interpolator, observed_fluxes, observed_vars, spec_res: float, labels,
+                                 search_radius=None) -> list:
+        """compute_uncertainty for many spectra of this fitter's wavelength
+        grid (lib.rs:1570-1600); every search of every spectrum shares one
+        batched chi2 evaluation per Brent step."""
+        fl = np.ascontiguousarray(np.stack([f32(x) for x in observed_fluxes]), dtype=np.float32)
+        vr = np.ascontiguousarray(np.stack([f32(x) for x in observed_vars]), dtype=np.float32)
+        if fl.shape != vr.shape:
+            raise ValueError("Flux and variance vectors must have the same length")
+        S, n = fl.shape
+        lab = f64(np.asarray(labels, dtype=np.float64).reshape(S, 5))
+        sr = None if search_radius is None else f64(np.asarray(search_radius, dtype=np.float64).reshape(5))
+        out = np.empty((S, 5, 2))
+        bst = np.zeros((S, 5, 2), np.int32)
+        sst = np.zeros(S, np.int32)
+        check(lib().pasta_compute_uncertainty(interpolator._grid._h, self.dispersion._h, self.continuum_fitter._h,
+                                              S, ptr(fl), ptr(vr), n, float(spec_res), ptr(lab),
+                                              ptr(sr) if sr is not None else None, ptr(out), ptr(bst), ptr(sst)))
+        _Interpolator._raise_status(sst, "compute_uncertainty")
+        res = []
+        for i in range(S):
+            pairs = [tuple(None if bst[i, k, j] else float(out[i, k, j]) for j in range(2)) for k in range(5)]
+            res.append(LabelUncertainties(*pairs))
+        return res
 
 
 def _write_trace(tr, trace_directory, best_particle_file):

@@ -232,3 +232,34 @@ def test_dispersion_convolve_matches_oracle(env):
     d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
     od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
     assert relmax(d.convolve(x), od.convolve(x, O.F32)) <= FLUX_TOL
+
+
+def test_compute_uncertainty_matches_oracle(env):
+    """Chi2-landscape bounds (fitting.rs:480-568): batched GPU Brent vs the oracle's sequential one."""
+    O, P, star = env["O"], env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(8, 2), (0.0, 300.0), (-150.0, 150.0))
+    sr = np.array([0.05, 0.3, 0.3, 0.5, 40.0])
+    u = fitter.compute_uncertainty(env["interp"], star.flux, star.var, 85000.0, star.label, sr)
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    oc = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    ref = O.compute_uncertainty(env["og"], od, oc, star.flux, star.var, 85000.0, star.label, sr)
+    radius = sr * np.array([star.label[0], 1, 1, 1, 1])
+    radius[3] = max(star.label[3] * sr[3], 100.0)
+    got = [u.teff, u.m, u.logg, u.vsini, u.rv]
+    for i in range(5):
+        for a, b in zip(got[i], ref[i]):
+            assert (a is None) == (b is None), (i, got[i], ref[i])
+            if a is not None:
+                assert abs(a - b) <= 5e-3 * radius[i], (i, a, b)
+    # the bulk form runs every search of every spectrum together; each result
+    # is the one computed alone
+    other = env["S"].make_star(env["spec"], [6900.0, -0.1, 4.1, 30.0, -10.0], 15000, 100.0, 85000.0, seed=12)
+    assert len(other.flux) == len(star.flux)
+    bulk = fitter.compute_uncertainty_bulk(env["interp"], [star.flux, other.flux], [star.var, other.var], 85000.0,
+                                           [star.label, other.label], sr)
+    assert bulk[0].to_dict() == u.to_dict()
+    alone = fitter.compute_uncertainty(env["interp"], other.flux, other.var, 85000.0, other.label, sr)
+    assert bulk[1].to_dict() == alone.to_dict()
+    assert set(u.to_dict()) == {"teff", "m", "logg", "vsini", "rv"}

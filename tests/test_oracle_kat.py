@@ -167,3 +167,44 @@ def test_seeded_fit_is_deterministic(small):
     assert rc1 == 0 and rc2 == 0
     np.testing.assert_array_equal(r1[0]["label"], r2[0]["label"])
     assert r1[0]["chi2"] == r2[0]["chi2"]
+
+
+def test_brent_root_known_answer():
+    # x^2 - 0.25 on [0, 1] has its root at 0.5; on [-1, 0] at -0.5
+    r = O._brent(lambda x: x * x - 0.25, 0.0, 1.0, tol=1e-10)
+    assert abs(r - 0.5) < 1e-9
+    r = O._brent(lambda x: x * x - 0.25, -1.0, 0.0, tol=1e-10)
+    assert abs(r + 0.5) < 1e-9
+    with pytest.raises(ValueError):
+        O._brent(lambda x: x * x + 1.0, 0.0, 1.0)
+
+
+def test_uncertainty_crossings_bracket_the_target(small):
+    spec, labels, spectra, g = small
+    star = S.make_star(spec, [7130.0, 0.07, 4.02, 50.0, 20.0], 3000, 100.0, 85000.0, seed=2)
+    d = O.Disp(g, O.DISP_FIXED, star.wl, 85000.0)
+    c = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    sr = np.array([0.05, 0.3, 0.3, 0.5, 40.0])
+    res = O.compute_uncertainty(g, d, c, star.flux, star.var, 85000.0, star.label, sr)
+    best, _ = O.chi2(g, d, c, star.flux, star.var, star.label, O.F64)
+    n = 4.0 * 85000.0 * (star.wl[-1] - star.wl[0]) / (star.wl[0] + star.wl[-1])
+    target = best[0] * (1.0 + np.sqrt(2.0 / n))
+    radius = sr * np.array([star.label[0], 1, 1, 1, 1])
+    radius[3] = max(star.label[3] * sr[3], 100.0)
+    found = 0
+    for i in range(5):
+        for side, dist in zip((-1, 1), res[i]):
+            if dist is None:
+                continue
+            # Brent stops with the crossing inside +-tol (1e-3 of the radius)
+            # of its estimate; chi2 may jump there (vsini changes the kernel width)
+            f = []
+            for off in (-2e-3, 2e-3):
+                lab = star.label.copy()
+                lab[i] += side * (dist + off * radius[i])
+                x, st = O.chi2(g, d, c, star.flux, star.var, lab, O.F64)
+                assert st[0] == 0
+                f.append(x[0] - target)
+            assert f[0] * f[1] <= 0.0, (i, side, dist, f)
+            found += 1
+    assert found >= 8
