@@ -186,7 +186,7 @@ int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d,
  * is complete when that stream reaches it.  The evaluation workspace is a
  * 32 MiB static device array inside the library, held by every GPU that
  * loads it until exit and shared by all calls: L is limited to what fits
- * (about 200 labels for a 20,000-pixel grid, 51 for 80,000 pixels) and larger
+ * (about 180 labels for a 20,000-pixel grid, 50 for 80,000 pixels) and larger
  * L is rejected with PASTA_E_ARG; calls whose work overlaps on the GPU race
  * on the array.  The first call on a device sets up the array's address and
  * should come before any stream capture.  Nothing is allocated: no

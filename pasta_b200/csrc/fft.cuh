@@ -59,7 +59,8 @@ __device__ __forceinline__ void dft8(cf v[8]) {
 // the stage happen before a barrier, all writes after it, so the transform
 // runs in place.  The caller must __syncthreads() after filling the input.
 // ld(i, a) returns input element i (a = its swizzled shared-memory slot),
-// st(i, a, v) stores output element i; SmemLoad / SmemStore use the
+// st(i, a, v, s) stores output element i, the thread's s-th output of the
+// stage (a compile-time constant after unrolling); SmemLoad / SmemStore use the
 // swizzled re/im arrays, other functors may read a staging buffer or write
 // outputs elsewhere.
 //
@@ -118,7 +119,7 @@ __device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD
       else if constexpr (NS == 8) a = (d ^ (j & 24)) ^ (9 * r);
       else if constexpr (NS == 64) a = (d ^ ((j >> 3) & 7)) ^ (64 * r ^ 8 * (r & 3));
       else a = p0 + q * FFT_T + r * NS;
-      st(d + r * NS, a, v[q][r]);
+      st(d + r * NS, a, v[q][r], q * R + r);
     }
   }
   __syncthreads();
@@ -130,7 +131,7 @@ struct SmemLoad {
 };
 struct SmemStore {
   float *re, *im;
-  __device__ __forceinline__ void operator()(int, int a, cf v) const {
+  __device__ __forceinline__ void operator()(int, int a, cf v, int) const {
     re[a] = v.x;
     im[a] = v.y;
   }

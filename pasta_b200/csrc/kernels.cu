@@ -311,6 +311,22 @@ __device__ __forceinline__ void stage_item(const EvalBatch &b, long long item, f
   if (w.has1) stage_row(stg1, row, w.j1, P.i_lo, P.i_hi);
 }
 
+// last forward stage with the product by the kernel spectrum in its stores:
+// its output s = 4 q + r is bin k = tid + 256 q + 512 r (Hermitian spectrum:
+// bins above 1024 are conjugates of bin 2048 - k)
+struct MulStore {
+  float *re, *im;
+  const float2 *__restrict__ H;  // 1025 bins
+  __device__ __forceinline__ void operator()(int, int a, cf v, int s) const {
+    const int k = (int)threadIdx.x + (s >> 2) * FFT_T + (s & 3) * 512;
+    float2 hh = k <= 1024 ? H[k] : H[FFTN - k];
+    if (k > 1024) hh.y = -hh.y;
+    const cf z = cmul(v, cf{hh.x, hh.y});
+    re[a] = z.x;
+    im[a] = z.y;
+  }
+};
+
 struct StageLoad {
   const float *s0, *s1;
   bool has1;
@@ -321,7 +337,7 @@ struct FoldStore {
   float *o0, *o1;
   int lo, V;
   float sc;
-  __device__ __forceinline__ void operator()(int i, int, cf v) const {
+  __device__ __forceinline__ void operator()(int i, int, cf v, int) const {
     const int u = i - lo;
     if ((unsigned)u < (unsigned)V) {
       o0[u] = v.x * sc;
@@ -330,7 +346,13 @@ struct FoldStore {
   }
 };
 
-__global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+#ifndef PB_BROADEN_MINB
+#define PB_BROADEN_MINB 4
+#endif
+#ifndef PB_BROADEN_FUSED_MUL
+#define PB_BROADEN_FUSED_MUL 0
+#endif
+__global__ void __launch_bounds__(FFT_T, PB_BROADEN_MINB) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) float br_smem[];
   float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
   float *re = stg1 + BR_STG, *im = re + FFT_SM;
@@ -370,9 +392,11 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
       cp_async_commit();
       fft_stage<8, 8, false>(re, im, tw);
       fft_stage<8, 64, false>(re, im, tw);
-      fft_stage<4, 512, false>(re, im, tw);
-      // the kernel spectrum (Hermitian: bins above 1024 are conjugates)
       const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
+#if PB_BROADEN_FUSED_MUL
+      fft_pass<4, 512, false>(tw, SmemLoad{re, im}, MulStore{re, im, H});
+#else
+      fft_stage<4, 512, false>(re, im, tw);
       for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
         float2 h = k <= 1024 ? H[k] : H[FFTN - k];
         if (k > 1024) h.y = -h.y;
@@ -382,6 +406,7 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
         im[a] = z.y;
       }
       __syncthreads();
+#endif
       fft_stage<8, 1, true>(re, im, tw);
       fft_stage<8, 8, true>(re, im, tw);
       fft_stage<8, 64, true>(re, im, tw);
@@ -466,15 +491,21 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cudaStream_t s) {
   if (b.E <= 0 || b.max_pairs <= 0) return;
   const size_t smem = BR_SMEM_FLOATS * sizeof(float);
-  static bool attr[64] = {};
+  static int per_sm[64] = {};  // resident CTAs per SM, per device
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !attr[dev]) {
-    cudaFuncSetAttribute(k_broaden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr[dev] = true;
+  int fit = 4;
+  if (dev >= 0 && dev < 64) {
+    if (!per_sm[dev]) {
+      cudaFuncSetAttribute(k_broaden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_broaden, FFT_T, smem) != cudaSuccess || n < 1) n = 1;
+      per_sm[dev] = n;
+    }
+    fit = per_sm[dev];
   }
   const long long total = (long long)b.E * b.max_pairs;
-  long long grid = (long long)num_sms() * 4;  // persistent: the CTAs that fit at once (64 regs x 256)
+  long long grid = (long long)num_sms() * fit;  // persistent: the CTAs that fit at once
   if (grid > total) grid = total;
   k_broaden<<<(unsigned)grid, FFT_T, smem, s>>>(G, b, tw);
   count_launch();
@@ -657,6 +688,7 @@ void launch_copy_broadened(const DevGrid &G, const EvalBatch &b, float *out, cud
 
 // ------------------------------------------------------------------ chi2
 constexpr int CT = 256, CW = CT / 32;
+constexpr int CU = 4;  // pixels per lane whose loads the chunk kernels issue together
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -777,14 +809,27 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
   double z[K];
 #pragma unroll
   for (int k = 0; k < K; k++) z[k] = 0.0;
-#pragma unroll 4
-  for (int i = lo + lane; i < hi; i += 32) {
-    const double y = (double)(flux[i] / mod[i]);
-    const float xf = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
-    float Pk[K];
-    legendre<K>(xf, Pk);
+  // loads of CU pixels are issued before any arithmetic on them (the f32
+  // division has a slow path the compiler will not schedule loads across)
+  for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
+    float fl[CU], md[CU], xf[CU];
 #pragma unroll
-    for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
+    for (int u = 0; u < CU; u++) {
+      const int i = min(i0 + 32 * u, hi - 1);
+      fl[u] = flux[i];
+      md[u] = mod[i];
+      xf[u] = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
+    }
+#pragma unroll
+    for (int u = 0; u < CU; u++) {
+      if (i0 + 32 * u < hi) {
+        const double y = (double)(fl[u] / md[u]);
+        float Pk[K];
+        legendre<K>(xf[u], Pk);
+#pragma unroll
+        for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
+      }
+    }
   }
 #pragma unroll
   for (int k = 0; k < K; k++) {
@@ -848,31 +893,57 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
     cp[k] = c > 0 ? coef[(c - 1) * MAX_P1 + k] : 0.0f;
   }
   double acc = 0.0;
-  if (c == 0) {
-#pragma unroll 4
-    for (int i = 50 + lane; i < st.cstart[1]; i += 32) {
-      const float p = poly_eval_r<K>(cc, st.xa[i]);
-      const float r = flux[i] - p * mod[i];
-      acc += (double)(r * r / var[i]);
+  // [lo, hi) with chunk c alone; loads of CU pixels before their arithmetic
+  auto alone = [&](int lo, int hi) {
+    for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
+      float fl[CU], md[CU], vr[CU], xa[CU];
+#pragma unroll
+      for (int u = 0; u < CU; u++) {
+        const int i = min(i0 + 32 * u, hi - 1);
+        fl[u] = flux[i];
+        md[u] = mod[i];
+        vr[u] = var[i];
+        xa[u] = st.xa[i];
+      }
+#pragma unroll
+      for (int u = 0; u < CU; u++) {
+        if (i0 + 32 * u < hi) {
+          const float p = poly_eval_r<K>(cc, xa[u]);
+          const float r = fl[u] - p * md[u];
+          acc += (double)(r * r / vr[u]);
+        }
+      }
     }
+  };
+  if (c == 0) {
+    alone(50, st.cstart[1]);
   } else {
     const int s0 = st.cstart[c], sp = st.cstop[c - 1];
     const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
-#pragma unroll 2
-    for (int i = s0 + lane; i < sp; i += 32) {
-      const float pv = poly_eval_r<K>(cp, st.xa[i]);
-      const float cu = poly_eval_r<K>(cc, st.xb[i]);
-      const float f = st.fac[i];
-      const float p = pv * f + cu * (1.0f - f);
-      const float r = flux[i] - p * mod[i];
-      acc += (double)(r * r / var[i]);
+    for (int i0 = s0 + lane; i0 < sp; i0 += 32 * 2) {  // overlap: blend previous and current
+      float fl[2], md[2], vr[2], xa[2], xb[2], fc[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int i = min(i0 + 32 * u, sp - 1);
+        fl[u] = flux[i];
+        md[u] = mod[i];
+        vr[u] = var[i];
+        xa[u] = st.xa[i];
+        xb[u] = st.xb[i];
+        fc[u] = st.fac[i];
+      }
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (i0 + 32 * u < sp) {
+          const float pv = poly_eval_r<K>(cp, xa[u]);
+          const float cu = poly_eval_r<K>(cc, xb[u]);
+          const float p = pv * fc[u] + cu * (1.0f - fc[u]);
+          const float r = fl[u] - p * md[u];
+          acc += (double)(r * r / vr[u]);
+        }
+      }
     }
-#pragma unroll 4
-    for (int i = sp + lane; i < nx; i += 32) {
-      const float p = poly_eval_r<K>(cc, st.xa[i]);
-      const float r = flux[i] - p * mod[i];
-      acc += (double)(r * r / var[i]);
-    }
+    alone(sp, nx);
   }
   acc = warp_sum(acc);
   if (lane == 0) b.cpart[(size_t)e * MAX_CHUNKS + c] = acc;
