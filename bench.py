@@ -54,7 +54,9 @@ PATH_BYTES_PER_WIN_PX, PATH_BYTES_PER_OBS = 128, 8
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # DRAM bytes per evaluation measured by ncu at full size (dram__bytes_read.sum +
 # dram__bytes_write.sum, one launch of 65,536 evaluations; profiles/dram_batched_fit_1024stars.md)
-DRAM_BYTES_PER_EVAL = {"k_interp": None, "k_broaden": None, "chi2": None}
+# (first evaluation step; k_broaden includes its block-bound search, chi2 the
+# resampling left over and both chunk kernels)
+DRAM_BYTES_PER_EVAL = {"k_interp": 710111, "k_broaden": 636944 + 4757, "chi2": 163697 + 149357 + 128}
 
 
 def log(*a):
@@ -269,6 +271,10 @@ def run_ours(args):
     interp_s = stage["interp_ms"] / 1000.0
     interp_bytes = stage["interp_px"] * INTERP_BYTES_PER_PX
     achieved = interp_bytes / interp_s / 1e9
+    # chunk continuum + chi2: per observed pixel the model, flux and chunk
+    # coordinate (moments) and the model, flux, var and coordinate (residuals)
+    chi2_bytes = stage["obs_px"] * (12 + 16)
+    chi2_gbs = chi2_bytes / (stage["chi2_ms"] / 1000.0) / 1e9
     # the path as a whole on the per-evaluation byte basis B_eval
     path_bytes = stage["interp_px"] * PATH_BYTES_PER_WIN_PX + stage["obs_px"] * PATH_BYTES_PER_OBS
     path_gbs = path_bytes / ev * evals_per_s / 1e9
@@ -302,6 +308,9 @@ def run_ours(args):
              "frac": achieved / peak, "traffic": traffic("k_interp"), "peak_kind": peak_kind,
              "algorithmic_bytes_per_launch": interp_bytes,
              "note": "neighbour rows shared by a star's particles hit in L2, so the algorithmic rate exceeds HBM"},
+            {"bound": "hbm", "kernel": "k_chunk_moments+k_chunk_resid", "achieved": chi2_gbs, "peak": peak,
+             "unit": "GB/s", "frac": chi2_gbs / peak, "traffic": traffic("chi2"), "peak_kind": peak_kind,
+             "algorithmic_bytes_per_launch": chi2_bytes},
         ],
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
