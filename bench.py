@@ -152,6 +152,47 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# ------------------------------------------------------------ served latency
+def serve_latency(P, interp, stars, settings, seeds, rate, n_req, seed):
+    """Submit n_req requests at Poisson arrival times (rate per second) to a
+    server stepping continuously; time-to-fit is submission to retirement."""
+    rng = np.random.default_rng(seed)
+    arrive = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    pick = rng.integers(0, len(stars), n_req)
+    chunks = rng.integers(4, 13, n_req)
+    degree = rng.integers(3, 9, n_req)
+    conts = [P.ChunkContinuumFitter(stars[j].wl, int(d), int(c), 0.2) for j, c, d in zip(pick, chunks, degree)]
+    disps = {}
+    for j in set(pick.tolist()):
+        disps[j] = P.FixedResolutionDispersion(stars[j].wl, RESOLUTION, interp.synth_wl)
+    srv = P.Server(interp, max_slots=len(stars))
+    t0 = time.perf_counter()
+    i = 0
+    ttf = []
+    while len(ttf) < n_req:
+        now = time.perf_counter() - t0
+        while i < n_req and arrive[i] <= now:
+            j = int(pick[i])
+            srv.submit(disps[j], conts[i], settings, stars[j].flux, stars[j].var, (0.0, 300.0), (-150.0, 150.0),
+                       seed=seeds[j] + 104729 * (i + 1))
+            i += 1
+        q, active, _ = srv.pending()
+        if q + active > 0:
+            srv.step()
+        elif i < n_req:
+            time.sleep(max(0.0, min(arrive[i] - now, 0.01)))
+        for _, st, res in srv.poll(4096):
+            ttf.append(res.time)
+    wall = time.perf_counter() - t0
+    del srv
+    ttf = np.array(ttf)
+    return {"p50": float(np.percentile(ttf, 50)), "p99": float(np.percentile(ttf, 99)),
+            "mean": float(ttf.mean()), "requests": n_req, "arrival_rate_per_s": rate,
+            "fits_per_s": n_req / wall,
+            "what": "served form: Poisson arrivals, config-1 stars, own continuum settings per request "
+                    "(4-12 chunks, degree 3-8), time from submission to result"}
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args):
     import torch
@@ -190,36 +231,62 @@ def run_ours(args):
     seeds = [int(7 + 100003 * rank + i) for i in range(n_stars)]
     log(f"[rank {rank}] {n_stars} stars in {time.time() - t:.1f}s")
 
-    # -------- device-timed steps (kernel throughput)
-    b = P.BatchFit(interp, disps, conts, settings, [s.flux for s in stars], [s.var for s in stars],
-                   (0.0, 300.0), (-150.0, 150.0), seeds=seeds)
-    info = b.info()
-    if args.warmup + args.steps + 3 > ITERS + 1:
-        raise SystemExit("steps + warmup exceed the fit's PSO steps")
-    b.step(args.warmup)
+    fl = [s.flux for s in stars]
+    vr = [s.var for s in stars]
+
+    # -------- timed region: the served form in steady state.  n_stars slots,
+    # refilled as fits finish, so the slots sit at every PSO iteration of the
+    # fit and a step costs what the average step of a whole fit costs.  The
+    # ramp-up that spreads the slots over the iterations is set-up, untimed.
+    srv = P.Server(interp, max_slots=n_stars)
+    per_step = -(-n_stars // (ITERS + 1))  # fits that finish per step in steady state
+    cursor = [0]
+
+    def feed(k):
+        for _ in range(k):
+            i = cursor[0] % n_stars
+            srv.submit(disps[i], conts[i], settings, fl[i], vr[i], (0.0, 300.0), (-150.0, 150.0),
+                       seed=seeds[i] + 7919 * (cursor[0] // n_stars))
+            cursor[0] += 1
+
+    t = time.time()
+    for _ in range(ITERS + 1):
+        feed(per_step)
+        srv.step()
+        srv.poll(4096)
+    log(f"[rank {rank}] served ramp-up in {time.time() - t:.1f}s, {srv.pending()[1]} slots active")
+    feed(per_step * (args.warmup + 2))
+    srv.run(args.warmup)
+    srv.poll(4096)
+    feed(per_step * (args.steps + 2))
     barrier()
     torch.cuda.synchronize(dev)
+    st0 = srv.stats()
     launches0 = _ffi.lib().pasta_kernel_launch_count()
     with ClockSampler(local) as clk:
-        dev_ms = b.step(args.steps)
+        dev_ms = srv.run(args.steps)
     torch.cuda.synchronize(dev)
     barrier()
-    launches = info["kernels_per_step"] * args.steps + (_ffi.lib().pasta_kernel_launch_count() - launches0)
+    launches = _ffi.lib().pasta_kernel_launch_count() - launches0
+    st1 = srv.stats()
+    fits_done = len(srv.poll(1 << 16))
+    del srv
     t_max = max_over_ranks(dev_ms / 1000.0, dev)
-    evals_step = info["evals_per_step"]
-    evals_total = sum_over_ranks(evals_step * args.steps, dev)
+    evals_step = (st1["evals"] - st0["evals"]) / args.steps
+    evals_total = sum_over_ranks(st1["evals"] - st0["evals"], dev)
     evals_per_s = evals_total / t_max
     fits_per_s = evals_per_s / EVALS_PER_FIT
 
-    # -------- per-stage breakdown (CUDA events between the stages, live)
+    # -------- per-stage breakdown (CUDA events between the stages, live) on a
+    # batch advanced to the middle of its fit
+    b = P.BatchFit(interp, disps, conts, settings, fl, vr, (0.0, 300.0), (-150.0, 150.0), seeds=seeds)
+    b.step(ITERS // 2)
     prof = [b.profile_step() for _ in range(3)]
     stage = {k: float(np.mean([p[k] for p in prof])) for k in prof[0]}
     b.finish()
     del b
 
     # -------- end to end: one complete fit of the batch through the public API
-    fl = [s.flux for s in stars]
-    vr = [s.var for s in stars]
     barrier()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -241,6 +308,12 @@ def run_ours(args):
     t_plain = time.perf_counter() - t0
     same = all(a.label.as_list() == r.label.as_list() and a.chi2 == r.chi2 for a, r in zip(plain, res[:n_plain]))
     plain_fits = n_plain / t_plain
+
+    # -------- served time-to-fit: Poisson arrivals, each request its own
+    # continuum settings (4-12 chunks, degree 3-8), stars of the workload
+    lat = serve_latency(P, interp, stars, settings, seeds, rate=args.serve_rate, n_req=args.serve_requests,
+                        seed=4242 + rank) if args.serve_requests > 0 else None
+    torch.cuda.synchronize(dev)
 
     # -------- CPU baseline (oracle, rank 0 at N=1)
     cpu = None
@@ -283,17 +356,22 @@ def run_ours(args):
         "metric": METRIC, "value": fits_per_s, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (u16 grid, f64 continuum solves)", "data": "synthetic (seeded)",
-        "config": {"workload": "batched fits: %d stars/GPU, grid 60x21x11 x %d px uint16 (%.1f GB), "
-                               "N_obs 10k-60k, vsini 0-300, RV +-150, R=85000, 8 chunks deg 5, PSO %dx%d"
+        "config": {"workload": "config-1 fits in steady state: %d slots/GPU refilled as fits finish (slots spread "
+                               "over all PSO iterations); grid 60x21x11 x %d px uint16 (%.1f GB), N_obs 10k-60k, "
+                               "vsini 0-300, RV +-150, R=85000, 8 chunks deg 5, PSO %dx%d"
                                % (n_stars, spec.n_px, spectra.nbytes / 1e9, PARTICLES, ITERS),
                    "stars_per_gpu": n_stars, "particles": PARTICLES, "iterations": ITERS,
-                   "evals_per_step": evals_step, "parallelism": "replicas x%d (stars sharded, no collective)" % world,
-                   "l2": "inputs larger than L2 (%.1f GB grid, ~%.0f GB read per step)"
+                   "evals_per_step": evals_step, "fits_finished_in_timed_steps": fits_done,
+                   "step": "one served step: PSO update, chi2 of every active particle, best update, "
+                           "admissions and retirements (final refit)",
+                   "parallelism": "replicas x%d (stars sharded, no collective)" % world,
+                   "l2": "inputs larger than L2 (%.1f GB grid, ~%.0f GB of interpolation reads per step)"
                          % (spectra.nbytes / 1e9, interp_bytes / 1e9)},
         "evals_per_s": evals_per_s,
         "e2e": {"value": e2e_fits, "unit": "fits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "seconds": t_e2e, "what": "fit_many of the whole batch (201 PSO steps + final refit), host arrays"},
-        "latency_s": {"p50": t_e2e, "p99": t_e2e, "note": "batched form: every star completes with the batch"},
+                "seconds": t_e2e, "what": "batched form: fit_many of %d stars from host arrays to results "
+                                          "(201 PSO steps + final refit); bytes are per call" % n_stars},
+        "latency_s": lat,
         "plain_gpu": {"fits_per_s": plain_fits, "stars": n_plain, "identical_results": same,
                       "batched_e2e_over_plain": e2e_fits / (plain_fits * world)},
         "label_error_vs_truth": {"median_abs": np.median(err, axis=0).tolist(),
@@ -424,6 +502,8 @@ def main():
     ap.add_argument("--plain-stars", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=30.0, help="served latency run: arrivals per second")
+    ap.add_argument("--serve-requests", type=int, default=300, help="served latency run: requests (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -292,6 +292,12 @@ int pasta_server_poll(pasta_server *s, int64_t *ids, pasta_fit_result *results,
 int pasta_server_pending(const pasta_server *s, int64_t *queued,
                          int64_t *active, int64_t *done);
 int pasta_server_destroy(pasta_server *s);
+/* `steps` server steps back to back (admitting queued requests as slots
+ * free up), timed between CUDA events on the library's stream (host work
+ * between the launches is inside the interval). */
+int pasta_server_run(pasta_server *s, int steps, double *device_ms);
+/* out3: chi2 evaluations run, steps run, particles per slot. */
+int pasta_server_stats(const pasta_server *s, int64_t *out3);
 
 #ifdef __cplusplus
 }

@@ -76,6 +76,8 @@ SIGNATURES = {
     "pasta_server_poll": (I, [P, P, P, P, I64, I, P]),
     "pasta_server_pending": (I, [P, P, P, P]),
     "pasta_server_destroy": (I, [P]),
+    "pasta_server_run": (I, [P, I, P]),
+    "pasta_server_stats": (I, [P, P]),
 }
 
 _lib = None

@@ -167,12 +167,14 @@ struct Workspace {
   DBuf<float2> H, HG;
   DBuf<EvalPrep> prep;
   DBuf<int> bnd;       // first observed pixel per broadening block
+  DBuf<GroupRec> grec; // interpolation groups, SEG slots per segment
+  DBuf<int> gcount;    // groups per segment
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   void ensure(int64_t want, int64_t str, int bstr) {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
-    bnd.release(); ccoef.release(); cpart.release();
+    bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
     cap = 0;
     A.alloc((size_t)want * str);
     B.alloc((size_t)want * str);
@@ -180,6 +182,8 @@ struct Workspace {
     HG.alloc((size_t)want * 1025);
     prep.alloc((size_t)want);
     bnd.alloc((size_t)want * bstr);
+    grec.alloc((size_t)(want + SEG - 1) / SEG * SEG);
+    gcount.alloc((size_t)(want + SEG - 1) / SEG);
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
     cap = want;
@@ -191,7 +195,7 @@ struct Workspace {
 
 // bytes of workspace one evaluation takes with rows of `stride` floats
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
-  return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)bnd_stride * 4 +
+  return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)bnd_stride * 4 +
          (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8);
 }
 
@@ -698,6 +702,8 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   // chi2 batches resample inside the broadening kernel unless a synth row is wanted
   b.obs_epi = a.need_chi2 && !a.out_obs && !a.out_synth && !a.full_window ? 1 : 0;
   b.bnd = g->ws.bnd.p;
+  b.grec = g->ws.grec.p;
+  b.gcount = g->ws.gcount.p;
   b.bnd_stride = g->ws.bnd_stride;
   b.ccoef = g->ws.ccoef.p;
   b.cpart = g->ws.cpart.p;
@@ -1061,6 +1067,7 @@ void batch_profile_step(Batch &B, double *out) {
   CK(cudaEventRecord(B.ev[2], s));
   if (a.max_m > 1) launch_rotker(g->d, b, C.tw.p, s);
   CK(cudaEventRecord(B.ev[3], s));
+  launch_group(g->d, b, s);
   launch_interp(g->d, b, s);
   CK(cudaEventRecord(B.ev[4], s));
   launch_obs_bounds(g->d, b, s);
@@ -1285,6 +1292,8 @@ struct pasta_server {
   };
   std::deque<Done> done;
   int64_t next_id = 1;
+  int64_t evals_total = 0, steps_total = 0;  // evaluations and steps run so far
+  int64_t graph_kernels = 0;                  // kernels in the captured step
   int max_m = 1, graph_max_m = 0;
   int64_t graph_gen = -1;
   uint32_t graph_mask = 0;  // continuum kinds / instrument width the captured step covers
@@ -2347,14 +2356,21 @@ int pasta_server_step(pasta_server *sv) {
       sv->graph_other = a.other_cont;
       sv->graph_hg = a.max_hg;
       sv->graph_chunks = a.max_chunks;
+      const int64_t k0 = kernel_launches();
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       launch_pso_update(g->d, sw, s);
       run_evals(g, a, s);
       launch_pso_best(sw, sv->W.ecost.p, sv->W.estatus.p, s);
       CK(cudaStreamEndCapture(s, &sv->graph));
+      sv->graph_kernels = kernel_launches() - k0;
+      count_launch(-(int)sv->graph_kernels);  // counted again at every replay
       CK(cudaGraphInstantiate(&sv->exec, sv->graph, 0));
     }
     CK(cudaGraphLaunch(sv->exec, s));
+    count_launch((int)sv->graph_kernels);
+    for (int i = 0; i < sv->slots; i++)
+      if (sv->slot_req[i]) sv->evals_total += sv->slot_req[i]->st.num_particles;
+    sv->steps_total++;
     std::vector<int> done(sv->slots), status(sv->slots);
     CK(cudaMemcpyAsync(done.data(), sv->W.done.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(status.data(), sv->W.status.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -2411,6 +2427,45 @@ int pasta_server_step(pasta_server *sv) {
     for (int i = 0; i < sv->slots; i++) active_after += sv->slot_req[i] ? 1 : 0;
   });
   return rc ? rc : active_after;
+}
+
+// `steps` server steps back to back, with the time between CUDA events on
+// the library's stream around them (host work between the launches, such as
+// admissions and retirements, is inside the interval).
+int pasta_server_run(pasta_server *sv, int steps, double *device_ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = guard([&] {
+    if (steps < 0) fail(PASTA_E_ARG, "steps must be >= 0");
+    cudaStream_t s = ctx().stream;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+  });
+  if (rc) return rc;
+  for (int k = 0; k < steps && !rc; k++) {
+    const int r = pasta_server_step(sv);
+    if (r < 0) rc = r;
+  }
+  const int rc2 = guard([&] {
+    cudaStream_t s = ctx().stream;
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (device_ms) *device_ms = ms;
+  });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc ? rc : rc2;
+}
+
+int pasta_server_stats(const pasta_server *sv, int64_t *out3) {
+  return guard([&] {
+    if (!out3) fail(PASTA_E_ARG, "output required");
+    out3[0] = sv->evals_total;
+    out3[1] = sv->steps_total;
+    out3[2] = sv->Pmax;
+  });
 }
 
 int pasta_server_poll(pasta_server *sv, int64_t *ids, pasta_fit_result *results, float *params, int64_t pstride,

@@ -36,107 +36,221 @@ static int num_sms() {
 
 // ---------------------------------------------------------------- interp
 // flux[px] = sum_n w_n * u16_n[px] * factor_n over the 64 neighbours
-// (interpolate.rs:954-981), 8 pixels per thread from one 128-bit load per
-// neighbour.  Grid: x = evaluation, y = 2048-pixel tile, so CTAs that run
-// together read the same 57 MB tile slab of the resident grid, which stays
-// in L2 across evaluations.  The weight and the dequantisation factor are
-// folded into one f32 (w * factor); the u16 -> f32 conversion is exact
-// (PRMT under the exponent of 2^23, one packed add), and the accumulation is
-// one packed f32x2 FMA per two pixels.  Neighbours with weight 0 (absent or
-// exactly at a node) contribute exactly 0 and are skipped.
-constexpr int IT_T = 256, IT_TILE = IT_T * 8;
+// (interpolate.rs:954-981).  Particles of one star soon sit in the same grid
+// cube and then read the same 64 rows, so evaluations are grouped first:
+// k_group finds, among SEG consecutive evaluations, those with identical
+// neighbour columns and records each group's rows once.  k_interp then
+// converts every row tile once per group and applies each member's weights
+// to it: the reads and the u16 -> f32 conversions are shared, each member
+// keeps its own accumulators, and each member's sum runs over its rows in
+// reference order (rows another member needs add exactly 0), so the result
+// is the same as interpolating every evaluation alone.
 
-__global__ void __launch_bounds__(IT_T) k_interp(DevGrid G, EvalBatch b) {
-  const int e = blockIdx.x;
-  const EvalPrep &P = b.prep[e];
-  if (P.status) return;
-  const int t0 = blockIdx.y * IT_TILE;
-  const int ilo = P.i_lo, ihi = P.i_hi;
-  if (t0 >= ihi || t0 + IT_TILE <= ilo) return;
-  // the neighbours with a non-zero weight, compacted and padded to a
-  // multiple of 8 with zero-weight entries (which add exactly 0), so the
-  // main loop issues its loads in branch-free groups of 8
-  __shared__ const uint16_t *rows[64];
-  __shared__ float ws[64], fs[64], wf[64];
-  __shared__ int nnz;
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    int base = 0;
-    for (int h = 0; h < 2; h++) {
-      const int n = h * 32 + lane;
-      const int c = P.cols[n];
-      const float f = c >= 0 ? G.factor[c] : 0.0f;
-      const float w = c >= 0 ? P.w[n] : 0.0f;
-      const bool keep = w * f != 0.0f;
-      const unsigned bal = __ballot_sync(0xffffffffu, keep);
-      if (keep) {
-        const int pos = base + __popc(bal & ((1u << lane) - 1u));
-        ws[pos] = w;
-        fs[pos] = f;
-        wf[pos] = w * f;
-        rows[pos] = G.spectra + (size_t)c * G.stride;
+__device__ __forceinline__ unsigned long long cols_hash(const int *c) {
+  unsigned long long h = 1469598103934665603ull;  // FNV-1a over the 64 indices
+  for (int n = 0; n < 64; n++) h = (h ^ (unsigned)c[n]) * 1099511628211ull;
+  return h;
+}
+
+// One CTA of SEG threads per segment of SEG consecutive evaluations.
+__global__ void __launch_bounds__(SEG) k_group(DevGrid G, EvalBatch b) {
+  __shared__ unsigned long long hs[SEG];
+  __shared__ int ok[SEG], lead[SEG], gid[SEG], slot[SEG], open_g[SEG], fill[SEG];
+  __shared__ int ng, cnt[2];
+  const int s = blockIdx.x, t = threadIdx.x, e = s * SEG + t;
+  const bool v = e < b.E && b.prep[e].status == 0;
+  ok[t] = v;
+  hs[t] = v ? cols_hash(b.prep[e].cols) : 0ull;
+  __syncthreads();
+  // leader: the first earlier evaluation with the same columns
+  int L = v ? t : -1;
+  if (v) {
+    const int *c = b.prep[e].cols;
+    for (int u = 0; u < t; u++) {
+      if (!ok[u] || hs[u] != hs[t]) continue;
+      const int *cu = b.prep[s * SEG + u].cols;
+      bool same = true;
+      for (int n = 0; n < 64 && same; n++) same = cu[n] == c[n];
+      if (same) {
+        L = u;
+        break;
       }
-      base += __popc(bal);
     }
-    const int padded = (base + 7) & ~7;
-    for (int pos = base + lane; pos < padded; pos += 32) {
-      ws[pos] = 0.0f;
-      fs[pos] = 0.0f;
-      wf[pos] = 0.0f;
-      rows[pos] = G.spectra;
+  }
+  lead[t] = L;
+  open_g[t] = -1;
+  fill[t] = 0;
+  __syncthreads();
+  if (t == 0) {  // groups in evaluation order, at most GROUP_MAX members each
+    int n = 0;
+    for (int u = 0; u < SEG; u++) {
+      gid[u] = -1;
+      if (!ok[u]) continue;
+      const int l = lead[u];
+      if (open_g[l] < 0 || fill[l] == GROUP_MAX) {
+        open_g[l] = n++;
+        fill[l] = 0;
+      }
+      gid[u] = open_g[l];
+      slot[u] = fill[l]++;
     }
-    if (lane == 0) nnz = padded;
+    ng = n;
+    b.gcount[s] = n;
   }
   __syncthreads();
-  const int px = t0 + threadIdx.x * 8;
-  if (px < ilo || px >= ihi) return;
-  float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e * b.stride + px);
-  const int nn = nnz;
-  if (px + 8 <= G.tail_start) {
-    float2 acc[4];
+  const int lane = t & 31, warp = t >> 5;
+  for (int g = 0; g < ng; g++) {
+    GroupRec &R = b.grec[(size_t)s * SEG + g];
+    // members in slot order
+    __shared__ int mem[GROUP_MAX];
+    if (t < GROUP_MAX) mem[t] = -1;
+    __syncthreads();
+    if (gid[t] == g) mem[slot[t]] = e;
+    __syncthreads();
+    int nm = 0;
+    for (int m = 0; m < GROUP_MAX; m++) nm += mem[m] >= 0;
+    // row t of the group: kept when any member weighs it
+    const int c = b.prep[mem[0]].cols[t];
+    const float f = c >= 0 ? G.factor[c] : 0.0f;
+    float w[GROUP_MAX], wf[GROUP_MAX];
+    bool keep = false;
 #pragma unroll
-    for (int k = 0; k < 4; k++) acc[k] = make_float2(0.0f, 0.0f);
+    for (int m = 0; m < GROUP_MAX; m++) {
+      w[m] = (mem[m] >= 0 && c >= 0) ? b.prep[mem[m]].w[t] : 0.0f;
+      wf[m] = w[m] * f;
+      keep |= wf[m] != 0.0f;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) cnt[warp] = __popc(bal);
+    __syncthreads();
+    const int pos = __popc(bal & ((1u << lane) - 1u)) + (warp ? cnt[0] : 0);
+    if (keep) {
+      R.wf[pos] = make_float4(wf[0], wf[1], wf[2], wf[3]);
+      R.w[pos] = make_float4(w[0], w[1], w[2], w[3]);
+      R.col[pos] = c;
+      R.f[pos] = f;
+    }
+    const int kept = cnt[0] + cnt[1];
+    const int padded = (kept + 7) & ~7;
+    if (t >= kept && t < padded) {  // zero-weight padding rows (add exactly 0)
+      R.wf[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      R.w[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      R.col[t] = 0;
+      R.f[t] = 0.0f;
+    }
+    if (t < GROUP_MAX) R.member[t] = mem[t];
+    if (t == 0) {
+      R.nmem = nm;
+      R.nn = padded;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
+  if (b.E <= 0) return;
+  k_group<<<(b.E + SEG - 1) / SEG, SEG, 0, s>>>(G, b);
+  count_launch();
+}
+
+constexpr int IT_T = 256, IT_TILE = IT_T * 8;
+
+// the NM members of a group on this thread's 8 pixels (one 128-bit load per row)
+template <int NM>
+__device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch &b, const GroupRec &R, int px) {
+  int e[NM];
+  bool in[NM], any = false;
+#pragma unroll
+  for (int m = 0; m < NM; m++) {
+    e[m] = R.member[m];
+    const EvalPrep &P = b.prep[e[m]];
+    in[m] = px >= P.i_lo && px < P.i_hi;
+    any |= in[m];
+  }
+  if (!any) return;
+  const int nn = R.nn;
+  if (px + 8 <= G.tail_start) {
+    float2 acc[NM][4];
+#pragma unroll
+    for (int m = 0; m < NM; m++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) acc[m][k] = make_float2(0.0f, 0.0f);
     const float2 bias = make_float2(-8388608.0f, -8388608.0f);
-#pragma unroll 8
+#pragma unroll 4
     for (int n = 0; n < nn; n++) {
-      const float w = wf[n];
-      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rows[n] + px));
-      const float2 w2 = make_float2(w, w);
+      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
+      const float4 w4 = R.wf[n];
+      const float ws[4] = {w4.x, w4.y, w4.z, w4.w};
       const uint32_t u[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         float2 v = make_float2(__int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7410)),
                                __int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7432)));
-        v = __fadd2_rn(v, bias);
-        acc[k] = __ffma2_rn(w2, v, acc[k]);
+        v = __fadd2_rn(v, bias);  // exact u16 -> f32
+#pragma unroll
+        for (int m = 0; m < NM; m++) acc[m][k] = __ffma2_rn(make_float2(ws[m], ws[m]), v, acc[m][k]);
       }
     }
-    out[0] = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
-    out[1] = make_float4(acc[2].x, acc[2].y, acc[3].x, acc[3].y);
+#pragma unroll
+    for (int m = 0; m < NM; m++) {
+      if (!in[m]) continue;
+      float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e[m] * b.stride + px);
+      out[0] = make_float4(acc[m][0].x, acc[m][0].y, acc[m][1].x, acc[m][1].y);
+      out[1] = make_float4(acc[m][2].x, acc[m][2].y, acc[m][3].x, acc[m][3].y);
+    }
     return;
   }
   // last tile: the final npx % 128 pixels carry an extra 1/65535 (interpolate.rs:978)
-  float acc[8];
 #pragma unroll
-  for (int k = 0; k < 8; k++) acc[k] = 0.0f;
-  for (int n = 0; n < nn; n++) {
-    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rows[n] + px));
-    const float wn = ws[n], fn = fs[n];
-    const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+  for (int m = 0; m < NM; m++) {
+    if (!in[m]) continue;
+    float acc[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const float x = (float)((u[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
-      const float v = px + k >= G.tail_start ? __fmul_rn(__fdiv_rn(x, 65535.0f), fn) : __fmul_rn(x, fn);
-      acc[k] = fmaf(wn, v, acc[k]);
+    for (int k = 0; k < 8; k++) acc[k] = 0.0f;
+    for (int n = 0; n < nn; n++) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
+      const float4 w4 = R.w[n];
+      const float wn = m == 0 ? w4.x : m == 1 ? w4.y : m == 2 ? w4.z : w4.w, fn = R.f[n];
+      const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const float x = (float)((u[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
+        const float v = px + k >= G.tail_start ? __fmul_rn(__fdiv_rn(x, 65535.0f), fn) : __fmul_rn(x, fn);
+        acc[k] = fmaf(wn, v, acc[k]);
+      }
     }
+    float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e[m] * b.stride + px);
+    out[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    out[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
   }
-  out[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-  out[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+}
+
+// Grid: x = segment, y = 2048-pixel tile, so CTAs that run together read
+// the same tile slab of the resident grid (57 MB for 13,860 x 80,000), which
+// stays in L2.  Each CTA walks its segment's groups.
+__global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
+  __shared__ GroupRec R;
+  const int s = blockIdx.x;
+  const int px = blockIdx.y * IT_TILE + threadIdx.x * 8;
+  const int ng = b.gcount[s];
+  for (int g = 0; g < ng; g++) {
+    const float4 *src = reinterpret_cast<const float4 *>(b.grec + (size_t)s * SEG + g);
+    float4 *dst = reinterpret_cast<float4 *>(&R);
+    for (int i = threadIdx.x; i < (int)(sizeof(GroupRec) / 16); i += IT_T) dst[i] = src[i];
+    __syncthreads();
+    switch (R.nmem) {
+      case 1: interp_members<1>(G, b, R, px); break;
+      case 2: interp_members<2>(G, b, R, px); break;
+      case 3: interp_members<3>(G, b, R, px); break;
+      default: interp_members<4>(G, b, R, px); break;
+    }
+    __syncthreads();
+  }
 }
 
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
-  dim3 grid(b.E, (G.npx + IT_TILE - 1) / IT_TILE);
+  dim3 grid((b.E + SEG - 1) / SEG, (G.npx + IT_TILE - 1) / IT_TILE);
   k_interp<<<grid, IT_T, 0, s>>>(G, b);
   count_launch();
 }
@@ -311,22 +425,6 @@ __device__ __forceinline__ void stage_item(const EvalBatch &b, long long item, f
   if (w.has1) stage_row(stg1, row, w.j1, P.i_lo, P.i_hi);
 }
 
-// last forward stage with the product by the kernel spectrum in its stores:
-// its output s = 4 q + r is bin k = tid + 256 q + 512 r (Hermitian spectrum:
-// bins above 1024 are conjugates of bin 2048 - k)
-struct MulStore {
-  float *re, *im;
-  const float2 *__restrict__ H;  // 1025 bins
-  __device__ __forceinline__ void operator()(int, int a, cf v, int s) const {
-    const int k = (int)threadIdx.x + (s >> 2) * FFT_T + (s & 3) * 512;
-    float2 hh = k <= 1024 ? H[k] : H[FFTN - k];
-    if (k > 1024) hh.y = -hh.y;
-    const cf z = cmul(v, cf{hh.x, hh.y});
-    re[a] = z.x;
-    im[a] = z.y;
-  }
-};
-
 struct StageLoad {
   const float *s0, *s1;
   bool has1;
@@ -346,13 +444,7 @@ struct FoldStore {
   }
 };
 
-#ifndef PB_BROADEN_MINB
-#define PB_BROADEN_MINB 4
-#endif
-#ifndef PB_BROADEN_FUSED_MUL
-#define PB_BROADEN_FUSED_MUL 0
-#endif
-__global__ void __launch_bounds__(FFT_T, PB_BROADEN_MINB) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) float br_smem[];
   float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
   float *re = stg1 + BR_STG, *im = re + FFT_SM;
@@ -392,11 +484,9 @@ __global__ void __launch_bounds__(FFT_T, PB_BROADEN_MINB) k_broaden(DevGrid G, E
       cp_async_commit();
       fft_stage<8, 8, false>(re, im, tw);
       fft_stage<8, 64, false>(re, im, tw);
-      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
-#if PB_BROADEN_FUSED_MUL
-      fft_pass<4, 512, false>(tw, SmemLoad{re, im}, MulStore{re, im, H});
-#else
       fft_stage<4, 512, false>(re, im, tw);
+      // the kernel spectrum (Hermitian: bins above 1024 are conjugates)
+      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
       for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
         float2 h = k <= 1024 ? H[k] : H[FFTN - k];
         if (k > 1024) h.y = -h.y;
@@ -406,7 +496,6 @@ __global__ void __launch_bounds__(FFT_T, PB_BROADEN_MINB) k_broaden(DevGrid G, E
         im[a] = z.y;
       }
       __syncthreads();
-#endif
       fft_stage<8, 1, true>(re, im, tw);
       fft_stage<8, 8, true>(re, im, tw);
       fft_stage<8, 64, true>(re, im, tw);
@@ -1164,6 +1253,7 @@ void launch_pipeline(const DevGrid &G, const EvalBatch &b, const float2 *tw, con
   if (o.full_window) launch_prep_full(G, b, s);
   else launch_prep(G, b, s);
   if (o.rot) launch_rotker(G, b, tw, s);
+  launch_group(G, b, s);
   launch_interp(G, b, s);
   launch_obs_bounds(G, b, s);
   launch_broaden(G, b, tw, s);

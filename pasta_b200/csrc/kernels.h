@@ -6,6 +6,21 @@
 
 namespace pb {
 
+// Evaluations that share all 64 neighbour rows (same grid cube), up to
+// GROUP_MAX per group, found among SEG consecutive evaluations (the
+// particles of one star in the batched engine), with the rows they use in
+// reference order (zero-weight rows of every member dropped, padded to a
+// multiple of 8 with zero weights).
+constexpr int GROUP_MAX = 4, SEG = 64;
+struct __align__(16) GroupRec {
+  float4 wf[64];          // per member weight x dequantisation factor (0: padding / not a member)
+  float4 w[64];           // per member weight (the exact tail path)
+  int col[64];            // grid row of compacted neighbour n
+  float f[64];            // its dequantisation factor
+  int member[GROUP_MAX];  // evaluation indices (-1: unused)
+  int nmem, nn;           // members, compacted rows
+};
+
 // Per-launch description of one batch of evaluations.
 struct EvalBatch {
   int E;                     // evaluations in this batch
@@ -33,6 +48,8 @@ struct EvalBatch {
   int bnd_stride;
   float *ccoef;              // [E][MAX_CHUNKS][MAX_P1] chunk polynomial coefficients (f32)
   double *cpart;             // [E][MAX_CHUNKS] chi2 partial sums per chunk section
+  GroupRec *grec;            // [ceil(E / SEG) * SEG] groups of each segment, in order
+  int *gcount;               // [ceil(E / SEG)] groups per segment
   const float *given;        // model given at the observed pixels (continuum utilities) or null
   int64_t given_stride;      // floats between the given rows of consecutive evaluations
 };
@@ -56,6 +73,8 @@ void launch_prep(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // same, for entry points that need every synthetic pixel and no resampling
 void launch_prep_full(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_rotker(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
+// groups of evaluations sharing their neighbour rows (after the preparation)
+void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // first observed pixel of every fused broadening block (chi2 batches)
 void launch_obs_bounds(const DevGrid &G, const EvalBatch &b, cudaStream_t s);

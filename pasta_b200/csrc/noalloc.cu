@@ -76,7 +76,8 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 size_t per_label_bytes(int64_t stride, int bnd_stride) {
   return align256(sizeof(EvalPrep)) + 2 * align256(1025 * sizeof(float2)) + align256(sizeof(int)) +
          2 * align256((size_t)stride * sizeof(float)) + align256((size_t)bnd_stride * sizeof(int)) +
-         align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float)) + align256((size_t)MAX_CHUNKS * sizeof(double));
+         align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float)) + align256((size_t)MAX_CHUNKS * sizeof(double)) +
+         align256(sizeof(GroupRec)) + align256(sizeof(int));
 }
 
 int setup_device(int dev, DeviceSetup **out) {
@@ -149,7 +150,8 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   }
   stride = std::max<int64_t>(stride, (n + 63) / 64 * 64);  // rows also hold the model at the observed pixels
   const int bstr = bnd_stride_for(G.npx);
-  const size_t fixed = align256(sizeof(DevStar));
+  // the star record, and the group slots of a partly filled last segment
+  const size_t fixed = align256(sizeof(DevStar)) + align256((size_t)(SEG - 1) * sizeof(GroupRec)) + 256;
   const size_t per = per_label_bytes(stride, bstr);
   const int64_t max_labels = NOALLOC_SCRATCH_BYTES > fixed ? (int64_t)((NOALLOC_SCRATCH_BYTES - fixed) / per) : 0;
   if (L > max_labels) {
@@ -190,6 +192,12 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   float *ccoef = (float *)p;
   p += align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float) * (size_t)L);
   double *cpart = (double *)p;
+  p += align256((size_t)MAX_CHUNKS * sizeof(double) * (size_t)L);
+  // SEG group slots per segment of SEG labels: L rounded up to SEG
+  const int64_t Lseg = (L + SEG - 1) / SEG * SEG;
+  GroupRec *grec = (GroupRec *)p;
+  p += align256(sizeof(GroupRec) * (size_t)Lseg);
+  int *gcount = (int *)p;
   cudaStream_t s = (cudaStream_t)stream;
   k_noalloc_init<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(star, dstar, eval_star, (int)L);
   EvalBatch b{};
@@ -220,6 +228,8 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   b.bnd_stride = bstr;
   b.ccoef = ccoef;
   b.cpart = cpart;
+  b.grec = grec;
+  b.gcount = gcount;
   launch_pipeline(G, b, S->twiddle, o, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) {

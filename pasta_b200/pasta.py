@@ -903,6 +903,18 @@ class Server:
                                                                         r.chi2, r.iterations, r.time)))
         return out
 
+    def run(self, steps: int) -> float:
+        """``steps`` steps back to back; returns the milliseconds between CUDA
+        events around them on the library's stream."""
+        ms = C.c_double()
+        check(lib().pasta_server_run(self._h, int(steps), C.byref(ms)))
+        return ms.value
+
+    def stats(self) -> dict:
+        out = np.zeros(3, np.int64)
+        check(lib().pasta_server_stats(self._h, ptr(out)))
+        return dict(zip(["evals", "steps", "particles_per_slot"], out.tolist()))
+
     def pending(self):
         q, a, d = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().pasta_server_pending(self._h, C.byref(q), C.byref(a), C.byref(d)))

@@ -263,3 +263,16 @@ def test_compute_uncertainty_matches_oracle(env):
     alone = fitter.compute_uncertainty(env["interp"], other.flux, other.var, 85000.0, other.label, sr)
     assert bulk[1].to_dict() == alone.to_dict()
     assert set(u.to_dict()) == {"teff", "m", "logg", "vsini", "rv"}
+
+
+def test_server_run_counts_steps_and_evaluations(env):
+    P, star = env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    srv = P.Server(env["interp"], max_slots=4)
+    for k in range(2):
+        srv.submit(d, cont, P.PSOSettings(8, 30), star.flux, star.var, (0.0, 300.0), (-150.0, 150.0), seed=5 + k)
+    ms = srv.run(3)
+    st = srv.stats()
+    assert ms > 0.0
+    assert st["steps"] == 3 and st["evals"] == 3 * 2 * 8
