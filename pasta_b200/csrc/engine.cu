@@ -2287,11 +2287,18 @@ int pasta_server_step(pasta_server *sv) {
       std::unique_ptr<pasta_server::Req> rp(new pasta_server::Req(std::move(r)));
       sv->queue.pop_front();
       sv->used += rp->bytes;
-      sv->slot_flux[i].reset(new DBuf<float>());
-      sv->slot_var[i].reset(new DBuf<float>());
-      sv->slot_flux[i]->upload(rp->flux);
-      sv->slot_var[i]->upload(rp->var);
-      sv->hstars[i] = make_star(rp->d, rp->c, sv->slot_flux[i]->p, sv->slot_var[i]->p, (int64_t)rp->flux.size());
+      // the slot's spectrum buffers are kept between requests and grow only
+      // for a longer spectrum (no allocation or free in the steady state)
+      const size_t nobs = rp->flux.size();
+      if (!sv->slot_flux[i] || sv->slot_flux[i]->n < nobs) {
+        sv->slot_flux[i].reset(new DBuf<float>());
+        sv->slot_var[i].reset(new DBuf<float>());
+        sv->slot_flux[i]->alloc(nobs);
+        sv->slot_var[i]->alloc(nobs);
+      }
+      CK(cudaMemcpyAsync(sv->slot_flux[i]->p, rp->flux.data(), nobs * sizeof(float), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sv->slot_var[i]->p, rp->var.data(), nobs * sizeof(float), cudaMemcpyHostToDevice, s));
+      sv->hstars[i] = make_star(rp->d, rp->c, sv->slot_flux[i]->p, sv->slot_var[i]->p, (int64_t)nobs);
       PsoParams P = make_pso_params(g, rp->st);
       sv->pp[i] = P;
       sv->max_m = std::max(sv->max_m, width_upper_bound(g, P.mx[3]));
@@ -2309,7 +2316,8 @@ int pasta_server_step(pasta_server *sv) {
       CK(cudaMemcpyAsync(sv->W.seed.p + i, &sd, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
       CK(cudaMemcpyAsync(sv->W.params.p + i, &P, sizeof(PsoParams), cudaMemcpyHostToDevice, s));
       CK(cudaMemcpyAsync(sv->dstars.p + i, &sv->hstars[i], sizeof(DevStar), cudaMemcpyHostToDevice, s));
-      CK(cudaStreamSynchronize(s));
+      // pageable sources are staged when the copies are issued; the step's
+      // launches follow on the same stream
       sv->slot_req[i] = std::move(rp);
       admitted.push_back(i);
     }
@@ -2422,7 +2430,6 @@ int pasta_server_step(pasta_server *sv) {
         CK(cudaMemcpyAsync(sv->W.active.p + i, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
       }
       CK(cudaStreamSynchronize(s));
-      for (int i : fin) { sv->slot_flux[i].reset(); sv->slot_var[i].reset(); }
     }
     for (int i = 0; i < sv->slots; i++) active_after += sv->slot_req[i] ? 1 : 0;
   });

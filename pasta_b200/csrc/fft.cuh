@@ -2,13 +2,14 @@
 //
 // Stockham autosort (Govindaraju et al., "High performance discrete Fourier
 // transforms on graphics processors", SC 2008) with radices 8, 8, 8, 4.
-// Data live in shared memory as separate real/imaginary float arrays whose
-// index is XOR-swizzled within each 32-word row (bits 0-4 ^= bits 3-7):
-// every stage's strided reads and scattered writes, and the linear
-// accesses, then touch 32 distinct banks per warp.  Twiddles
-// W_2048^k = exp(-2 pi i k / 2048) come from a table the host computed in
-// double.  Forward is unnormalised; the inverse is unnormalised too
-// (caller scales by 1/2048, like convolve_rv.rs:153-154).
+// Data live in shared memory as 2048 interleaved complex values (float2,
+// one 64-bit access each) whose index is XOR-swizzled within each 16-value
+// row (bits 0-3 ^= bits 3-6): a 64-bit warp access is served as two
+// half-warps, and every stage's strided reads and scattered writes, and the
+// linear accesses, then touch 16 distinct 8-byte bank pairs per half-warp.
+// Twiddles W_2048^k = exp(-2 pi i k / 2048) come from a table the host
+// computed in double.  Forward is unnormalised; the inverse is unnormalised
+// too (caller scales by 1/2048, like convolve_rv.rs:153-154).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -16,7 +17,7 @@ namespace pb {
 
 constexpr int FFT_T = 256;
 constexpr int FFT_SM = 2048;
-__device__ __forceinline__ int pidx(int i) { return (i & ~31) | ((i ^ (i >> 3)) & 31); }
+__device__ __forceinline__ int pidx(int i) { return i ^ ((i >> 3) & 15); }
 
 struct cf {
   float x, y;
@@ -64,15 +65,16 @@ __device__ __forceinline__ void dft8(cf v[8]) {
 // swizzled re/im arrays, other functors may read a staging buffer or write
 // outputs elsewhere.
 //
-// Slot arithmetic: the swizzle only mixes bits 3-7 into bits 0-4, so
+// Slot arithmetic: the swizzle only mixes bits 3-6 into bits 0-3, so
 // pidx(j + c) = pidx(j) + c for every multiple c of 256, and the writes of
 // the four stages of fft2048 reduce to one XOR with a per-thread base:
-//   NS = 1:   pidx(8j + r)           = (8j ^ (j & 31)) ^ r
-//   NS = 8:   pidx(d + 8r)           = (d ^ (j & 24)) ^ 9r
-//   NS = 64:  pidx(d + 64r)          = (d ^ ((j >> 3) & 7)) ^ (64r ^ 8(r & 3))
+//   NS = 1:   pidx(8j + r)           = (8j ^ (j & 15)) ^ r
+//   NS = 8:   pidx(d + 8r)           = (d ^ (j & 8)) ^ 9r
+//   NS = 64:  pidx(d + 64r)          = (d ^ ((j >> 3) & 7)) ^ (64r ^ 8(r & 1))
 //   NS = 512: pidx(j + 512r)         = pidx(j) + 512r
 // with d the first output index of the thread's butterfly.  The identities
-// hold for every thread and r of these stages (checked exhaustively).
+// and the absence of bank conflicts hold for every thread and r of these
+// stages (checked exhaustively).
 template <int R, int NS, bool INV, class LD, class ST>
 __device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD &ld, const ST &st) {
   static_assert((R == 8 && (NS == 1 || NS == 8 || NS == 64)) || (R == 4 && NS == 512), "fft2048 stage");
@@ -115,9 +117,9 @@ __device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD
 #pragma unroll
     for (int r = 0; r < R; r++) {
       int a;
-      if constexpr (NS == 1) a = (d ^ (j & 31)) ^ r;
-      else if constexpr (NS == 8) a = (d ^ (j & 24)) ^ (9 * r);
-      else if constexpr (NS == 64) a = (d ^ ((j >> 3) & 7)) ^ (64 * r ^ 8 * (r & 3));
+      if constexpr (NS == 1) a = (d ^ (j & 15)) ^ r;
+      else if constexpr (NS == 8) a = (d ^ (j & 8)) ^ (9 * r);
+      else if constexpr (NS == 64) a = (d ^ ((j >> 3) & 7)) ^ (64 * r ^ 8 * (r & 1));
       else a = p0 + q * FFT_T + r * NS;
       st(d + r * NS, a, v[q][r], q * R + r);
     }
@@ -126,28 +128,28 @@ __device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD
 }
 
 struct SmemLoad {
-  const float *re, *im;
-  __device__ __forceinline__ cf operator()(int, int a) const { return cf{re[a], im[a]}; }
+  const float2 *c;
+  __device__ __forceinline__ cf operator()(int, int a) const {
+    const float2 v = c[a];
+    return cf{v.x, v.y};
+  }
 };
 struct SmemStore {
-  float *re, *im;
-  __device__ __forceinline__ void operator()(int, int a, cf v, int) const {
-    re[a] = v.x;
-    im[a] = v.y;
-  }
+  float2 *c;
+  __device__ __forceinline__ void operator()(int, int a, cf v, int) const { c[a] = make_float2(v.x, v.y); }
 };
 
 template <int R, int NS, bool INV>
-__device__ __forceinline__ void fft_stage(float *re, float *im, const float2 *__restrict__ tw) {
-  fft_pass<R, NS, INV>(tw, SmemLoad{re, im}, SmemStore{re, im});
+__device__ __forceinline__ void fft_stage(float2 *c, const float2 *__restrict__ tw) {
+  fft_pass<R, NS, INV>(tw, SmemLoad{c}, SmemStore{c});
 }
 
 template <bool INV>
-__device__ __forceinline__ void fft2048(float *re, float *im, const float2 *__restrict__ tw) {
-  fft_stage<8, 1, INV>(re, im, tw);
-  fft_stage<8, 8, INV>(re, im, tw);
-  fft_stage<8, 64, INV>(re, im, tw);
-  fft_stage<4, 512, INV>(re, im, tw);
+__device__ __forceinline__ void fft2048(float2 *c, const float2 *__restrict__ tw) {
+  fft_stage<8, 1, INV>(c, tw);
+  fft_stage<8, 8, INV>(c, tw);
+  fft_stage<8, 64, INV>(c, tw);
+  fft_stage<4, 512, INV>(c, tw);
 }
 
 }  // namespace pb

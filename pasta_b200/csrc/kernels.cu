@@ -369,7 +369,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 constexpr int BR_STG = 2064;
 // dynamic shared memory of k_broaden (floats): two staging rows, the
 // swizzled FFT arrays, the two blocks' outputs, the instrument taps
-constexpr int BR_SMEM_FLOATS = 2 * BR_STG + 2 * FFT_SM + 2 * FFT_SM + 512;
+constexpr int BR_SMEM_FLOATS = 2 * BR_STG + 2 * FFT_SM + 2 * FFT_SM + 512;  // staging, FFT (float2), outputs, taps
 
 // pixels outside [ilo, ihi) are zero; ilo and ihi are multiples of 8, so
 // every 16-byte chunk is wholly inside or outside
@@ -387,18 +387,18 @@ struct BroadenItem {
   bool has1;
 };
 
-// the work item `item` of this batch, or false when it has nothing to do
-__device__ __forceinline__ bool broaden_item(const EvalBatch &b, long long item, BroadenItem &w) {
-  w.e = (int)(item / b.max_pairs);
-  w.pair = (int)(item % b.max_pairs);
-  const EvalPrep &P = b.prep[w.e];
-  if (P.status || !P.fused || 2 * w.pair >= P.nblk) return false;
+// the work item (evaluation e, block pair), or false when it has nothing to do
+__device__ __forceinline__ bool broaden_item(const EvalBatch &b, int e, int pair, BroadenItem &w) {
+  w.e = e;
+  w.pair = pair;
+  const EvalPrep &P = b.prep[e];
+  if (P.status || !P.fused || 2 * pair >= P.nblk) return false;
   w.m = P.m;
   w.hg = P.hg;
   w.V = FFTN - (w.m - 1) - 2 * w.hg;
-  w.s0 = P.o_lo + 2 * w.pair * (w.V - 1);
+  w.s0 = P.o_lo + 2 * pair * (w.V - 1);
   w.s1 = w.s0 + (w.V - 1);
-  w.has1 = 2 * w.pair + 1 < P.nblk;
+  w.has1 = 2 * pair + 1 < P.nblk;
   // input t of a block is synth pixel (s - hg - hw + t) for the rotation,
   // (s - hg + t) for the identity
   const int shift = w.m > 1 ? w.hg + (w.m - 1) / 2 : w.hg;
@@ -407,20 +407,42 @@ __device__ __forceinline__ bool broaden_item(const EvalBatch &b, long long item,
   return true;
 }
 
-// this CTA's first item at or after `item` that has work (total: none)
-__device__ __forceinline__ long long next_item(const EvalBatch &b, long long item, long long total) {
-  BroadenItem w;
-  for (; item < total; item += gridDim.x)
-    if (broaden_item(b, item, w)) return item;
-  return total;
-}
+// The items of a CTA, item = e * max_pairs + pair for item = blockIdx.x,
+// blockIdx.x + gridDim.x, ...: stepping (e, pair) by the precomputed
+// quotient and remainder of gridDim.x needs no division per item.
+struct ItemCursor {
+  int e, pair;
+  int de, dp, mp, E;
+  __device__ __forceinline__ void init(const EvalBatch &b) {
+    mp = b.max_pairs;
+    E = b.E;
+    e = (int)blockIdx.x / mp;
+    pair = (int)blockIdx.x % mp;
+    de = (int)gridDim.x / mp;
+    dp = (int)gridDim.x % mp;
+  }
+  __device__ __forceinline__ void advance() {
+    pair += dp;
+    e += de;
+    if (pair >= mp) {
+      pair -= mp;
+      e++;
+    }
+  }
+  __device__ __forceinline__ bool done() const { return e >= E; }
+  // move to the first item with work at or after the current one
+  __device__ __forceinline__ void settle(const EvalBatch &b) {
+    BroadenItem w;
+    while (!done() && !broaden_item(b, e, pair, w)) advance();
+  }
+};
 
 // start the copies of an item's input into the staging rows
-__device__ __forceinline__ void stage_item(const EvalBatch &b, long long item, float *stg0, float *stg1) {
+__device__ __forceinline__ void stage_item(const EvalBatch &b, int e, int pair, float *stg0, float *stg1) {
   BroadenItem w;
-  broaden_item(b, item, w);
-  const EvalPrep &P = b.prep[w.e];
-  const float *row = b.bufA + (size_t)w.e * b.stride;
+  broaden_item(b, e, pair, w);
+  const EvalPrep &P = b.prep[e];
+  const float *row = b.bufA + (size_t)e * b.stride;
   stage_row(stg0, row, w.j0, P.i_lo, P.i_hi);
   if (w.has1) stage_row(stg1, row, w.j1, P.i_lo, P.i_hi);
 }
@@ -447,19 +469,22 @@ struct FoldStore {
 __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) float br_smem[];
   float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
-  float *re = stg1 + BR_STG, *im = re + FFT_SM;
-  float *ob0 = im + FFT_SM, *ob1 = ob0 + FFT_SM;
+  float2 *c = reinterpret_cast<float2 *>(stg1 + BR_STG);  // FFT data (BR_STG keeps 16-byte alignment)
+  float *ob0 = reinterpret_cast<float *>(c + FFT_SM), *ob1 = ob0 + FFT_SM;
   float *gks = ob1 + FFT_SM;  // the fixed instrument kernel of the current item
-  const long long total = (long long)b.E * b.max_pairs;
   const int N = G.npx;
   const int p0 = pidx(threadIdx.x);
-  long long item = next_item(b, blockIdx.x, total);
-  if (item < total) stage_item(b, item, stg0, stg1);
+  ItemCursor cur;
+  cur.init(b);
+  cur.settle(b);
+  if (!cur.done()) stage_item(b, cur.e, cur.pair, stg0, stg1);
   cp_async_commit();
-  while (item < total) {
-    const long long nxt = next_item(b, item + gridDim.x, total);
+  while (!cur.done()) {
+    ItemCursor nxt = cur;
+    nxt.advance();
+    nxt.settle(b);
     BroadenItem w;
-    broaden_item(b, item, w);
+    broaden_item(b, cur.e, cur.pair, w);
     cp_async_wait_all();
     __syncthreads();  // the item's input is staged
     const int e = w.e, pair = w.pair, m = w.m, hg = w.hg, V = w.V, s0 = w.s0, s1 = w.s1;
@@ -479,47 +504,46 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     if (m > 1) {
-      fft_pass<8, 1, false>(tw, ld, SmemStore{re, im});  // first stage straight from the staging rows
-      if (nxt < total) stage_item(b, nxt, stg0, stg1);
+      fft_pass<8, 1, false>(tw, ld, SmemStore{c});  // first stage straight from the staging rows
+      if (!nxt.done()) stage_item(b, nxt.e, nxt.pair, stg0, stg1);
       cp_async_commit();
-      fft_stage<8, 8, false>(re, im, tw);
-      fft_stage<8, 64, false>(re, im, tw);
-      fft_stage<4, 512, false>(re, im, tw);
+      fft_stage<8, 8, false>(c, tw);
+      fft_stage<8, 64, false>(c, tw);
+      fft_stage<4, 512, false>(c, tw);
       // the kernel spectrum (Hermitian: bins above 1024 are conjugates)
       const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
       for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
         float2 h = k <= 1024 ? H[k] : H[FFTN - k];
         if (k > 1024) h.y = -h.y;
         const int a = p0 + (k - threadIdx.x);  // pidx(k), k - threadIdx.x a multiple of 256
-        const cf z = cmul(cf{re[a], im[a]}, cf{h.x, h.y});
-        re[a] = z.x;
-        im[a] = z.y;
+        const float2 x = c[a];
+        const cf z = cmul(cf{x.x, x.y}, cf{h.x, h.y});
+        c[a] = make_float2(z.x, z.y);
       }
       __syncthreads();
-      fft_stage<8, 1, true>(re, im, tw);
-      fft_stage<8, 8, true>(re, im, tw);
-      fft_stage<8, 64, true>(re, im, tw);
+      fft_stage<8, 1, true>(c, tw);
+      fft_stage<8, 8, true>(c, tw);
+      fft_stage<8, 64, true>(c, tw);
       base = m - 1;
       const float sc = 1.0f / 2048.0f;
       if (fold) {  // output u sits at base + 2 hg + u
-        fft_pass<4, 512, true>(tw, SmemLoad{re, im}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
+        fft_pass<4, 512, true>(tw, SmemLoad{c}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
       } else {
-        fft_stage<4, 512, true>(re, im, tw);
+        fft_stage<4, 512, true>(c, tw);
         for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
           const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
-          re[pidx(t)] = (i0 >= 0 && i0 < N) ? re[pidx(t)] * sc : 0.0f;
-          im[pidx(t)] = (i1 >= 0 && i1 < N) ? im[pidx(t)] * sc : 0.0f;
+          const float2 x = c[pidx(t)];
+          c[pidx(t)] = make_float2((i0 >= 0 && i0 < N) ? x.x * sc : 0.0f, (i1 >= 0 && i1 < N) ? x.y * sc : 0.0f);
         }
         __syncthreads();
       }
     } else {  // identity rotation: the staged input is the rotation output
       for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
         const cf v = ld(t, 0);
-        re[p0 + (t - threadIdx.x)] = v.x;
-        im[p0 + (t - threadIdx.x)] = v.y;
+        c[p0 + (t - threadIdx.x)] = make_float2(v.x, v.y);
       }
       __syncthreads();
-      if (nxt < total) stage_item(b, nxt, stg0, stg1);
+      if (!nxt.done()) stage_item(b, nxt.e, nxt.pair, stg0, stg1);
       cp_async_commit();
     }
     if (!fold) {
@@ -527,21 +551,22 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
         const int i0 = s0 + u, i1 = s1 + u;
         float v0, v1;
         if (hg == 0) {
-          v0 = re[pidx(base + u)];
-          v1 = im[pidx(base + u)];
+          const float2 x = c[pidx(base + u)];
+          v0 = x.x;
+          v1 = x.y;
         } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at base + (i - s + hg)
           float a0 = 0.0f, a1 = 0.0f;
           for (int k = 0; k < gw; k++) {
             const float g = gks[k];
-            const int t = pidx(base + u + 2 * hg - k);
-            a0 = fmaf(g, re[t], a0);
-            a1 = fmaf(g, im[t], a1);
+            const float2 x = c[pidx(base + u + 2 * hg - k)];
+            a0 = fmaf(g, x.x, a0);
+            a1 = fmaf(g, x.y, a1);
           }
           v0 = a0;
           v1 = a1;
         } else {
-          v0 = instrument(st, N, i0, hg, [&](int i) { return re[pidx(base + i - (s0 - hg))]; });
-          v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return im[pidx(base + i - (s1 - hg))]; }) : 0.0f;
+          v0 = instrument(st, N, i0, hg, [&](int i) { return c[pidx(base + i - (s0 - hg))].x; });
+          v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return c[pidx(base + i - (s1 - hg))].y; }) : 0.0f;
         }
         ob0[u] = v0;
         ob1[u] = v1;
@@ -572,7 +597,7 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
         if (has1 && u < n1 && i1 < ohi) y[i1] = ob1[u];
       }
     }
-    item = nxt;
+    cur = nxt;
   }
   cp_async_wait_all();
 }
@@ -637,7 +662,7 @@ void launch_obs_bounds(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
 // Overlap-save with the rotation kernel alone: block b produces rotation
 // outputs [g_lo + b V, g_lo + (b+1) V), V = 2048 - (m - 1), into B.
 __global__ void __launch_bounds__(FFT_T, 3) k_rot(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
-  __shared__ float re[FFT_SM], im[FFT_SM];
+  __shared__ float2 c[FFT_SM];
   const long long total = (long long)b.E * b.max_pairs_unfused;
   for (long long item = blockIdx.x; item < total; item += gridDim.x) {
     const int e = (int)(item / b.max_pairs_unfused), pair = (int)(item % b.max_pairs_unfused);
@@ -651,30 +676,29 @@ __global__ void __launch_bounds__(FFT_T, 3) k_rot(DevGrid G, EvalBatch b, const 
     const float *x = b.bufA + (size_t)e * b.stride;
     for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
       const int j0 = s0 - hw + t, j1 = s1 - hw + t;
-      re[pidx(t)] = (j0 >= ilo && j0 < ihi) ? x[j0] : 0.0f;
-      im[pidx(t)] = (has1 && j1 >= ilo && j1 < ihi) ? x[j1] : 0.0f;
+      c[pidx(t)] = make_float2((j0 >= ilo && j0 < ihi) ? x[j0] : 0.0f, (has1 && j1 >= ilo && j1 < ihi) ? x[j1] : 0.0f);
     }
     __syncthreads();
-    fft2048<false>(re, im, tw);
+    fft2048<false>(c, tw);
     const float2 *H = b.H + (size_t)e * 1025;
     for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
       float2 h = k <= 1024 ? H[k] : H[FFTN - k];
       if (k > 1024) h.y = -h.y;
       const int a = pidx(k);
-      const cf z = cmul(cf{re[a], im[a]}, cf{h.x, h.y});
-      re[a] = z.x;
-      im[a] = z.y;
+      const float2 v = c[a];
+      const cf z = cmul(cf{v.x, v.y}, cf{h.x, h.y});
+      c[a] = make_float2(z.x, z.y);
     }
     __syncthreads();
-    fft2048<true>(re, im, tw);
+    fft2048<true>(c, tw);
     float *y = b.bufB + (size_t)e * b.stride;
     const float sc = 1.0f / 2048.0f;
     for (int t = m - 1 + threadIdx.x; t < FFTN; t += FFT_T) {
       const int i0 = s0 + t - (m - 1);
-      if (i0 < ghi) y[i0] = re[pidx(t)] * sc;
+      if (i0 < ghi) y[i0] = c[pidx(t)].x * sc;
       if (has1) {
         const int i1 = s1 + t - (m - 1);
-        if (i1 < ghi) y[i1] = im[pidx(t)] * sc;
+        if (i1 < ghi) y[i1] = c[pidx(t)].y * sc;
       }
     }
     __syncthreads();

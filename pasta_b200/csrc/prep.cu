@@ -135,7 +135,7 @@ __global__ void k_prep(DevGrid G, EvalBatch b, int full_window) {
 // (convolve_rv.rs:438-475), normalised by its f32 sum, zero padded to 2048
 // and transformed; the 1025-bin half spectrum goes to H.
 __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
-  __shared__ float re[FFT_SM], im[FFT_SM];
+  __shared__ float2 c[FFT_SM];
   __shared__ float red[FFT_T];
   const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
@@ -155,8 +155,7 @@ __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const 
       double y = 1.0 - r * r;
       if (y > 0.0) val = (float)((2.0 * (1.0 - eps) * sqrt(y) + pi * eps / 2.0 * y) / den);
     }
-    re[pidx(t)] = val;
-    im[pidx(t)] = 0.0f;
+    c[pidx(t)] = make_float2(val, 0.0f);
     local += val;
   }
   red[threadIdx.x] = local;
@@ -166,11 +165,11 @@ __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const 
     __syncthreads();
   }
   const float total = red[0];
-  for (int t = threadIdx.x; t < m; t += FFT_T) re[pidx(t)] = re[pidx(t)] / total;
+  for (int t = threadIdx.x; t < m; t += FFT_T) c[pidx(t)].x = c[pidx(t)].x / total;
   __syncthreads();
-  fft2048<false>(re, im, tw);
+  fft2048<false>(c, tw);
   float2 *H = b.H + (size_t)e * 1025;
-  for (int k = threadIdx.x; k <= 1024; k += FFT_T) H[k] = make_float2(re[pidx(k)], im[pidx(k)]);
+  for (int k = threadIdx.x; k <= 1024; k += FFT_T) H[k] = c[pidx(k)];
   // rotation x instrument spectrum for the blocks of the broadening kernel
   // that apply both as one convolution
   const DevStar &st = b.stars[P.star];
@@ -178,7 +177,8 @@ __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const 
     float2 *HG = b.HG + (size_t)e * 1025;
     for (int k = threadIdx.x; k <= 1024; k += FFT_T) {
       const float2 g = st.gspec[k];
-      const cf z = cmul(cf{re[pidx(k)], im[pidx(k)]}, cf{g.x, g.y});
+      const float2 x = c[pidx(k)];
+      const cf z = cmul(cf{x.x, x.y}, cf{g.x, g.y});
       HG[k] = make_float2(z.x, z.y);
     }
   }
