@@ -362,6 +362,8 @@ def run_ours(args):
                                % (n_stars, spec.n_px, spectra.nbytes / 1e9, PARTICLES, ITERS),
                    "stars_per_gpu": n_stars, "particles": PARTICLES, "iterations": ITERS,
                    "evals_per_step": evals_step, "fits_finished_in_timed_steps": fits_done,
+                   "host_ms_per_step": {k: (st1[k + "_us"] - st0[k + "_us"]) / 1000.0 / args.steps
+                                        for k in ("admit", "device", "retire", "refit")},
                    "step": "one served step: PSO update, chi2 of every active particle, best update, "
                            "admissions and retirements (final refit)",
                    "parallelism": "replicas x%d (stars sharded, no collective)" % world,

@@ -296,8 +296,11 @@ int pasta_server_destroy(pasta_server *s);
  * free up), timed between CUDA events on the library's stream (host work
  * between the launches is inside the interval). */
 int pasta_server_run(pasta_server *s, int steps, double *device_ms);
-/* out3: chi2 evaluations run, steps run, particles per slot. */
-int pasta_server_stats(const pasta_server *s, int64_t *out3);
+/* out7: chi2 evaluations run, steps run, particles per slot, and the host
+ * microseconds spent in steps before the device loop is launched
+ * (admissions), waiting for it, after it (retirements), and of those in
+ * the final refits. */
+int pasta_server_stats(const pasta_server *s, int64_t *out7);
 
 #ifdef __cplusplus
 }

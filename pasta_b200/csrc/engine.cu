@@ -876,8 +876,26 @@ struct SwarmBuffers {
 };
 
 // Final refit at the best labels (fitting.rs:436-440) -> continuum params.
+// Device buffers of a final refit, kept by callers that refit often (the
+// server retires a few stars every step) so that no step allocates.
+struct RefitScratch {
+  DBuf<double> lab, cost, par;
+  DBuf<int> es, ea, st;
+  void ensure(int S, int pstride) {
+    if (cost.n < (size_t)S) {
+      lab.alloc((size_t)S * 5);
+      cost.alloc(S);
+      es.alloc(S);
+      ea.alloc(S);
+      st.alloc(S);
+    }
+    if (par.n < (size_t)S * pstride) par.alloc((size_t)S * pstride);
+  }
+};
+
 void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, const std::vector<double> &best,
-                 const std::vector<int> &ok, std::vector<std::vector<float>> &params, cudaStream_t s) {
+                 const std::vector<int> &ok, std::vector<std::vector<float>> &params, cudaStream_t s,
+                 RefitScratch *scratch = nullptr, const DevStar *dstars = nullptr) {
   const int S = (int)in.size();
   int pstride = 1, max_m = 1;
   for (auto &x : in) {
@@ -886,18 +904,18 @@ void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, c
     if (x.st->ckind[3] == 1) vhi = x.st->ca[3];
     max_m = std::max(max_m, width_upper_bound(g, vhi));
   }
-  DBuf<double> lab, cost, par;
-  DBuf<int> es, ea, st;
-  lab.upload(best);
+  RefitScratch local;
+  RefitScratch &R = scratch ? *scratch : local;
+  R.ensure(S, pstride);
   std::vector<int> star(S);
   for (int i = 0; i < S; i++) star[i] = i;
-  es.upload(star);
-  ea.upload(ok);
-  cost.alloc(S);
-  st.alloc(S);
-  par.alloc((size_t)S * pstride);
+  CK(cudaMemcpyAsync(R.lab.p, best.data(), (size_t)S * 5 * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(R.es.p, star.data(), (size_t)S * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(R.ea.p, ok.data(), (size_t)S * sizeof(int), cudaMemcpyHostToDevice, s));
+  DBuf<double> &lab = R.lab, &cost = R.cost, &par = R.par;
+  DBuf<int> &es = R.es, &ea = R.ea, &st = R.st;
   EvalArgs a;
-  a.stars = ss.dstars.p;
+  a.stars = dstars ? dstars : ss.dstars.p;
   a.labels = lab.p;
   a.eval_star = es.p;
   a.eval_active = ea.p;
@@ -1294,6 +1312,10 @@ struct pasta_server {
   int64_t next_id = 1;
   int64_t evals_total = 0, steps_total = 0;  // evaluations and steps run so far
   int64_t graph_kernels = 0;                  // kernels in the captured step
+  RefitScratch refit;                         // final-refit buffers reused by every retirement
+  double t_before = 0, t_step = 0, t_after = 0;  // host seconds: admission, graph run, retirement
+  double t_refit = 0;                              // of which the final refits
+  DBuf<DevStar> refit_stars;
   int max_m = 1, graph_max_m = 0;
   int64_t graph_gen = -1;
   uint32_t graph_mask = 0;  // continuum kinds / instrument width the captured step covers
@@ -2266,6 +2288,7 @@ void server_rebuild(pasta_server *sv, int Pmax) {
 int pasta_server_step(pasta_server *sv) {
   int active_after = 0;
   int rc = guard([&] {
+    const double t0 = now_s();
     std::lock_guard<std::mutex> lk(sv->mu);
     pasta_grid *g = sv->g;
     std::lock_guard<std::mutex> lg(g->mu);
@@ -2374,6 +2397,7 @@ int pasta_server_step(pasta_server *sv) {
       count_launch(-(int)sv->graph_kernels);  // counted again at every replay
       CK(cudaGraphInstantiate(&sv->exec, sv->graph, 0));
     }
+    const double t1 = now_s();
     CK(cudaGraphLaunch(sv->exec, s));
     count_launch((int)sv->graph_kernels);
     for (int i = 0; i < sv->slots; i++)
@@ -2383,6 +2407,9 @@ int pasta_server_step(pasta_server *sv) {
     CK(cudaMemcpyAsync(done.data(), sv->W.done.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(status.data(), sv->W.status.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    const double t2 = now_s();
+    sv->t_before += t1 - t0;
+    sv->t_step += t2 - t1;
     // retire finished requests: final refit for their params, free the slot
     std::vector<int> fin;
     for (int i = 0; i < sv->slots; i++)
@@ -2405,10 +2432,13 @@ int pasta_server_step(pasta_server *sv) {
         for (int d = 0; d < 5; d++) best.push_back(gx[(size_t)i * 5 + d]);
         ok.push_back(status[i] == 0 ? 1 : 0);
       }
-      ss.dstars.upload(hs);
+      if (sv->refit_stars.n < hs.size()) sv->refit_stars.alloc(sv->slots);
+      CK(cudaMemcpyAsync(sv->refit_stars.p, hs.data(), hs.size() * sizeof(DevStar), cudaMemcpyHostToDevice, s));
       ss.h = hs;
       std::vector<std::vector<float>> params;
-      final_refit(g, ss, in, best, ok, params, s);
+      const double tr0 = now_s();
+      final_refit(g, ss, in, best, ok, params, s, &sv->refit, sv->refit_stars.p);
+      sv->t_refit += now_s() - tr0;
       const double tnow = now_s();
       for (size_t q = 0; q < fin.size(); q++) {
         const int i = fin[q];
@@ -2432,6 +2462,7 @@ int pasta_server_step(pasta_server *sv) {
       CK(cudaStreamSynchronize(s));
     }
     for (int i = 0; i < sv->slots; i++) active_after += sv->slot_req[i] ? 1 : 0;
+    sv->t_after += now_s() - t2;
   });
   return rc ? rc : active_after;
 }
@@ -2466,12 +2497,17 @@ int pasta_server_run(pasta_server *sv, int steps, double *device_ms) {
   return rc ? rc : rc2;
 }
 
-int pasta_server_stats(const pasta_server *sv, int64_t *out3) {
+int pasta_server_stats(const pasta_server *sv, int64_t *out7) {
   return guard([&] {
-    if (!out3) fail(PASTA_E_ARG, "output required");
-    out3[0] = sv->evals_total;
-    out3[1] = sv->steps_total;
-    out3[2] = sv->Pmax;
+    if (!out7) fail(PASTA_E_ARG, "output required");
+    int64_t *out6 = out7;
+    out6[0] = sv->evals_total;
+    out6[1] = sv->steps_total;
+    out6[2] = sv->Pmax;
+    out6[3] = (int64_t)(sv->t_before * 1e6);
+    out6[4] = (int64_t)(sv->t_step * 1e6);
+    out6[5] = (int64_t)(sv->t_after * 1e6);
+    out6[6] = (int64_t)(sv->t_refit * 1e6);
   });
 }
 

@@ -911,9 +911,10 @@ class Server:
         return ms.value
 
     def stats(self) -> dict:
-        out = np.zeros(3, np.int64)
+        out = np.zeros(7, np.int64)
         check(lib().pasta_server_stats(self._h, ptr(out)))
-        return dict(zip(["evals", "steps", "particles_per_slot"], out.tolist()))
+        return dict(zip(["evals", "steps", "particles_per_slot", "admit_us", "device_us", "retire_us", "refit_us"],
+                        out.tolist()))
 
     def pending(self):
         q, a, d = C.c_int64(), C.c_int64(), C.c_int64()
