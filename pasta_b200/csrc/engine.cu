@@ -855,6 +855,7 @@ struct SwarmBuffers {
     w.gx = gx.p; w.gcost = gcost.p; w.iter = iter.p; w.status = status.p; w.done = done.p;
     w.active = active.p; w.seed = seed.p; w.params = params.p; w.labels = labels.p;
     w.eval_active = eval_active.p;
+    w.refit = nullptr;
     return w;
   }
   void alloc(int S_, int Pmax_) {
@@ -1282,6 +1283,10 @@ void fit_plain(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result
 }  // namespace
 
 // ================================================================ serving
+// continuum parameters per slot of the in-graph refit: the most any
+// continuum fitter has (chunks x coefficients, or linear-model columns)
+constexpr int SERVER_REFIT_STRIDE = MAX_CHUNKS * MAX_P1 > MAX_LIN_K ? MAX_CHUNKS * MAX_P1 : MAX_LIN_K;
+
 struct pasta_server {
   pasta_grid *g = nullptr;
   int slots = 0, Pmax = 0;
@@ -1312,10 +1317,12 @@ struct pasta_server {
   int64_t next_id = 1;
   int64_t evals_total = 0, steps_total = 0;  // evaluations and steps run so far
   int64_t graph_kernels = 0;                  // kernels in the captured step
-  RefitScratch refit;                         // final-refit buffers reused by every retirement
   double t_before = 0, t_step = 0, t_after = 0;  // host seconds: admission, graph run, retirement
-  double t_refit = 0;                              // of which the final refits
-  DBuf<DevStar> refit_stars;
+  double t_refit = 0;                              // of which reading the refits back
+  // in-graph final refit: per slot the finished flag, identity star index,
+  // chi2, status and continuum parameters
+  DBuf<int> rf_flag, rf_star, rf_status;
+  DBuf<double> rf_cost, rf_params;
   int max_m = 1, graph_max_m = 0;
   int64_t graph_gen = -1;
   uint32_t graph_mask = 0;  // continuum kinds / instrument width the captured step covers
@@ -2271,6 +2278,14 @@ void server_rebuild(pasta_server *sv, int Pmax) {
   // (re)allocate slot swarm arrays for a larger particle count; only when empty
   sv->Pmax = Pmax;
   sv->W.alloc(sv->slots, Pmax);
+  std::vector<int> ident(sv->slots);
+  for (int i = 0; i < sv->slots; i++) ident[i] = i;
+  sv->rf_star.upload(ident);
+  sv->rf_flag.alloc(sv->slots);
+  CK(cudaMemset(sv->rf_flag.p, 0, sv->slots * sizeof(int)));
+  sv->rf_status.alloc(sv->slots);
+  sv->rf_cost.alloc(sv->slots);
+  sv->rf_params.alloc((size_t)sv->slots * SERVER_REFIT_STRIDE);
   std::vector<int> z(sv->slots, 0), done1(sv->slots, 1), im(sv->slots, -1);
   CK(cudaMemcpy(sv->W.active.p, z.data(), z.size() * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(sv->W.done.p, done1.data(), z.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -2349,6 +2364,7 @@ int pasta_server_step(pasta_server *sv) {
     if (!any) return;
     const int64_t E = (int64_t)sv->slots * sv->Pmax;
     Swarm sw = sv->W.view();
+    sw.refit = sv->rf_flag.p;
     EvalArgs a;
     a.stars = sv->dstars.p;
     a.labels = sv->W.labels.p;
@@ -2392,6 +2408,18 @@ int pasta_server_step(pasta_server *sv) {
       launch_pso_update(g->d, sw, s);
       run_evals(g, a, s);
       launch_pso_best(sw, sv->W.ecost.p, sv->W.estatus.p, s);
+      // final refit (fitting.rs:436-440) of the swarms that finished in this
+      // step: chi2 at the best label with the continuum parameters written
+      EvalArgs r = a;
+      r.labels = sv->W.gx.p;
+      r.eval_star = sv->rf_star.p;
+      r.eval_active = sv->rf_flag.p;
+      r.E = sv->slots;
+      r.cost = sv->rf_cost.p;
+      r.status = sv->rf_status.p;
+      r.params = sv->rf_params.p;
+      r.param_stride = SERVER_REFIT_STRIDE;
+      run_evals(g, r, s);
       CK(cudaStreamEndCapture(s, &sv->graph));
       sv->graph_kernels = kernel_launches() - k0;
       count_launch(-(int)sv->graph_kernels);  // counted again at every replay
@@ -2403,9 +2431,13 @@ int pasta_server_step(pasta_server *sv) {
     for (int i = 0; i < sv->slots; i++)
       if (sv->slot_req[i]) sv->evals_total += sv->slot_req[i]->st.num_particles;
     sv->steps_total++;
+    // the step's flags and every slot's best (small) in one wait
     std::vector<int> done(sv->slots), status(sv->slots);
+    std::vector<double> gx((size_t)sv->slots * 5), gc(sv->slots);
     CK(cudaMemcpyAsync(done.data(), sv->W.done.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(status.data(), sv->W.status.p, sv->slots * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(gx.data(), sv->W.gx.p, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(gc.data(), sv->W.gcost.p, gc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     const double t2 = now_s();
     sv->t_before += t1 - t0;
@@ -2415,29 +2447,20 @@ int pasta_server_step(pasta_server *sv) {
     for (int i = 0; i < sv->slots; i++)
       if (sv->slot_req[i] && done[i]) fin.push_back(i);
     if (!fin.empty()) {
-      std::vector<double> gx((size_t)sv->slots * 5), gc(sv->slots);
-      CK(cudaMemcpyAsync(gx.data(), sv->W.gx.p, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(gc.data(), sv->W.gcost.p, gc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      std::vector<StarInput> in;
-      std::vector<double> best;
-      std::vector<int> ok;
-      StarSet ss;
-      ss.h.clear();
-      std::vector<DevStar> hs;
-      for (int i : fin) {
-        auto &r = *sv->slot_req[i];
-        in.push_back(StarInput{r.d, r.c, &r.st, r.flux.data(), r.var.data(), (int64_t)r.flux.size(), r.seed});
-        hs.push_back(sv->hstars[i]);
-        for (int d = 0; d < 5; d++) best.push_back(gx[(size_t)i * 5 + d]);
-        ok.push_back(status[i] == 0 ? 1 : 0);
-      }
-      if (sv->refit_stars.n < hs.size()) sv->refit_stars.alloc(sv->slots);
-      CK(cudaMemcpyAsync(sv->refit_stars.p, hs.data(), hs.size() * sizeof(DevStar), cudaMemcpyHostToDevice, s));
-      ss.h = hs;
-      std::vector<std::vector<float>> params;
+      // the step's graph refitted every swarm that finished successfully
+      // (chi2 at its best label with the continuum parameters written)
       const double tr0 = now_s();
-      final_refit(g, ss, in, best, ok, params, s, &sv->refit, sv->refit_stars.p);
+      std::vector<std::vector<double>> rows(fin.size());
+      std::vector<int> rst(fin.size(), 0);
+      for (size_t q = 0; q < fin.size(); q++) {
+        const int i = fin[q];
+        if (status[i] != 0) continue;
+        rows[q].resize(device_param_stride(sv->slot_req[i]->c));
+        CK(cudaMemcpyAsync(rows[q].data(), sv->rf_params.p + (size_t)i * SERVER_REFIT_STRIDE,
+                           rows[q].size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&rst[q], sv->rf_status.p + i, sizeof(int), cudaMemcpyDeviceToHost, s));
+      }
+      CK(cudaStreamSynchronize(s));
       sv->t_refit += now_s() - tr0;
       const double tnow = now_s();
       for (size_t q = 0; q < fin.size(); q++) {
@@ -2451,7 +2474,7 @@ int pasta_server_step(pasta_server *sv) {
         dn.r.iterations = r.st.max_iters;
         dn.r.status = status[i];
         dn.r.time = tnow - r.t_submit;
-        dn.params = params[q];
+        if (status[i] == 0 && rst[q] == 0) dn.params = params_from_device(r.c, rows[q].data());
         dn.r.n_params = (int)dn.params.size();
         sv->done.push_back(std::move(dn));
         sv->used -= r.bytes;
@@ -2459,7 +2482,6 @@ int pasta_server_step(pasta_server *sv) {
         int zero = 0;
         CK(cudaMemcpyAsync(sv->W.active.p + i, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
       }
-      CK(cudaStreamSynchronize(s));
     }
     for (int i = 0; i < sv->slots; i++) active_after += sv->slot_req[i] ? 1 : 0;
     sv->t_after += now_s() - t2;

@@ -285,10 +285,17 @@ struct Resampler {
       else if (k == N) idx = (double)N - 1.0;
       else idx = __dadd_rn(__dadd_rn(__ddiv_rn(wl - wl_vals[k - 1], wl_vals[k] - wl_vals[k - 1]), (double)k), -1.0);
     }
+    return from_index(idx);
+  }
+  __device__ __forceinline__ ResPos from_index(double idx) const {
     const double fl = floor(idx);
     int j = fl > 0 ? (int)fl : 0;
     if (j > N - 2) j = N - 2;  // the preparation kernel rejected j + 1 >= N already
     return ResPos{j, (float)idx - (float)j};
+  }
+  // position from an already loaded float index (uniform grids)
+  __device__ __forceinline__ ResPos pos_from_fidx(double fx) const {
+    return from_index(kind == WL_LOG ? fx + shift_log : __dadd_rn(__dmul_rn(shift_factor, fx), lin_offset));
   }
   __device__ __forceinline__ float operator()(int i) const {
     if (given) return given[i];
@@ -580,13 +587,23 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
       const int *bd = b.bnd + (size_t)e * b.bnd_stride + 2 * pair;
       const int q0 = bd[0], q1 = bd[1], q2 = has1 ? bd[2] : q1;
       const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
-#pragma unroll 4
-      for (int i = q0 + threadIdx.x; i < q2; i += FFT_T) {
-        const ResPos q = R.pos(i);
-        const bool k1 = i >= q1;
-        const float *o = k1 ? ob1 : ob0;
-        const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
-        y[i] = resample_value(q.w, o[u], o[u + 1]);
+      constexpr int EU = 8;  // observed pixels per thread whose float indices load together
+      for (int i0 = q0 + threadIdx.x; i0 < q2; i0 += FFT_T * EU) {
+        double fx[EU];
+        if (R.kind != WL_NONUNI) {
+#pragma unroll
+          for (int k = 0; k < EU; k++) fx[k] = R.fidx[min(i0 + k * FFT_T, q2 - 1)];
+        }
+#pragma unroll
+        for (int k = 0; k < EU; k++) {
+          const int i = i0 + k * FFT_T;
+          if (i >= q2) break;
+          const ResPos q = R.kind != WL_NONUNI ? R.pos_from_fidx(fx[k]) : R.pos(i);
+          const bool k1 = i >= q1;
+          const float *o = k1 ? ob1 : ob0;
+          const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
+          y[i] = resample_value(q.w, o[u], o[u + 1]);
+        }
       }
     } else {
       // owned pixels; the last block also writes its final output

@@ -108,6 +108,7 @@ struct Swarm {
   PsoParams *params;         // [S]
   double *labels;            // [S*Pmax][5] evaluation labels
   int *eval_active;          // [S*Pmax]
+  int *refit;                // [S] or null: 1 for a swarm that finished successfully in this step
 };
 // positions for this step (update, or publish host-placed initial positions)
 void launch_pso_update(const DevGrid &G, const Swarm &w, cudaStream_t s);

@@ -306,6 +306,7 @@ __global__ void __launch_bounds__(MAX_PARTICLES) k_pso_best(Swarm W, const doubl
   __shared__ double skey[MAX_PARTICLES];
   __shared__ int sidx[MAX_PARTICLES];
   const int s = blockIdx.x, p = threadIdx.x;
+  if (W.refit && p == 0) W.refit[s] = 0;
   if (!(W.active[s] && !W.done[s] && W.status[s] == 0)) return;
   const PsoParams &S = W.params[s];
   const int P = S.P;
@@ -355,7 +356,10 @@ __global__ void __launch_bounds__(MAX_PARTICLES) k_pso_best(Swarm W, const doubl
     __syncthreads();
     if (p == 0) {
       W.iter[s] = 0;
-      if (S.max_iters <= 0) W.done[s] = 1;
+      if (S.max_iters <= 0) {
+        W.done[s] = 1;
+        if (W.refit) W.refit[s] = 1;
+      }
     }
     return;
   }
@@ -378,7 +382,10 @@ __global__ void __launch_bounds__(MAX_PARTICLES) k_pso_best(Swarm W, const doubl
   }
   if (p == 0) {
     W.iter[s] = it + 1;
-    if (it + 1 >= S.max_iters) W.done[s] = 1;
+    if (it + 1 >= S.max_iters) {
+      W.done[s] = 1;
+      if (W.refit) W.refit[s] = 1;
+    }
   }
 }
 

@@ -209,6 +209,8 @@ def test_server_result_same_alone_and_in_mix(env):
     for i, rid in enumerate(ids):
         assert done[rid].label.as_list() == alone[i].label.as_list()
         assert done[rid].chi2 == alone[i].chi2
+        # the server refits inside its step graph, the batched fit after its last step
+        assert done[rid].continuum_params == alone[i].continuum_params
 
 
 def test_continuum_utilities(env):
