@@ -282,8 +282,12 @@ int pasta_server_submit(pasta_server *s, const pasta_dispersion *d,
                         const pasta_pso_settings *settings, const float *flux,
                         const float *var, int64_t n, uint64_t seed,
                         int64_t *request_id);
-/* advance the device loop by one step (admit, iterate, retire); returns the
- * number of active slots after the step */
+/* advance the device loop by one step: one PSO step of every occupied slot
+ * (finished swarms are refitted in the same step), admission of queued
+ * requests into free slots (while the step runs on the device; the new
+ * slots join the next step, except that an idle server admits first) and
+ * retirement of the finished requests; returns the number of active slots
+ * after the step */
 int pasta_server_step(pasta_server *s);
 /* collect up to max finished results (non-blocking) */
 int pasta_server_poll(pasta_server *s, int64_t *ids, pasta_fit_result *results,

@@ -745,6 +745,8 @@ void ensure_workspace(pasta_grid *g, int64_t E, int64_t max_nobs) {
   const int64_t need = std::max<int64_t>(g->stride, (max_nobs + 63) / 64 * 64);
   const int64_t stride = std::max(need, g->ws.stride);  // rows never shrink
   const int bstr = bnd_stride_for((int)g->npx);
+  // enough already (no device-memory query on this path: it runs every step)
+  if (g->ws.cap >= std::max<int64_t>(E, 1) && g->ws.stride == stride && g->ws.bnd_stride == bstr) return;
   const int64_t want = workspace_cap(g, E, stride);
   if (g->ws.cap >= want && g->ws.stride == stride && g->ws.bnd_stride == bstr) return;
   g->ws.ensure(want, stride, bstr);
@@ -2315,50 +2317,58 @@ int pasta_server_step(pasta_server *sv) {
     int needP = sv->Pmax;
     for (auto &r : sv->queue) needP = std::max(needP, r.st.num_particles);
     if (needP != sv->Pmax && !any_active) server_rebuild(sv, needP);
-    // admit queued requests into free slots within the HBM budget
+    // admit queued requests into free slots within the HBM budget: the
+    // slot state is uploaded on the stream (pageable sources are staged
+    // when the copies are issued)
     std::vector<int> admitted;
-    for (int i = 0; i < sv->slots && !sv->queue.empty(); i++) {
-      if (sv->slot_req[i]) continue;
-      auto &r = sv->queue.front();
-      if (r.st.num_particles > sv->Pmax) break;
-      if (sv->used + r.bytes > sv->budget && any_active) break;
-      std::unique_ptr<pasta_server::Req> rp(new pasta_server::Req(std::move(r)));
-      sv->queue.pop_front();
-      sv->used += rp->bytes;
-      // the slot's spectrum buffers are kept between requests and grow only
-      // for a longer spectrum (no allocation or free in the steady state)
-      const size_t nobs = rp->flux.size();
-      if (!sv->slot_flux[i] || sv->slot_flux[i]->n < nobs) {
-        sv->slot_flux[i].reset(new DBuf<float>());
-        sv->slot_var[i].reset(new DBuf<float>());
-        sv->slot_flux[i]->alloc(nobs);
-        sv->slot_var[i]->alloc(nobs);
+    auto admit = [&]() {
+      for (int i = 0; i < sv->slots && !sv->queue.empty(); i++) {
+        if (sv->slot_req[i]) continue;
+        auto &r = sv->queue.front();
+        if (r.st.num_particles > sv->Pmax) break;
+        if (sv->used + r.bytes > sv->budget && any_active) break;
+        std::unique_ptr<pasta_server::Req> rp(new pasta_server::Req(std::move(r)));
+        sv->queue.pop_front();
+        sv->used += rp->bytes;
+        // the slot's spectrum buffers are kept between requests and grow only
+        // for a longer spectrum (no allocation or free in the steady state)
+        const size_t nobs = rp->flux.size();
+        if (!sv->slot_flux[i] || sv->slot_flux[i]->n < nobs) {
+          sv->slot_flux[i].reset(new DBuf<float>());
+          sv->slot_var[i].reset(new DBuf<float>());
+          sv->slot_flux[i]->alloc(nobs);
+          sv->slot_var[i]->alloc(nobs);
+        }
+        CK(cudaMemcpyAsync(sv->slot_flux[i]->p, rp->flux.data(), nobs * sizeof(float), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->slot_var[i]->p, rp->var.data(), nobs * sizeof(float), cudaMemcpyHostToDevice, s));
+        sv->hstars[i] = make_star(rp->d, rp->c, sv->slot_flux[i]->p, sv->slot_var[i]->p, (int64_t)nobs);
+        PsoParams P = make_pso_params(g, rp->st);
+        sv->pp[i] = P;
+        sv->max_m = std::max(sv->max_m, width_upper_bound(g, P.mx[3]));
+        std::vector<double> x((size_t)sv->Pmax * 5, 0.0), v((size_t)sv->Pmax * 5, 0.0);
+        int st = init_swarm_host(g, P, rp->seed, x.data(), v.data());
+        const size_t base = (size_t)i * sv->Pmax * 5;
+        CK(cudaMemcpyAsync(sv->W.x.p + base, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->W.v.p + base, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        int one = 1, zero = 0, m1 = -1, done0 = st ? 1 : 0;
+        uint64_t sd = rp->seed;
+        CK(cudaMemcpyAsync(sv->W.active.p + i, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->W.done.p + i, &done0, sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->W.status.p + i, st ? &st : &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->W.iter.p + i, &m1, sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->W.seed.p + i, &sd, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->W.params.p + i, &P, sizeof(PsoParams), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(sv->dstars.p + i, &sv->hstars[i], sizeof(DevStar), cudaMemcpyHostToDevice, s));
+        // pageable sources are staged when the copies are issued; the step's
+        // launches follow on the same stream
+        sv->slot_req[i] = std::move(rp);
+        admitted.push_back(i);
       }
-      CK(cudaMemcpyAsync(sv->slot_flux[i]->p, rp->flux.data(), nobs * sizeof(float), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->slot_var[i]->p, rp->var.data(), nobs * sizeof(float), cudaMemcpyHostToDevice, s));
-      sv->hstars[i] = make_star(rp->d, rp->c, sv->slot_flux[i]->p, sv->slot_var[i]->p, (int64_t)nobs);
-      PsoParams P = make_pso_params(g, rp->st);
-      sv->pp[i] = P;
-      sv->max_m = std::max(sv->max_m, width_upper_bound(g, P.mx[3]));
-      std::vector<double> x((size_t)sv->Pmax * 5, 0.0), v((size_t)sv->Pmax * 5, 0.0);
-      int st = init_swarm_host(g, P, rp->seed, x.data(), v.data());
-      const size_t base = (size_t)i * sv->Pmax * 5;
-      CK(cudaMemcpyAsync(sv->W.x.p + base, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->W.v.p + base, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-      int one = 1, zero = 0, m1 = -1, done0 = st ? 1 : 0;
-      uint64_t sd = rp->seed;
-      CK(cudaMemcpyAsync(sv->W.active.p + i, &one, sizeof(int), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->W.done.p + i, &done0, sizeof(int), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->W.status.p + i, st ? &st : &zero, sizeof(int), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->W.iter.p + i, &m1, sizeof(int), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->W.seed.p + i, &sd, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->W.params.p + i, &P, sizeof(PsoParams), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(sv->dstars.p + i, &sv->hstars[i], sizeof(DevStar), cudaMemcpyHostToDevice, s));
-      // pageable sources are staged when the copies are issued; the step's
-      // launches follow on the same stream
-      sv->slot_req[i] = std::move(rp);
-      admitted.push_back(i);
-    }
+    };
+    // an idle server admits before its launch; a busy one after it, so the
+    // host work overlaps the step on the device and the new slots join the
+    // next step
+    if (!any_active) admit();
     bool any = false;
     for (int i = 0; i < sv->slots; i++) any |= (bool)sv->slot_req[i];
     if (!any) return;
@@ -2431,6 +2441,7 @@ int pasta_server_step(pasta_server *sv) {
     for (int i = 0; i < sv->slots; i++)
       if (sv->slot_req[i]) sv->evals_total += sv->slot_req[i]->st.num_particles;
     sv->steps_total++;
+    if (any_active) admit();
     // the step's flags and every slot's best (small) in one wait
     std::vector<int> done(sv->slots), status(sv->slots);
     std::vector<double> gx((size_t)sv->slots * 5), gc(sv->slots);
