@@ -53,10 +53,11 @@ PATH_BYTES_PER_WIN_PX, PATH_BYTES_PER_OBS = 128, 8
 # nominal FP32 CUDA-core peak of a B200: 148 SMs x 128 FMA/clk x 2 flops x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # DRAM bytes per evaluation measured by ncu at full size (dram__bytes_read.sum +
-# dram__bytes_write.sum, one launch of 65,536 evaluations; profiles/dram_batched_fit_1024stars.md)
-# (first evaluation step; k_broaden includes its block-bound search, chi2 the
-# resampling left over and both chunk kernels)
-DRAM_BYTES_PER_EVAL = {"k_interp": 710111, "k_broaden": 636944 + 4757, "chi2": 163697 + 149357 + 128}
+# dram__bytes_write.sum of one mid-fit step of 65,536 evaluations;
+# profiles/step_launches_dram_1024stars.md): k_broaden includes its
+# block-bound search, chi2 both chunk kernels, the leftover resampling and
+# the final sums
+DRAM_BYTES_PER_EVAL = {"k_interp": 481230, "k_broaden": 608154 + 921, "chi2": 163516 + 149386 + 128 + 259}
 
 
 def log(*a):
@@ -232,6 +233,18 @@ def run_ours(args):
     settings = P.PSOSettings(PARTICLES, ITERS)
     seeds = [int(7 + 100003 * rank + i) for i in range(n_stars)]
     log(f"[rank {rank}] {n_stars} stars in {time.time() - t:.1f}s")
+    if args.stages_only:
+        # one mid-fit step run stage by stage inside an NVTX range "stages"
+        # (what ncu --nvtx --nvtx-include "stages/" captures)
+        b = P.BatchFit(interp, disps, conts, settings, [s.flux for s in stars], [s.var for s in stars],
+                       (0.0, 300.0), (-150.0, 150.0), seeds=seeds)
+        b.step(ITERS // 2)
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_push("stages")
+        st = b.profile_step()
+        torch.cuda.nvtx.range_pop()
+        b.finish()
+        return {"stages_only": True, "stars": n_stars, "stage": st} if rank == 0 else None
 
     fl = [s.flux for s in stars]
     vr = [s.var for s in stars]
@@ -508,6 +521,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=30.0, help="served latency run: arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=300, help="served latency run: requests (0: skip)")
+    ap.add_argument("--stages-only", action="store_true",
+                    help="profiling aid: one mid-fit batched step, stage by stage, in an NVTX range 'stages'")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
