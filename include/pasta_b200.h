@@ -132,6 +132,16 @@ int pasta_dispersion_destroy(pasta_dispersion *d);
 /* PyWavelengthDispersion.convolve (lib.rs:671-680): in/out n = synth n */
 int pasta_dispersion_convolve(const pasta_dispersion *d, const float *in,
                               int64_t n, float *out);
+/* The arithmetic of PyWavelengthDispersion.convolve_and_resample_directory
+ * (lib.rs:686-755) for M grid spectra at once: each row of in [M x n_in]
+ * (dequantised flux on the input wavelength grid in_kind/in_a/in_b, which
+ * has the dispersion's synth length) is convolved with the dispersion's
+ * instrument profile and resampled at RV 0 to its observed wavelengths,
+ * out [M x n_obs] (shift_and_resample, convolve_rv.rs:532-604).  Linspace
+ * and Logspace input grids; a non-uniform one is PASTA_E_UNSUPPORTED. */
+int pasta_dispersion_convolve_resample(const pasta_dispersion *d, int in_kind,
+                                       double in_a, double in_b, int64_t n_in,
+                                       const float *in, int64_t M, float *out);
 /* kernel width (odd) and, if out != NULL, the kernels width x n_synth
  * row-major as get_kernels returns them (lib.rs:1043-1060) */
 int pasta_dispersion_kernels(const pasta_dispersion *d, int64_t *width,

@@ -52,6 +52,7 @@ SIGNATURES = {
     "pasta_dispersion_destroy": (I, [P]),
     "pasta_dispersion_convolve": (I, [P, P, I64, P]),
     "pasta_dispersion_kernels": (I, [P, P, P]),
+    "pasta_dispersion_convolve_resample": (I, [P, I, D, D, I64, P, I64, P]),
     "pasta_continuum_create": (I, [I, P, I64, I, I, D, P, I, P, I, P]),
     "pasta_continuum_destroy": (I, [P]),
     "pasta_continuum_nparams": (I, [P]),

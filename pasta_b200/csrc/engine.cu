@@ -1882,6 +1882,54 @@ int pasta_dispersion_convolve(const pasta_dispersion *d, const float *in, int64_
   });
 }
 
+int pasta_dispersion_convolve_resample(const pasta_dispersion *d, int in_kind, double in_a, double in_b,
+                                       int64_t n_in, const float *in, int64_t M, float *out) {
+  return guard([&] {
+    if (!d || !in || !out || M < 0) fail(PASTA_E_ARG, "dispersion, input and output are required");
+    if (M == 0) return;
+    if (n_in != d->synth_n)
+      fail(PASTA_E_ARG, "flux_arr and wavelength grid don't match. flux_arr: %lld, synth_wl: %lld", (long long)n_in,
+           (long long)d->synth_n);
+    if (in_kind != WL_LOG && in_kind != WL_LIN)
+      fail(PASTA_E_UNSUPPORTED, "resampling from a non-uniform input wavelength grid is not supported");
+    // the range checks of shift_and_resample at RV 0 (convolve_rv.rs:548-567);
+    // WlGrid::get_first_and_last ends one step past the last pixel (interpolate.rs:695-698)
+    const double first = in_kind == WL_LOG ? std::pow(10.0, in_a) : in_a;
+    const double last = in_kind == WL_LOG ? std::pow(10.0, in_a + in_b * (double)n_in) : in_a + in_b * (double)n_in;
+    if (d->wl.front() < first)
+      fail(PASTA_E_RV_RANGE, "Observed wavelength is smaller than synthetic wavelength (RV=0, %.1f < %.1f)",
+           d->wl.front(), first);
+    if (d->wl.back() > last)
+      fail(PASTA_E_RV_RANGE, "Observed wavelength is larger than synthetic wavelength (RV=0, %.1f > %.1f)",
+           d->wl.back(), last);
+    // the reference reads pixel floor(index) + 1 (an index panic past the end)
+    if (std::floor(d->fidx_max) + 1.0 >= (double)n_in) fail(PASTA_E_RESAMPLE, "resampling index out of range");
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    DevStar st = make_star(d, nullptr, nullptr, nullptr, (int64_t)d->wl.size());
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    const int64_t nobs = (int64_t)d->wl.size();
+    // spectra per launch: device buffers of about 1 GB
+    const int64_t per = (2 * n_in + nobs) * (int64_t)sizeof(float);
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(M, (1ll << 30) / per));
+    DBuf<float> di, dc, dout;
+    di.alloc((size_t)chunk * n_in);
+    dc.alloc((size_t)chunk * n_in);
+    dout.alloc((size_t)chunk * nobs);
+    for (int64_t m0 = 0; m0 < M; m0 += chunk) {
+      const int64_t k = std::min(chunk, M - m0);
+      CK(cudaMemcpyAsync(di.p, in + (size_t)m0 * n_in, (size_t)k * n_in * sizeof(float), cudaMemcpyHostToDevice, s));
+      launch_gauss_batch((int)n_in, ds.p, di.p, dc.p, (int)k, s);
+      launch_resample_rows((int)n_in, in_kind, ds.p, (int)nobs, dc.p, dout.p, (int)k, s);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(out + (size_t)m0 * nobs, dout.p, (size_t)k * nobs * sizeof(float), cudaMemcpyDeviceToHost,
+                         s));
+      CK(cudaStreamSynchronize(s));
+    }
+  });
+}
+
 // ------------------------------------------------------------- fit
 static int fit_common(const pasta_grid *gc, std::vector<StarInput> &in, int mode, pasta_fit_result *results,
                       float *const *params, double *trace) {

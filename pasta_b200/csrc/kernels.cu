@@ -763,9 +763,9 @@ void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
 }
 
 // standalone PyWavelengthDispersion.convolve (lib.rs:671-680): in -> out, all pixels
-__global__ void __launch_bounds__(GT) k_gauss_alone(int N, const DevStar *stp, const float *in, float *out) {
+// tile blockIdx.x of one spectrum: in -> out, all pixels
+__device__ __forceinline__ void k_gauss_alone_body(int N, const DevStar &st, const float *in, float *out) {
   __shared__ float sbuf[G_TILE + 2 * G_HMAX];
-  const DevStar &st = *stp;
   const int t0 = blockIdx.x * G_TILE, t1 = min(t0 + G_TILE, N);
   if (st.disp_kind == DISP_NONE) {
     for (int i = t0 + threadIdx.x; i < t1; i += blockDim.x) out[i] = in[i];
@@ -780,6 +780,45 @@ __global__ void __launch_bounds__(GT) k_gauss_alone(int N, const DevStar *stp, c
   for (int i = t0 + threadIdx.x; i < t1; i += blockDim.x)
     out[i] = instrument(st, N, i, h, [&](int t) { return sbuf[t - base]; });
 }
+__global__ void __launch_bounds__(GT) k_gauss_alone(int N, const DevStar *stp, const float *in, float *out) {
+  k_gauss_alone_body(N, *stp, in, out);
+}
+// M spectra of N pixels at once: grid y = spectrum
+__global__ void __launch_bounds__(GT) k_gauss_batch(int N, const DevStar *stp, const float *in, float *out) {
+  const size_t off = (size_t)blockIdx.y * N;
+  k_gauss_alone_body(N, *stp, in + off, out + off);
+}
+void launch_gauss_batch(int N, const DevStar *star, const float *in, float *out, int M, cudaStream_t s) {
+  if (M <= 0 || N <= 0) return;
+  k_gauss_batch<<<dim3((N + G_TILE - 1) / G_TILE, M), GT, 0, s>>>(N, star, in, out);
+  count_launch();
+}
+
+// shift_and_resample at RV 0 (convolve_rv.rs:532-604) of M rows of N synth
+// pixels to the star's observed pixels: out [M][n_obs]
+__global__ void k_resample_rows(int N, int kind, const DevStar *stp, const float *in, float *out) {
+  const DevStar &st = *stp;
+  Resampler R;
+  R.s = in + (size_t)blockIdx.y * N;
+  R.N = N;
+  R.kind = kind;
+  R.shift_log = 0.0;
+  R.shift_factor = 1.0;
+  R.lin_offset = 0.0;
+  R.fidx = st.fidx;
+  R.wl_obs = st.wl_obs;
+  R.wl_vals = nullptr;
+  R.given = nullptr;
+  float *o = out + (size_t)blockIdx.y * st.n_obs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n_obs; i += gridDim.x * blockDim.x) o[i] = R(i);
+}
+void launch_resample_rows(int N, int kind, const DevStar *star, int n_obs, const float *in, float *out, int M,
+                          cudaStream_t s) {
+  if (M <= 0 || n_obs <= 0) return;
+  k_resample_rows<<<dim3((n_obs + 255) / 256, M), 256, 0, s>>>(N, kind, star, in, out);
+  count_launch();
+}
+
 void launch_gauss_standalone(const DevGrid &G, const DevStar *star, const float *in, float *out, cudaStream_t s) {
   k_gauss_alone<<<(G.npx + G_TILE - 1) / G_TILE, GT, 0, s>>>(G.npx, star, in, out);
   count_launch();

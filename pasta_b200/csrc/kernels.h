@@ -95,6 +95,11 @@ void launch_copy_broadened(const DevGrid &G, const EvalBatch &b, float *out, cud
 void launch_build_chunk(const DevStar *star, const double *coef, int n, float *out, cudaStream_t s);
 void launch_gauss_standalone(const DevGrid &G, const DevStar *star, const float *in, float *out,
                              cudaStream_t s);
+// instrument profile of M spectra of N pixels: in, out [M][N]
+void launch_gauss_batch(int N, const DevStar *star, const float *in, float *out, int M, cudaStream_t s);
+// resampling at RV 0 of M rows of N synth pixels (grid kind WL_*) to the star's n_obs observed pixels
+void launch_resample_rows(int N, int kind, const DevStar *star, int n_obs, const float *in, float *out, int M,
+                          cudaStream_t s);
 
 // swarm state of S stars x Pmax particles (structure of arrays)
 struct Swarm {

@@ -181,6 +181,44 @@ class PyWavelengthDispersion:
     def wavelength(self) -> list:
         return list(self.wl)
 
+    def convolve_and_resample_spectra(self, spectra, input_wavelength: WlGrid) -> np.ndarray:
+        """Instrument broadening and resampling at RV 0 to this dispersion's
+        wavelengths of many dequantised grid spectra at once (M x n_synth -> M x n_obs)."""
+        x = np.ascontiguousarray(np.atleast_2d(spectra), dtype=np.float32)
+        out = np.empty((x.shape[0], len(self.wl)), np.float32)
+        k, a, b, n, _ = input_wavelength._c()
+        check(lib().pasta_dispersion_convolve_resample(self._h, k, a, b, x.shape[1], ptr(x), x.shape[0], ptr(out)))
+        return out
+
+    def convolve_and_resample_directory(self, input_directory: str, output_directory: str, includes_factor: bool,
+                                        input_wavelength: WlGrid, batch: int = 256) -> None:
+        """Pre-convolve a grid directory (lib.rs:686-755): every model file is
+        convolved with this dispersion and resampled to its wavelengths, then
+        written under the same name, requantised to uint16 (with the f32
+        maximum prefix when includes_factor).  Existing outputs are kept.
+        The arithmetic runs on the GPU, ``batch`` files per launch."""
+        files = sorted(os.listdir(input_directory))
+        todo = [f for f in files if not os.path.exists(os.path.join(output_directory, f))]
+        for i0 in range(0, len(todo), batch):
+            names = todo[i0:i0 + batch]
+            rows, facs = [], []
+            for name in names:
+                arr = np.load(os.path.join(input_directory, name))
+                u, mx = _split_factor(arr, includes_factor)
+                x = u.astype(np.float32) / np.float32(65535.0)
+                if includes_factor:
+                    x = x * np.float32(mx)
+                rows.append(x)
+            res = self.convolve_and_resample_spectra(np.stack(rows), input_wavelength)
+            for name, r in zip(names, res):
+                if includes_factor:
+                    mx = np.float32(r.max())
+                    q = _as_u16(np.maximum(r, np.float32(0.0)) / mx * np.float32(65535.0))
+                    out = np.concatenate([np.frombuffer(mx.astype("<f4").tobytes(), dtype="<u2"), q])
+                else:
+                    out = _as_u16(np.clip(r, np.float32(0.0), np.float32(1.0)) * np.float32(65535.0))
+                np.save(os.path.join(output_directory, name), out.astype(np.uint16))
+
     def kernels(self) -> np.ndarray:
         w = C.c_int64()
         check(lib().pasta_dispersion_kernels(self._h, C.byref(w), None))
@@ -373,6 +411,12 @@ def _label_from_filename(filename: str):
         raise ValueError("Invalid filename: %s" % filename)
     sign = -1.0 if parts[0].startswith("lm") else 1.0
     return float(parts[1]), sign * float(parts[0][2:]) / 100.0, float(parts[2]) / 100.0
+
+
+def _as_u16(x: np.ndarray) -> np.ndarray:
+    """Rust's `f32 as u16`: truncation toward zero, saturating at 0 and 65535, NaN -> 0."""
+    x = np.nan_to_num(np.asarray(x, np.float32), nan=0.0, posinf=65535.0, neginf=0.0)
+    return np.trunc(np.clip(x, 0.0, 65535.0)).astype(np.uint16)
 
 
 def _split_factor(arr: np.ndarray, includes_factor: bool):

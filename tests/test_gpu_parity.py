@@ -8,6 +8,8 @@ Tolerances (stated per test):
 * seeded PSO replay: vs the oracle on the same draw stream, dTeff <= 1 K,
   d[M/H], dlogg <= 1e-3, dvsini, dRV <= 0.01 km/s.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -296,3 +298,49 @@ def test_grouped_interpolation_is_each_label_alone(env):
     od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
     for i in (0, 4, 9):
         assert relmax(bulk[i], od.produce_model(lab[i], O.F32)) <= FLUX_TOL
+
+
+def _resample_rv0(x, wl_obs, log_first, log_step):
+    """shift_and_resample at RV 0 on a Logspace grid (convolve_rv.rs:569-590), numpy."""
+    idx = (np.log10(wl_obs) - log_first) / log_step
+    j = np.floor(idx).astype(np.int64)
+    w = idx.astype(np.float32) - j.astype(np.float32)
+    x = np.asarray(x, np.float32)
+    return (np.float32(1.0) - w) * x[j] + w * x[j + 1]
+
+
+def test_convolve_and_resample_directory(env, tmp_path):
+    """Grid pre-convolution (lib.rs:686-755) with and without the f32 maximum prefix."""
+    O, P, S, star = env["O"], env["P"], env["S"], env["star"]
+    spec = env["spec"]
+    labels, spectra = env["labels"][:3], env["spectra"][:3]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    for with_factor in (False, True):
+        src, dst = tmp_path / ("in%d" % with_factor), tmp_path / ("out%d" % with_factor)
+        os.makedirs(dst)
+        maxima = np.array([1.5, 0.8, 2.25], np.float32) if with_factor else None
+        S.write_grid_dir(str(src), labels, spectra, maxima)
+        d.convolve_and_resample_directory(str(src), str(dst), with_factor, env["wl"])
+        for i, (t, m, g) in enumerate(labels):
+            name = S.filename_from_labels(t, m, g)
+            got = np.load(os.path.join(dst, name))
+            x = spectra[i].astype(np.float32) / np.float32(65535.0)
+            if with_factor:
+                x = x * maxima[i]
+            ref = _resample_rv0(od.convolve(x, O.F32), star.wl, spec.log_first, spec.log_step).astype(np.float32)
+            assert relmax(d.convolve_and_resample_spectra(x[None], env["wl"])[0], ref) <= FLUX_TOL
+            if with_factor:
+                mx = np.frombuffer(got[:2].tobytes(), dtype="<f4")[0]
+                assert abs(mx - ref.max()) <= 1e-5 * ref.max()
+                expect = np.trunc(np.maximum(ref, 0) / ref.max() * np.float32(65535.0))
+                body = got[2:]
+            else:
+                expect = np.trunc(np.clip(ref, 0, 1) * np.float32(65535.0))
+                body = got
+            assert body.dtype == np.uint16 and len(body) == len(star.wl)
+            assert np.abs(body.astype(np.int64) - expect.astype(np.int64)).max() <= 2
+        # existing outputs are kept
+        before = os.path.getmtime(os.path.join(dst, S.filename_from_labels(*labels[0])))
+        d.convolve_and_resample_directory(str(src), str(dst), with_factor, env["wl"])
+        assert os.path.getmtime(os.path.join(dst, S.filename_from_labels(*labels[0]))) == before

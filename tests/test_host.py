@@ -150,3 +150,10 @@ def test_replica_sharding_over_two_gloo_ranks(tmp_path):
     outs = [p.communicate(timeout=120)[0] for p in procs]
     assert all(p.returncode == 0 for p in procs), outs
     assert "OK" in outs[0]
+
+
+def test_rust_style_u16_cast():
+    """`f32 as u16` truncates toward zero and saturates; NaN becomes 0."""
+    from pasta_b200.pasta import _as_u16
+    x = np.array([-3.0, 0.0, 0.99, 1.0, 65534.9, 65535.0, 70000.0, np.nan, np.inf], np.float32)
+    np.testing.assert_array_equal(_as_u16(x), [0, 0, 0, 1, 65534, 65535, 65535, 0, 65535])
