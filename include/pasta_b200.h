@@ -316,6 +316,65 @@ int pasta_server_run(pasta_server *s, int steps, double *device_ms);
  * the final refits. */
 int pasta_server_stats(const pasta_server *s, int64_t *out7);
 
+/* ---------------------------------------------------------- binaries
+ * A binary label is star 1 (teff, m, logg, vsini, rv), star 2 (the same)
+ * and the light ratio: 11 doubles.  cont_grid is the interpolator of the
+ * unnormalised models that supplies each star's continuum; it must have the
+ * same number of pixels as g (the reference indexes both with the same
+ * synthetic pixel). */
+
+/* Interpolator::interpolate_linear (interpolate.rs:985-1028; lib.rs:1127):
+ * labels L x 3 (teff, m, logg), out L x n_synth. */
+int pasta_interpolate_linear(const pasta_grid *g, const double *tml,
+                             int64_t L, float *out, int32_t *status);
+/* Interpolator::produce_binary_model_norm (interpolate.rs:822-893,
+ * convolve_rv.rs:606-700; lib.rs:1019-1041): labels L x 11, out L x n_obs. */
+int pasta_binary_model(const pasta_grid *g, const pasta_grid *cont_grid,
+                       const pasta_dispersion *d, const double *labels,
+                       int64_t L, float *out, int32_t *status);
+/* BinaryFitter::chi2 via BinaryCostFunction::cost (fitting.rs:584-600,
+ * 699-717; lib.rs:1673-1698): out[L] chi2 (NaN where status != 0). */
+int pasta_binary_chi2(const pasta_grid *g, const pasta_grid *cont_grid,
+                      const pasta_dispersion *d, const pasta_continuum *c,
+                      const float *flux, const float *var, int64_t n,
+                      const double *labels, int64_t L, double *out,
+                      int32_t *status);
+
+typedef struct {
+  int32_t num_particles;
+  int32_t max_iters;
+  double inertia_factor, cognitive_factor, social_factor, delta;
+  double vsini_lo, vsini_hi, rv_lo, rv_hi;
+  /* per-parameter constraint over the 11 binary parameters:
+   * 0 none, 1 fixed at a, 2 range [a, b] (lib.rs:817-835) */
+  int32_t ckind[11];
+  double ca[11], cb[11];
+} pasta_binary_settings;
+
+typedef struct {
+  double label1[5], label2[5];
+  double light_ratio;
+  double chi2;
+  double time;     /* seconds */
+  int32_t iterations;
+  int32_t status;  /* 0 ok, else PASTA_E_* of the failing particle */
+  int32_t n_params;
+  int32_t _pad;
+} pasta_binary_result;
+
+/* BinaryFitter::fit (fitting.rs:633-697; lib.rs:1636-1671): particle swarm
+ * over the 11 parameters with the light ratio in (0, 1), on the draw stream
+ * of `seed` (the single-star phases, dimensions 0..10).  Every particle of
+ * an iteration is evaluated in one batch on the device.  params receives
+ * pasta_continuum_nparams(c) floats (or is NULL); trace (or NULL) receives
+ * (max_iters + 1) x num_particles x 12 doubles (position, cost). */
+int pasta_binary_fit(const pasta_grid *g, const pasta_grid *cont_grid,
+                     const pasta_dispersion *d, const pasta_continuum *c,
+                     const pasta_binary_settings *settings,
+                     const float *flux, const float *var, int64_t n,
+                     uint64_t seed, pasta_binary_result *result,
+                     float *params, double *trace);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,20 @@ class FitResult(C.Structure):
                 ("status", C.c_int), ("n_params", C.c_int), ("params", C.c_double * 512)]
 
 
+class BinarySettings(C.Structure):
+    _fields_ = [("num_particles", C.c_int), ("max_iters", C.c_int), ("inertia", C.c_double),
+                ("cognitive", C.c_double), ("social", C.c_double), ("delta", C.c_double),
+                ("vsini_lo", C.c_double), ("vsini_hi", C.c_double), ("rv_lo", C.c_double),
+                ("rv_hi", C.c_double), ("ckind", C.c_int * 11), ("ca", C.c_double * 11),
+                ("cb", C.c_double * 11)]
+
+
+class BinaryResult(C.Structure):
+    _fields_ = [("label1", C.c_double * 5), ("label2", C.c_double * 5), ("light_ratio", C.c_double),
+                ("chi2", C.c_double), ("iterations", C.c_int), ("status", C.c_int), ("n_params", C.c_int),
+                ("params", C.c_double * 512)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -76,6 +90,11 @@ def lib():
             "or_chi2": (i, [P, P, P, i, P, P, i64, P, i64, P, P, i]),
             "or_fit": (i, [P, P, P, i, P, P, P, i64, i64, P, i, i, P, P]),
             "or_draw_u01": (d, [C.c_uint64] * 5),
+            "or_local_grid_linear": (i, [P, d, d, d, P, P]),
+            "or_interpolate_linear": (i, [P, i, d, d, d, P]),
+            "or_binary_model": (i, [P, P, P, i, P, P]),
+            "or_binary_chi2": (i, [P, P, P, P, i, P, P, i64, P, i64, P, P, i]),
+            "or_binary_fit": (i, [P, P, P, P, i, P, P, P, i64, C.c_uint64, i, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(_lib, name)
@@ -134,6 +153,19 @@ class Grid:
     def interpolate(self, t, m, g, prec=F32):
         out = np.zeros(self.npx)
         if lib().or_interpolate(self.h, prec, t, m, g, _p(out)):
+            raise _err()
+        return out
+
+    def local_grid_linear(self, t, m, g):
+        cols = np.zeros(8, dtype=np.int64)
+        w = np.zeros(8)
+        if lib().or_local_grid_linear(self.h, t, m, g, _p(cols), _p(w)):
+            raise _err()
+        return cols, w
+
+    def interpolate_linear(self, t, m, g, prec=F32):
+        out = np.zeros(self.npx)
+        if lib().or_interpolate_linear(self.h, prec, t, m, g, _p(out)):
             raise _err()
         return out
 
@@ -371,3 +403,57 @@ def compute_uncertainty(grid, disp, cont, flux, var, spec_res, label, search_rad
                 pair.append(None)
         res[i] = tuple(pair)
     return res
+
+
+# ------------------------------------------------------------------ binaries
+def binary_model(grid, cont_grid, disp, lab, prec=F32):
+    """produce_binary_model_norm (interpolate.rs:868): lab = star 1 [5],
+    star 2 [5], light ratio."""
+    lab = np.ascontiguousarray(lab, dtype=np.float64)
+    out = np.zeros(len(disp.wl))
+    if lib().or_binary_model(grid.h, cont_grid.h, disp.h, prec, _p(lab), _p(out)):
+        raise _err()
+    return out
+
+
+def binary_chi2(grid, cont_grid, disp, cont, flux, var, labels, prec=F32, nthreads=0):
+    flux = np.ascontiguousarray(flux, dtype=np.float32)
+    var = np.ascontiguousarray(var, dtype=np.float32)
+    labels = np.ascontiguousarray(np.atleast_2d(labels), dtype=np.float64)
+    out = np.zeros(len(labels))
+    st = np.zeros(len(labels), dtype=np.int32)
+    nt = nthreads or os.cpu_count()
+    if lib().or_binary_chi2(grid.h, cont_grid.h, disp.h, cont.h, prec, _p(flux), _p(var), len(flux),
+                            _p(labels), len(labels), _p(out), _p(st), nt):
+        raise _err()
+    return out, st
+
+
+def binary_settings(num_particles, max_iters, vsini_range, rv_range, inertia=0.7213475204,
+                    cognitive=1.1931471806, social=1.1931471806, delta=1e-7, constraints=()):
+    s = BinarySettings()
+    s.num_particles, s.max_iters = num_particles, max_iters
+    s.inertia, s.cognitive, s.social, s.delta = inertia, cognitive, social, delta
+    s.vsini_lo, s.vsini_hi = vsini_range
+    s.rv_lo, s.rv_hi = rv_range
+    for (idx, kind, a, b) in constraints:
+        s.ckind[idx], s.ca[idx], s.cb[idx] = kind, a, b
+    return s
+
+
+def binary_fit(grid, cont_grid, disp, cont, st, flux, var, seed, prec=F32, nthreads=0, trace=False):
+    """BinaryFitter::fit (fitting.rs:633-697) on the shared draw stream."""
+    flux = np.ascontiguousarray(flux, dtype=np.float32)
+    var = np.ascontiguousarray(var, dtype=np.float32)
+    res = BinaryResult()
+    tr = np.zeros((st.max_iters + 1, st.num_particles, 12)) if trace else None
+    nt = nthreads or os.cpu_count()
+    rc = lib().or_binary_fit(grid.h, cont_grid.h, disp.h, cont.h, prec, C.byref(st), _p(flux), _p(var),
+                             len(flux), seed, nt, C.byref(res), _p(tr))
+    out = dict(label1=np.array(res.label1[:]), label2=np.array(res.label2[:]), light_ratio=res.light_ratio,
+               chi2=res.chi2, iterations=res.iterations, status=res.status,
+               params=np.array(res.params[:res.n_params]),
+               error=lib().or_last_error().decode() if rc else "")
+    if trace:
+        return out, rc, tr
+    return out, rc

@@ -327,6 +327,94 @@ std::vector<T> interpolate(const OGrid &g, double t, double mm, double lg) {
   return out;
 }
 
+// Range::find_neighbors_linear (interpolate.rs:161-213): the two grid points
+// around x.  A grid point at the right limit takes its left partner; a right
+// limit at index 0 has none (the reference's usize subtraction panics).
+void find_neighbors_linear(const Range &r, double x, int left, int right, int out[2]) {
+  auto s = r.search(x);
+  int i = s.second;
+  if (s.first) {
+    if (i < left) fail("Index %d out of left bound, x=%g", i, x);
+    if (i > right) fail("Index %d out of right bound, x=%g", i, x);
+    if (i == right) {
+      if (i == 0) fail("no left neighbour for x=%g", x);
+      out[0] = i - 1; out[1] = i;
+    } else {
+      out[0] = i; out[1] = i + 1;
+    }
+  } else {
+    if (i <= left) fail("Index %d out of left bound, x=%g", i, x);
+    if (i > right) fail("Index %d out of right bound, x=%g", i, x);
+    out[0] = i - 1; out[1] = i;
+  }
+}
+
+// Grid::get_local_grid_linear (interpolate.rs:536-600) and
+// calculate_interpolation_coefficients_linear (cubic.rs:6-10, 246-270):
+// the 2 x 2 x 2 cube around the label, teff outer, logg middle, [M/H] inner,
+// weights (a * b * c) in f64 before the f32 cast.  A (teff, logg) corner
+// outside that teff's logg limits has no model; the reference would read a
+// neighbouring column there, the oracle stops.
+void local_grid_linear(const OGrid &g, double t, double mm, double lg, int64_t cols[8], double w64[8]) {
+  if (t != t || mm != mm || lg != lg) fail("NaN label");
+  if (!g.teff_logg_ok(t, lg)) fail("Teff, logg out of bounds (%g, %g)", t, lg);
+  if (!g.m_ok(mm)) fail("M out of bounds (%g)", mm);
+  auto tl = g.teff_index_limits_at(lg);
+  auto ll = g.logg_index_limits_at(t);
+  int tn[2], mn[2], ln[2];
+  find_neighbors_linear(g.teff, t, tl.first, tl.second, tn);
+  find_neighbors_linear(g.m, mm, 0, g.m.n() - 1, mn);
+  find_neighbors_linear(g.logg, lg, ll.first, ll.second, ln);
+  auto lin = [](double x, double x0, double x1, double f[2]) {  // cubic.rs:6-10
+    f[0] = (x - x1) / (x0 - x1);
+    f[1] = (x - x0) / (x1 - x0);
+  };
+  double ft[2], fl[2], fm[2];
+  lin(t, g.teff.v[tn[0]], g.teff.v[tn[1]], ft);
+  lin(lg, g.logg.v[ln[0]], g.logg.v[ln[1]], fl);
+  lin(mm, g.m.v[mn[0]], g.m.v[mn[1]], fm);
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      auto lim = g.logg_limits[tn[a]];
+      if (ln[b] < lim.first || ln[b] > lim.second)
+        fail("no model at teff index %d, logg index %d", tn[a], ln[b]);
+      for (int c = 0; c < 2; c++) {
+        const int idx = (a * 2 + b) * 2 + c;
+        w64[idx] = ft[a] * fl[b] * fm[c];
+        cols[idx] = g.column(tn[a], mn[c], ln[b]);
+      }
+    }
+}
+
+// GridInterpolator::interpolate_linear (interpolate.rs:985-1028): every
+// pixel (the batched part and the tail alike) is u16 / 65535 * factor,
+// summed over the 8 corners in order.
+template <class T>
+std::vector<T> interpolate_linear(const OGrid &g, double t, double mm, double lg) {
+  int64_t cols[8];
+  double w64[8];
+  local_grid_linear(g, t, mm, lg, cols, w64);
+  const int64_t n = g.npx;
+  const bool f32 = std::is_same<T, float>::value;
+  T w[8], fac[8];
+  const uint16_t *col[8];
+  for (int j = 0; j < 8; j++) {
+    w[j] = f32 ? (T)(float)w64[j] : (T)w64[j];
+    fac[j] = f32 ? (T)g.factors[cols[j]] : (T)g.factors64[cols[j]];
+    col[j] = &g.spectra[(size_t)cols[j] * n];
+  }
+  std::vector<T> out(n);
+  for (int64_t i = 0; i < n; i++) {
+    T acc = T(0);
+    for (int j = 0; j < 8; j++) {
+      T mval = (T)col[j][i] / T(65535.0) * fac[j];
+      acc = acc + mval * w[j];
+    }
+    out[i] = acc;
+  }
+  return out;
+}
+
 // ------------------------------------------------------------------ FFT
 // Own radix-2 real FFT of 2048 (stand-in for realfft/rustfft).
 struct Fft2048 {
@@ -666,6 +754,80 @@ std::vector<T> produce_model(const OGrid &g, const ODisp &d, const double *lab) 
   auto rot = convolve_rotation<T>(g, interp, lab[3]);
   auto conv = disp_convolve<T>(d, rot);
   return shift_and_resample<T>(g, conv, d, lab[4]);
+}
+
+// ---------------------------------------------------------------- binary
+// DVector::mean: sum in order, times 1 / n
+template <class T>
+T row_mean(const std::vector<T> &v) {
+  T s = T(0);
+  for (T x : v) s = s + x;
+  return s * (T(1) / (T)v.size());
+}
+
+// Interpolator::produce_binary_model_norm (interpolate.rs:868-893):
+// produce_binary_components (822-866) -- each star's normalised model
+// broadened on the synthetic grid, its continuum linearly interpolated in
+// the continuum grid, lr = light_ratio * mean(c1) / mean(c2) -- then
+// shift_resample_and_add_binary_components (convolve_rv.rs:606-700):
+// per observed pixel (n1 c1 + lr n2 c2) / (c1 + lr c2), each factor
+// resampled at its star's RV.  lab = (star 1 [5], star 2 [5], light ratio).
+// The FP32 mirror casts the light ratio to f32 as the reference does
+// (fitting.rs:596); the FP64 mode keeps it in double.
+template <class T>
+std::vector<T> binary_model(const OGrid &g, const OGrid &gc, const ODisp &d, const double *lab) {
+  const bool f32 = std::is_same<T, float>::value;
+  auto norm = [&](const double *p) {
+    auto interp = interpolate<T>(g, p[0], p[1], p[2]);
+    auto rot = convolve_rotation<T>(g, interp, p[3]);
+    return disp_convolve<T>(d, rot);
+  };
+  auto n1 = norm(lab);
+  auto c1 = interpolate_linear<T>(gc, lab[0], lab[1], lab[2]);
+  auto n2 = norm(lab + 5);
+  auto c2 = interpolate_linear<T>(gc, lab[5], lab[6], lab[7]);
+  const T lr0 = f32 ? (T)(float)lab[10] : (T)lab[10];
+  const T lr = lr0 * row_mean(c1) / row_mean(c2);
+
+  const int64_t N = g.wl.n;
+  if ((int64_t)n1.size() != N) fail("Length of input_array and wavelength grid don't match");
+  const double rv1 = lab[4], rv2 = lab[9];
+  if (rv1 != rv1 || rv2 != rv2) fail("NaN RV");
+  const double sf1 = 1.0 - rv1 / C_KMS, sf2 = 1.0 - rv2 / C_KMS;
+  auto fl = g.wl.first_last();
+  const double first_src = d.wl[0] * std::min(sf1, sf2);
+  if (first_src < fl.first) fail("Observed wavelength is smaller than synthetic wavelength (%.1f < %.1f)", first_src, fl.first);
+  const double last_src = d.wl[d.wl.size() - 1] * std::max(sf1, sf2);
+  if (last_src > fl.second) fail("Observed wavelength is larger than synthetic wavelength (%.1f > %.1f)", last_src, fl.second);
+  const int64_t NC = (int64_t)c1.size();
+  auto at = [&](double index, const std::vector<T> &a, const std::vector<T> &c, T &av, T &cv) {
+    const double f = std::floor(index);
+    const int64_t j = f > 0 ? (int64_t)f : 0;  // `as usize` saturates at 0
+    if (j + 1 >= N || j + 1 >= NC) fail("resampling index %lld out of range (%lld)", (long long)(j + 1), (long long)N);
+    const T w = (T)(float)index - (T)(float)j;
+    av = (T(1) - w) * a[j] + w * a[j + 1];
+    cv = (T(1) - w) * c[j] + w * c[j + 1];
+  };
+  const int64_t L = (int64_t)d.wl.size();
+  std::vector<T> out(L);
+  for (int64_t i = 0; i < L; i++) {
+    double i1, i2;
+    if (g.wl.kind == OWL_LINSPACE) {
+      i1 = sf1 * d.fidx[i] + (g.wl.a / g.wl.b) * (sf1 - 1.0);
+      i2 = sf2 * d.fidx[i] + (g.wl.a / g.wl.b) * (sf2 - 1.0);
+    } else if (g.wl.kind == OWL_LOGSPACE) {
+      i1 = d.fidx[i] + std::log10(sf1) / g.wl.b;
+      i2 = d.fidx[i] + std::log10(sf2) / g.wl.b;
+    } else {
+      i1 = g.wl.float_index(d.wl[i] * sf1);
+      i2 = g.wl.float_index(d.wl[i] * sf2);
+    }
+    T a1, k1, a2, k2;
+    at(i1, n1, c1, a1, k1);
+    at(i2, n2, c2, a2, k2);
+    out[i] = (a1 * k1 + lr * a2 * k2) / (k1 + lr * k2);
+  }
+  return out;
 }
 
 // ------------------------------------------------------- least squares
@@ -1136,6 +1298,170 @@ void fit_one(const OGrid &g, const ODisp &d, const OCont &c, const OPsoSettings 
   for (int i = 0; i < res.n_params; i++) res.params[i] = params[i];
 }
 
+// BinaryCostFunction::cost (fitting.rs:584-600)
+template <class T>
+double binary_cost(const OGrid &g, const OGrid &gc, const ODisp &d, const OCont &c, const float *flux,
+                   const float *var, const double *lab) {
+  auto mdl = binary_model<T>(g, gc, d, lab);
+  std::vector<double> params;
+  double chi2;
+  fit_continuum<T>(c, flux, var, mdl, params, chi2);
+  return chi2;
+}
+
+// BinaryBounds (bounds.rs:188-275) wrapped in ConstrainedPSOBounds
+// (bounds.rs:69-130): star 1 at 0..5, star 2 at 5..10, light ratio at 10
+// with the range (0, 1) BinaryFitter::fit gives it (fitting.rs:649-655).
+struct BinaryBoundsO {
+  const OGrid *g;
+  const OBinarySettings *st;
+  static constexpr double lr_lo = 0.0, lr_hi = 1.0;
+  std::pair<double, double> raw(const double *p, int i) const {
+    if (i == 3 || i == 8) return {st->vsini_lo, st->vsini_hi};
+    if (i == 4 || i == 9) return {st->rv_lo, st->rv_hi};
+    if (i == 10) return {lr_lo, lr_hi};
+    return i < 5 ? g->limits_at(p, i) : g->limits_at(p + 5, i - 5);
+  }
+  std::pair<double, double> constrain(int i, std::pair<double, double> l) const {
+    if (st->ckind[i] == 1) return {st->ca[i], st->ca[i]};
+    if (st->ckind[i] == 2) return {std::max(l.first, st->ca[i]), std::min(l.second, st->cb[i])};
+    return l;
+  }
+  void outer(double mn[11], double mx[11]) const {
+    for (int k = 0; k < 2; k++) {
+      mn[5 * k + 0] = g->teff.v.front(); mx[5 * k + 0] = g->teff.v.back();
+      mn[5 * k + 1] = g->m.v.front(); mx[5 * k + 1] = g->m.v.back();
+      mn[5 * k + 2] = g->logg.v.front(); mx[5 * k + 2] = g->logg.v.back();
+      mn[5 * k + 3] = st->vsini_lo; mx[5 * k + 3] = st->vsini_hi;
+      mn[5 * k + 4] = st->rv_lo; mx[5 * k + 4] = st->rv_hi;
+    }
+    mn[10] = lr_lo; mx[10] = lr_hi;
+    for (int i = 0; i < 11; i++) {
+      auto l = constrain(i, {mn[i], mx[i]});
+      mn[i] = l.first; mx[i] = l.second;
+    }
+  }
+  double clamp_1d(const double *p, int i) const {
+    auto l = constrain(i, raw(p, i));
+    if (!(l.first <= l.second)) fail("clamp limits invalid (%g > %g) in dim %d", l.first, l.second, i);
+    return std::min(std::max(p[i], l.first), l.second);
+  }
+  bool within(const double *p) const {
+    if (!g->within(p) || !g->within(p + 5)) return false;
+    for (int k = 0; k < 2; k++) {
+      const double vs = p[5 * k + 3], rv = p[5 * k + 4];
+      if (!(vs >= st->vsini_lo && vs <= st->vsini_hi && rv >= st->rv_lo && rv <= st->rv_hi)) return false;
+    }
+    if (!(p[10] >= lr_lo && p[10] <= lr_hi)) return false;
+    for (int i = 0; i < 11; i++) {
+      if (st->ckind[i] == 1 && !(std::fabs(p[i] - st->ca[i]) <= 2.220446049250313e-16)) return false;
+      if (st->ckind[i] == 2 && !(p[i] >= st->ca[i] && p[i] <= st->cb[i])) return false;
+    }
+    return true;
+  }
+};
+
+// BinaryFitter::fit (fitting.rs:633-697) with the particle swarm of
+// particleswarm.rs:111-307 over 11 dimensions, on the shared draw stream
+// (the same phases and counters as the single-star fit, dimension d < 11).
+template <class T>
+void fit_binary(const OGrid &g, const OGrid &gc, const ODisp &d, const OCont &c, const OBinarySettings &st,
+                const float *flux, const float *var, uint64_t seed, int nthreads, OBinaryResult &res,
+                double *trace) {
+  constexpr int D = 11;
+  BinaryBoundsO B{&g, &st};
+  const int P = st.num_particles;
+  if (P <= 0) fail("num_particles must be positive");
+  double mn[D], mx[D];
+  B.outer(mn, mx);
+  struct Pt {
+    double x[D], v[D], bx[D];
+    double cost, bcost;
+  };
+  std::vector<Pt> ps(P);
+  uint64_t cand = 0;
+  for (int p = 0; p < P;) {  // bounds.rs:21-35
+    if (cand > 10000000ull) fail("could not place particles within bounds");
+    double x[D];
+    for (int k = 0; k < D; k++)
+      x[k] = mn[k] == mx[k] ? mn[k] : uniform_between(mn[k], mx[k], draw_u01(seed, 1, cand, 0, k));
+    cand++;
+    if (B.within(x)) { std::memcpy(ps[p].x, x, sizeof x); p++; }
+  }
+  for (int p = 0; p < P; p++)
+    for (int k = 0; k < D; k++) {
+      double w = mx[k] - mn[k];
+      ps[p].v[k] = (-w == w) ? -w : uniform_between(-w, w, draw_u01(seed, 2, p, 0, k));
+    }
+  auto evaluate = [&]() {
+    std::vector<std::string> errs(P);
+    std::vector<int> bad(P, 0);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+    for (int i = 0; i < P; i++) {
+      try {
+        ps[i].cost = binary_cost<T>(g, gc, d, c, flux, var, ps[i].x);
+      } catch (const std::exception &e) {
+        bad[i] = 1;
+        errs[i] = e.what();
+      }
+    }
+    for (int i = 0; i < P; i++) if (bad[i]) fail("particle %d: %s", i, errs[i].c_str());
+  };
+  evaluate();
+  for (auto &q : ps) { std::memcpy(q.bx, q.x, sizeof q.x); q.bcost = q.cost; }
+  std::stable_sort(ps.begin(), ps.end(), [](const Pt &a, const Pt &b) { return a.cost < b.cost; });
+  double gx[D];
+  std::memcpy(gx, ps[0].x, sizeof gx);
+  double gcost = ps[0].cost;
+  auto dump = [&](int it) {
+    if (!trace) return;
+    double *t = trace + (size_t)it * P * (D + 1);
+    for (int p = 0; p < P; p++) {
+      for (int k = 0; k < D; k++) t[p * (D + 1) + k] = ps[p].x[k];
+      t[p * (D + 1) + D] = ps[p].cost;
+    }
+  };
+  dump(0);
+  for (int it = 0; it < st.max_iters; it++) {
+    for (int p = 0; p < P; p++) {
+      Pt &q = ps[p];
+      for (int k = 0; k < D; k++) {
+        double momentum = q.v[k] * st.inertia;
+        double to_opt = q.bx[k] - q.x[k];
+        double pull = (to_opt == 0.0 ? 0.0 : uniform_between(0.0, to_opt, draw_u01(seed, 3, it, p, 2 * k))) * st.cognitive;
+        double to_g = gx[k] - q.x[k];
+        double pullg = (to_g == 0.0 ? 0.0 : uniform_between(0.0, to_g, draw_u01(seed, 3, it, p, 2 * k + 1))) * st.social;
+        q.v[k] = momentum + pull + pullg;
+        double nx[D];
+        std::memcpy(nx, q.x, sizeof nx);
+        nx[k] += q.v[k];
+        q.x[k] = B.clamp_1d(nx, k);
+        if (!B.within(q.x)) fail("Particle %d is not within bounds", p);
+      }
+    }
+    evaluate();
+    for (auto &q : ps) {
+      if (q.cost < q.bcost) {
+        std::memcpy(q.bx, q.x, sizeof q.x);
+        q.bcost = q.cost;
+        if (q.cost < gcost) { std::memcpy(gx, q.x, sizeof gx); gcost = q.cost; }
+      }
+    }
+    dump(it + 1);
+  }
+  std::memcpy(res.label1, gx, 5 * sizeof(double));
+  std::memcpy(res.label2, gx + 5, 5 * sizeof(double));
+  res.light_ratio = gx[10];
+  res.chi2 = gcost;
+  res.iterations = st.max_iters;
+  auto mdl = binary_model<T>(g, gc, d, gx);
+  std::vector<double> params;
+  double chi2;
+  fit_continuum<T>(c, flux, var, mdl, params, chi2);
+  res.n_params = (int)std::min<size_t>(params.size(), 512);
+  for (int i = 0; i < res.n_params; i++) res.params[i] = params[i];
+}
+
 template <class F>
 int guard(F &&f) {
   try {
@@ -1425,6 +1751,51 @@ int or_fit(const OGrid *g, const ODisp *d, const OCont *c, int prec, const OPsoS
   }
   if (any) for (int64_t s = 0; s < S; s++) if (out[s].status) { g_err = errs[s]; break; }
   return any ? -1 : 0;
+}
+
+int or_local_grid_linear(const OGrid *g, double t, double m, double l, int64_t *cols, double *w) {
+  return guard([&] { local_grid_linear(*g, t, m, l, cols, w); });
+}
+int or_interpolate_linear(const OGrid *g, int prec, double t, double m, double l, double *out) {
+  return guard([&] {
+    if (prec == OP_F32) { auto v = interpolate_linear<float>(*g, t, m, l); std::copy(v.begin(), v.end(), out); }
+    else { auto v = interpolate_linear<double>(*g, t, m, l); std::copy(v.begin(), v.end(), out); }
+  });
+}
+int or_binary_model(const OGrid *g, const OGrid *gc, const ODisp *d, int prec, const double *lab, double *out) {
+  return guard([&] {
+    if (prec == OP_F32) { auto v = binary_model<float>(*g, *gc, *d, lab); std::copy(v.begin(), v.end(), out); }
+    else { auto v = binary_model<double>(*g, *gc, *d, lab); std::copy(v.begin(), v.end(), out); }
+  });
+}
+int or_binary_chi2(const OGrid *g, const OGrid *gc, const ODisp *d, const OCont *c, int prec, const float *flux,
+                   const float *var, int64_t n, const double *labels, int64_t L, double *out, int *status,
+                   int nthreads) {
+  if (n != (int64_t)d->wl.size()) { g_err = "Observed spectrum and target dispersion must have the same length"; return -1; }
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int64_t i = 0; i < L; i++) {
+    try {
+      out[i] = prec == OP_F32 ? binary_cost<float>(*g, *gc, *d, *c, flux, var, labels + 11 * i)
+                              : binary_cost<double>(*g, *gc, *d, *c, flux, var, labels + 11 * i);
+      status[i] = 0;
+    } catch (const std::exception &e) {
+      out[i] = NAN;
+      status[i] = -1;
+    }
+  }
+  return 0;
+}
+int or_binary_fit(const OGrid *g, const OGrid *gc, const ODisp *d, const OCont *c, int prec,
+                  const OBinarySettings *st, const float *flux, const float *var, int64_t n, uint64_t seed,
+                  int nthreads, OBinaryResult *out, double *trace) {
+  if (n != (int64_t)d->wl.size()) { g_err = "Observed spectrum and target dispersion must have the same length"; return -1; }
+  std::memset(out, 0, sizeof(OBinaryResult));
+  int rc = guard([&] {
+    if (prec == OP_F32) fit_binary<float>(*g, *gc, *d, *c, *st, flux, var, seed, nthreads, *out, trace);
+    else fit_binary<double>(*g, *gc, *d, *c, *st, flux, var, seed, nthreads, *out, trace);
+  });
+  out->status = rc;
+  return rc;
 }
 
 }  // extern "C"

@@ -137,6 +137,51 @@ int or_fit(const OGrid *g, const ODisp *d, const OCont *c, int prec,
            int64_t n, int64_t S, const uint64_t *seeds, int nthreads,
            int threads_over_stars, OFitResult *out, double *trace);
 
+/* ------------------------------------------------------------- binaries */
+/* 8 column indices and f64 weights of the linear interpolation
+ * (interpolate.rs:536-600, cubic.rs:246-270) */
+int or_local_grid_linear(const OGrid *g, double teff, double m, double logg,
+                         int64_t *cols, double *w);
+/* interpolate_linear(teff, m, logg) -> npx values (interpolate.rs:985) */
+int or_interpolate_linear(const OGrid *g, int prec, double teff, double m,
+                          double logg, double *out);
+/* produce_binary_model_norm (interpolate.rs:868): lab = star 1 [5],
+ * star 2 [5], light ratio; gc is the continuum grid; out [n_obs] */
+int or_binary_model(const OGrid *g, const OGrid *gc, const ODisp *d, int prec,
+                    const double *lab, double *out);
+/* BinaryCostFunction::cost (fitting.rs:584) for L labels [L x 11] */
+int or_binary_chi2(const OGrid *g, const OGrid *gc, const ODisp *d,
+                   const OCont *c, int prec, const float *flux,
+                   const float *var, int64_t n, const double *labels,
+                   int64_t L, double *out, int *status, int nthreads);
+
+typedef struct {
+  int num_particles;
+  int max_iters;
+  double inertia, cognitive, social, delta;
+  double vsini_lo, vsini_hi, rv_lo, rv_hi;
+  int ckind[11];
+  double ca[11], cb[11];
+} OBinarySettings;
+
+typedef struct {
+  double label1[5], label2[5];
+  double light_ratio;
+  double chi2;
+  int iterations;
+  int status;
+  int n_params;
+  double params[512];
+} OBinaryResult;
+
+/* BinaryFitter::fit (fitting.rs:633-697); particles threaded over
+ * nthreads.  trace (optional): (max_iters+1) x P x 12 (position, cost). */
+int or_binary_fit(const OGrid *g, const OGrid *gc, const ODisp *d,
+                  const OCont *c, int prec, const OBinarySettings *st,
+                  const float *flux, const float *var, int64_t n,
+                  uint64_t seed, int nthreads, OBinaryResult *out,
+                  double *trace);
+
 /* the shared PSO draw stream */
 double or_draw_u01(uint64_t seed, uint64_t phase, uint64_t a, uint64_t b,
                    uint64_t c);

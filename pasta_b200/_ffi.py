@@ -31,6 +31,20 @@ class FitResultC(C.Structure):
                 ("_pad", C.c_int32)]
 
 
+class BinarySettingsC(C.Structure):
+    _fields_ = [("num_particles", C.c_int32), ("max_iters", C.c_int32), ("inertia_factor", C.c_double),
+                ("cognitive_factor", C.c_double), ("social_factor", C.c_double), ("delta", C.c_double),
+                ("vsini_lo", C.c_double), ("vsini_hi", C.c_double), ("rv_lo", C.c_double),
+                ("rv_hi", C.c_double), ("ckind", C.c_int32 * 11), ("ca", C.c_double * 11),
+                ("cb", C.c_double * 11)]
+
+
+class BinaryResultC(C.Structure):
+    _fields_ = [("label1", C.c_double * 5), ("label2", C.c_double * 5), ("light_ratio", C.c_double),
+                ("chi2", C.c_double), ("time", C.c_double), ("iterations", C.c_int32), ("status", C.c_int32),
+                ("n_params", C.c_int32), ("_pad", C.c_int32)]
+
+
 # name -> (restype, argtypes); every symbol of include/pasta_b200.h
 P, D, I64, I, F = C.c_void_p, C.c_double, C.c_int64, C.c_int, C.c_float
 SIGNATURES = {
@@ -79,6 +93,10 @@ SIGNATURES = {
     "pasta_server_destroy": (I, [P]),
     "pasta_server_run": (I, [P, I, P]),
     "pasta_server_stats": (I, [P, P]),
+    "pasta_interpolate_linear": (I, [P, P, I64, P, P]),
+    "pasta_binary_model": (I, [P, P, P, P, I64, P, P]),
+    "pasta_binary_chi2": (I, [P, P, P, P, P, P, I64, P, I64, P, P]),
+    "pasta_binary_fit": (I, [P, P, P, P, P, P, P, I64, C.c_uint64, P, P, P]),
 }
 
 _lib = None

@@ -1,9 +1,9 @@
 """Builds libpasta_b200.so in-tree for sm_100a (nvcc, no JIT cache).
 
-prep.cu is compiled with -fmad=false so that its double-precision geometry
-(neighbour search, kernel widths, windows, swarm clamps) is evaluated exactly
-as written, like the host and the reference; the bandwidth/FFT kernels keep
-FMA contraction.
+prep.cu and binary.cu are compiled with -fmad=false so that their
+double-precision geometry (neighbour search, kernel widths, windows, swarm
+clamps, shifts) is evaluated exactly as written, like the host and the
+reference; the bandwidth/FFT kernels keep FMA contraction.
 """
 from __future__ import annotations
 
@@ -19,7 +19,8 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
           "-I" + os.path.join(ROOT, "include")]
-UNITS = [("prep.cu", ["-fmad=false"]), ("kernels.cu", []), ("engine.cu", []), ("noalloc.cu", [])]
+UNITS = [("prep.cu", ["-fmad=false"]), ("kernels.cu", []), ("binary.cu", ["-fmad=false"]), ("engine.cu", []),
+         ("noalloc.cu", [])]
 DEPS = ["common.cuh", "fft.cuh", "kernels.h"]
 
 

@@ -325,6 +325,66 @@ PB_HD int local_grid(const GridGeom &G, double t, double m, double lg, int cols[
   return S_OK;
 }
 
+// Range::find_neighbors_linear (interpolate.rs:161-213): the two grid
+// points around x.  A grid point at the right limit takes its left partner
+// (none at index 0, where the reference's usize subtraction panics).
+PB_HD int find_neighbors_linear(const double *v, int n, double x, int left, int right, int out[2]) {
+  bool found;
+  int i = lower_bound(v, n, x, found);
+  if (found) {
+    if (i < left || i > right) return S_NEIGHBORS;
+    if (i == right) {
+      if (i == 0) return S_NEIGHBORS;
+      out[0] = i - 1; out[1] = i;
+    } else {
+      out[0] = i; out[1] = i + 1;
+    }
+  } else {
+    if (i <= left || i > right) return S_NEIGHBORS;
+    out[0] = i - 1; out[1] = i;
+  }
+  return S_OK;
+}
+
+// Grid::get_local_grid_linear + calculate_interpolation_coefficients_linear
+// (interpolate.rs:536-600; cubic.rs:6-10, 246-270): the 8 corners of the
+// cube around the label, teff outer, logg middle, [M/H] inner, with f32
+// weights (a * b * c).  A corner whose logg index lies outside its teff's
+// logg limits has no model: S_NEIGHBORS (the reference would read a
+// neighbouring column there).
+PB_HD int local_grid_linear(const GridGeom &G, double t, double m, double lg, int cols[8], float w[8]) {
+  if (t != t || m != m || lg != lg) return S_NAN;
+  if (!teff_logg_ok(G, t, lg)) return S_OUT_OF_GRID;
+  if (!m_ok(G, m)) return S_OUT_OF_GRID;
+  int tlo, thi, llo, lhi;
+  int st = teff_index_limits_at(G, lg, tlo, thi);
+  if (st) return st;
+  st = logg_index_limits_at(G, t, llo, lhi);
+  if (st) return st;
+  int tn[2], mn[2], ln[2];
+  if (find_neighbors_linear(G.tv, G.nt, t, tlo, thi, tn)) return S_NEIGHBORS;
+  if (find_neighbors_linear(G.mv, G.nm, m, 0, G.nm - 1, mn)) return S_NEIGHBORS;
+  if (find_neighbors_linear(G.lv, G.nl, lg, llo, lhi, ln)) return S_NEIGHBORS;
+  double ft[2], fl[2], fm[2];
+  ft[0] = (t - G.tv[tn[1]]) / (G.tv[tn[0]] - G.tv[tn[1]]);
+  ft[1] = (t - G.tv[tn[0]]) / (G.tv[tn[1]] - G.tv[tn[0]]);
+  fl[0] = (lg - G.lv[ln[1]]) / (G.lv[ln[0]] - G.lv[ln[1]]);
+  fl[1] = (lg - G.lv[ln[0]]) / (G.lv[ln[1]] - G.lv[ln[0]]);
+  fm[0] = (m - G.mv[mn[1]]) / (G.mv[mn[0]] - G.mv[mn[1]]);
+  fm[1] = (m - G.mv[mn[0]]) / (G.mv[mn[1]] - G.mv[mn[0]]);
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      const int i = tn[a];
+      if (ln[b] < G.llo[i] || ln[b] > G.lhi[i]) return S_NEIGHBORS;
+      for (int c = 0; c < 2; c++) {
+        const int idx = (a * 2 + b) * 2 + c;
+        w[idx] = (float)(ft[a] * fl[b] * fm[c]);
+        cols[idx] = (int)((G.cum[i] + ln[b] - G.llo[i]) * (int64_t)G.nm + mn[c]);
+      }
+    }
+  return S_OK;
+}
+
 // Grid::get_limits_at (interpolate.rs:647-664)
 PB_HD int grid_limits_at(const GridGeom &G, const double *p, int index, double &lo, double &hi) {
   int a, b, st;

@@ -1930,6 +1930,462 @@ int pasta_dispersion_convolve_resample(const pasta_dispersion *d, int in_kind, d
   });
 }
 
+// ============================================================= binaries
+namespace {
+
+// Device buffers for binary labels: up to cap labels of an observed
+// spectrum of nobs pixels on a grid with `tiles` continuum tiles.
+struct BinaryScratch {
+  int64_t cap = 0, nobs = 0;
+  int tiles = 0;
+  DBuf<double> labels;  // [cap][11]
+  DBuf<double> comp;    // [2 cap][5]
+  DBuf<int> star0;      // [2 cap] all zero: every component belongs to star 0
+  DBuf<LinRec> lin;     // [2 cap]
+  DBuf<double> part;    // [2 cap][tiles]
+  DBuf<EvalPrep> cprep; // [cap]
+  DBuf<float> model;    // [cap][nobs]
+  DBuf<double> cost;    // [cap]
+  DBuf<int> status;     // [cap]
+  void ensure(int64_t L, int t, int64_t n) {
+    if (L <= cap && t == tiles && n == nobs) return;
+    labels.alloc((size_t)L * 11);
+    comp.alloc((size_t)L * 10);
+    star0.alloc((size_t)L * 2);
+    CK(cudaMemset(star0.p, 0, (size_t)L * 2 * sizeof(int)));
+    lin.alloc((size_t)L * 2);
+    part.alloc((size_t)L * 2 * t);
+    cprep.alloc((size_t)L);
+    CK(cudaMemset(cprep.p, 0, (size_t)L * sizeof(EvalPrep)));
+    model.alloc((size_t)L * n);
+    cost.alloc((size_t)L);
+    status.alloc((size_t)L);
+    cap = L;
+    tiles = t;
+    nobs = n;
+  }
+};
+
+void check_binary_grids(const pasta_grid *g, const pasta_grid *gc) {
+  if (!gc) fail(PASTA_E_ARG, "a continuum interpolator is required");
+  if (gc->npx != g->npx)
+    fail(PASTA_E_ARG, "continuum grid has %lld pixels and the model grid %lld: they must be equal",
+         (long long)gc->npx, (long long)g->npx);
+  if (gc->dev != g->dev) fail(PASTA_E_ARG, "the continuum grid lives on another device");
+}
+
+// The L binary labels in bs.labels (device): the components through the
+// regular pipeline on the whole synthetic grid, the continua, the combined
+// model at the observed pixels (bs.model, status in bs.cprep) and, when
+// chi2, the continuum fit (bs.cost, bs.status; params when given).  Runs in
+// sub-batches of half the workspace (two components per label);
+// asynchronous on s, no allocation.
+void run_binary(pasta_grid *g, const pasta_grid *gc, const DevStar *dstar, const DevStar &hstar,
+                BinaryScratch &bs, int64_t L, double vs_max, bool chi2, double *dparams, int param_stride,
+                cudaStream_t s) {
+  EvalArgs a;
+  a.stars = dstar;
+  a.eval_star = bs.star0.p;
+  a.need_chi2 = 0;
+  a.full_window = 1;
+  a.max_m = width_upper_bound(g, vs_max);
+  star_kinds({hstar}, a);
+  const int64_t capL = std::min<int64_t>(g->ws.cap / 2, bs.cap);
+  if (capL < 1) fail(PASTA_E_NOMEM, "the evaluation workspace holds fewer than two evaluations");
+  const int64_t nobs = hstar.n_obs;
+  for (int64_t off = 0; off < L; off += capL) {
+    const int64_t cnt = std::min(capL, L - off);
+    BinaryBatch bb{};
+    bb.L = (int)cnt;
+    bb.labels = bs.labels.p + (size_t)off * 11;
+    bb.comp_labels = bs.comp.p;
+    bb.lin = bs.lin.p;
+    bb.part = bs.part.p;
+    bb.lin_tiles = bs.tiles;
+    bb.cprep = bs.cprep.p + off;
+    bb.model = bs.model.p + (size_t)off * nobs;
+    bb.model_stride = nobs;
+    launch_binary_split(gc->d, bb, s);
+    a.labels = bs.comp.p;
+    a.E = 2 * cnt;
+    run_evals(g, a, s);  // 2 cnt <= workspace capacity: rows [0, 2 cnt)
+    const EvalBatch comp = make_batch(g, a, 0, 2 * cnt);
+    launch_interp_linear(gc->d, comp, bb, s);
+    launch_binary_combine(g->d, (int)gc->npx, comp, bb, (int)nobs, s);
+    if (chi2) {
+      EvalBatch cb{};
+      cb.E = (int)cnt;
+      cb.stars = dstar;
+      cb.prep = bb.cprep;
+      cb.cost = bs.cost.p + off;
+      cb.status = bs.status.p + off;
+      cb.params = dparams ? dparams + (size_t)off * param_stride : nullptr;
+      cb.param_stride = param_stride;
+      cb.need_chi2 = 1;
+      cb.chunk_p1_mask = a.chunk_p1_mask;
+      cb.max_chunks = a.max_chunks;
+      cb.other_cont = a.other_cont;
+      cb.ccoef = g->ws.ccoef.p;
+      cb.cpart = g->ws.cpart.p;
+      cb.given = bb.model;
+      cb.given_stride = nobs;
+      launch_chi2(g->d, cb, s);
+    }
+  }
+  CK(cudaGetLastError());
+}
+
+double max_binary_vsini(const double *labels, int64_t L) {
+  double v = 0.0;
+  for (int64_t i = 0; i < L; i++)
+    for (int k : {3, 8}) {
+      const double x = labels[(size_t)i * 11 + k];
+      if (x > v) v = x;
+    }
+  return v;
+}
+
+// statuses of the L labels whose combination ran (model entry point)
+std::vector<int> binary_status(const BinaryScratch &bs, int64_t L, cudaStream_t s) {
+  std::vector<EvalPrep> hp((size_t)L);
+  CK(cudaMemcpyAsync(hp.data(), bs.cprep.p, (size_t)L * sizeof(EvalPrep), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::vector<int> st((size_t)L);
+  for (int64_t i = 0; i < L; i++) st[i] = hp[i].status;
+  return st;
+}
+
+}  // namespace
+
+int pasta_interpolate_linear(const pasta_grid *gc_, const double *tml, int64_t L, float *out, int32_t *status) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(gc_);
+    if (L < 0) fail(PASTA_E_ARG, "negative label count");
+    if (L == 0) return;
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    const int64_t npx = g->npx, str = (npx + 63) / 64 * 64;
+    const int tiles = linear_tiles((int)npx);
+    DBuf<double> dl;
+    DBuf<LinRec> lin;
+    DBuf<double> part;
+    DBuf<float> dout;
+    dl.upload(tml, (size_t)L * 3);
+    lin.alloc((size_t)L);
+    part.alloc((size_t)L * tiles);
+    dout.alloc((size_t)L * str);
+    launch_linear_prep(g->d, dl.p, (int)L, lin.p, s);
+    launch_interp_linear_rows(g->d, lin.p, (int)L, dout.p, str, part.p, s);
+    CK(cudaGetLastError());
+    std::vector<LinRec> hl((size_t)L);
+    CK(cudaMemcpyAsync(hl.data(), lin.p, (size_t)L * sizeof(LinRec), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpy2DAsync(out, npx * sizeof(float), dout.p, str * sizeof(float), npx * sizeof(float), (size_t)L,
+                         cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < L; i++) {
+      if (status) status[i] = hl[i].status;
+      if (hl[i].status) std::fill(out + i * npx, out + (i + 1) * npx, NAN);
+    }
+  });
+}
+
+int pasta_binary_model(const pasta_grid *g_, const pasta_grid *cg, const pasta_dispersion *d, const double *labels,
+                       int64_t L, float *out, int32_t *status) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(g_);
+    if (!d) fail(PASTA_E_ARG, "dispersion required");
+    if (L < 0) fail(PASTA_E_ARG, "negative label count");
+    if (L == 0) return;
+    check_disp_grid(g, d);
+    check_binary_grids(g, cg);
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    std::lock_guard<std::mutex> lk(g->mu);
+    const int64_t nobs = (int64_t)d->wl.size();
+    DevStar st = make_star(d, nullptr, nullptr, nullptr, nobs);
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    ensure_workspace(g, 2 * L, nobs);
+    BinaryScratch bs;
+    bs.ensure(L, linear_tiles((int)g->npx), nobs);
+    CK(cudaMemcpyAsync(bs.labels.p, labels, (size_t)L * 11 * sizeof(double), cudaMemcpyHostToDevice, s));
+    run_binary(g, cg, ds.p, st, bs, L, max_binary_vsini(labels, L), false, nullptr, 0, s);
+    CK(cudaMemcpyAsync(out, bs.model.p, (size_t)L * nobs * sizeof(float), cudaMemcpyDeviceToHost, s));
+    const std::vector<int> hs = binary_status(bs, L, s);
+    for (int64_t i = 0; i < L; i++) {
+      if (status) status[i] = hs[i];
+      if (hs[i]) std::fill(out + i * nobs, out + (i + 1) * nobs, NAN);
+    }
+  });
+}
+
+int pasta_binary_chi2(const pasta_grid *g_, const pasta_grid *cg, const pasta_dispersion *d,
+                      const pasta_continuum *c, const float *flux, const float *var, int64_t n,
+                      const double *labels, int64_t L, double *out, int32_t *status) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(g_);
+    if (!d || !c || !flux || !var) fail(PASTA_E_ARG, "dispersion, continuum and data required");
+    if (L < 0) fail(PASTA_E_ARG, "negative label count");
+    if (L == 0) return;
+    check_disp_grid(g, d);
+    check_binary_grids(g, cg);
+    if (n != (int64_t)d->wl.size()) fail(PASTA_E_ARG, "Observed spectrum and target dispersion must have the same length");
+    if (c->kind != PASTA_CONT_CONSTANT && c->n != n)
+      fail(PASTA_E_ARG, "continuum fitter and dispersion have different lengths");
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    std::lock_guard<std::mutex> lk(g->mu);
+    DBuf<float> df, dv;
+    df.upload(flux, n);
+    dv.upload(var, n);
+    DevStar st = make_star(d, c, df.p, dv.p, n);
+    DBuf<DevStar> ds;
+    ds.upload(&st, 1);
+    ensure_workspace(g, 2 * L, n);
+    BinaryScratch bs;
+    bs.ensure(L, linear_tiles((int)g->npx), n);
+    CK(cudaMemcpyAsync(bs.labels.p, labels, (size_t)L * 11 * sizeof(double), cudaMemcpyHostToDevice, s));
+    run_binary(g, cg, ds.p, st, bs, L, max_binary_vsini(labels, L), true, nullptr, 0, s);
+    std::vector<double> hc((size_t)L);
+    std::vector<int> hs((size_t)L);
+    CK(cudaMemcpyAsync(hc.data(), bs.cost.p, (size_t)L * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hs.data(), bs.status.p, (size_t)L * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < L; i++) {
+      out[i] = hs[i] ? NAN : hc[i];
+      if (status) status[i] = hs[i];
+    }
+  });
+}
+
+namespace {
+
+// BinaryBounds (bounds.rs:188-275) inside ConstrainedPSOBounds
+// (bounds.rs:69-130): star 1 at 0..5, star 2 at 5..10, the light ratio at
+// 10 in (0, 1) as BinaryFitter::fit sets it (fitting.rs:649-655).
+struct BinaryBoundsH {
+  const GridGeom *G = nullptr;
+  pasta_binary_settings S{};
+  double mn[11], mx[11];
+  void constrain(int i, double &lo, double &hi) const {
+    if (S.ckind[i] == 1) { lo = S.ca[i]; hi = S.ca[i]; }
+    else if (S.ckind[i] == 2) { lo = std::max(lo, S.ca[i]); hi = std::min(hi, S.cb[i]); }
+  }
+  void init(const pasta_grid *g, const pasta_binary_settings &st) {
+    G = &g->hg;
+    S = st;
+    for (int k = 0; k < 2; k++) {
+      mn[5 * k] = g->tv.front(); mx[5 * k] = g->tv.back();
+      mn[5 * k + 1] = g->mv.front(); mx[5 * k + 1] = g->mv.back();
+      mn[5 * k + 2] = g->lv.front(); mx[5 * k + 2] = g->lv.back();
+      mn[5 * k + 3] = st.vsini_lo; mx[5 * k + 3] = st.vsini_hi;
+      mn[5 * k + 4] = st.rv_lo; mx[5 * k + 4] = st.rv_hi;
+    }
+    mn[10] = 0.0; mx[10] = 1.0;
+    for (int i = 0; i < 11; i++) constrain(i, mn[i], mx[i]);
+  }
+  int limits_at(const double *p, int i, double &lo, double &hi) const {
+    if (i == 3 || i == 8) { lo = S.vsini_lo; hi = S.vsini_hi; }
+    else if (i == 4 || i == 9) { lo = S.rv_lo; hi = S.rv_hi; }
+    else if (i == 10) { lo = 0.0; hi = 1.0; }
+    else {
+      const int st = grid_limits_at(*G, i < 5 ? p : p + 5, i < 5 ? i : i - 5, lo, hi);
+      if (st) return st;
+    }
+    constrain(i, lo, hi);
+    return S_OK;
+  }
+  int clamp_1d(const double *p, int i, double &out) const {  // bounds.rs:13-16
+    double lo, hi;
+    const int st = limits_at(p, i, lo, hi);
+    if (st) return st;
+    if (!(lo <= hi)) return S_CLAMP;
+    out = p[i] < lo ? lo : (p[i] > hi ? hi : p[i]);
+    return S_OK;
+  }
+  bool within(const double *p) const {
+    for (int k = 0; k < 2; k++) {
+      const double *q = p + 5 * k;
+      if (!(m_ok(*G, q[1]) && teff_logg_ok(*G, q[0], q[2]))) return false;
+      if (!(q[3] >= S.vsini_lo && q[3] <= S.vsini_hi && q[4] >= S.rv_lo && q[4] <= S.rv_hi)) return false;
+    }
+    if (!(p[10] >= 0.0 && p[10] <= 1.0)) return false;
+    for (int i = 0; i < 11; i++) {
+      if (S.ckind[i] == 1 && !(std::fabs(p[i] - S.ca[i]) <= 2.220446049250313e-16)) return false;
+      if (S.ckind[i] == 2 && !(p[i] >= S.ca[i] && p[i] <= S.cb[i])) return false;
+    }
+    return true;
+  }
+};
+
+}  // namespace
+
+// BinaryFitter::fit: the swarm runs on the host (11-dimensional positions on
+// the draw stream of the single-star fit), every iteration's particles are
+// evaluated as one batch on the device.
+int pasta_binary_fit(const pasta_grid *g_, const pasta_grid *cg, const pasta_dispersion *d,
+                     const pasta_continuum *c, const pasta_binary_settings *settings, const float *flux,
+                     const float *var, int64_t n, uint64_t seed, pasta_binary_result *res, float *params,
+                     double *trace) {
+  return guard([&] {
+    pasta_grid *g = const_cast<pasta_grid *>(g_);
+    if (!d || !c || !settings || !flux || !var || !res) fail(PASTA_E_ARG, "dispersion, continuum, settings and data required");
+    const pasta_binary_settings &st = *settings;
+    if (st.num_particles < 1 || st.num_particles > MAX_PARTICLES)
+      fail(PASTA_E_ARG, "num_particles must be in 1..%d", MAX_PARTICLES);
+    if (st.max_iters < 0) fail(PASTA_E_ARG, "max_iters must be >= 0");
+    if (st.social_factor < 0.0) fail(PASTA_E_ARG, "`ParticleSwarm`: social factor must be >=0.");
+    if (st.delta < 0.0) fail(PASTA_E_ARG, "`ParticleSwarm`: delta must be >=0.");
+    check_disp_grid(g, d);
+    check_binary_grids(g, cg);
+    if (n != (int64_t)d->wl.size()) fail(PASTA_E_ARG, "Observed spectrum and target dispersion must have the same length");
+    if (c->kind != PASTA_CONT_CONSTANT && c->n != n)
+      fail(PASTA_E_ARG, "continuum fitter and dispersion have different lengths");
+    const double t0 = now_s();
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    std::lock_guard<std::mutex> lk(g->mu);
+    constexpr int D = 11;
+    const int P = st.num_particles;
+    BinaryBoundsH B;
+    B.init(g, st);
+    DBuf<float> df, dv;
+    df.upload(flux, n);
+    dv.upload(var, n);
+    DevStar hstar = make_star(d, c, df.p, dv.p, n);
+    DBuf<DevStar> ds;
+    ds.upload(&hstar, 1);
+    ensure_workspace(g, 2 * (int64_t)P, n);
+    BinaryScratch bs;
+    bs.ensure(P, linear_tiles((int)g->npx), n);
+    const double vs_max = std::max(B.mx[3], B.mx[8]);
+    std::vector<double> x((size_t)P * D), v((size_t)P * D), bx, cost(P), bcost, gx(D);
+    std::vector<int> est(P);
+    double gcost = 0.0;
+    int status = S_OK;
+    // bounds.rs:21-35 (rejection sampling) and particleswarm.rs:137-150
+    uint64_t cand = 0;
+    for (int p = 0; p < P && !status;) {
+      if (cand > 20000000ull) { status = S_BOUNDS; break; }
+      double t[D];
+      for (int k = 0; k < D; k++)
+        t[k] = B.mn[k] == B.mx[k] ? B.mn[k] : uniform_between(B.mn[k], B.mx[k], draw_u01(seed, PH_INIT_POS, cand, 0, k));
+      cand++;
+      if (B.within(t)) {
+        std::copy(t, t + D, &x[(size_t)p * D]);
+        p++;
+      }
+    }
+    for (int p = 0; p < P; p++)
+      for (int k = 0; k < D; k++) {
+        const double w = B.mx[k] - B.mn[k];
+        v[(size_t)p * D + k] = (-w == w) ? -w : uniform_between(-w, w, draw_u01(seed, PH_INIT_VEL, p, 0, k));
+      }
+    auto evaluate = [&]() -> int {
+      CK(cudaMemcpyAsync(bs.labels.p, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      run_binary(g, cg, ds.p, hstar, bs, P, vs_max, true, nullptr, 0, s);
+      CK(cudaMemcpyAsync(cost.data(), bs.cost.p, P * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(est.data(), bs.status.p, P * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int p = 0; p < P; p++)
+        if (est[p]) return est[p];
+      return S_OK;
+    };
+    auto dump = [&](int it) {
+      if (!trace) return;
+      for (int p = 0; p < P; p++) {
+        double *t = trace + ((size_t)it * P + p) * (D + 1);
+        for (int k = 0; k < D; k++) t[k] = x[(size_t)p * D + k];
+        t[D] = cost[p];
+      }
+    };
+    if (!status) status = evaluate();
+    if (!status) {  // particleswarm.rs:111-134: sorted by cost once (stable, NaN last)
+      std::vector<int> idx(P);
+      for (int p = 0; p < P; p++) idx[p] = p;
+      auto key = [&](int p) { return cost[p] != cost[p] ? INFINITY : cost[p]; };
+      std::stable_sort(idx.begin(), idx.end(), [&](int a_, int b_) { return key(a_) < key(b_); });
+      std::vector<double> x2(x.size()), v2(v.size()), c2(P);
+      for (int r = 0; r < P; r++) {
+        for (int k = 0; k < D; k++) {
+          x2[(size_t)r * D + k] = x[(size_t)idx[r] * D + k];
+          v2[(size_t)r * D + k] = v[(size_t)idx[r] * D + k];
+        }
+        c2[r] = cost[idx[r]];
+      }
+      x = x2; v = v2; cost = c2;
+      bx = x; bcost = cost;
+      std::copy(x.begin(), x.begin() + D, gx.begin());
+      gcost = cost[0];
+      dump(0);
+    }
+    for (int it = 0; it < st.max_iters && !status; it++) {  // particleswarm.rs:219-307
+      for (int p = 0; p < P && !status; p++) {
+        double *xp = &x[(size_t)p * D], *vp = &v[(size_t)p * D];
+        const double *bp = &bx[(size_t)p * D];
+        for (int k = 0; k < D; k++) {
+          const double momentum = vp[k] * st.inertia_factor;
+          const double to_opt = bp[k] - xp[k];
+          const double pull = (to_opt == 0.0 ? 0.0 : uniform_between(0.0, to_opt, draw_u01(seed, PH_ITER, it, p, 2 * k))) * st.cognitive_factor;
+          const double to_g = gx[k] - xp[k];
+          const double pullg = (to_g == 0.0 ? 0.0 : uniform_between(0.0, to_g, draw_u01(seed, PH_ITER, it, p, 2 * k + 1))) * st.social_factor;
+          vp[k] = momentum + pull + pullg;
+          double nx[D];
+          std::copy(xp, xp + D, nx);
+          nx[k] += vp[k];
+          double cl;
+          const int cs = B.clamp_1d(nx, k, cl);
+          if (cs) { status = cs; break; }
+          xp[k] = cl;
+          if (!B.within(xp)) { status = S_BOUNDS; break; }
+        }
+      }
+      if (status) break;
+      status = evaluate();
+      if (status) break;
+      for (int p = 0; p < P; p++) {
+        if (cost[p] < bcost[p]) {
+          std::copy(&x[(size_t)p * D], &x[(size_t)p * D] + D, &bx[(size_t)p * D]);
+          bcost[p] = cost[p];
+          if (cost[p] < gcost) {
+            std::copy(&x[(size_t)p * D], &x[(size_t)p * D] + D, gx.begin());
+            gcost = cost[p];
+          }
+        }
+      }
+      dump(it + 1);
+    }
+    // continuum parameters at the best position (fitting.rs:674-686)
+    std::vector<float> pv;
+    if (!status) {
+      const int ps = device_param_stride(c);
+      DBuf<double> dpar;
+      dpar.alloc(ps);
+      CK(cudaMemcpyAsync(bs.labels.p, gx.data(), D * sizeof(double), cudaMemcpyHostToDevice, s));
+      run_binary(g, cg, ds.p, hstar, bs, 1, std::max(gx[3], gx[8]), true, dpar.p, ps, s);
+      std::vector<double> hp(ps);
+      int hs = 0;
+      CK(cudaMemcpyAsync(hp.data(), dpar.p, ps * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&hs, bs.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (hs) status = hs;
+      else pv = params_from_device(c, hp.data());
+    }
+    std::memset(res, 0, sizeof *res);
+    for (int k = 0; k < 5; k++) {
+      res->label1[k] = gx[k];
+      res->label2[k] = gx[5 + k];
+    }
+    res->light_ratio = gx[10];
+    res->chi2 = gcost;
+    res->iterations = st.max_iters;
+    res->status = status;
+    res->n_params = (int)pv.size();
+    res->time = now_s() - t0;
+    if (params) std::copy(pv.begin(), pv.end(), params);
+  });
+}
+
 // ------------------------------------------------------------- fit
 static int fit_common(const pasta_grid *gc, std::vector<StarInput> &in, int mode, pasta_fit_result *results,
                       float *const *params, double *trace) {

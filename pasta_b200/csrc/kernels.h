@@ -101,6 +101,42 @@ void launch_gauss_batch(int N, const DevStar *star, const float *in, float *out,
 void launch_resample_rows(int N, int kind, const DevStar *star, int n_obs, const float *in, float *out, int M,
                           cudaStream_t s);
 
+// ---------------------------------------------------------------- binaries
+// Linear interpolation corners of one component's continuum
+// (interpolate.rs:536-600): 8 grid rows, their f32 weights and factors.
+struct LinRec {
+  int cols[8];
+  float w[8];
+  float f[8];
+  int status;
+};
+// L binary labels (star 1 [5], star 2 [5], light ratio) evaluated as 2L
+// component evaluations: star 1 of every label, then star 2 of every label.
+struct BinaryBatch {
+  int L;
+  const double *labels;   // [L][11]
+  double *comp_labels;    // [2L][5] (RV 0: the shift is applied per observed pixel)
+  LinRec *lin;            // [2L]
+  double *part;           // [2L][lin_tiles] partial sums of the continuum rows
+  int lin_tiles;
+  EvalPrep *cprep;        // [L] status and star of every label for the continuum fit
+  float *model;           // [L][model_stride] binary model at the observed pixels
+  int64_t model_stride;
+};
+int linear_tiles(int npx);
+// component labels and continuum corners (Gc: the continuum grid)
+void launch_binary_split(const DevGrid &Gc, const BinaryBatch &bb, cudaStream_t s);
+// continuum rows into the workspace buffer without the broadened row
+void launch_interp_linear(const DevGrid &Gc, const EvalBatch &comp, const BinaryBatch &bb, cudaStream_t s);
+// interpolate_linear entry point: corners of L labels [L][3], then R rows into
+// out [R][stride] with the per-tile sums part [R][linear_tiles(npx)]
+void launch_linear_prep(const DevGrid &Gc, const double *tml, int L, LinRec *lin, cudaStream_t s);
+void launch_interp_linear_rows(const DevGrid &Gc, const LinRec *lin, int R, float *out, int64_t stride,
+                               double *part, cudaStream_t s);
+// light ratio, shift, resampling and sum of the two stars (Nc continuum pixels)
+void launch_binary_combine(const DevGrid &G, int Nc, const EvalBatch &comp, const BinaryBatch &bb, int n_obs,
+                           cudaStream_t s);
+
 // swarm state of S stars x Pmax particles (structure of arrays)
 struct Swarm {
   int S, Pmax;

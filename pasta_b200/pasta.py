@@ -38,7 +38,7 @@ __all__ = [
     "LinearModelContinuumFitter", "FixedContinuum", "ConstantContinuum", "FixConstraint",
     "RangeConstraint", "get_vsini_kernel", "InMemInterpolator", "OnDiskInterpolator",
     "CachedInterpolator", "PyWavelengthDispersion", "PyContinuumFitter", "SingleFitter",
-    "Server", "PastaError", "LabelUncertainties",
+    "Server", "PastaError", "LabelUncertainties", "BinaryFitter", "BinaryOptimizationResult",
 ]
 
 PastaError = _ffi.PastaError
@@ -149,6 +149,34 @@ class OptimizationResult:
     def from_dict(d):
         return OptimizationResult(Label.from_dict(d["label"]), d["continuum_params"], d["chi2"], d["iterations"],
                                   d["time"])
+
+
+class BinaryOptimizationResult:
+    """lib.rs:296-360."""
+
+    def __init__(self, label1: Label, label2: Label, light_ratio: float, continuum_params, chi2: float,
+                 iterations: int, time: float):
+        self.label1 = label1
+        self.label2 = label2
+        self.light_ratio = float(light_ratio)
+        self.continuum_params = [float(x) for x in continuum_params]
+        self.chi2 = float(chi2)
+        self.iterations = int(iterations)
+        self.time = float(time)
+
+    def to_dict(self):
+        return dict(label1=self.label1.to_dict(), label2=self.label2.to_dict(), light_ratio=self.light_ratio,
+                    continuum_params=list(self.continuum_params), chi2=self.chi2, iterations=self.iterations,
+                    time=self.time)
+
+    def to_json(self):
+        return json.dumps(self.to_dict(), separators=(",", ":"))
+
+    @staticmethod
+    def from_dict(d):
+        return BinaryOptimizationResult(Label.from_dict(d["label1"]), Label.from_dict(d["label2"]),
+                                        d["light_ratio"], d["continuum_params"], d["chi2"], d["iterations"],
+                                        d["time"])
 
 
 # ------------------------------------------------------------ dispersions
@@ -555,6 +583,36 @@ class _Interpolator:
         self._raise_status(st)
         return out[0]
 
+    def interpolate_linear(self, teff, m, logg) -> np.ndarray:
+        """Trilinear interpolation over the 8 surrounding models
+        (interpolate.rs:985-1028; lib.rs:1127-1139)."""
+        lab = self._labels([teff, m, logg], 3)
+        out = np.empty((1, self._grid.npx), np.float32)
+        st = np.zeros(1, np.int32)
+        check(lib().pasta_interpolate_linear(self._grid._h, ptr(lab), 1, ptr(out), ptr(st)))
+        self._raise_status(st, "linear interpolation")
+        return out[0]
+
+    def produce_binary_model_norm(self, continuum_interpolator, dispersion, labels1, labels2,
+                                  light_ratio: float) -> np.ndarray:
+        """Normalised model of a binary (lib.rs:1013-1041): each star's
+        normalised model weighted by its continuum from the continuum
+        interpolator (a grid of unnormalised models), light ratio
+        light_ratio * mean(c1) / mean(c2) (interpolate.rs:822-893)."""
+        lab = f64(np.concatenate([np.asarray(labels1, np.float64).reshape(5),
+                                  np.asarray(labels2, np.float64).reshape(5), [float(light_ratio)]])[None, :])
+        out = np.empty((1, len(dispersion.wl)), np.float32)
+        st = np.zeros(1, np.int32)
+        check(lib().pasta_binary_model(self._grid._h, continuum_interpolator._grid._h, dispersion._h, ptr(lab), 1,
+                                       ptr(out), ptr(st)))
+        self._raise_status(st, "binary model production")
+        return out[0]
+
+    def get_binary_fitter(self, dispersion, continuum_fitter, settings: PSOSettings, vsini_range,
+                          rv_range) -> "BinaryFitter":
+        """lib.rs:1177-1193."""
+        return BinaryFitter(dispersion, continuum_fitter, settings, vsini_range, rv_range)
+
     def get_kernels(self, wl, disp) -> np.ndarray:
         """Variable-resolution kernels, width x n_synth (lib.rs:1043-1060)."""
         return VariableResolutionDispersion(wl, disp, self.synth_wl).kernels()
@@ -858,6 +916,84 @@ class SingleFitter:
         return res
 
 
+class BinaryFitter:
+    """InMemBinaryFitter / OnDiskBinaryFitter / CachedBinaryFitter
+    (lib.rs:1630-1699; fitting.rs:571-717): 11 parameters, star 1
+    (teff, m, logg, vsini, rv), star 2 (the same) and the light ratio."""
+
+    def __init__(self, dispersion, continuum_fitter, settings: PSOSettings, vsini_range, rv_range):
+        self.dispersion = dispersion
+        self.continuum_fitter = continuum_fitter
+        self.settings = settings
+        self.vsini_range = tuple(map(float, vsini_range))
+        self.rv_range = tuple(map(float, rv_range))
+
+    def _st(self, constraints) -> _ffi.BinarySettingsC:
+        st = _ffi.BinarySettingsC()
+        s = self.settings
+        st.num_particles, st.max_iters = s.num_particles, s.max_iters
+        st.inertia_factor, st.cognitive_factor = s.inertia_factor, s.cognitive_factor
+        st.social_factor, st.delta = s.social_factor, s.delta
+        st.vsini_lo, st.vsini_hi = self.vsini_range
+        st.rv_lo, st.rv_hi = self.rv_range
+        for c in constraints or ():
+            if not 0 <= c.parameter < 11:
+                raise IndexError("constraint parameter index out of range")
+            st.ckind[c.parameter], st.ca[c.parameter], st.cb[c.parameter] = c.kind, c.a, c.b
+        return st
+
+    def fit(self, interpolator, continuum_interpolator, observed_flux, observed_var,
+            trace_directory: Optional[str] = None, best_particle_file: Optional[str] = None,
+            parallelize: Optional[bool] = None, constraints=None, seed: Optional[int] = None,
+            _trace: bool = False) -> BinaryOptimizationResult:
+        """PSO fit of a binary (lib.rs:1636-1671).  ``parallelize`` is accepted
+        for API compatibility (every particle of an iteration is evaluated in
+        one device batch)."""
+        if trace_directory is not None and best_particle_file is not None:
+            raise RuntimeError("Cannot specify both trace_directory and best_particle_file")
+        fl, vr = f32(observed_flux), f32(observed_var)
+        if fl.shape != vr.shape:
+            raise ValueError("Flux and variance vectors must have the same length")
+        if len(fl) != len(self.dispersion.wl):
+            raise PastaError(-1, "Observed spectrum and target dispersion must have the same length")
+        st = self._st(constraints)
+        res = _ffi.BinaryResultC()
+        params = np.zeros(max(self.continuum_fitter.nparams(), 1), np.float32)
+        want_trace = _trace or trace_directory is not None or best_particle_file is not None
+        tr = np.zeros((st.max_iters + 1, st.num_particles, 12)) if want_trace else None
+        check(lib().pasta_binary_fit(interpolator._grid._h, continuum_interpolator._grid._h, self.dispersion._h,
+                                     self.continuum_fitter._h, C.byref(st), ptr(fl), ptr(vr), len(fl),
+                                     _seed(seed), C.byref(res), ptr(params), ptr(tr)))
+        if res.status:
+            raise PastaError(int(res.status), "binary fit failed (status %d)" % res.status)
+        if trace_directory is not None or best_particle_file is not None:
+            _write_trace(tr, trace_directory, best_particle_file)
+        out = BinaryOptimizationResult(Label(*res.label1), Label(*res.label2), res.light_ratio,
+                                       params[:res.n_params], res.chi2, res.iterations, res.time)
+        if _trace:
+            out._trace = tr
+        return out
+
+    def chi2(self, interpolator, continuum_interpolator, observed_flux, observed_var, labels,
+             allow_nan: Optional[bool] = None) -> list:
+        """Chi2 at fixed 11-parameter labels (lib.rs:1673-1698); failures give
+        NaN unless allow_nan is False."""
+        fl, vr = f32(observed_flux), f32(observed_var)
+        if len(fl) != len(vr):
+            raise ValueError("Flux and variance vectors must have the same length")
+        lab = f64(np.atleast_2d(np.asarray(labels, dtype=np.float64)))
+        if lab.shape[1] != 11:
+            raise ValueError("binary labels have 11 columns")
+        out = np.empty(len(lab))
+        st = np.zeros(len(lab), np.int32)
+        check(lib().pasta_binary_chi2(interpolator._grid._h, continuum_interpolator._grid._h, self.dispersion._h,
+                                      self.continuum_fitter._h, ptr(fl), ptr(vr), len(fl), ptr(lab), len(lab),
+                                      ptr(out), ptr(st)))
+        if allow_nan is False:
+            _Interpolator._raise_status(st, "chi2")
+        return [float(x) for x in out]
+
+
 def _write_trace(tr, trace_directory, best_particle_file):
     """PSOobserver / BestParticleObserver output (fitting.rs:217-296)."""
     if tr is None:
@@ -866,7 +1002,7 @@ def _write_trace(tr, trace_directory, best_particle_file):
     if trace_directory is not None:
         os.makedirs(trace_directory, exist_ok=True)
         for it in range(n_it):
-            vals = [{"position": list(map(float, p[:5])), "cost": float(p[5])} for p in tr[it + 1]]
+            vals = [{"position": list(map(float, p[:-1])), "cost": float(p[-1])} for p in tr[it + 1]]
             with open(os.path.join(trace_directory, "it_%d.json" % it), "w") as f:
                 json.dump(vals, f, separators=(",", ":"))
     if best_particle_file is not None:
@@ -874,9 +1010,9 @@ def _write_trace(tr, trace_directory, best_particle_file):
         hist = []
         for it in range(n_it):
             for p in tr[it + 1]:
-                if p[5] < best[5]:
+                if p[-1] < best[-1]:
                     best = p
-            hist.append({"position": list(map(float, best[:5])), "cost": float(best[5])})
+            hist.append({"position": list(map(float, best[:-1])), "cost": float(best[-1])})
             with open(best_particle_file, "w") as f:
                 json.dump(hist, f, separators=(",", ":"))
 

@@ -234,12 +234,8 @@ def observed_window(spec: GridSpec, rv_max: float, vsini_max: float, resolution:
     return float(wl[margin]), float(wl[spec.n_px - 1 - margin - spec.n_px % 128])
 
 
-def make_star(spec: GridSpec, label, n_obs: int, snr: float, resolution: float, seed: int,
-              rv_max: float = 150.0, vsini_max: float = 300.0, lm: Optional[LineModel] = None,
-              profiles=None) -> Star:
-    """Noisy observed spectrum for label = (teff, m, logg, vsini, rv)."""
-    rng = np.random.default_rng(seed)
-    lm = lm or LineModel(spec)
+def _broadened(spec: GridSpec, label, resolution: float, lm: "LineModel", profiles=None) -> np.ndarray:
+    """Noiseless model at label on the synthetic grid, rotated and broadened."""
     wl = spec.wl()
     f = lm.flux(np.asarray(label[:3])[None, :], wl, profiles)[0]
     if spec.includes_factor:
@@ -255,6 +251,17 @@ def make_star(spec: GridSpec, label, n_obs: int, snr: float, resolution: float, 
         x = np.arange(n) - (n - 1) / 2
         g = np.exp(-0.5 * (x / sig) ** 2)
         f = _fft_convolve_same(f, g / g.sum())
+    return f
+
+
+def make_star(spec: GridSpec, label, n_obs: int, snr: float, resolution: float, seed: int,
+              rv_max: float = 150.0, vsini_max: float = 300.0, lm: Optional[LineModel] = None,
+              profiles=None) -> Star:
+    """Noisy observed spectrum for label = (teff, m, logg, vsini, rv)."""
+    rng = np.random.default_rng(seed)
+    lm = lm or LineModel(spec)
+    wl = spec.wl()
+    f = _broadened(spec, label, resolution, lm, profiles)
     lo, hi = observed_window(spec, rv_max, vsini_max, resolution)
     wl_obs = np.geomspace(lo, hi, n_obs)
     src = wl_obs * (1.0 - label[4] / C_KMS)
@@ -344,3 +351,58 @@ def make_stars(spec: GridSpec, labels: np.ndarray, n_obs, snr, resolution: float
             out.append(Star(wl_obs, flux.astype(np.float32), (sigma ** 2).astype(np.float32), lab[k].copy(),
                             float(snr[i])))
     return out
+
+
+# ------------------------------------------------------------------ binaries
+def continuum_shape(wl: np.ndarray, teff: float, m: float, logg: float) -> np.ndarray:
+    """Unnormalised continuum of a model: the blackbody at Teff relative to a
+    5772 K blackbody at 5000 A, scaled smoothly with [M/H] and logg."""
+    ref = blackbody(np.array([5000.0]), 5772.0)[0]
+    return blackbody(wl, teff) / ref * (1.0 + 0.05 * m + 0.02 * (logg - 4.0))
+
+
+def make_continuum_grid(spec: GridSpec):
+    """Grid of unnormalised continua on the axes and wavelengths of spec,
+    stored like an includes_factor grid (u16 of flux / max, f32 max per
+    model).  Returns (labels, spectra, maxima)."""
+    labels = gridpoints(spec)
+    wl = spec.wl()
+    n = len(labels)
+    spectra = np.empty((n, spec.n_px), dtype=np.uint16)
+    maxima = np.empty(n, dtype=np.float32)
+    for i, (t, m, g) in enumerate(labels):
+        f = continuum_shape(wl, t, m, g).astype(np.float32)
+        mx = np.float32(f.max())
+        maxima[i] = mx
+        spectra[i] = np.clip(np.rint(f / mx * 65535.0), 0, 65535).astype(np.uint16)
+    return labels, spectra, maxima
+
+
+def make_binary_star(spec: GridSpec, label1, label2, light_ratio: float, n_obs: int, snr: float,
+                     resolution: float, seed: int, rv_max: float = 150.0, vsini_max: float = 300.0) -> Star:
+    """Noisy normalised spectrum of a binary: each star's broadened model
+    weighted by its continuum, (n1 c1 + lr n2 c2) / (c1 + lr c2) with
+    lr = light_ratio mean(c1) / mean(c2), each star shifted by its own RV."""
+    rng = np.random.default_rng(seed)
+    lm = LineModel(spec)
+    wl = spec.wl()
+    n1 = _broadened(spec, label1, resolution, lm)
+    n2 = _broadened(spec, label2, resolution, lm)
+    c1 = continuum_shape(wl, *label1[:3])
+    c2 = continuum_shape(wl, *label2[:3])
+    lr = light_ratio * c1.mean() / c2.mean()
+    lo, hi = observed_window(spec, rv_max, vsini_max, resolution)
+    wl_obs = np.geomspace(lo, hi, n_obs)
+
+    def at(arr, rv):
+        return np.interp(np.log10(wl_obs * (1.0 - rv / C_KMS)), np.log10(wl), arr)
+
+    a1, k1, a2, k2 = at(n1, label1[4]), at(c1, label1[4]), at(n2, label2[4]), at(c2, label2[4])
+    model = (a1 * k1 + lr * a2 * k2) / (k1 + lr * k2)
+    x = np.linspace(-1.0, 1.0, n_obs)
+    b1, b2 = rng.uniform(-0.2, 0.2, 2)
+    signal = model * (1.0 + b1 * x + b2 * x * x)
+    sigma = np.abs(signal) / snr + 1e-6
+    flux = signal + sigma * rng.standard_normal(n_obs)
+    lab = np.concatenate([np.asarray(label1, np.float64), np.asarray(label2, np.float64), [light_ratio]])
+    return Star(wl_obs, flux.astype(np.float32), (sigma ** 2).astype(np.float32), lab, snr)

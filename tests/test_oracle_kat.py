@@ -208,3 +208,86 @@ def test_uncertainty_crossings_bracket_the_target(small):
             assert f[0] * f[1] <= 0.0, (i, side, dist, f)
             found += 1
     assert found >= 8
+
+
+# ------------------------------------------------------------------ binaries
+def test_linear_interpolation_known_answers():
+    """interpolate_linear (interpolate.rs:985-1028, cubic.rs:6-10): at a node the
+    weights are one-hot, every pixel is u16 / 65535 * factor; spectra linear in
+    each label (a trilinear field) are reproduced anywhere inside the grid;
+    the weights sum to one; outside the grid is an error."""
+    pts, spectra, coef = _poly_grid(1)
+    g = O.Grid(pts, spectra, None, O.WL_LOGSPACE, 3.6, 1e-5)
+    for i in (0, 17, 240, len(pts) - 1):
+        out = g.interpolate_linear(*pts[i], O.F64)
+        np.testing.assert_allclose(out, spectra[i] / 65535.0 / 65535.0, rtol=1e-12)
+    for lab in [(7130.0, 0.07, 4.02), (6000.0, -0.5, 3.5), (7999.0, 0.49, 4.49), (6250.0, 0.0, 3.75)]:
+        cols, w = g.local_grid_linear(*lab)
+        assert abs(w.sum() - 1.0) < 1e-12
+        assert (cols >= 0).all()
+        out = g.interpolate_linear(*lab, O.F64) * 65535.0 * 65535.0
+        x = np.array([(lab[0] - 6000) / 2000, lab[1] + 0.5, lab[2] - 3.5])
+        exact = (0.1 + 0.25 * (x[0] * coef[:, 0] + x[1] * coef[:, 1] + x[2] * coef[:, 2])) * 65535.0
+        assert np.abs(out - exact).max() <= 0.51  # quantisation of the nodes
+    for bad in [(5999.0, 0.0, 4.0), (7000.0, 0.6, 4.0), (7000.0, 0.0, 4.6)]:
+        with pytest.raises(O.OracleError):
+            g.interpolate_linear(*bad)
+
+
+@pytest.fixture(scope="module")
+def binary_small(small):
+    spec, labels, spectra, g = small
+    cl, cs, cf = S.make_continuum_grid(spec)
+    gc = O.Grid(cl, cs, cf, O.WL_LOGSPACE, spec.log_first, spec.log_step)
+    star = S.make_binary_star(spec, [7600.0, 0.1, 4.1, 30.0, -40.0], [6300.0, -0.2, 3.8, 10.0, 45.0], 0.6,
+                              3000, 150.0, 85000.0, seed=5)
+    d = O.Disp(g, O.DISP_FIXED, star.wl, 85000.0)
+    return spec, g, gc, d, star
+
+
+def test_binary_model_identities(binary_small):
+    """produce_binary_model_norm (interpolate.rs:868-893): two identical stars
+    give the single-star model, a zero light ratio gives star 1 alone, and
+    swapping the stars with light ratio r -> the model with 1/r."""
+    spec, g, gc, d, star = binary_small
+    l1 = [7600.0, 0.1, 4.1, 30.0, -40.0]
+    l2 = [6300.0, -0.2, 3.8, 10.0, 45.0]
+    single = d.produce_model(l1, O.F64)
+    np.testing.assert_allclose(O.binary_model(g, gc, d, l1 + l1 + [0.4], O.F64), single, rtol=1e-12)
+    np.testing.assert_allclose(O.binary_model(g, gc, d, l1 + l2 + [0.0], O.F64), single, rtol=1e-12)
+    a = O.binary_model(g, gc, d, l1 + l2 + [0.5], O.F64)
+    b = O.binary_model(g, gc, d, l2 + l1 + [2.0], O.F64)
+    np.testing.assert_allclose(a, b, rtol=1e-12)
+    m32 = O.binary_model(g, gc, d, l1 + l2 + [0.5], O.F32)
+    assert np.abs(m32 - a).max() / np.abs(a).max() < 1e-5
+
+
+def test_binary_chi2_is_smallest_at_the_truth(binary_small):
+    spec, g, gc, d, star = binary_small
+    oc = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    truth = list(star.label)
+    labs = [truth]
+    for k, dx in [(0, 150.0), (4, 8.0), (5, -150.0), (9, -8.0), (10, 0.2)]:
+        x = list(truth)
+        x[k] += dx
+        labs.append(x)
+    c, st = O.binary_chi2(g, gc, d, oc, star.flux, star.var, labs, O.F64)
+    assert (st == 0).all()
+    assert c[0] < 1.1 and (c[1:] > c[0]).all(), c
+    bad = list(truth)
+    bad[5] = 9000.0  # star 2 outside the grid
+    c, st = O.binary_chi2(g, gc, d, oc, star.flux, star.var, [bad], O.F64)
+    assert st[0] != 0 and np.isnan(c[0])
+
+
+def test_binary_fit_is_deterministic_and_bounded(binary_small):
+    spec, g, gc, d, star = binary_small
+    oc = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    st = O.binary_settings(12, 4, (0.0, 100.0), (-100.0, 100.0), constraints=[(10, 1, 0.6, 0.6)])
+    r1, rc1 = O.binary_fit(g, gc, d, oc, st, star.flux, star.var, 9, O.F64, nthreads=2)
+    r2, rc2 = O.binary_fit(g, gc, d, oc, st, star.flux, star.var, 9, O.F64, nthreads=3)
+    assert rc1 == 0 and rc2 == 0
+    assert r1["chi2"] == r2["chi2"]
+    np.testing.assert_array_equal(r1["label1"], r2["label1"])
+    assert r1["light_ratio"] == 0.6
+    assert 0.0 <= r1["label1"][3] <= 100.0 and -100.0 <= r1["label2"][4] <= 100.0
