@@ -197,6 +197,65 @@ def serve_latency(P, interp, stars, settings, seeds, rate, n_req, seed):
 
 
 # ------------------------------------------------------------------ our arm
+def binary_leg(P, S, n_stars, cpu, seed):
+    """BinaryFitter on the config-0 grid (9 x 11 x 5 x 20,000 px) with a
+    continuum grid of unnormalised models on the same axes: n_stars synthetic
+    binaries (15,000 observed pixels, SNR 100, R = 85,000), 5 chunks of degree
+    8, PSO 40 x 100, each fit through the public API (BinaryFitter.fit, the
+    reference's per-star call).  cpu: the oracle's binary fit (FP32 mirror,
+    particles on all host threads as with parallelize=true) on a bounded
+    sample: one star, initial swarm + 2 iterations, scaled to 101 rounds."""
+    import torch
+    spec0 = S.config0_grid(n_px=20000)
+    labels, spectra, factors = S.make_grid(spec0)
+    cl, cs, cf = S.make_continuum_grid(spec0)
+    wl = P.WlGrid(spec0.log_first, spec0.log_step, spec0.n_px, log=True)
+    interp = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+    cint = P.InMemInterpolator.from_arrays(cl, cs, cf, wl)
+    rng = np.random.default_rng(seed)
+
+    def lab():
+        return [rng.uniform(6000.0, 8000.0), rng.uniform(-0.5, 0.5), rng.uniform(3.5, 4.5),
+                rng.uniform(0.0, 100.0), rng.uniform(-100.0, 100.0)]
+
+    stars = [S.make_binary_star(spec0, lab(), lab(), rng.uniform(0.2, 0.9), 15000, 100.0, RESOLUTION, seed=seed + i,
+                                rv_max=100.0, vsini_max=100.0) for i in range(n_stars)]
+    fitters = [interp.get_binary_fitter(P.FixedResolutionDispersion(s.wl, RESOLUTION, wl),
+                                        P.ChunkContinuumFitter(s.wl, 5, 8, 0.2), P.PSOSettings(40, 100),
+                                        (0.0, 100.0), (-100.0, 100.0)) for s in stars]
+    warm = interp.get_binary_fitter(fitters[0].dispersion, fitters[0].continuum_fitter, P.PSOSettings(40, 3),
+                                    (0.0, 100.0), (-100.0, 100.0))
+    warm.fit(interp, cint, stars[0].flux, stars[0].var, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = [f.fit(interp, cint, s.flux, s.var, seed=seed + 17 * i) for i, (f, s) in enumerate(zip(fitters, stars))]
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    evals = n_stars * 40 * 101
+    out = {"workload": "binary fits (BinaryFitter.fit per star): config-0 grid 9x11x5 x 20000 px + continuum grid, "
+                       "N_obs 15000, 5 chunks deg 8, PSO 40x100 over 11 parameters",
+           "stars": n_stars, "fits_per_s": n_stars / t, "chi2_evals_per_s": evals / t, "seconds": t,
+           "median_chi2": float(np.median([r.chi2 for r in res]))}
+    if cpu:
+        O = _oracle()
+        og = O.Grid(labels, spectra, factors, O.WL_LOGSPACE, spec0.log_first, spec0.log_step)
+        ogc = O.Grid(cl, cs, cf, O.WL_LOGSPACE, spec0.log_first, spec0.log_step)
+        s = stars[0]
+        od = O.Disp(og, O.DISP_FIXED, s.wl, RESOLUTION)
+        oc = O.Cont(O.CONT_CHUNK, s.wl, 5, 8, 0.2)
+        st = O.binary_settings(40, 2, (0.0, 100.0), (-100.0, 100.0))
+        nthreads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        r, rc = O.binary_fit(og, ogc, od, oc, st, s.flux, s.var, seed, O.F32, nthreads=nthreads)
+        tc = time.perf_counter() - t0
+        per_fit = tc / 3 * 101
+        out["cpu_baseline"] = {"value": 1.0 / per_fit, "unit": "binary fits/s", "cores": nthreads, "kind": "port",
+                               "sample": "1 star, initial swarm + 2 iterations (3 x 40 binary chi2 evals) in %.2fs, "
+                                         "scaled to 101 rounds" % tc}
+        out["gpu_over_cpu"] = out["fits_per_s"] * per_fit
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -324,6 +383,11 @@ def run_ours(args):
     same = all(a.label.as_list() == r.label.as_list() and a.chi2 == r.chi2 for a, r in zip(plain, res[:n_plain]))
     plain_fits = n_plain / t_plain
 
+    # -------- binary fits (BinaryFitter, config-0 sizes)
+    binary = binary_leg(P, S, args.binary_stars, rank == 0 and world == 1 and not args.no_cpu,
+                        seed=5150 + rank) if args.binary_stars > 0 else None
+    torch.cuda.synchronize(dev)
+
     # -------- served time-to-fit: Poisson arrivals, each request its own
     # continuum settings (4-12 chunks, degree 3-8), stars of the workload
     lat = serve_latency(P, interp, stars, settings, seeds, rate=args.serve_rate, n_req=args.serve_requests,
@@ -389,6 +453,7 @@ def run_ours(args):
                 "seconds": t_e2e, "what": "batched form: fit_many of %d stars from host arrays to results "
                                           "(201 PSO steps + final refit); bytes are per call" % n_stars},
         "latency_s": lat,
+        "binary": binary,
         "plain_gpu": {"fits_per_s": plain_fits, "stars": n_plain, "identical_results": same,
                       "batched_e2e_over_plain": e2e_fits / (plain_fits * world)},
         "label_error_vs_truth": {"median_abs": np.median(err, axis=0).tolist(),
@@ -521,6 +586,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=30.0, help="served latency run: arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=300, help="served latency run: requests (0: skip)")
+    ap.add_argument("--binary-stars", type=int, default=16, help="binary-fit leg: stars (0: skip)")
     ap.add_argument("--stages-only", action="store_true",
                     help="profiling aid: one mid-fit batched step, stage by stage, in an NVTX range 'stages'")
     args = ap.parse_args()

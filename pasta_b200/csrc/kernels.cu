@@ -13,6 +13,8 @@
 //   k_resample_out / k_copy_broadened serve the model entry points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "fft.cuh"
 #include "kernels.h"
@@ -52,36 +54,45 @@ __device__ __forceinline__ unsigned long long cols_hash(const int *c) {
   return h;
 }
 
-// One CTA of SEG threads per segment of SEG consecutive evaluations.
-__global__ void __launch_bounds__(SEG) k_group(DevGrid G, EvalBatch b) {
+// One CTA per segment of SEG consecutive evaluations: slice 0 (SEG threads)
+// finds the groups, then GROUP_SLICES slices of SEG threads write the group
+// records, one group per slice at a time (thread t of a slice handles
+// neighbour row t).
+constexpr int GROUP_SLICES = 4;
+__global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatch b) {
   __shared__ unsigned long long hs[SEG];
   __shared__ int ok[SEG], lead[SEG], gid[SEG], slot[SEG], open_g[SEG], fill[SEG];
-  __shared__ int ng, cnt[2];
-  const int s = blockIdx.x, t = threadIdx.x, e = s * SEG + t;
-  const bool v = e < b.E && b.prep[e].status == 0;
-  ok[t] = v;
-  hs[t] = v ? cols_hash(b.prep[e].cols) : 0ull;
+  __shared__ int ng;
+  __shared__ int cnt[GROUP_SLICES][2];
+  __shared__ int mem[GROUP_SLICES][GROUP_MAX];
+  const int s = blockIdx.x, tid = threadIdx.x, t = tid % SEG, sl = tid / SEG, e = s * SEG + t;
+  if (sl == 0) {
+    const bool v = e < b.E && b.prep[e].status == 0;
+    ok[t] = v;
+    hs[t] = v ? cols_hash(b.prep[e].cols) : 0ull;
+  }
   __syncthreads();
-  // leader: the first earlier evaluation with the same columns
-  int L = v ? t : -1;
-  if (v) {
-    const int *c = b.prep[e].cols;
-    for (int u = 0; u < t; u++) {
-      if (!ok[u] || hs[u] != hs[t]) continue;
-      const int *cu = b.prep[s * SEG + u].cols;
-      bool same = true;
-      for (int n = 0; n < 64 && same; n++) same = cu[n] == c[n];
-      if (same) {
-        L = u;
-        break;
+  if (sl == 0) {  // leader: the first earlier evaluation with the same columns
+    int L = ok[t] ? t : -1;
+    if (ok[t]) {
+      const int *c = b.prep[e].cols;
+      for (int u = 0; u < t; u++) {
+        if (!ok[u] || hs[u] != hs[t]) continue;
+        const int *cu = b.prep[s * SEG + u].cols;
+        bool same = true;
+        for (int n = 0; n < 64 && same; n++) same = cu[n] == c[n];
+        if (same) {
+          L = u;
+          break;
+        }
       }
     }
+    lead[t] = L;
+    open_g[t] = -1;
+    fill[t] = 0;
   }
-  lead[t] = L;
-  open_g[t] = -1;
-  fill[t] = 0;
   __syncthreads();
-  if (t == 0) {  // groups in evaluation order, at most GROUP_MAX members each
+  if (tid == 0) {  // groups in evaluation order, at most GROUP_MAX members each
     int n = 0;
     for (int u = 0; u < SEG; u++) {
       gid[u] = -1;
@@ -98,50 +109,55 @@ __global__ void __launch_bounds__(SEG) k_group(DevGrid G, EvalBatch b) {
     b.gcount[s] = n;
   }
   __syncthreads();
-  const int lane = t & 31, warp = t >> 5;
-  for (int g = 0; g < ng; g++) {
-    GroupRec &R = b.grec[(size_t)s * SEG + g];
-    // members in slot order
-    __shared__ int mem[GROUP_MAX];
-    if (t < GROUP_MAX) mem[t] = -1;
+  const int lane = tid & 31, wsl = t >> 5;  // warp within the slice
+  for (int base = 0; base < ng; base += GROUP_SLICES) {
+    const int g = base + sl;
+    const bool act = g < ng;
+    if (t < GROUP_MAX) mem[sl][t] = -1;
     __syncthreads();
-    if (gid[t] == g) mem[slot[t]] = e;
+    if (act && gid[t] == g) mem[sl][slot[t]] = s * SEG + t;
     __syncthreads();
-    int nm = 0;
-    for (int m = 0; m < GROUP_MAX; m++) nm += mem[m] >= 0;
-    // row t of the group: kept when any member weighs it
-    const int c = b.prep[mem[0]].cols[t];
-    const float f = c >= 0 ? G.factor[c] : 0.0f;
-    float w[GROUP_MAX], wf[GROUP_MAX];
+    GroupRec &R = b.grec[(size_t)s * SEG + (act ? g : 0)];
+    int c = -1, nm = 0;
+    float f = 0.0f, w[GROUP_MAX], wf[GROUP_MAX];
+    unsigned bal = 0u;
     bool keep = false;
+    if (act) {
+      for (int m = 0; m < GROUP_MAX; m++) nm += mem[sl][m] >= 0;
+      // row t of the group: kept when any member weighs it
+      c = b.prep[mem[sl][0]].cols[t];
+      f = c >= 0 ? G.factor[c] : 0.0f;
 #pragma unroll
-    for (int m = 0; m < GROUP_MAX; m++) {
-      w[m] = (mem[m] >= 0 && c >= 0) ? b.prep[mem[m]].w[t] : 0.0f;
-      wf[m] = w[m] * f;
-      keep |= wf[m] != 0.0f;
+      for (int m = 0; m < GROUP_MAX; m++) {
+        w[m] = (mem[sl][m] >= 0 && c >= 0) ? b.prep[mem[sl][m]].w[t] : 0.0f;
+        wf[m] = w[m] * f;
+        keep |= wf[m] != 0.0f;
+      }
+      bal = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) cnt[sl][wsl] = __popc(bal);
     }
-    const unsigned bal = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) cnt[warp] = __popc(bal);
     __syncthreads();
-    const int pos = __popc(bal & ((1u << lane) - 1u)) + (warp ? cnt[0] : 0);
-    if (keep) {
-      R.wf[pos] = make_float4(wf[0], wf[1], wf[2], wf[3]);
-      R.w[pos] = make_float4(w[0], w[1], w[2], w[3]);
-      R.col[pos] = c;
-      R.f[pos] = f;
-    }
-    const int kept = cnt[0] + cnt[1];
-    const int padded = (kept + 7) & ~7;
-    if (t >= kept && t < padded) {  // zero-weight padding rows (add exactly 0)
-      R.wf[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      R.w[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      R.col[t] = 0;
-      R.f[t] = 0.0f;
-    }
-    if (t < GROUP_MAX) R.member[t] = mem[t];
-    if (t == 0) {
-      R.nmem = nm;
-      R.nn = padded;
+    if (act) {
+      const int pos = __popc(bal & ((1u << lane) - 1u)) + (wsl ? cnt[sl][0] : 0);
+      if (keep) {
+        R.wf[pos] = make_float4(wf[0], wf[1], wf[2], wf[3]);
+        R.w[pos] = make_float4(w[0], w[1], w[2], w[3]);
+        R.col[pos] = c;
+        R.f[pos] = f;
+      }
+      const int kept = cnt[sl][0] + cnt[sl][1];
+      const int padded = (kept + 7) & ~7;
+      if (t >= kept && t < padded) {  // zero-weight padding rows (add exactly 0)
+        R.wf[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        R.w[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        R.col[t] = 0;
+        R.f[t] = 0.0f;
+      }
+      if (t < GROUP_MAX) R.member[t] = mem[sl][t];
+      if (t == 0) {
+        R.nmem = nm;
+        R.nn = padded;
+      }
     }
     __syncthreads();
   }
@@ -149,7 +165,7 @@ __global__ void __launch_bounds__(SEG) k_group(DevGrid G, EvalBatch b) {
 
 void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
-  k_group<<<(b.E + SEG - 1) / SEG, SEG, 0, s>>>(G, b);
+  k_group<<<(b.E + SEG - 1) / SEG, SEG * GROUP_SLICES, 0, s>>>(G, b);
   count_launch();
 }
 
@@ -227,13 +243,15 @@ __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch
 
 // Grid: x = segment, y = 2048-pixel tile, so CTAs that run together read
 // the same tile slab of the resident grid (57 MB for 13,860 x 80,000), which
-// stays in L2.  Each CTA walks its segment's groups.
+// stays in L2; z = slice of the segment's groups (groups z, z + Z, ...), more
+// than one only for batches too small to fill the GPU otherwise.  Groups have
+// disjoint members, so the slicing does not change any result.
 __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
   __shared__ GroupRec R;
   const int s = blockIdx.x;
   const int px = blockIdx.y * IT_TILE + threadIdx.x * 8;
   const int ng = b.gcount[s];
-  for (int g = 0; g < ng; g++) {
+  for (int g = blockIdx.z; g < ng; g += gridDim.z) {
     const float4 *src = reinterpret_cast<const float4 *>(b.grec + (size_t)s * SEG + g);
     float4 *dst = reinterpret_cast<float4 *>(&R);
     for (int i = threadIdx.x; i < (int)(sizeof(GroupRec) / 16); i += IT_T) dst[i] = src[i];
@@ -250,7 +268,10 @@ __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
 
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
-  dim3 grid((b.E + SEG - 1) / SEG, (G.npx + IT_TILE - 1) / IT_TILE);
+  const int segs = (b.E + SEG - 1) / SEG, tiles = (G.npx + IT_TILE - 1) / IT_TILE;
+  const int want = num_sms() * 6;  // two waves of the 3 CTAs an SM holds
+  const int z = segs * tiles >= want ? 1 : std::min(SEG, (want + segs * tiles - 1) / (segs * tiles));
+  dim3 grid(segs, tiles, z);
   k_interp<<<grid, IT_T, 0, s>>>(G, b);
   count_launch();
 }
