@@ -587,11 +587,18 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=30.0, help="served latency run: arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=300, help="served latency run: requests (0: skip)")
     ap.add_argument("--binary-stars", type=int, default=16, help="binary-fit leg: stars (0: skip)")
+    ap.add_argument("--binary-only", action="store_true",
+                    help="run only the binary-fit leg (with its CPU baseline unless --no-cpu) and print it")
     ap.add_argument("--stages-only", action="store_true",
                     help="profiling aid: one mid-fit batched step, stage by stage, in an NVTX range 'stages'")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.binary_only:
+        from pasta_b200 import pasta as P
+        from pasta_b200 import synth as S
+        print(json.dumps(binary_leg(P, S, max(args.binary_stars, 1), not args.no_cpu, seed=5150)), flush=True)
+        return
     line = run_reference(args) if args.impl == "reference" else run_ours(args)
     if line is not None:
         print(json.dumps(line), flush=True)
