@@ -90,12 +90,19 @@ int64_t pasta_kernel_launch_count(void);
  * (lib.rs:1875-1931).  labels: n x (teff, m, logg) in any order; spectra:
  * n x n_px uint16, row i for labels[i]; maxima: the includes_factor f32
  * maxima (model_fetchers.rs:53-63) or NULL.  The grid is uploaded once and
- * stays resident in HBM. */
+ * stays resident in HBM.  Creation also measures, on this device, up to
+ * which combined broadening width (rotation taps + 2 x instrument half
+ * width) a direct convolution beats the FFT blocks; the environment
+ * variable PASTA_DIRECT_MAX_TAPS fixes that width instead (0: FFT only). */
 int pasta_grid_create(const double *labels, const uint16_t *spectra,
                       const float *maxima, int64_t n_models, int64_t n_px,
                       int wl_kind, double wl_a, double wl_b,
                       const double *wl_values, pasta_grid **out);
 int pasta_grid_destroy(pasta_grid *g);
+/* the measured direct/FFT crossover in taps (no counterpart in the
+ * reference); set: 0..512, for the batches and fits started afterwards */
+int pasta_grid_direct_max(const pasta_grid *g, int32_t *taps);
+int pasta_grid_set_direct_max(pasta_grid *g, int32_t taps);
 /* sizes: n_teff, n_m, n_logg, n_px, n_models (lib.rs:1436-1461) */
 int pasta_grid_shape(const pasta_grid *g, int64_t *out5);
 int pasta_grid_axis(const pasta_grid *g, int axis, double *out);

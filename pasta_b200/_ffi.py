@@ -54,6 +54,8 @@ SIGNATURES = {
     "pasta_kernel_launch_count": (I64, []),
     "pasta_grid_create": (I, [P, P, P, I64, I64, I, D, D, P, P]),
     "pasta_grid_destroy": (I, [P]),
+    "pasta_grid_direct_max": (I, [P, P]),
+    "pasta_grid_set_direct_max": (I, [P, C.c_int32]),
     "pasta_grid_shape": (I, [P, P]),
     "pasta_grid_axis": (I, [P, I, P]),
     "pasta_grid_logg_limits": (I, [P, P, P]),

@@ -26,6 +26,10 @@ constexpr int MAX_LIN_K = 128;      // linear-model columns
 constexpr int MAX_PARTICLES = 1024;
 // the fused broadening kernel needs this many outputs per 2048-point block
 constexpr int MIN_FUSED_OUTPUTS = 128;
+// direct (non-FFT) broadening: outputs per tile, and the widest combined
+// kernel (rotation taps + 2 x instrument half width) it takes
+constexpr int DIRECT_TILE = 2048;
+constexpr int DIRECT_MAX_TAPS = 512;
 
 // Legendre recurrence in f32 with explicit rounding, evaluated identically
 // by the host (Gram matrices) and the device (moments, continuum):
@@ -121,6 +125,8 @@ struct EvalPrep {
   int final_in_b; // 1: the broadened spectrum ends in buffer B, else in A
   int epi;        // 1: k_broaden resamples to the observed pixels itself (no synth row)
   int mobs_in_b;  // model at the observed pixels: 1 = row of B, 0 = row of A
+  int direct;     // 1: broadened by direct convolution (k_direct) into B instead of the FFT kernels
+  int ndt;        // direct tiles of (DIRECT_TILE - 2 hg) & ~3 outputs over [o_lo & ~3, o_hi)
   int o_lo, o_hi; // synth pixels the resampler reads [o_lo, o_hi)
   int g_lo, g_hi; // rotation outputs the Gaussian reads [g_lo, g_hi)
   int i_lo, i_hi; // interpolated pixels needed [i_lo, i_hi) (multiples of 8)

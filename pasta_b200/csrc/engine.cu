@@ -216,6 +216,7 @@ struct pasta_grid {
   DBuf<int64_t> dcum;
   std::mutex mu;
   Workspace ws;
+  int direct_max = 0;  // combined kernels of at most this many taps are broadened directly (measured)
 };
 
 namespace {
@@ -709,6 +710,8 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.cpart = g->ws.cpart.p;
   b.given = a.given ? a.given + (size_t)off * a.given_stride : nullptr;
   b.given_stride = a.given_stride;
+  b.direct_max = g->direct_max;
+  b.max_dtiles = (int)((g->npx + DIRECT_TILE - DIRECT_MAX_TAPS - 1) / (DIRECT_TILE - DIRECT_MAX_TAPS));
   return b;
 }
 
@@ -1354,6 +1357,93 @@ int pasta_set_device(int device) {
 }
 
 // interpolate.rs:267-331 (Grid::new) + model_fetchers.rs:136-166 (column order)
+namespace {
+
+// Autotuner of the broadening path: the crossover between the direct and the
+// FFT broadening on this device.  For rotation widths on a ladder, the
+// pipeline runs 256 evaluations of one grid label over the whole synthetic
+// grid with either path, timed with CUDA events (best of 3 after a warm-up);
+// direct_max is the widest kernel up to which the direct path won at every
+// rung.  PASTA_DIRECT_MAX_TAPS fixes the value instead (0: FFT only);
+// PASTA_TUNE_VERBOSE prints the measured ladder.
+void tune_direct(pasta_grid *g) {
+  g->direct_max = 0;
+  if (const char *ev = getenv("PASTA_DIRECT_MAX_TAPS")) {
+    g->direct_max = std::max(0, std::min(DIRECT_MAX_TAPS, atoi(ev)));
+    return;
+  }
+  if (g->wl_kind == WL_NONUNI || !(g->d.dvelo > 0.0)) return;
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
+  const int E = 256;
+  const int ti = (int)g->tv.size() / 2;
+  const double t = g->tv[ti], mh = g->mv[g->mv.size() / 2], lg = g->lv[(g->llo[ti] + g->lhi[ti]) / 2];
+  DevStar st = make_star(nullptr, nullptr, nullptr, nullptr, 0);
+  st.disp_kind = DISP_NONE;
+  DBuf<DevStar> ds;
+  ds.upload(&st, 1);
+  DBuf<double> dl;
+  dl.alloc((size_t)E * 5);
+  DBuf<int> de;
+  de.upload(std::vector<int>(E, 0));
+  ensure_workspace(g, E, 0);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int ladder[] = {17, 33, 65, 97, 129, 193, 257, 385, 511};
+  int best = 0;
+  std::vector<double> lab((size_t)E * 5);
+  for (int w : ladder) {
+    double lo = 0.0, hi = 1e5;  // the largest vsini whose kernel has at most w taps
+    for (int it = 0; it < 80; it++) {
+      const double mid = 0.5 * (lo + hi);
+      if (rotation_width(mid, g->d.dvelo) <= w) lo = mid;
+      else hi = mid;
+    }
+    const int mw = rotation_width(lo, g->d.dvelo);
+    if (mw < 3 || mw > w) continue;
+    for (int i = 0; i < E; i++) {
+      double *q = &lab[(size_t)i * 5];
+      q[0] = t; q[1] = mh; q[2] = lg; q[3] = lo; q[4] = 0.0;
+    }
+    CK(cudaMemcpy(dl.p, lab.data(), lab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    EvalArgs a;
+    a.stars = ds.p;
+    a.labels = dl.p;
+    a.eval_star = de.p;
+    a.E = E;
+    a.full_window = 1;
+    a.max_m = mw;
+    star_kinds({st}, a);
+    float tm[2];
+    for (int mode = 0; mode < 2; mode++) {
+      g->direct_max = mode ? DIRECT_MAX_TAPS : 0;
+      run_evals(g, a, s);
+      float bt = 1e30f;
+      for (int rep = 0; rep < 3; rep++) {
+        CK(cudaEventRecord(e0, s));
+        run_evals(g, a, s);
+        CK(cudaEventRecord(e1, s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        bt = std::min(bt, ms);
+      }
+      tm[mode] = bt;
+    }
+    if (getenv("PASTA_TUNE_VERBOSE"))
+      fprintf(stderr, "pasta_b200 tune: %lld px, rotation %d taps: FFT %.4f ms, direct %.4f ms (%d evaluations)\n",
+              (long long)g->npx, mw, tm[0], tm[1], E);
+    if (tm[1] < tm[0]) best = mw;
+    else break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g->direct_max = best;
+}
+
+}  // namespace
+
 int pasta_grid_create(const double *labels, const uint16_t *spectra, const float *maxima, int64_t n_models,
                       int64_t n_px, int wl_kind, double wl_a, double wl_b, const double *wl_values,
                       pasta_grid **out) {
@@ -1451,7 +1541,19 @@ int pasta_grid_create(const double *labels, const uint16_t *spectra, const float
     if (wl_kind == WL_LIN) d.dvelo = wl_b / ((wl_a + wl_a + wl_b * (double)n_px) / 2.0);
     else if (wl_kind == WL_LOG) d.dvelo = M_LN10 * wl_b;
     else d.dvelo = 0.0;
+    tune_direct(g.get());
     *out = g.release();
+  });
+}
+
+int pasta_grid_direct_max(const pasta_grid *g, int32_t *out) {
+  return guard([&] { *out = g->direct_max; });
+}
+int pasta_grid_set_direct_max(pasta_grid *g, int32_t taps) {
+  return guard([&] {
+    if (taps < 0 || taps > DIRECT_MAX_TAPS) fail(PASTA_E_ARG, "direct_max must be in 0..%d", DIRECT_MAX_TAPS);
+    std::lock_guard<std::mutex> lk(g->mu);
+    g->direct_max = taps;
   });
 }
 

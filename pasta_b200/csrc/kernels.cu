@@ -663,6 +663,242 @@ void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cuda
   count_launch();
 }
 
+// ----------------------------------------------- direct broadening (narrow)
+// Evaluations whose combined kernel (m rotation taps + 2 hg instrument taps)
+// is narrow are convolved directly: per tile of DIRECT_TILE - 2 hg final
+// outputs [t0, t0 + n) the DIRECT_TILE rotation outputs [t0 - hg, t0 + n + hg) (zero outside the
+// grid, like the reference's cropped segment) and then the instrument
+// profile, both from shared memory, into B.  The result is the same linear
+// convolution the FFT path computes (convolve_rv.rs:121-157, 207-210,
+// 414-430, 484-529), to f32 roundoff.
+constexpr int DT_T = 256;
+constexpr int DT_X = DIRECT_TILE + DIRECT_MAX_TAPS + 32;  // staged input / rotation output (floats)
+constexpr int DT_HALF = DT_X / 2;                          // 1296 = 16 mod 32 (see dchunk)
+constexpr int DT_K = DIRECT_MAX_TAPS + 32;                // zero-padded taps
+static_assert(DT_X % 8 == 0 && DT_HALF % 32 == 16, "direct tile layout");
+
+// Rows of the direct path sit in shared memory chunk-interleaved: float4
+// chunk c (elements 4c..4c+3) at (c & 1) * DT_HALF + (c >> 1) * 4.  The
+// chunks 2t + q that the threads t of a warp read together are then
+// consecutive 16-byte words (no bank conflicts), and so are the chunks 2t,
+// 2t + 1 each thread writes.
+__device__ __forceinline__ int dchunk(int c) { return ((c & 1) ? DT_HALF : 0) + ((c >> 1) << 2); }
+__device__ __forceinline__ int dperm(int i) { return dchunk(i >> 2) + (i & 3); }
+
+// out(v) = sum_{j=-h..h} k[h + j] x(D + v - j), v in [0, n), n <= 8 DT_T: the
+// eight consecutive outputs v0 = 8t.. of thread t.  x (chunk-interleaved) is
+// readable (finite) over [0, n + 2h + 16); D - h is 0..3; kp holds k[0..2h]
+// at offset zp = 12 + the amount that makes 2h + (D - h) + zp a multiple of
+// 4, zeros around it, so every window of 12 taps is three aligned float4
+// reads and taps outside the kernel are exact zeros.  Each chunk of 4 inputs
+// costs 2 shared-memory reads (the input, one new tap float4) for 32 FMAs.
+__device__ __forceinline__ int direct_zp(int h, int pl) { return 12 + ((4 - ((2 * h + pl) & 3)) & 3); }
+
+__device__ __forceinline__ void conv_step(const float4 a, const float4 lo, float4 &mid, float4 &hi, float (&acc)[8]) {
+  const float T[12] = {lo.x, lo.y, lo.z, lo.w, mid.x, mid.y, mid.z, mid.w, hi.x, hi.y, hi.z, hi.w};
+  const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+#pragma unroll
+    for (int r = 0; r < 4; r++) acc[c] = fmaf(T[4 + c - r], av[r], acc[c]);
+  hi = mid;
+  mid = lo;
+}
+
+template <class Store>
+__device__ __forceinline__ void conv_blocked(const float *__restrict__ x, int D, int h, const float *__restrict__ kp,
+                                             int n, const Store &st) {
+  const int v0 = 8 * threadIdx.x;
+  if (v0 >= n) return;
+  const int pl = D - h;
+  const int z0 = 2 * h + pl + direct_zp(h, pl);  // multiple of 4
+  const int Q = (pl + 7 + 2 * h) / 4 + 1;
+  const float4 *xe = reinterpret_cast<const float4 *>(x) + threadIdx.x;            // chunks 2t, 2t + 2, ...
+  const float4 *xo = reinterpret_cast<const float4 *>(x + DT_HALF) + threadIdx.x;  // chunks 2t + 1, ...
+  const float4 *k4 = reinterpret_cast<const float4 *>(kp) + z0 / 4;
+  float acc[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) acc[c] = 0.0f;
+  // chunk q: inputs x(v0 + 4q + r), taps kp[z0 - 4q - 4 + i], i = 4 + c - r in 1..10
+  float4 hi = k4[1], mid = k4[0];
+  int q = 0;
+  for (; q + 1 < Q; q += 2) {
+    conv_step(xe[q >> 1], k4[-q - 1], mid, hi, acc);
+    conv_step(xo[q >> 1], k4[-q - 2], mid, hi, acc);
+  }
+  if (q < Q) conv_step(xe[q >> 1], k4[-q - 1], mid, hi, acc);
+  st(v0, acc);
+}
+
+// taps k[0..2h] (or the single tap 1 when taps == null) into kp with the
+// padding of conv_blocked for this D - h
+__device__ __forceinline__ void direct_taps(float *kp, const float *taps, int h, int pl) {
+  const int zp = direct_zp(h, pl);
+  for (int t = threadIdx.x; t < DT_K; t += DT_T) {
+    const int u = t - zp;
+    kp[t] = (u >= 0 && u <= 2 * h) ? (taps ? taps[u] : 1.0f) : 0.0f;
+  }
+}
+
+// final outputs per direct tile of an evaluation: a multiple of 4, so the
+// input alignment (and with it the padding of the rotation taps) is the same
+// for every tile of the evaluation; tiles start at o_lo rounded down to 4,
+// so the outputs are 16-byte aligned in the row
+__device__ __forceinline__ int direct_td(int hg) { return (DIRECT_TILE - 2 * hg) & ~3; }
+
+struct DirectTile {
+  int e, tile, m, hw, hg, t0, n, p0, nr, pl, x0;
+};
+__device__ __forceinline__ bool direct_tile(const EvalBatch &b, int e, int tile, DirectTile &d) {
+  const EvalPrep &P = b.prep[e];
+  if (P.status || !P.direct || tile >= P.ndt) return false;
+  d.e = e;
+  d.tile = tile;
+  d.m = P.m;
+  d.hw = (d.m - 1) / 2;
+  d.hg = P.hg;
+  const int td = direct_td(d.hg);
+  d.t0 = (P.o_lo & ~3) + tile * td;
+  d.n = min(td, P.o_hi - d.t0);
+  d.p0 = d.t0 - d.hg;  // rotation outputs [p0, p0 + nr)
+  d.nr = d.n + 2 * d.hg;
+  d.pl = (((d.p0 - d.hw) % 4) + 4) % 4;
+  d.x0 = d.p0 - d.hw - d.pl;  // inputs staged from x0, a multiple of 4
+  return true;
+}
+__device__ __forceinline__ void direct_stage(const EvalBatch &b, const DirectTile &d, float *xs) {
+  const EvalPrep &P = b.prep[d.e];
+  const float *row = b.bufA + (size_t)d.e * b.stride;
+  const int nx = (d.nr + 2 * d.hw + 16 + 3) & ~3;
+  for (int c = threadIdx.x; c < nx / 4; c += DT_T) {
+    const int g = d.x0 + 4 * c;
+    const bool ok = g >= P.i_lo && g + 4 <= P.i_hi;
+    cp_async16(xs + dchunk(c), ok ? row + g : row + P.i_lo, ok);
+  }
+}
+// the next item with work in [i, i1) as (e, tile), or false
+__device__ __forceinline__ bool direct_next(const EvalBatch &b, int &e, int &tile, long long &i, long long i1,
+                                            DirectTile &d) {
+  while (i < i1) {
+    if (direct_tile(b, e, tile, d)) return true;
+    i++;
+    if (++tile == b.max_dtiles) {
+      tile = 0;
+      e++;
+    }
+  }
+  return false;
+}
+
+// One CTA walks a contiguous range of (evaluation, tile) items, so the taps
+// are loaded once per evaluation; the next item's input is copied in
+// (cp.async) while the current one is convolved.
+__global__ void __launch_bounds__(DT_T) k_direct(DevGrid G, EvalBatch b) {
+  __shared__ __align__(16) float xs[2][DT_X];
+  __shared__ __align__(16) float rs[DT_X];
+  __shared__ __align__(16) float kr[DT_K];
+  __shared__ __align__(16) float kg[DT_K];
+  const int N = G.npx;
+  const long long total = (long long)b.E * b.max_dtiles;
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  long long ic = (long long)blockIdx.x * per;
+  const long long i1 = min(total, ic + per);
+  int ce = (int)(ic / b.max_dtiles), ct = (int)(ic % b.max_dtiles);
+  DirectTile cur, nxt;
+  bool have = direct_next(b, ce, ct, ic, i1, cur);
+  if (have) direct_stage(b, cur, xs[0]);
+  cp_async_commit();
+  int buf = 0, taps_e = -1;
+  while (have) {
+    long long in = ic + 1;
+    int ne = ce, nt = ct + 1;
+    if (nt == b.max_dtiles) {
+      nt = 0;
+      ne++;
+    }
+    const bool more = direct_next(b, ne, nt, in, i1, nxt);
+    if (more) direct_stage(b, nxt, xs[buf ^ 1]);
+    cp_async_commit();
+    const EvalPrep &P = b.prep[cur.e];
+    const DevStar &st = b.stars[P.star];
+    const bool fixedk = st.disp_kind == DISP_FIXED && cur.hg > 0;
+    if (cur.e != taps_e) {
+      direct_taps(kr, cur.m > 1 ? reinterpret_cast<const float *>(b.H + (size_t)cur.e * 1025) : nullptr,
+                  cur.m > 1 ? cur.hw : 0, cur.pl);
+      direct_taps(kg, fixedk ? st.gk : nullptr, fixedk ? cur.hg : 0, 0);
+      taps_e = cur.e;
+    }
+    const int p0 = cur.p0, nr = cur.nr, n = cur.n, hg = cur.hg;
+    for (int t = nr + threadIdx.x; t < nr + 16; t += DT_T) rs[dperm(t)] = 0.0f;
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this item's input (the next may be in flight)
+    __syncthreads();
+    const float *x = xs[buf];
+    if (cur.m > 1) {
+      conv_blocked(x, cur.hw + cur.pl, cur.hw, kr, nr, [&](int v0, float (&acc)[8]) {
+#pragma unroll
+        for (int c = 0; c < 8; c++) {  // zero outside the grid and past the tile
+          const int v = v0 + c, p = p0 + v;
+          if (!(v < nr && p >= 0 && p < N)) acc[c] = 0.0f;
+        }
+        float4 *r4 = reinterpret_cast<float4 *>(rs);
+        r4[dchunk(v0 >> 2) >> 2] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        r4[dchunk((v0 >> 2) + 1) >> 2] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+      });
+    } else {  // identity rotation: the staged input itself (zero outside the grid)
+      for (int v = threadIdx.x; v < nr; v += DT_T) {
+        const int p = p0 + v;
+        rs[dperm(v)] = (p >= 0 && p < N) ? x[dperm(v + cur.pl)] : 0.0f;
+      }
+    }
+    __syncthreads();
+    float *y = b.bufB + (size_t)cur.e * b.stride + cur.t0;  // 16-byte aligned
+    if (hg == 0 || fixedk) {
+      conv_blocked(rs, fixedk ? hg : 0, fixedk ? hg : 0, kg, n, [&](int v0, float (&acc)[8]) {
+        if (v0 + 8 <= n) {
+          reinterpret_cast<float4 *>(y + v0)[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+          reinterpret_cast<float4 *>(y + v0)[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 8; c++)
+            if (v0 + c < n) y[v0 + c] = acc[c];
+        }
+      });
+    } else {  // per-pixel instrument kernels (edge pixels pass through)
+      for (int v = threadIdx.x; v < n; v += DT_T)
+        y[v] = instrument(st, N, cur.t0 + v, hg, [&](int i) { return rs[dperm(i - p0)]; });
+    }
+    __syncthreads();  // rs and this buffer are rewritten for the item after next
+    buf ^= 1;
+    have = more;
+    ic = in;
+    ce = ne;
+    ct = nt;
+    cur = nxt;
+  }
+  cp_async_wait_all();
+}
+
+void launch_direct(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
+  if (b.E <= 0 || b.direct_max <= 0 || b.max_dtiles <= 0) return;
+  static int per_sm[64] = {};  // resident CTAs per SM, per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int fit = 4;
+  if (dev >= 0 && dev < 64) {
+    if (!per_sm[dev]) {
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_direct, DT_T, 0) != cudaSuccess || n < 1) n = 1;
+      per_sm[dev] = n;
+    }
+    fit = per_sm[dev];
+  }
+  const long long total = (long long)b.E * b.max_dtiles;
+  long long grid = (long long)num_sms() * fit;
+  if (grid > total) grid = total;
+  k_direct<<<(unsigned)grid, DT_T, 0, s>>>(G, b);
+  count_launch();
+}
+
 // First observed pixel of every fused broadening block: bnd[k] = the
 // smallest i whose left synth pixel is >= s_k (binary search on the
 // monotone resampling index); bnd[0] = 0, bnd[nblk] = n_obs.
@@ -1358,6 +1594,7 @@ void launch_pipeline(const DevGrid &G, const EvalBatch &b, const float2 *tw, con
   launch_interp(G, b, s);
   launch_obs_bounds(G, b, s);
   launch_broaden(G, b, tw, s);
+  launch_direct(G, b, s);
   if (o.may_unfuse) {
     launch_rot(G, b, tw, s);
     launch_gauss(G, b, s);

@@ -52,6 +52,8 @@ struct EvalBatch {
   int *gcount;               // [ceil(E / SEG)] groups per segment
   const float *given;        // model given at the observed pixels (continuum utilities) or null
   int64_t given_stride;      // floats between the given rows of consecutive evaluations
+  int direct_max;            // combined kernels of at most this many taps are convolved directly (0: never)
+  int max_dtiles;            // direct tiles per evaluation at most (at least DIRECT_TILE - DIRECT_MAX_TAPS outputs each)
 };
 
 // int entries per evaluation of EvalBatch::bnd for a grid of npx pixels
@@ -79,6 +81,8 @@ void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // first observed pixel of every fused broadening block (chi2 batches)
 void launch_obs_bounds(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
+// direct convolution of the evaluations k_prep routed to it (EvalPrep::direct)
+void launch_direct(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_rot(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);
 void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // model at the observed pixels for the evaluations k_broaden did not resample

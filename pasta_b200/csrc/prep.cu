@@ -125,6 +125,19 @@ __global__ void k_prep(DevGrid G, EvalBatch b, int full_window) {
     P.nblk = m > 1 ? (g_hi - g_lo + V - 1) / V : 0;
     P.final_in_b = hg > 0 ? (m > 1 ? 0 : 1) : (m > 1 ? 1 : 0);
   }
+  // narrow combined kernels: direct convolution (k_direct) into B, resampled
+  // afterwards by k_resample_obs; the FFT kernels skip these evaluations
+  P.direct = 0;
+  P.ndt = 0;
+  const int taps = m + 2 * hg;
+  if (work && P.fused && b.direct_max > 0 && taps <= b.direct_max && taps <= DIRECT_MAX_TAPS) {
+    P.direct = 1;
+    P.nblk = 0;
+    P.final_in_b = 1;
+    P.epi = 0;
+    const int td = (DIRECT_TILE - 2 * hg) & ~3;  // final outputs per direct tile
+    P.ndt = (o_hi - (o_lo & ~3) + td - 1) / td;  // tiles start at o_lo rounded down to 4
+  }
   // the model at the observed pixels goes where no live data is: B when
   // k_broaden resamples (it reads A), else the buffer without the synth row
   P.mobs_in_b = P.epi ? 1 : (P.final_in_b ? 0 : 1);
@@ -167,6 +180,11 @@ __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const 
   const float total = red[0];
   for (int t = threadIdx.x; t < m; t += FFT_T) c[pidx(t)].x = c[pidx(t)].x / total;
   __syncthreads();
+  if (P.direct) {  // the direct path takes the taps themselves (first m floats of H)
+    float *taps = reinterpret_cast<float *>(b.H + (size_t)e * 1025);
+    for (int t = threadIdx.x; t < m; t += FFT_T) taps[t] = c[pidx(t)].x;
+    return;
+  }
   fft2048<false>(c, tw);
   float2 *H = b.H + (size_t)e * 1025;
   for (int k = threadIdx.x; k <= 1024; k += FFT_T) H[k] = c[pidx(k)];

@@ -583,6 +583,19 @@ class _Interpolator:
         self._raise_status(st)
         return out[0]
 
+    @property
+    def direct_max(self) -> int:
+        """Widest combined broadening kernel (rotation taps + 2 x instrument
+        half width) convolved directly instead of by FFT blocks; measured on
+        this device when the grid was loaded (no counterpart in the reference)."""
+        v = C.c_int32()
+        check(lib().pasta_grid_direct_max(self._grid._h, C.byref(v)))
+        return int(v.value)
+
+    @direct_max.setter
+    def direct_max(self, taps: int):
+        check(lib().pasta_grid_set_direct_max(self._grid._h, int(taps)))
+
     def interpolate_linear(self, teff, m, logg) -> np.ndarray:
         """Trilinear interpolation over the 8 surrounding models
         (interpolate.rs:985-1028; lib.rs:1127-1139)."""

@@ -78,6 +78,44 @@ def test_produce_model_matches_oracle(env, disp_kind, vsini, rv):
     assert relmax(gpu, ref) <= FLUX_TOL
 
 
+@pytest.mark.parametrize("disp_kind", ["fixed", "none", "variable"])
+@pytest.mark.parametrize("vsini,rv", [(0.0, 0.0), (3.0, -40.0), (20.0, 10.0), (50.0, 20.0), (140.0, -90.0)])
+def test_direct_broadening_matches_fft_and_oracle(env, disp_kind, vsini, rv):
+    """The direct-convolution path (narrow kernels) and the FFT path give the
+    same model: forced on and off, both against the oracle's FP32 mirror."""
+    O, P, star = env["O"], env["P"], env["star"]
+    if disp_kind == "fixed":
+        d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+        od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    elif disp_kind == "none":
+        d = P.NoConvolutionDispersion(star.wl, env["wl"])
+        od = O.Disp(env["og"], O.DISP_NONE, star.wl)
+    else:
+        sig = (star.wl / np.linspace(60000.0, 90000.0, len(star.wl)) / 2.355).astype(np.float32)
+        d = P.VariableResolutionDispersion(star.wl, sig, env["wl"])
+        od = O.Disp(env["og"], O.DISP_VARIABLE, star.wl, disp=sig)
+    lab = [7130.0, 0.07, 4.02, vsini, rv]
+    interp = env["interp"]
+    keep = interp.direct_max
+    try:
+        interp.direct_max = 512
+        direct = interp.produce_model(d, *lab)
+        interp.direct_max = 0
+        fft = interp.produce_model(d, *lab)
+    finally:
+        interp.direct_max = keep
+    ref = od.produce_model(lab, O.F32)
+    assert relmax(direct, ref) <= FLUX_TOL
+    assert relmax(fft, ref) <= FLUX_TOL
+    assert relmax(direct, fft) <= FLUX_TOL
+
+
+def test_direct_crossover_is_measured(env):
+    v = env["interp"].direct_max
+    assert 0 <= v <= 512
+    print("direct/FFT crossover on this device: %d taps" % v)
+
+
 def _fitters(env, kind):
     O, P, star, S = env["O"], env["P"], env["star"], env["S"]
     n = len(star.wl)
