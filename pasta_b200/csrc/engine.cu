@@ -171,10 +171,13 @@ struct Workspace {
   DBuf<int> gcount;    // groups per segment
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
+  DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
+  DBuf<int> dcount;
   void ensure(int64_t want, int64_t str, int bstr) {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
+    dlist.release(); dcount.release();
     cap = 0;
     A.alloc((size_t)want * str);
     B.alloc((size_t)want * str);
@@ -186,6 +189,8 @@ struct Workspace {
     gcount.alloc((size_t)(want + SEG - 1) / SEG);
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
+    dlist.alloc((size_t)want);
+    dcount.alloc(1);
     cap = want;
     stride = str;
     bnd_stride = bstr;
@@ -196,7 +201,7 @@ struct Workspace {
 // bytes of workspace one evaluation takes with rows of `stride` floats
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
   return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)bnd_stride * 4 +
-         (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8);
+         (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8) + 4;
 }
 
 struct pasta_grid {
@@ -712,6 +717,8 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.given_stride = a.given_stride;
   b.direct_max = g->direct_max;
   b.max_dtiles = (int)((g->npx + DIRECT_TILE - DIRECT_MAX_TAPS - 1) / (DIRECT_TILE - DIRECT_MAX_TAPS));
+  b.direct_list = g->ws.dlist.p;
+  b.direct_count = g->ws.dcount.p;
   return b;
 }
 
@@ -1097,6 +1104,7 @@ void batch_profile_step(Batch &B, double *out) {
   launch_obs_bounds(g->d, b, s);
   launch_broaden(g->d, b, C.tw.p, s);
   CK(cudaEventRecord(B.ev[5], s));
+  launch_direct(g->d, b, s);
   if (may_unfuse) {
     launch_rot(g->d, b, C.tw.p, s);
     launch_gauss(g->d, b, s);

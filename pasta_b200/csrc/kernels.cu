@@ -776,47 +776,34 @@ __device__ __forceinline__ void direct_stage(const EvalBatch &b, const DirectTil
     cp_async16(xs + dchunk(c), ok ? row + g : row + P.i_lo, ok);
   }
 }
-// the next item with work in [i, i1) as (e, tile), or false
-__device__ __forceinline__ bool direct_next(const EvalBatch &b, int &e, int &tile, long long &i, long long i1,
-                                            DirectTile &d) {
-  while (i < i1) {
-    if (direct_tile(b, e, tile, d)) return true;
-    i++;
-    if (++tile == b.max_dtiles) {
-      tile = 0;
-      e++;
-    }
-  }
+// the next item with work at or after i in steps of gridDim.x, or false;
+// item i is tile i % max_dtiles of the listed evaluation i / max_dtiles
+__device__ __forceinline__ bool direct_next(const EvalBatch &b, long long &i, long long total, DirectTile &d) {
+  for (; i < total; i += gridDim.x)
+    if (direct_tile(b, b.direct_list[i / b.max_dtiles], (int)(i % b.max_dtiles), d)) return true;
   return false;
 }
 
-// One CTA walks a contiguous range of (evaluation, tile) items, so the taps
-// are loaded once per evaluation; the next item's input is copied in
-// (cp.async) while the current one is convolved.
+// CTAs take the tiles of the evaluations k_prep listed in grid strides, so
+// those tiles (often all particles of a few stars) spread over the whole GPU;
+// the next item's input is copied in (cp.async) while the current one is
+// convolved.
 __global__ void __launch_bounds__(DT_T) k_direct(DevGrid G, EvalBatch b) {
   __shared__ __align__(16) float xs[2][DT_X];
   __shared__ __align__(16) float rs[DT_X];
   __shared__ __align__(16) float kr[DT_K];
   __shared__ __align__(16) float kg[DT_K];
   const int N = G.npx;
-  const long long total = (long long)b.E * b.max_dtiles;
-  const long long per = (total + gridDim.x - 1) / gridDim.x;
-  long long ic = (long long)blockIdx.x * per;
-  const long long i1 = min(total, ic + per);
-  int ce = (int)(ic / b.max_dtiles), ct = (int)(ic % b.max_dtiles);
+  const long long total = (long long)*b.direct_count * b.max_dtiles;
+  long long ic = blockIdx.x;
   DirectTile cur, nxt;
-  bool have = direct_next(b, ce, ct, ic, i1, cur);
+  bool have = direct_next(b, ic, total, cur);
   if (have) direct_stage(b, cur, xs[0]);
   cp_async_commit();
   int buf = 0, taps_e = -1;
   while (have) {
-    long long in = ic + 1;
-    int ne = ce, nt = ct + 1;
-    if (nt == b.max_dtiles) {
-      nt = 0;
-      ne++;
-    }
-    const bool more = direct_next(b, ne, nt, in, i1, nxt);
+    long long in = ic + gridDim.x;
+    const bool more = direct_next(b, in, total, nxt);
     if (more) direct_stage(b, nxt, xs[buf ^ 1]);
     cp_async_commit();
     const EvalPrep &P = b.prep[cur.e];
@@ -871,15 +858,13 @@ __global__ void __launch_bounds__(DT_T) k_direct(DevGrid G, EvalBatch b) {
     buf ^= 1;
     have = more;
     ic = in;
-    ce = ne;
-    ct = nt;
     cur = nxt;
   }
   cp_async_wait_all();
 }
 
 void launch_direct(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
-  if (b.E <= 0 || b.direct_max <= 0 || b.max_dtiles <= 0) return;
+  if (b.E <= 0 || b.direct_max <= 0 || b.max_dtiles <= 0 || !b.direct_list) return;
   static int per_sm[64] = {};  // resident CTAs per SM, per device
   int dev = 0;
   cudaGetDevice(&dev);

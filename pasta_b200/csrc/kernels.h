@@ -54,6 +54,8 @@ struct EvalBatch {
   int64_t given_stride;      // floats between the given rows of consecutive evaluations
   int direct_max;            // combined kernels of at most this many taps are convolved directly (0: never)
   int max_dtiles;            // direct tiles per evaluation at most (at least DIRECT_TILE - DIRECT_MAX_TAPS outputs each)
+  int *direct_list;          // [E] evaluations k_prep routed to the direct path (in any order)
+  int *direct_count;         // [1] their number (zeroed before k_prep)
 };
 
 // int entries per evaluation of EvalBatch::bnd for a grid of npx pixels

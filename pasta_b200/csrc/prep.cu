@@ -130,13 +130,14 @@ __global__ void k_prep(DevGrid G, EvalBatch b, int full_window) {
   P.direct = 0;
   P.ndt = 0;
   const int taps = m + 2 * hg;
-  if (work && P.fused && b.direct_max > 0 && taps <= b.direct_max && taps <= DIRECT_MAX_TAPS) {
+  if (work && P.fused && b.direct_max > 0 && b.direct_list && taps <= b.direct_max && taps <= DIRECT_MAX_TAPS) {
     P.direct = 1;
     P.nblk = 0;
     P.final_in_b = 1;
     P.epi = 0;
     const int td = (DIRECT_TILE - 2 * hg) & ~3;  // final outputs per direct tile
     P.ndt = (o_hi - (o_lo & ~3) + td - 1) / td;  // tiles start at o_lo rounded down to 4
+    b.direct_list[atomicAdd(b.direct_count, 1)] = e;
   }
   // the model at the observed pixels goes where no live data is: B when
   // k_broaden resamples (it reads A), else the buffer without the synth row
@@ -204,11 +205,13 @@ __global__ void __launch_bounds__(FFT_T) k_rotker(DevGrid G, EvalBatch b, const 
 
 void launch_prep(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
+  if (b.direct_max > 0 && b.direct_count) cudaMemsetAsync(b.direct_count, 0, sizeof(int), s);
   k_prep<<<(b.E + 127) / 128, 128, 0, s>>>(G, b, 0);
   count_launch();
 }
 void launch_prep_full(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
+  if (b.direct_max > 0 && b.direct_count) cudaMemsetAsync(b.direct_count, 0, sizeof(int), s);
   k_prep<<<(b.E + 127) / 128, 128, 0, s>>>(G, b, 1);
   count_launch();
 }

@@ -1157,7 +1157,7 @@ class BatchFit:
     def profile_step(self) -> dict:
         out = np.zeros(12)
         check(lib().pasta_batch_profile_step(self._h, ptr(out)))
-        names = ["update_ms", "prep_ms", "rotker_ms", "interp_ms", "broaden_ms", "unfused_ms", "chi2_ms", "best_ms",
+        names = ["update_ms", "prep_ms", "rotker_ms", "interp_ms", "broaden_ms", "direct_unfused_ms", "chi2_ms", "best_ms",
                  "interp_px", "evals", "obs_px", "broaden_blocks"]
         return dict(zip(names, out.tolist()))
 
