@@ -23,8 +23,16 @@ struct cf {
   float x, y;
 };
 __device__ __forceinline__ cf cmul(cf a, cf b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
-__device__ __forceinline__ cf cadd(cf a, cf b) { return {a.x + b.x, a.y + b.y}; }
-__device__ __forceinline__ cf csub(cf a, cf b) { return {a.x - b.x, a.y - b.y}; }
+// complex add / subtract as one packed f32x2 instruction each (a - b as
+// b * (-1) + a: the product is exact, so this rounds like a - b)
+__device__ __forceinline__ cf cadd(cf a, cf b) {
+  const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  return {r.x, r.y};
+}
+__device__ __forceinline__ cf csub(cf a, cf b) {
+  const float2 r = __ffma2_rn(make_float2(b.x, b.y), make_float2(-1.0f, -1.0f), make_float2(a.x, a.y));
+  return {r.x, r.y};
+}
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>
 __device__ __forceinline__ cf rot90(cf a) {
