@@ -82,6 +82,12 @@ const char *pasta_last_error(void);
 int pasta_set_device(int device);
 /* Number of launches of this library's kernels since load (all threads). */
 int64_t pasta_kernel_launch_count(void);
+/* Linear-model continua (LinearModelFitter, continuum_fitting.rs:44-107)
+ * with at most 64 design columns run on the tensor cores (tcgen05, f32
+ * accuracy by split tf32 operands); 0 selects the CUDA-core path instead,
+ * for the calls and batches started afterwards (no counterpart in the
+ * reference; the environment variable PASTA_LINEAR_TC=0 sets the default). */
+int pasta_set_linear_tensor_cores(int on);
 
 /* ----------------------------------------------------------- the grid
  * Replaces InMemFetcher::new / from_tar_zstd + GridInterpolator::new

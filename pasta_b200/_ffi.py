@@ -52,6 +52,7 @@ SIGNATURES = {
     "pasta_last_error": (C.c_char_p, []),
     "pasta_set_device": (I, [I]),
     "pasta_kernel_launch_count": (I64, []),
+    "pasta_set_linear_tensor_cores": (I, [I]),
     "pasta_grid_create": (I, [P, P, P, I64, I64, I, D, D, P, P]),
     "pasta_grid_destroy": (I, [P]),
     "pasta_grid_direct_max": (I, [P, P]),

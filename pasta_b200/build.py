@@ -19,8 +19,8 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
           "-I" + os.path.join(ROOT, "include")]
-UNITS = [("prep.cu", ["-fmad=false"]), ("kernels.cu", []), ("binary.cu", ["-fmad=false"]), ("engine.cu", []),
-         ("noalloc.cu", [])]
+UNITS = [("prep.cu", ["-fmad=false"]), ("kernels.cu", []), ("binary.cu", ["-fmad=false"]), ("lintc.cu", []),
+         ("engine.cu", []), ("noalloc.cu", [])]
 DEPS = ["common.cuh", "fft.cuh", "kernels.h"]
 
 

@@ -110,7 +110,9 @@ struct DevStar {
   const int *cstart, *cstop;  // chunk bounds
   const float *xa, *xb, *fac; // per observed pixel: coordinate in lower/upper chunk, blend factor
   const double *chol;   // per chunk: p1 x p1 lower Cholesky factor of the Legendre Gram (row-major)
-  const float *q;       // linear: n_obs x k orthonormal basis (row-major)
+  const float *q;       // linear: k x n_obs orthonormal basis (each basis vector contiguous)
+  const float *qt;      // linear: the same basis pixel-major, kp columns (zero padded), for the tensor cores
+  int kp;               // linear: basis columns padded to a multiple of 16 (0: no tensor-core path)
   const float *cont;    // fixed continuum
 };
 

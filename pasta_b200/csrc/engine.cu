@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <limits>
 #include <chrono>
 #include <cmath>
@@ -359,11 +360,13 @@ struct pasta_continuum {
   int k = 0;
   std::vector<float> qcol;  // k x n column-major
   std::vector<double> R;    // k x k upper (row-major)
+  int kp = 0;               // k padded to a multiple of 16 for the tensor-core path (0: k > 64)
+  std::vector<float> qt;    // n x kp pixel-major copy of the basis (zero padded)
   // fixed
   std::vector<float> cont;
   int ignore = 0;
   DBuf<int> dcs, dce;
-  DBuf<float> dxa, dxb, dfac, dq, dcont;
+  DBuf<float> dxa, dxb, dfac, dq, dqt, dcont;
   DBuf<double> dchol;
 };
 
@@ -551,6 +554,13 @@ void linear_setup(pasta_continuum *c, const float *design, int k) {
     }
     for (int64_t i = 0; i < n; i++) c->qcol[(size_t)col * n + i] = (float)q[i];
   }
+  // pixel-major copy for the tensor-core products (at most 64 columns)
+  c->kp = k <= 64 ? (k + 15) / 16 * 16 : 0;
+  if (c->kp) {
+    c->qt.assign((size_t)n * c->kp, 0.0f);
+    for (int col = 0; col < k; col++)
+      for (int64_t i = 0; i < n; i++) c->qt[(size_t)i * c->kp + col] = c->qcol[(size_t)col * n + i];
+  }
 }
 
 // Host result of a continuum solve -> the reference's parameter vector.
@@ -622,6 +632,8 @@ DevStar make_star(const pasta_dispersion *d, const pasta_continuum *c, const flo
     s.xa = c->dxa.p; s.xb = c->dxb.p; s.fac = c->dfac.p;
     s.chol = c->dchol.p;
     s.q = c->dq.p;
+    s.qt = c->dqt.p;
+    s.kp = c->dqt.p ? c->kp : 0;
     s.cont = c->dcont.p;
   } else {
     s.cont_kind = CONT_CONSTANT;
@@ -660,6 +672,8 @@ struct EvalArgs {
   float *out_synth = nullptr;
   const float *given = nullptr;  // model given at observed pixels
   int64_t given_stride = 0;      // floats between the given rows of consecutive evaluations
+  int lin_group = 0;             // consecutive evaluations sharing a star (tensor-core linear continua), or 0
+  uint32_t lin_kp_mask = 0;      // tensor-core bases present (bit kp / 16)
 };
 
 // continuum kinds and instrument widths of the stars a batch can touch
@@ -673,7 +687,23 @@ void star_kinds(const std::vector<DevStar> &h, EvalArgs &a) {
     }
     a.max_nobs = std::max<int64_t>(a.max_nobs, st.n_obs);
     if (st.disp_kind != DISP_NONE) a.max_hg = std::max(a.max_hg, (st.gw - 1) / 2);
+    if (st.cont_kind == CONT_LINEAR && st.kp > 0) a.lin_kp_mask |= 1u << (st.kp / 16);
   }
+}
+
+// tensor-core linear continua: on unless PASTA_LINEAR_TC=0 or
+// pasta_set_linear_tensor_cores(0) selects the CUDA-core path
+std::atomic<int> g_linear_tc{-1};
+bool linear_tc_enabled() {
+  int v = g_linear_tc.load();
+  if (v < 0) {
+    const char *e = getenv("PASTA_LINEAR_TC");
+    v = (e && e[0] == '0') ? 0 : 1;
+    int expect = -1;
+    g_linear_tc.compare_exchange_strong(expect, v);
+    v = g_linear_tc.load();
+  }
+  return v != 0;
 }
 
 int width_upper_bound(const pasta_grid *g, double vsini_hi) {
@@ -719,6 +749,11 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.max_dtiles = (int)((g->npx + DIRECT_TILE - DIRECT_MAX_TAPS - 1) / (DIRECT_TILE - DIRECT_MAX_TAPS));
   b.direct_list = g->ws.dlist.p;
   b.direct_count = g->ws.dcount.p;
+  // groups must start at star boundaries: sub-batches that begin inside a
+  // group take the CUDA-core path
+  const bool lin = linear_tc_enabled() && a.lin_group > 0 && a.lin_group <= 128 && off % a.lin_group == 0;
+  b.lin_group = lin ? a.lin_group : 0;
+  b.lin_kp_mask = lin ? a.lin_kp_mask : 0u;
   return b;
 }
 
@@ -940,6 +975,7 @@ void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, c
   a.need_chi2 = 1;
   a.max_m = max_m;
   star_kinds(ss.h, a);
+  a.lin_group = 1;  // one evaluation per star
   ensure_workspace(g, S, a.max_nobs);
   run_evals(g, a, s);
   std::vector<double> hp((size_t)S * pstride);
@@ -1032,6 +1068,7 @@ void batch_init(Batch &B, pasta_grid *g, const std::vector<StarInput> &in) {
   a.need_chi2 = 1;
   a.max_m = B.max_m;
   star_kinds(B.ss.h, a);
+  a.lin_group = B.Pmax <= 128 ? B.Pmax : 0;  // star s owns evaluations [s Pmax, (s + 1) Pmax)
   ensure_workspace(g, (int64_t)E, a.max_nobs);
   for (auto &e : B.ev) CK(cudaEventCreate(&e));
   if (!getenv("PASTA_NO_GRAPH")) {
@@ -1208,6 +1245,7 @@ void fit_plain(pasta_grid *g, const std::vector<StarInput> &in, pasta_fit_result
     a.need_chi2 = 1;
     a.max_m = width_upper_bound(g, pp.mx[3]);
     star_kinds(ss.h, a);
+    a.lin_group = 128;  // the particles of the one star
     ensure_workspace(g, P, a.max_nobs);
     std::vector<int> est(P);
     auto evaluate = [&]() -> int {
@@ -1340,6 +1378,7 @@ struct pasta_server {
   int64_t graph_gen = -1;
   uint32_t graph_mask = 0;  // continuum kinds / instrument width the captured step covers
   int graph_other = 0, graph_hg = 0, graph_chunks = 0;
+  uint32_t graph_lin = 0;   // tensor-core linear bases the captured step covers
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   std::mutex mu;
@@ -1353,6 +1392,10 @@ struct pasta_server {
 extern "C" {
 
 int pasta_abi_version(void) { return PASTA_B200_ABI_VERSION; }
+int pasta_set_linear_tensor_cores(int on) {
+  g_linear_tc.store(on ? 1 : 0);
+  return PASTA_OK;
+}
 const char *pasta_last_error(void) { return g_last_error.c_str(); }
 int64_t pasta_kernel_launch_count(void) { return kernel_launches(); }
 
@@ -1745,6 +1788,7 @@ int pasta_continuum_create(int kind, const double *wl, int64_t n, int n_chunks, 
       if (!design) fail(PASTA_E_ARG, "linear fitter needs a design matrix");
       linear_setup(c.get(), design, k);
       c->dq.upload(c->qcol);
+      if (c->kp) c->dqt.upload(c->qt);
     } else if (kind == PASTA_CONT_FIXED) {
       if (!continuum) fail(PASTA_E_ARG, "fixed continuum needs values");
       c->cont.assign(continuum, continuum + n);
@@ -1922,6 +1966,7 @@ static int run_label_batch(const pasta_grid *gc, const pasta_dispersion *d, cons
     a.full_window = full_window;
     a.max_m = width_upper_bound(g, vmax);
     star_kinds({st}, a);
+    a.lin_group = 128;  // every evaluation belongs to the one star
     if (out_obs) { dout.alloc((size_t)L * nobs); a.out_obs = dout.p; a.out_stride = nobs; }
     if (out_synth) { dout.alloc((size_t)L * g->npx); a.out_synth = dout.p; }
     ensure_workspace(g, L, a.max_nobs);
@@ -2135,6 +2180,8 @@ void run_binary(pasta_grid *g, const pasta_grid *gc, const DevStar *dstar, const
       cb.chunk_p1_mask = a.chunk_p1_mask;
       cb.max_chunks = a.max_chunks;
       cb.other_cont = a.other_cont;
+      cb.lin_group = linear_tc_enabled() ? 128 : 0;  // every label belongs to the one star
+      cb.lin_kp_mask = a.lin_kp_mask;
       cb.ccoef = g->ws.ccoef.p;
       cb.cpart = g->ws.cpart.p;
       cb.given = bb.model;
@@ -3008,11 +3055,13 @@ int pasta_server_step(pasta_server *sv) {
       if (sv->graph_other) a.other_cont = 1;
       a.max_hg = std::max(a.max_hg, sv->graph_hg);
       a.max_chunks = std::max(a.max_chunks, sv->graph_chunks);
+      a.lin_kp_mask |= sv->graph_lin;
+      a.lin_group = sv->Pmax <= 128 ? sv->Pmax : 0;
     }
     ensure_workspace(g, E, a.max_nobs);
     const bool grown = sv->graph_max_m < sv->max_m || (a.chunk_p1_mask & ~sv->graph_mask) ||
                        (a.other_cont && !sv->graph_other) || a.max_hg > sv->graph_hg ||
-                       a.max_chunks > sv->graph_chunks;
+                       a.max_chunks > sv->graph_chunks || (a.lin_kp_mask & ~sv->graph_lin);
     if (sv->exec && (grown || sv->graph_gen != g->ws.gen)) {
       // a wider kernel or a new continuum kind was admitted, or the workspace moved
       cudaGraphExecDestroy(sv->exec);
@@ -3027,6 +3076,7 @@ int pasta_server_step(pasta_server *sv) {
       sv->graph_other = a.other_cont;
       sv->graph_hg = a.max_hg;
       sv->graph_chunks = a.max_chunks;
+      sv->graph_lin = a.lin_kp_mask;
       const int64_t k0 = kernel_launches();
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       launch_pso_update(g->d, sw, s);

@@ -1390,6 +1390,7 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b) {
   const EvalPrep &P = b.prep[e];
   const DevStar &st = b.stars[P.star];
   if (st.cont_kind == CONT_CHUNK) return;
+  if (st.cont_kind == CONT_LINEAR && st.kp > 0 && b.lin_group > 0) return;  // k_linear_tc
   if (P.status) {
     write_result(b, e, 0.0, P.status);
     return;
@@ -1488,6 +1489,9 @@ void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
     count_launch();
   }
   if (b.other_cont) {
+    if (b.lin_group > 0)
+      for (int kp = 16; kp <= 64; kp += 16)
+        if (b.lin_kp_mask & (1u << (kp / 16))) launch_linear_tc(b, kp, s);
     k_chi2_other<<<b.E, CT, 0, s>>>(G, b);
     count_launch();
   }

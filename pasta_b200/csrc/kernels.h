@@ -56,6 +56,9 @@ struct EvalBatch {
   int max_dtiles;            // direct tiles per evaluation at most (at least DIRECT_TILE - DIRECT_MAX_TAPS outputs each)
   int *direct_list;          // [E] evaluations k_prep routed to the direct path (in any order)
   int *direct_count;         // [1] their number (zeroed before k_prep)
+  int lin_group;             // linear continua on the tensor cores: groups of this many consecutive
+                             // evaluations share a star (0: the CUDA-core path)
+  uint32_t lin_kp_mask;      // bit kp / 16: a linear continuum with a kp-column tensor-core basis is present
 };
 
 // int entries per evaluation of EvalBatch::bnd for a grid of npx pixels
@@ -91,6 +94,8 @@ void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // chi2 from the model at the observed pixels (b.given when set)
 void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// linear-model continua with a kp-column basis on the tensor cores (lintc.cu)
+void launch_linear_tc(const EvalBatch &b, int kp, cudaStream_t s);
 // copy the preparation status to b.status (batches without chi2)
 void launch_prep_status(const EvalBatch &b, cudaStream_t s);
 // model at the observed pixels: out [E][out_stride]

@@ -382,3 +382,53 @@ def test_convolve_and_resample_directory(env, tmp_path):
         before = os.path.getmtime(os.path.join(dst, S.filename_from_labels(*labels[0])))
         d.convolve_and_resample_directory(str(src), str(dst), with_factor, env["wl"])
         assert os.path.getmtime(os.path.join(dst, S.filename_from_labels(*labels[0]))) == before
+
+
+@pytest.mark.parametrize("k", [12, 40, 64])
+def test_linear_continuum_tensor_core_many_labels(env, k):
+    """Linear-model continua run as tcgen05 tf32 (split hi/lo) products per
+    group of 128 evaluations: chi2 of 300 random labels (three groups).
+    Against the CUDA-core path on the same models: relative 5e-6.  Against
+    the FP64 oracle: relative 3e-5; for the worst-fitting labels (chi2 in the
+    thousands) the model's own f32 roundoff is amplified past 1e-5, and the
+    CUDA-core path deviates by the same amount on the same labels."""
+    from pasta_b200 import _ffi
+    O, P, S, star = env["O"], env["P"], env["S"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    D = S.legendre_design(star.wl, k)
+    cont, oc = P.LinearModelContinuumFitter(D), O.Cont(O.CONT_LINEAR, design=D)
+    rng = np.random.default_rng(k)
+    labs = np.stack([rng.uniform(6000, 8000, 300), rng.uniform(-0.5, 0.5, 300), rng.uniform(3.5, 4.5, 300),
+                     rng.uniform(0, 200, 300), rng.uniform(-100, 100, 300)], axis=1)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(8, 2), (0, 300), (-150, 150))
+    gpu = np.array(fitter.chi2(env["interp"], star.flux, star.var, labs))
+    _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(0))
+    try:
+        cuda_cores = np.array(fitter.chi2(env["interp"], star.flux, star.var, labs))
+    finally:
+        _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(1))
+    np.testing.assert_allclose(gpu, cuda_cores, rtol=5e-6)
+    ref, st = O.chi2(env["og"], od, oc, star.flux, star.var, labs, O.F64)
+    assert (st == 0).all()
+    np.testing.assert_allclose(gpu, ref, rtol=3e-5)
+    good = ref < 1000.0
+    np.testing.assert_allclose(gpu[good], ref[good], rtol=CHI2_TOL)
+
+
+def test_linear_continuum_fit_params(env):
+    """A fit with a linear-model continuum: the continuum parameters of the
+    result against the oracle's fit at the returned label."""
+    O, P, S, star = env["O"], env["P"], env["S"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
+    D = S.legendre_design(star.wl, 40)
+    cont, oc = P.LinearModelContinuumFitter(D), O.Cont(O.CONT_LINEAR, design=D)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(16, 4), (0, 300), (-150, 150))
+    r = fitter.fit(env["interp"], star.flux, star.var, seed=77)
+    lab = r.label.as_list()
+    mdl = od.produce_model(lab, O.F64)
+    params, chi2 = oc.fit(star.flux, star.var, mdl, O.F64)
+    assert len(r.continuum_params) == 40
+    np.testing.assert_allclose(r.continuum_params, params, rtol=1e-3, atol=1e-4 * np.abs(params).max())
+    assert abs(r.chi2 - chi2) <= 1e-4 * chi2
