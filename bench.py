@@ -256,6 +256,40 @@ def binary_leg(P, S, n_stars, cpu, seed):
     return out
 
 
+def linear_leg(P, S, n_labels, k, reps=5):
+    """Linear-model continuum (design of k Legendre columns) on the config-0
+    grid (20,000 px), one star of 15,000 observed pixels: chi2 of n_labels
+    random labels per call through SingleFitter.chi2, with the tensor-core
+    path and with the CUDA-core path (best of reps calls each, host clock,
+    host arrays in and out)."""
+    from pasta_b200 import _ffi
+    spec0 = S.config0_grid(n_px=20000)
+    labels, spectra, factors = S.make_grid(spec0)
+    wl = P.WlGrid(spec0.log_first, spec0.log_step, spec0.n_px, log=True)
+    interp = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+    star = S.make_star(spec0, [7130.0, 0.07, 4.02, 50.0, 20.0], 15000, 100.0, RESOLUTION, seed=11)
+    d = P.FixedResolutionDispersion(star.wl, RESOLUTION, wl)
+    cont = P.LinearModelContinuumFitter(S.legendre_design(star.wl, k))
+    fitter = interp.get_fitter(d, cont, P.PSOSettings(8, 2), (0.0, 300.0), (-150.0, 150.0))
+    rng = np.random.default_rng(5)
+    labs = np.stack([rng.uniform(6000, 8000, n_labels), rng.uniform(-0.5, 0.5, n_labels),
+                     rng.uniform(3.5, 4.5, n_labels), rng.uniform(0, 200, n_labels),
+                     rng.uniform(-100, 100, n_labels)], axis=1)
+    out = {"workload": "chi2 of %d labels, linear-model continuum with %d Legendre columns, config-0 grid, "
+                       "N_obs 15000" % (n_labels, k)}
+    for name, on in (("tensor_cores", 1), ("cuda_cores", 0)):
+        _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(on))
+        fitter.chi2(interp, star.flux, star.var, labs)
+        best = 1e30
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fitter.chi2(interp, star.flux, star.var, labs)
+            best = min(best, time.perf_counter() - t0)
+        out[name] = {"chi2_evals_per_s": n_labels / best, "seconds": best}
+    _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(1))
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -587,6 +621,10 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=30.0, help="served latency run: arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=300, help="served latency run: requests (0: skip)")
     ap.add_argument("--binary-stars", type=int, default=16, help="binary-fit leg: stars (0: skip)")
+    ap.add_argument("--linear-only", action="store_true",
+                    help="time chi2 with a linear-model continuum, tensor-core and CUDA-core paths, and print it")
+    ap.add_argument("--linear-labels", type=int, default=1024)
+    ap.add_argument("--linear-k", type=int, default=40)
     ap.add_argument("--binary-only", action="store_true",
                     help="run only the binary-fit leg (with its CPU baseline unless --no-cpu) and print it")
     ap.add_argument("--stages-only", action="store_true",
@@ -594,6 +632,11 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.linear_only:
+        from pasta_b200 import pasta as P
+        from pasta_b200 import synth as S
+        print(json.dumps(linear_leg(P, S, args.linear_labels, args.linear_k)), flush=True)
+        return
     if args.binary_only:
         from pasta_b200 import pasta as P
         from pasta_b200 import synth as S

@@ -173,12 +173,13 @@ struct Workspace {
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
+  DBuf<double> zpart;  // tensor-core linear continua: partial coefficients [cap][LIN_MAX_SLICES][64]
   DBuf<int> dcount;
   void ensure(int64_t want, int64_t str, int bstr) {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
-    dlist.release(); dcount.release();
+    dlist.release(); dcount.release(); zpart.release();
     cap = 0;
     A.alloc((size_t)want * str);
     B.alloc((size_t)want * str);
@@ -191,6 +192,7 @@ struct Workspace {
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
     dlist.alloc((size_t)want);
+    zpart.alloc((size_t)want * LIN_MAX_SLICES * 64);
     dcount.alloc(1);
     cap = want;
     stride = str;
@@ -202,7 +204,7 @@ struct Workspace {
 // bytes of workspace one evaluation takes with rows of `stride` floats
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
   return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)bnd_stride * 4 +
-         (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8) + 4;
+         (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8) + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8;
 }
 
 struct pasta_grid {
@@ -691,6 +693,24 @@ void star_kinds(const std::vector<DevStar> &h, EvalArgs &a) {
   }
 }
 
+// pixel slices per group of the tensor-core linear continua: enough CTAs
+// for two waves of two per SM, at most LIN_MAX_SLICES
+void set_lin_slices(pasta_grid *g, EvalBatch &b) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  b.lin_zpart = g->ws.zpart.p;
+  if (b.lin_group <= 0) {
+    b.lin_slices = 1;
+    return;
+  }
+  const int groups = (b.E + b.lin_group - 1) / b.lin_group;
+  b.lin_slices = std::max(1, std::min(LIN_MAX_SLICES, (4 * sms + groups - 1) / groups));
+}
+
 // tensor-core linear continua: on unless PASTA_LINEAR_TC=0 or
 // pasta_set_linear_tensor_cores(0) selects the CUDA-core path
 std::atomic<int> g_linear_tc{-1};
@@ -754,6 +774,7 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   const bool lin = linear_tc_enabled() && a.lin_group > 0 && a.lin_group <= 128 && off % a.lin_group == 0;
   b.lin_group = lin ? a.lin_group : 0;
   b.lin_kp_mask = lin ? a.lin_kp_mask : 0u;
+  set_lin_slices(g, b);
   return b;
 }
 
@@ -2182,6 +2203,7 @@ void run_binary(pasta_grid *g, const pasta_grid *gc, const DevStar *dstar, const
       cb.other_cont = a.other_cont;
       cb.lin_group = linear_tc_enabled() ? 128 : 0;  // every label belongs to the one star
       cb.lin_kp_mask = a.lin_kp_mask;
+      set_lin_slices(g, cb);
       cb.ccoef = g->ws.ccoef.p;
       cb.cpart = g->ws.cpart.p;
       cb.given = bb.model;

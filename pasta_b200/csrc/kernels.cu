@@ -1489,9 +1489,7 @@ void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
     count_launch();
   }
   if (b.other_cont) {
-    if (b.lin_group > 0)
-      for (int kp = 16; kp <= 64; kp += 16)
-        if (b.lin_kp_mask & (1u << (kp / 16))) launch_linear_tc(b, kp, s);
+    if (b.lin_group > 0) launch_linear_tc(b, s);
     k_chi2_other<<<b.E, CT, 0, s>>>(G, b);
     count_launch();
   }

@@ -21,6 +21,8 @@ struct __align__(16) GroupRec {
   int nmem, nn;           // members, compacted rows
 };
 
+constexpr int LIN_MAX_SLICES = 32;  // at most MAX_CHUNKS: the slices' residual sums use EvalBatch::cpart
+
 // Per-launch description of one batch of evaluations.
 struct EvalBatch {
   int E;                     // evaluations in this batch
@@ -59,6 +61,8 @@ struct EvalBatch {
   int lin_group;             // linear continua on the tensor cores: groups of this many consecutive
                              // evaluations share a star (0: the CUDA-core path)
   uint32_t lin_kp_mask;      // bit kp / 16: a linear continuum with a kp-column tensor-core basis is present
+  int lin_slices;            // pixel slices per group (1..LIN_MAX_SLICES)
+  double *lin_zpart;         // [E][LIN_MAX_SLICES][64] partial coefficients of the slices
 };
 
 // int entries per evaluation of EvalBatch::bnd for a grid of npx pixels
@@ -94,8 +98,8 @@ void launch_gauss(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 // chi2 from the model at the observed pixels (b.given when set)
 void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
-// linear-model continua with a kp-column basis on the tensor cores (lintc.cu)
-void launch_linear_tc(const EvalBatch &b, int kp, cudaStream_t s);
+// linear-model continua on the tensor cores, every basis width present (lintc.cu)
+void launch_linear_tc(const EvalBatch &b, cudaStream_t s);
 // copy the preparation status to b.status (batches without chi2)
 void launch_prep_status(const EvalBatch &b, cudaStream_t s);
 // model at the observed pixels: out [E][out_stride]

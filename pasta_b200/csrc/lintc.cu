@@ -9,7 +9,10 @@
 // particles of a swarm) these are two dense products:
 //   GEMM1  Z^T [128 x KP]  = B^T [128 x N] . Q [N x KP]      (B = flux / model per evaluation)
 //   GEMM2  F^T [128 x 32]  = Z^T [128 x KP] . Q^T [KP x 32]  per tile of 32 pixels,
-// and the residual sum is the epilogue of GEMM2.  Both run as
+// and the residual sum is the epilogue of GEMM2.  Each group's pixels are
+// split into slices (more when there are fewer groups) worked by separate
+// CTAs; the slices' partial coefficients and residual sums are added in
+// slice order, so the result does not depend on scheduling.  Both run as
 // tcgen05.mma kind::tf32 with M = 128 from shared-memory operands in the
 // canonical K-major layout (8-row x 16-byte core matrices, no swizzle).  To
 // keep f32 accuracy each operand is split into a tf32 head and an exact
@@ -38,6 +41,8 @@ constexpr int LT_TN = 32;   // pixels per GEMM2 tile (MMA N)
 // columns; GEMM2: up to 8 regions of 32 columns), summed in f64 on read-back
 constexpr uint32_t LT_TMEM_COLS = 256;
 constexpr int S_MMA_TIMEOUT = -99;      // PASTA_E_INTERNAL
+// partial coefficient of a slice whose barrier wait ran out (never a real value)
+constexpr double LT_FAILED = -1e300;
 
 // shared-memory map (bytes)
 constexpr int G1_AH = 0, G1_AL = 16384, G1_BH = 32768, G1_BL = 40960;  // B^T stage 128 x 32, Q stage 64 x 32
@@ -45,7 +50,8 @@ constexpr int G2_AH = 0, G2_AL = 32768;                                // Z^T 12
 constexpr int G2_BH = 65536, G2_BL = 81920;                            // Q^T tile 32 x 64
 constexpr int LT_MISC = 98304;                                         // barrier, tensor-memory slot, flags
 constexpr int LT_RED = LT_MISC + 64;                                   // 128 doubles: half-1 residual sums
-constexpr int LT_SMEM = LT_RED + LT_M * 8;
+constexpr int LT_RFAIL = LT_RED + LT_M * 8;                            // 128 ints: half-1 failure flags
+constexpr int LT_SMEM = LT_RFAIL + LT_M * 4;
 
 // byte offset of element (row, k) in a K-major tile with kt elements per
 // row: core matrix (row / 8, k / 4) of 8 rows x 16 bytes, row-group stride
@@ -131,9 +137,13 @@ __device__ __forceinline__ const float *lt_model_row(const EvalBatch &b, const E
 
 }  // namespace
 
-// One CTA per group of b.lin_group consecutive evaluations of one star whose
-// continuum is a linear model with a tensor-core basis (DevStar::kp > 0).
-template <int KP>
+// One CTA per (group of b.lin_group consecutive evaluations of one star whose
+// continuum is a linear model with a tensor-core basis, pixel slice): the
+// slices spread a group over the GPU when there are few groups.
+// MODE 0: GEMM1 over the slice -> f64 partial coefficients lin_zpart[e][slice].
+// MODE 1: the coefficients (partials summed in slice order), GEMM2 and the
+//         residual sum over the slice -> cpart[e][slice].
+template <int KP, int MODE>
 __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
   static_assert(KP % 16 == 0 && KP >= 16 && KP <= 64, "basis columns");
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -145,15 +155,17 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
   const DevStar &st = b.stars[star];
   if (st.cont_kind != CONT_LINEAR || st.kp != KP) return;
   const int N = st.n_obs, K = st.k_lin;
+  const int S = gridDim.y, sl = blockIdx.y;
+  const int per = ((N + S - 1) / S + LT_TK - 1) / LT_TK * LT_TK;
+  const int x0 = min(N, sl * per), x1 = min(N, x0 + per);
   const int e = e0 + p;
   const bool member = p < LG && e < b.E;
   const EvalPrep *P = member ? &b.prep[e] : nullptr;
-  int status = member ? P->status : 0;
-  if (member && !status && P->star != star) status = S_MMA_TIMEOUT;
-  if (member && !status && st.cont_bad) status = S_CONTINUUM;
-  const bool live = member && status == 0;
+  const bool live = member && P->status == 0 && P->star == star && !st.cont_bad;
   const float *mod = live ? lt_model_row(b, *P, e) : nullptr;
   const float *flux = st.flux, *var = st.var, *q = st.q, *qt = st.qt;
+  constexpr int HALF = KP / 2;
+  double *zp = b.lin_zpart + ((size_t)e * LIN_MAX_SLICES) * 64;
 
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
   const uint32_t mbar = sbase + LT_MISC;
@@ -178,92 +190,102 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
   const uint32_t lane_off = (uint32_t)((w & 3) * 32) << 16;
   uint32_t phase = 0;
   bool ok = true;
-
-  // ------------------------------------------------ GEMM1: Z^T = B^T Q
-  // Each k-step of a 32-pixel stage goes to its own accumulator (3 MMAs)
-  // and the four are read back and added into the f64 coefficients.
-  constexpr int HALF = KP / 2;
   double z[HALF];
 #pragma unroll
   for (int c = 0; c < HALF; c++) z[c] = 0.0;
-  const uint32_t id1 = idesc_tf32(LT_M, KP);
-  for (int i0 = 0; i0 < N && ok; i0 += LT_TK) {
-    // B^T stage: row p, pixels i0 + 16 h .. + 16
+
+  if (MODE == 0) {
+    // ---------------------------------------------- GEMM1: Z^T = B^T Q over the slice
+    // Each k-step of a 32-pixel stage goes to its own accumulator (3 MMAs)
+    // and the four are read back and added into the f64 coefficients.
+    const uint32_t id1 = idesc_tf32(LT_M, KP);
+    for (int i0 = x0; i0 < x1 && ok; i0 += LT_TK) {
+      // B^T stage: row p, pixels i0 + 16 h .. + 16
 #pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const int k = 16 * h + 4 * g;
-      float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      if (live) {
-        float a[4];
+      for (int g = 0; g < 4; g++) {
+        const int k = 16 * h + 4 * g;
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (live) {
+          float a[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int i = i0 + k + j;
-          a[j] = i < N ? flux[i] / mod[i] : 0.0f;
+          for (int j = 0; j < 4; j++) {
+            const int i = i0 + k + j;
+            a[j] = i < x1 ? flux[i] / mod[i] : 0.0f;
+          }
+          v = make_float4(a[0], a[1], a[2], a[3]);
         }
-        v = make_float4(a[0], a[1], a[2], a[3]);
+        store_split4(sm, G1_AH + kmaj(p, k, LT_TK), G1_AL + kmaj(p, k, LT_TK), v);
       }
-      store_split4(sm, G1_AH + kmaj(p, k, LT_TK), G1_AL + kmaj(p, k, LT_TK), v);
-    }
-    // Q stage: basis row r = t / 4, pixels 8 (t % 4) .. + 8
-    {
-      const int r = t >> 2, k = 8 * (t & 3);
+      // Q stage: basis row r = t / 4, pixels 8 (t % 4) .. + 8
+      {
+        const int r = t >> 2, k = 8 * (t & 3);
 #pragma unroll
-      for (int g = 0; g < 2; g++) {
-        float a[4];
+        for (int g = 0; g < 2; g++) {
+          float a[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int i = i0 + k + 4 * g + j;
-          a[j] = (r < K && i < N) ? q[(size_t)r * N + i] : 0.0f;
+          for (int j = 0; j < 4; j++) {
+            const int i = i0 + k + 4 * g + j;
+            a[j] = (r < K && i < x1) ? q[(size_t)r * N + i] : 0.0f;
+          }
+          if (r < KP) store_split4(sm, G1_BH + kmaj(r, k + 4 * g, LT_TK), G1_BL + kmaj(r, k + 4 * g, LT_TK),
+                                   make_float4(a[0], a[1], a[2], a[3]));
         }
-        if (r < KP) store_split4(sm, G1_BH + kmaj(r, k + 4 * g, LT_TK), G1_BL + kmaj(r, k + 4 * g, LT_TK),
-                                 make_float4(a[0], a[1], a[2], a[3]));
       }
-    }
-    proxy_fence();
-    __syncthreads();
-    if (t == 0) {
+      proxy_fence();
+      __syncthreads();
+      if (t == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int s = 0; s < LT_TK / 8; s++) {
+          const uint32_t off = (uint32_t)(s * 256);
+          const uint64_t ah = smem_desc(sbase + G1_AH + off, LT_TK), al = smem_desc(sbase + G1_AL + off, LT_TK);
+          const uint64_t bh = smem_desc(sbase + G1_BH + off, LT_TK), bl = smem_desc(sbase + G1_BL + off, LT_TK);
+          const uint32_t d = tmem + (uint32_t)(s * 64);
+          mma_tf32(d, ah, bh, id1, 0u);
+          mma_tf32(d, ah, bl, id1, 1u);
+          mma_tf32(d, al, bh, id1, 1u);
+        }
+        mma_commit(mbar);
+      }
+      if (!mbar_wait(mbar, phase)) atomicOr(err, 1);
+      phase ^= 1u;
+      __syncthreads();
+      ok = *err == 0;
+      if (!ok) break;
       tc_fence_after();
 #pragma unroll
-      for (int s = 0; s < LT_TK / 8; s++) {
-        const uint32_t off = (uint32_t)(s * 256);
-        const uint64_t ah = smem_desc(sbase + G1_AH + off, LT_TK), al = smem_desc(sbase + G1_AL + off, LT_TK);
-        const uint64_t bh = smem_desc(sbase + G1_BH + off, LT_TK), bl = smem_desc(sbase + G1_BL + off, LT_TK);
-        const uint32_t d = tmem + (uint32_t)(s * 64);
-        mma_tf32(d, ah, bh, id1, 0u);
-        mma_tf32(d, ah, bl, id1, 1u);
-        mma_tf32(d, al, bh, id1, 1u);
-      }
-      mma_commit(mbar);
+      for (int ks = 0; ks < LT_TK / 8; ks++)
+#pragma unroll
+        for (int c = 0; c < HALF; c += 8) {
+          float v[8];
+          tmem_ld8(tmem + lane_off + (uint32_t)(ks * 64 + h * HALF + c), v);
+#pragma unroll
+          for (int j = 0; j < 8; j++) z[c + j] += (double)v[j];
+        }
+      tc_fence_before();
     }
-    if (!mbar_wait(mbar, phase)) atomicOr(err, 1);
-    phase ^= 1u;
-    __syncthreads();
-    ok = *err == 0;
-    if (!ok) break;
-    // the stage's k-step sums into the f64 coefficients (row p, columns h KP/2 ..)
-    tc_fence_after();
+    if (live) {
 #pragma unroll
-    for (int ks = 0; ks < LT_TK / 8; ks++)
-#pragma unroll
-      for (int c = 0; c < HALF; c += 8) {
-        float v[8];
-        tmem_ld8(tmem + lane_off + (uint32_t)(ks * 64 + h * HALF + c), v);
-#pragma unroll
-        for (int j = 0; j < 8; j++) z[c + j] += (double)v[j];
-      }
-    tc_fence_before();
-  }
-
-  // ------------------------------------------------ GEMM2 + residual epilogue
-  double acc = 0.0;
-  if (ok) {
-    if (live && b.params) {
-      double *par = b.params + (size_t)e * b.param_stride;
-#pragma unroll
-      for (int c = 0; c < HALF; c++)
-        if (h * HALF + c < K) par[h * HALF + c] = z[c];
+      for (int c = 0; c < HALF; c++) zp[(size_t)sl * 64 + h * HALF + c] = ok ? z[c] : LT_FAILED;
     }
-    __syncthreads();  // GEMM1 operands are no longer read
+  } else {
+    // ---------------------------------------------- GEMM2 + residual epilogue over the slice
+    bool zfail = false;
+    if (live) {
+      for (int s2 = 0; s2 < S; s2++)
+#pragma unroll
+        for (int c = 0; c < HALF; c++) {
+          const double v = zp[(size_t)s2 * 64 + h * HALF + c];
+          zfail |= v == LT_FAILED;
+          z[c] += v;
+        }
+      if (b.params && sl == 0) {
+        double *par = b.params + (size_t)e * b.param_stride;
+#pragma unroll
+        for (int c = 0; c < HALF; c++)
+          if (h * HALF + c < K) par[h * HALF + c] = z[c];
+      }
+    }
 #pragma unroll
     for (int c = 0; c < HALF; c += 4) {
       const int k = h * HALF + c;
@@ -271,8 +293,9 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
       if (live) v = make_float4((float)z[c], (float)z[c + 1], (float)z[c + 2], (float)z[c + 3]);
       store_split4(sm, G2_AH + kmaj(p, k, KP), G2_AL + kmaj(p, k, KP), v);
     }
+    double acc = 0.0;
     const uint32_t id2 = idesc_tf32(LT_M, LT_TN);
-    for (int i0 = 0; i0 < N && ok; i0 += LT_TN) {
+    for (int i0 = x0; i0 < x1 && ok; i0 += LT_TN) {
       // Q^T tile: pixel row r = t / 8 (of 32), basis columns 8 (t % 8) .. + 8
       {
         const int r = t >> 3, k = 8 * (t & 7), i = i0 + r;
@@ -280,7 +303,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
         for (int g = 0; g < 2; g++) {
           if (k + 4 * g >= KP) break;
           float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          if (i < N) v = *reinterpret_cast<const float4 *>(qt + (size_t)i * KP + k + 4 * g);
+          if (i < x1) v = *reinterpret_cast<const float4 *>(qt + (size_t)i * KP + k + 4 * g);
           store_split4(sm, G2_BH + kmaj(r, k + 4 * g, KP), G2_BL + kmaj(r, k + 4 * g, KP), v);
         }
       }
@@ -323,7 +346,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
 #pragma unroll
           for (int j = 0; j < 8; j++) {
             const int i = i0 + 16 * h + c + j;
-            if (i >= 50 && i < N - 50) {
+            if (i >= 50 && i < N - 50 && i < x1) {
               const float bb = flux[i] / mod[i];
               const float r = (float)f[j] - bb;
               acc += (double)(r / var[i] * r);
@@ -333,47 +356,68 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
       }
       tc_fence_before();
     }
+    int *rfail = reinterpret_cast<int *>(sm + LT_RFAIL);
+    if (h == 1) {
+      red[p] = acc;
+      rfail[p] = zfail ? 1 : 0;
+    }
+    __syncthreads();
+    // a residual sum is never negative: -1 marks a failed slice (a NaN sum stays a NaN chi2, as in the reference)
+    if (h == 0 && live) b.cpart[(size_t)e * MAX_CHUNKS + sl] = (ok && !zfail && !rfail[p]) ? acc + red[p] : -1.0;
   }
-  // ------------------------------------------------ results, tensor memory
-  if (h == 1) red[p] = acc;
+  // ------------------------------------------------ tensor memory
   tc_fence_before();
   __syncthreads();
   if (w == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(LT_TMEM_COLS) : "memory");
   }
-  if (h == 0 && member) {
-    int s = status;
-    if (!s && !ok) s = S_MMA_TIMEOUT;
-    const double chi2 = (acc + red[p]) / (double)N;
-    b.cost[e] = s ? __longlong_as_double(0x7FF8000000000000ll) : chi2;
-    b.status[e] = s;
-  }
 }
 
-void launch_linear_tc(const EvalBatch &b, int kp, cudaStream_t s) {
-  if (b.E <= 0 || b.lin_group <= 0 || b.lin_group > LT_M) return;
-  const int groups = (b.E + b.lin_group - 1) / b.lin_group;
-  switch (kp) {
-    case 16:
-      cudaFuncSetAttribute(k_linear_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
-      k_linear_tc<16><<<groups, LT_T, LT_SMEM, s>>>(b);
-      break;
-    case 32:
-      cudaFuncSetAttribute(k_linear_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
-      k_linear_tc<32><<<groups, LT_T, LT_SMEM, s>>>(b);
-      break;
-    case 48:
-      cudaFuncSetAttribute(k_linear_tc<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
-      k_linear_tc<48><<<groups, LT_T, LT_SMEM, s>>>(b);
-      break;
-    case 64:
-      cudaFuncSetAttribute(k_linear_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
-      k_linear_tc<64><<<groups, LT_T, LT_SMEM, s>>>(b);
-      break;
-    default:
-      return;
+// chi2 = the slices' residual sums in slice order / N, and the statuses, of
+// the evaluations of tensor-core linear continua
+__global__ void k_linear_final(EvalBatch b) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= b.E) return;
+  const int LG = b.lin_group;
+  const int star = b.prep[(e / LG) * LG].star;
+  const DevStar &st = b.stars[star];
+  if (st.cont_kind != CONT_LINEAR || st.kp == 0) return;
+  const EvalPrep &P = b.prep[e];
+  int s = P.status;
+  if (!s && P.star != star) s = S_MMA_TIMEOUT;
+  if (!s && st.cont_bad) s = S_CONTINUUM;
+  double chi2 = 0.0;
+  if (!s) {
+    for (int k = 0; k < b.lin_slices; k++) {
+      const double v = b.cpart[(size_t)e * MAX_CHUNKS + k];
+      if (v < 0.0) s = S_MMA_TIMEOUT;  // a residual sum is never negative: a slice's barrier wait ran out
+      chi2 += v;
+    }
+    chi2 /= (double)st.n_obs;
   }
+  b.cost[e] = s ? __longlong_as_double(0x7FF8000000000000ll) : chi2;
+  b.status[e] = s;
+}
+
+template <int KP>
+static void launch_kp(const EvalBatch &b, dim3 grid, cudaStream_t s) {
+  cudaFuncSetAttribute(k_linear_tc<KP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
+  cudaFuncSetAttribute(k_linear_tc<KP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
+  k_linear_tc<KP, 0><<<grid, LT_T, LT_SMEM, s>>>(b);
+  k_linear_tc<KP, 1><<<grid, LT_T, LT_SMEM, s>>>(b);
+  count_launch(2);
+}
+
+void launch_linear_tc(const EvalBatch &b, cudaStream_t s) {
+  if (b.E <= 0 || b.lin_group <= 0 || b.lin_group > LT_M || !b.lin_kp_mask) return;
+  const int groups = (b.E + b.lin_group - 1) / b.lin_group;
+  const dim3 grid(groups, b.lin_slices);
+  if (b.lin_kp_mask & (1u << 1)) launch_kp<16>(b, grid, s);
+  if (b.lin_kp_mask & (1u << 2)) launch_kp<32>(b, grid, s);
+  if (b.lin_kp_mask & (1u << 3)) launch_kp<48>(b, grid, s);
+  if (b.lin_kp_mask & (1u << 4)) launch_kp<64>(b, grid, s);
+  k_linear_final<<<(b.E + 255) / 256, 256, 0, s>>>(b);
   count_launch();
 }
 
