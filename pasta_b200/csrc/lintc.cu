@@ -197,39 +197,34 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
   if (MODE == 0) {
     // ---------------------------------------------- GEMM1: Z^T = B^T Q over the slice
     // Each k-step of a 32-pixel stage goes to its own accumulator (3 MMAs)
-    // and the four are read back and added into the f64 coefficients.
+    // and the four are read back and added into the f64 coefficients.  The
+    // next stage's operands are loaded into registers while the MMAs run.
     const uint32_t id1 = idesc_tf32(LT_M, KP);
-    for (int i0 = x0; i0 < x1 && ok; i0 += LT_TK) {
-      // B^T stage: row p, pixels i0 + 16 h .. + 16
+    const int r = t >> 2, kq = 8 * (t & 3);  // Q stage: basis row r, pixels kq .. kq + 8
+    float av[16], qv[8];
+    auto load_stage = [&](int i0) {
 #pragma unroll
-      for (int g = 0; g < 4; g++) {
-        const int k = 16 * h + 4 * g;
-        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (live) {
-          float a[4];
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int i = i0 + k + j;
-            a[j] = i < x1 ? flux[i] / mod[i] : 0.0f;
-          }
-          v = make_float4(a[0], a[1], a[2], a[3]);
-        }
-        store_split4(sm, G1_AH + kmaj(p, k, LT_TK), G1_AL + kmaj(p, k, LT_TK), v);
+      for (int j = 0; j < 16; j++) {
+        const int i = i0 + 16 * h + j;
+        av[j] = (live && i < x1) ? flux[i] / mod[i] : 0.0f;
       }
-      // Q stage: basis row r = t / 4, pixels 8 (t % 4) .. + 8
-      {
-        const int r = t >> 2, k = 8 * (t & 3);
 #pragma unroll
-        for (int g = 0; g < 2; g++) {
-          float a[4];
+      for (int j = 0; j < 8; j++) {
+        const int i = i0 + kq + j;
+        qv[j] = (r < K && i < x1) ? q[(size_t)r * N + i] : 0.0f;
+      }
+    };
+    if (x0 < x1) load_stage(x0);
+    for (int i0 = x0; i0 < x1 && ok; i0 += LT_TK) {
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int i = i0 + k + 4 * g + j;
-            a[j] = (r < K && i < x1) ? q[(size_t)r * N + i] : 0.0f;
-          }
-          if (r < KP) store_split4(sm, G1_BH + kmaj(r, k + 4 * g, LT_TK), G1_BL + kmaj(r, k + 4 * g, LT_TK),
-                                   make_float4(a[0], a[1], a[2], a[3]));
-        }
+      for (int g = 0; g < 4; g++)
+        store_split4(sm, G1_AH + kmaj(p, 16 * h + 4 * g, LT_TK), G1_AL + kmaj(p, 16 * h + 4 * g, LT_TK),
+                     make_float4(av[4 * g], av[4 * g + 1], av[4 * g + 2], av[4 * g + 3]));
+      if (r < KP) {
+#pragma unroll
+        for (int g = 0; g < 2; g++)
+          store_split4(sm, G1_BH + kmaj(r, kq + 4 * g, LT_TK), G1_BL + kmaj(r, kq + 4 * g, LT_TK),
+                       make_float4(qv[4 * g], qv[4 * g + 1], qv[4 * g + 2], qv[4 * g + 3]));
       }
       proxy_fence();
       __syncthreads();
@@ -247,6 +242,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
         }
         mma_commit(mbar);
       }
+      if (i0 + LT_TK < x1) load_stage(i0 + LT_TK);  // in flight while the MMAs run
       if (!mbar_wait(mbar, phase)) atomicOr(err, 1);
       phase ^= 1u;
       __syncthreads();
@@ -295,18 +291,20 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
     }
     double acc = 0.0;
     const uint32_t id2 = idesc_tf32(LT_M, LT_TN);
-    for (int i0 = x0; i0 < x1 && ok; i0 += LT_TN) {
-      // Q^T tile: pixel row r = t / 8 (of 32), basis columns 8 (t % 8) .. + 8
-      {
-        const int r = t >> 3, k = 8 * (t & 7), i = i0 + r;
+    const int r = t >> 3, kq = 8 * (t & 7);  // Q^T tile: pixel row r (of 32), basis columns kq .. kq + 8
+    float4 qv[2];
+    auto load_tile = [&](int i0) {
+      const int i = i0 + r;
 #pragma unroll
-        for (int g = 0; g < 2; g++) {
-          if (k + 4 * g >= KP) break;
-          float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          if (i < x1) v = *reinterpret_cast<const float4 *>(qt + (size_t)i * KP + k + 4 * g);
-          store_split4(sm, G2_BH + kmaj(r, k + 4 * g, KP), G2_BL + kmaj(r, k + 4 * g, KP), v);
-        }
-      }
+      for (int g = 0; g < 2; g++)
+        qv[g] = (i < x1 && kq + 4 * g < KP) ? *reinterpret_cast<const float4 *>(qt + (size_t)i * KP + kq + 4 * g)
+                                            : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    };
+    if (x0 < x1) load_tile(x0);
+    for (int i0 = x0; i0 < x1 && ok; i0 += LT_TN) {
+#pragma unroll
+      for (int g = 0; g < 2; g++)
+        if (kq + 4 * g < KP) store_split4(sm, G2_BH + kmaj(r, kq + 4 * g, KP), G2_BL + kmaj(r, kq + 4 * g, KP), qv[g]);
       proxy_fence();
       __syncthreads();
       if (t == 0) {
@@ -322,6 +320,16 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
           mma_tf32(d, al, bh, id2, 1u);
         }
         mma_commit(mbar);
+      }
+      // while the MMAs run: the next tile's basis and this tile's ratios and variances
+      if (i0 + LT_TN < x1) load_tile(i0 + LT_TN);
+      float bb[16], vv[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int i = i0 + 16 * h + j;
+        const bool use = live && i >= 50 && i < N - 50 && i < x1;
+        bb[j] = use ? flux[i] / mod[i] : 0.0f;
+        vv[j] = use ? var[i] : 0.0f;
       }
       if (!mbar_wait(mbar, phase)) atomicOr(err, 1);
       phase ^= 1u;
@@ -347,9 +355,8 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
           for (int j = 0; j < 8; j++) {
             const int i = i0 + 16 * h + c + j;
             if (i >= 50 && i < N - 50 && i < x1) {
-              const float bb = flux[i] / mod[i];
-              const float r = (float)f[j] - bb;
-              acc += (double)(r / var[i] * r);
+              const float rr = (float)f[j] - bb[c + j];
+              acc += (double)(rr / vv[c + j] * rr);
             }
           }
         }
