@@ -422,6 +422,10 @@ def run_ours(args):
                         seed=5150 + rank) if args.binary_stars > 0 else None
     torch.cuda.synchronize(dev)
 
+    # -------- linear-model continuum: tensor-core vs CUDA-core path (config-0 sizes)
+    linear = linear_leg(P, S, args.linear_labels, args.linear_k) if args.linear_labels > 0 and rank == 0 else None
+    torch.cuda.synchronize(dev)
+
     # -------- served time-to-fit: Poisson arrivals, each request its own
     # continuum settings (4-12 chunks, degree 3-8), stars of the workload
     lat = serve_latency(P, interp, stars, settings, seeds, rate=args.serve_rate, n_req=args.serve_requests,
@@ -488,6 +492,7 @@ def run_ours(args):
                                           "(201 PSO steps + final refit); bytes are per call" % n_stars},
         "latency_s": lat,
         "binary": binary,
+        "linear_continuum": linear,
         "plain_gpu": {"fits_per_s": plain_fits, "stars": n_plain, "identical_results": same,
                       "batched_e2e_over_plain": e2e_fits / (plain_fits * world)},
         "label_error_vs_truth": {"median_abs": np.median(err, axis=0).tolist(),
@@ -623,7 +628,7 @@ def main():
     ap.add_argument("--binary-stars", type=int, default=16, help="binary-fit leg: stars (0: skip)")
     ap.add_argument("--linear-only", action="store_true",
                     help="time chi2 with a linear-model continuum, tensor-core and CUDA-core paths, and print it")
-    ap.add_argument("--linear-labels", type=int, default=1024)
+    ap.add_argument("--linear-labels", type=int, default=1024, help="linear-continuum leg: labels per call (0: skip)")
     ap.add_argument("--linear-k", type=int, default=40)
     ap.add_argument("--binary-only", action="store_true",
                     help="run only the binary-fit leg (with its CPU baseline unless --no-cpu) and print it")
