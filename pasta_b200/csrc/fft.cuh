@@ -64,9 +64,11 @@ __device__ __forceinline__ void dft8(cf v[8]) {
   v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 
-// One Stockham stage of radix R at sub-transform length NS.  All reads of
-// the stage happen before a barrier, all writes after it, so the transform
-// runs in place.  The caller must __syncthreads() after filling the input.
+// One Stockham stage of radix R at sub-transform length NS.  With MID all
+// reads of the stage happen before a barrier, all writes after it, so the
+// transform runs in place; without it the stage must read and write
+// different buffers (ping-pong) and only the closing barrier remains.  The
+// caller must __syncthreads() after filling the input.
 // ld(i, a) returns input element i (a = its swizzled shared-memory slot),
 // st(i, a, v, s) stores output element i, the thread's s-th output of the
 // stage (a compile-time constant after unrolling); SmemLoad / SmemStore use the
@@ -83,7 +85,7 @@ __device__ __forceinline__ void dft8(cf v[8]) {
 // with d the first output index of the thread's butterfly.  The identities
 // and the absence of bank conflicts hold for every thread and r of these
 // stages (checked exhaustively).
-template <int R, int NS, bool INV, class LD, class ST>
+template <int R, int NS, bool INV, class LD, class ST, bool MID = true>
 __device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD &ld, const ST &st) {
   static_assert((R == 8 && (NS == 1 || NS == 8 || NS == 64)) || (R == 4 && NS == 512), "fft2048 stage");
   constexpr int N = 2048, J = N / R, PER = J / FFT_T, STEP = N / (NS * R);
@@ -115,7 +117,7 @@ __device__ __forceinline__ void fft_pass(const float2 *__restrict__ tw, const LD
       }
     }
   }
-  __syncthreads();
+  if constexpr (MID) __syncthreads();
 #pragma unroll
   for (int q = 0; q < PER; q++) {
     const int j = t + q * FFT_T;
@@ -150,6 +152,11 @@ struct SmemStore {
 template <int R, int NS, bool INV>
 __device__ __forceinline__ void fft_stage(float2 *c, const float2 *__restrict__ tw) {
   fft_pass<R, NS, INV>(tw, SmemLoad{c}, SmemStore{c});
+}
+// one stage from buffer src to buffer dst (no barrier between reads and writes)
+template <int R, int NS, bool INV>
+__device__ __forceinline__ void fft_stage_pp(const float2 *src, float2 *dst, const float2 *__restrict__ tw) {
+  fft_pass<R, NS, INV, SmemLoad, SmemStore, false>(tw, SmemLoad{src}, SmemStore{dst});
 }
 
 template <bool INV>

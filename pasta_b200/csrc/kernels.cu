@@ -395,9 +395,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // staging row: synth pixels [a0, a0 + BR_STG) with a0 = j0 rounded down to
 // 4, so a block's 2048 inputs start at offset j0 - a0 in 0..3
 constexpr int BR_STG = 2064;
-// dynamic shared memory of k_broaden (floats): two staging rows, the
-// swizzled FFT arrays, the two blocks' outputs, the instrument taps
-constexpr int BR_SMEM_FLOATS = 2 * BR_STG + 2 * FFT_SM + 2 * FFT_SM + 512;  // staging, FFT (float2), outputs, taps
+// dynamic shared memory of k_broaden (floats): two staging rows, two
+// swizzled FFT arrays (float2; the blocks' outputs reuse one of them), the
+// instrument taps
+constexpr int BR_SMEM_FLOATS = 2 * BR_STG + 2 * FFT_SM + 2 * FFT_SM + 512;
 
 // pixels outside [ilo, ihi) are zero; ilo and ihi are multiples of 8, so
 // every 16-byte chunk is wholly inside or outside
@@ -480,6 +481,31 @@ struct StageLoad {
   bool has1;
   __device__ __forceinline__ cf operator()(int i, int) const { return cf{s0[i], has1 ? s1[i] : 0.0f}; }
 };
+// last forward stage: the spectrum times the kernel spectrum H (1025 bins of
+// a real kernel; bins above 1024 are the conjugates of 2048 - k).  The stage
+// writes output k to the slot it read input k from, so the product takes the
+// place of a separate pass.
+struct SpecStore {
+  float2 *c;
+  const float2 *__restrict__ H;
+  __device__ __forceinline__ void operator()(int k, int a, cf v, int) const {
+    float2 h = __ldg(&H[k <= 1024 ? k : FFTN - k]);
+    if (k > 1024) h.y = -h.y;
+    const cf z = cmul(v, cf{h.x, h.y});
+    c[a] = make_float2(z.x, z.y);
+  }
+};
+// last inverse stage of the unfolded path: rotation output t (data index
+// s - hg + t - base of each block) scaled, zero outside the grid
+struct MaskStore {
+  float2 *c;
+  int base, r0, r1, N;
+  float sc;
+  __device__ __forceinline__ void operator()(int t, int a, cf v, int) const {
+    const int i0 = r0 + (t - base), i1 = r1 + (t - base);
+    c[a] = make_float2((i0 >= 0 && i0 < N) ? v.x * sc : 0.0f, (i1 >= 0 && i1 < N) ? v.y * sc : 0.0f);
+  }
+};
 // last inverse stage of the folded path: FFT index i is output i - lo
 struct FoldStore {
   float *o0, *o1;
@@ -497,9 +523,12 @@ struct FoldStore {
 __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) float br_smem[];
   float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
-  float2 *c = reinterpret_cast<float2 *>(stg1 + BR_STG);  // FFT data (BR_STG keeps 16-byte alignment)
-  float *ob0 = reinterpret_cast<float *>(c + FFT_SM), *ob1 = ob0 + FFT_SM;
-  float *gks = ob1 + FFT_SM;  // the fixed instrument kernel of the current item
+  // two FFT buffers (BR_STG keeps 16-byte alignment); the stages alternate
+  // between them, so each needs one barrier.  The transform ends in fb; the
+  // outputs then take the other buffer (fa), or fb itself on the folded path
+  float2 *fa = reinterpret_cast<float2 *>(stg1 + BR_STG);
+  float2 *fb = fa + FFT_SM;
+  float *gks = reinterpret_cast<float *>(fb + FFT_SM);  // the fixed instrument kernel of the current item
   const int N = G.npx;
   const int p0 = pidx(threadIdx.x);
   ItemCursor cur;
@@ -514,7 +543,7 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
     BroadenItem w;
     broaden_item(b, cur.e, cur.pair, w);
     cp_async_wait_all();
-    __syncthreads();  // the item's input is staged
+    __syncthreads();  // the item's input is staged; the last item's outputs are written
     const int e = w.e, pair = w.pair, m = w.m, hg = w.hg, V = w.V, s0 = w.s0, s1 = w.s1;
     const bool has1 = w.has1;
     const EvalPrep &P = b.prep[e];
@@ -531,49 +560,36 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
     // with the combined kernel: multiply the spectra and skip the taps.
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
+    float *ob0 = reinterpret_cast<float *>(fold ? fb : fa), *ob1 = ob0 + FFT_SM;
     if (m > 1) {
-      fft_pass<8, 1, false>(tw, ld, SmemStore{c});  // first stage straight from the staging rows
+      // first stage straight from the staging rows
+      fft_pass<8, 1, false, StageLoad, SmemStore, false>(tw, ld, SmemStore{fa});
       if (!nxt.done()) stage_item(b, nxt.e, nxt.pair, stg0, stg1);
       cp_async_commit();
-      fft_stage<8, 8, false>(c, tw);
-      fft_stage<8, 64, false>(c, tw);
-      fft_stage<4, 512, false>(c, tw);
-      // the kernel spectrum (Hermitian: bins above 1024 are conjugates)
+      fft_stage_pp<8, 8, false>(fa, fb, tw);
+      fft_stage_pp<8, 64, false>(fb, fa, tw);
       const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
-      for (int k = threadIdx.x; k < FFTN; k += FFT_T) {
-        float2 h = k <= 1024 ? H[k] : H[FFTN - k];
-        if (k > 1024) h.y = -h.y;
-        const int a = p0 + (k - threadIdx.x);  // pidx(k), k - threadIdx.x a multiple of 256
-        const float2 x = c[a];
-        const cf z = cmul(cf{x.x, x.y}, cf{h.x, h.y});
-        c[a] = make_float2(z.x, z.y);
-      }
-      __syncthreads();
-      fft_stage<8, 1, true>(c, tw);
-      fft_stage<8, 8, true>(c, tw);
-      fft_stage<8, 64, true>(c, tw);
+      fft_pass<4, 512, false, SmemLoad, SpecStore, false>(tw, SmemLoad{fa}, SpecStore{fb, H});
+      fft_stage_pp<8, 1, true>(fb, fa, tw);
+      fft_stage_pp<8, 8, true>(fa, fb, tw);
+      fft_stage_pp<8, 64, true>(fb, fa, tw);
       base = m - 1;
       const float sc = 1.0f / 2048.0f;
-      if (fold) {  // output u sits at base + 2 hg + u
-        fft_pass<4, 512, true>(tw, SmemLoad{c}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
-      } else {
-        fft_stage<4, 512, true>(c, tw);
-        for (int t = base + threadIdx.x; t < FFTN; t += FFT_T) {
-          const int i0 = s0 - hg + (t - base), i1 = s1 - hg + (t - base);
-          const float2 x = c[pidx(t)];
-          c[pidx(t)] = make_float2((i0 >= 0 && i0 < N) ? x.x * sc : 0.0f, (i1 >= 0 && i1 < N) ? x.y * sc : 0.0f);
-        }
-        __syncthreads();
-      }
+      if (fold)  // output u sits at base + 2 hg + u
+        fft_pass<4, 512, true, SmemLoad, FoldStore, false>(tw, SmemLoad{fa}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
+      else
+        fft_pass<4, 512, true, SmemLoad, MaskStore, false>(tw, SmemLoad{fa},
+                                                           MaskStore{fb, base, s0 - hg, s1 - hg, N, sc});
     } else {  // identity rotation: the staged input is the rotation output
       for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
         const cf v = ld(t, 0);
-        c[p0 + (t - threadIdx.x)] = make_float2(v.x, v.y);
+        fb[p0 + (t - threadIdx.x)] = make_float2(v.x, v.y);
       }
       __syncthreads();
       if (!nxt.done()) stage_item(b, nxt.e, nxt.pair, stg0, stg1);
       cp_async_commit();
     }
+    const float2 *c = fb;  // rotation outputs of the unfolded paths
     if (!fold) {
       for (int u = threadIdx.x; u < V; u += FFT_T) {
         const int i0 = s0 + u, i1 = s1 + u;
@@ -599,8 +615,8 @@ __global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, co
         ob0[u] = v0;
         ob1[u] = v1;
       }
+      __syncthreads();  // (the folded path's last stage ended with one)
     }
-    __syncthreads();
     float *y = b.bufB + (size_t)e * b.stride;
     if (P.epi) {
       // observed pixels [bnd[2 pair], bnd[2 pair + 2]) have their left synth
