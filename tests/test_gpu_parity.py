@@ -388,12 +388,20 @@ def test_convolve_and_resample_directory(env, tmp_path):
 def test_linear_continuum_tensor_core_many_labels(env, k):
     """Linear-model continua run as tcgen05 tf32 (split hi/lo) products per
     group of 128 evaluations: chi2 of 300 random labels (three groups).
-    Against the CUDA-core path on the same models: relative 5e-6.  Against
-    the FP64 oracle: relative 3e-5; for the worst-fitting labels (chi2 in the
-    thousands) the model's own f32 roundoff is amplified past 1e-5, and the
-    CUDA-core path deviates by the same amount on the same labels."""
+
+    The broadening path is pinned (the timed direct/FFT crossover can fall
+    either way on this small grid).  Direct convolution for every kernel:
+    against the CUDA-core path on the same models relative 5e-6, against the
+    FP64 oracle relative 3e-5 (NaN where the oracle's 64-column solve
+    breaks down), good fits (chi2 < 1000) 1e-5.  FFT blocks for every
+    kernel: good fits 1e-5.  The narrow-kernel labels that fit badly (chi2
+    up to 1e9) are ill-conditioned in the model: the FFT's f32 roundoff of
+    4e-7 in the flux moves their chi2 by up to 1e-2 at 12-40 columns and 0.3
+    at 64, and the oracle's own FP32 mirror of the reference deviates from
+    its FP64 mode by up to 2.4% (7e12 where FP64 gives NaN), so they carry
+    no tolerance on that path beyond being finite."""
     from pasta_b200 import _ffi
-    O, P, S, star = env["O"], env["P"], env["S"], env["star"]
+    O, P, S, star, interp = env["O"], env["P"], env["S"], env["star"], env["interp"]
     d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
     od = O.Disp(env["og"], O.DISP_FIXED, star.wl, 85000.0)
     D = S.legendre_design(star.wl, k)
@@ -401,19 +409,28 @@ def test_linear_continuum_tensor_core_many_labels(env, k):
     rng = np.random.default_rng(k)
     labs = np.stack([rng.uniform(6000, 8000, 300), rng.uniform(-0.5, 0.5, 300), rng.uniform(3.5, 4.5, 300),
                      rng.uniform(0, 200, 300), rng.uniform(-100, 100, 300)], axis=1)
-    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(8, 2), (0, 300), (-150, 150))
-    gpu = np.array(fitter.chi2(env["interp"], star.flux, star.var, labs))
-    _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(0))
+    fitter = interp.get_fitter(d, cont, P.PSOSettings(8, 2), (0, 300), (-150, 150))
+    saved = interp.direct_max
     try:
-        cuda_cores = np.array(fitter.chi2(env["interp"], star.flux, star.var, labs))
+        interp.direct_max = 512  # every kernel of the test (at most 512 taps) convolved directly
+        gpu = np.array(fitter.chi2(interp, star.flux, star.var, labs))
+        _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(0))
+        try:
+            cuda_cores = np.array(fitter.chi2(interp, star.flux, star.var, labs))
+        finally:
+            _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(1))
+        interp.direct_max = 0  # every kernel through the FFT blocks
+        gpu_fft = np.array(fitter.chi2(interp, star.flux, star.var, labs))
     finally:
-        _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(1))
+        interp.direct_max = saved
     np.testing.assert_allclose(gpu, cuda_cores, rtol=5e-6)
     ref, st = O.chi2(env["og"], od, oc, star.flux, star.var, labs, O.F64)
     assert (st == 0).all()
     np.testing.assert_allclose(gpu, ref, rtol=3e-5)
     good = ref < 1000.0
     np.testing.assert_allclose(gpu[good], ref[good], rtol=CHI2_TOL)
+    np.testing.assert_allclose(gpu_fft[good], ref[good], rtol=CHI2_TOL)
+    assert (np.isfinite(gpu_fft) | ~np.isfinite(ref)).all()
 
 
 def test_linear_continuum_fit_params(env):
