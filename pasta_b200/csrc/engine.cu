@@ -120,6 +120,43 @@ struct DBuf {
   void upload(const std::vector<T> &v) { upload(v.data(), v.size()); }
 };
 
+// page-locked host buffer: copies from and to it are asynchronous and can
+// be captured in a CUDA graph
+template <class T>
+struct HostBuf {
+  T *p = nullptr;
+  HostBuf() = default;
+  HostBuf(const HostBuf &) = delete;
+  HostBuf &operator=(const HostBuf &) = delete;
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  void alloc(size_t count) {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    if (count == 0) return;
+    cudaError_t e = cudaMallocHost(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      fail(PASTA_E_NOMEM, "cudaMallocHost of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+  }
+};
+
+// an instantiated CUDA graph, destroyed with its owner
+struct GraphHold {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  GraphHold() = default;
+  GraphHold(const GraphHold &) = delete;
+  GraphHold &operator=(const GraphHold &) = delete;
+  ~GraphHold() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
 struct Ctx {
   int dev = 0;
   cudaStream_t stream = nullptr;
@@ -1433,8 +1470,8 @@ namespace {
 
 // Autotuner of the broadening path: the crossover between the direct and the
 // FFT broadening on this device.  For rotation widths on a ladder, the
-// pipeline runs 256 evaluations of one grid label over the whole synthetic
-// grid with either path, timed with CUDA events (best of 3 after a warm-up);
+// pipeline runs 256 or more evaluations of one grid label over the whole
+// synthetic grid with either path, timed with CUDA events (best of 3 after a warm-up);
 // direct_max is the widest kernel up to which the direct path won at every
 // rung.  PASTA_DIRECT_MAX_TAPS fixes the value instead (0: FFT only);
 // PASTA_TUNE_VERBOSE prints the measured ladder.
@@ -1447,7 +1484,10 @@ void tune_direct(pasta_grid *g) {
   if (g->wl_kind == WL_NONUNI || !(g->d.dvelo > 0.0)) return;
   Ctx &C = ctx();
   cudaStream_t s = C.stream;
-  const int E = 256;
+  // at least ~15M window pixels per run (256 evaluations at 80,000 px, 768
+  // at 20,000), so that small grids are timed on throughput rather than on
+  // launch latency, where both paths tie and the comparison is noise
+  const int E = std::max(256, std::min(2048, (int)(20000000LL / std::max<int64_t>(g->npx, 1)) / 256 * 256));
   const int ti = (int)g->tv.size() / 2;
   const double t = g->tv[ti], mh = g->mv[g->mv.size() / 2], lg = g->lv[(g->llo[ti] + g->lhi[ti]) / 2];
   DevStar st = make_star(nullptr, nullptr, nullptr, nullptr, 0);
@@ -1506,11 +1546,7 @@ void tune_direct(pasta_grid *g) {
     if (getenv("PASTA_TUNE_VERBOSE"))
       fprintf(stderr, "pasta_b200 tune: %lld px, rotation %d taps: FFT %.4f ms, direct %.4f ms (%d evaluations)\n",
               (long long)g->npx, mw, tm[0], tm[1], E);
-    // Near-ties go to direct convolution: its roundoff stays relative to the
-    // local flux (an FFT block's is relative to the block's largest value),
-    // and a 3% margin keeps the choice stable against timing noise where
-    // both paths are launch-bound (small grids).
-    if (tm[1] <= 1.03f * tm[0]) best = mw;
+    if (tm[1] < tm[0]) best = mw;
     else break;
   }
   cudaEventDestroy(e0);
@@ -2464,12 +2500,45 @@ int pasta_binary_fit(const pasta_grid *g_, const pasta_grid *cg, const pasta_dis
         const double w = B.mx[k] - B.mn[k];
         v[(size_t)p * D + k] = (-w == w) ? -w : uniform_between(-w, w, draw_u01(seed, PH_INIT_VEL, p, 0, k));
       }
-    auto evaluate = [&]() -> int {
-      CK(cudaMemcpyAsync(bs.labels.p, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    // One evaluation of the swarm: positions in, costs and statuses out,
+    // through page-locked buffers.  The sequence is the same every
+    // iteration, so it is captured once as a CUDA graph and replayed (one
+    // launch per iteration instead of a dozen kernels and three copies).
+    HostBuf<double> hx, hcost;
+    HostBuf<int> hest;
+    hx.alloc((size_t)P * D);
+    hcost.alloc(P);
+    hest.alloc(P);
+    auto enqueue = [&]() {
+      CK(cudaMemcpyAsync(bs.labels.p, hx.p, (size_t)P * D * sizeof(double), cudaMemcpyHostToDevice, s));
       run_binary(g, cg, ds.p, hstar, bs, P, vs_max, true, nullptr, 0, s);
-      CK(cudaMemcpyAsync(cost.data(), bs.cost.p, P * sizeof(double), cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(est.data(), bs.status.p, P * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hcost.p, bs.cost.p, P * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hest.p, bs.status.p, P * sizeof(int), cudaMemcpyDeviceToHost, s));
+    };
+    GraphHold gh;
+    bool try_graph = !getenv("PASTA_NO_GRAPH");
+    auto evaluate = [&]() -> int {
+      std::copy(x.begin(), x.end(), hx.p);
+      if (try_graph) {
+        try_graph = false;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+          enqueue();
+        } catch (...) {
+          cudaGraph_t dead = nullptr;
+          cudaStreamEndCapture(s, &dead);  // leave capture mode before the error propagates
+          if (dead) cudaGraphDestroy(dead);
+          cudaGetLastError();
+          throw;
+        }
+        CK(cudaStreamEndCapture(s, &gh.graph));
+        CK(cudaGraphInstantiate(&gh.exec, gh.graph, 0));
+      }
+      if (gh.exec) CK(cudaGraphLaunch(gh.exec, s));
+      else enqueue();
       CK(cudaStreamSynchronize(s));
+      std::copy(hcost.p, hcost.p + P, cost.begin());
+      std::copy(hest.p, hest.p + P, est.begin());
       for (int p = 0; p < P; p++)
         if (est[p]) return est[p];
       return S_OK;

@@ -1216,7 +1216,11 @@ void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
 // flux/model over the chunk (216-226) is the projection onto the chunk's
 // polynomial space; it is solved here in a Legendre basis with the FP64
 // Cholesky factor of its Gram matrix (the same space as the reference's
-// monomial SVD, far better conditioned).  Moments accumulate in FP64.
+// monomial SVD, far better conditioned).  A lane sums the products
+// P_k(x) y of its CU pixels in f32 and adds that partial to its running
+// FP64 moment: one f32 -> f64 conversion per moment per CU pixels instead of
+// one per pixel (the conversions share the narrow XU pipe with the
+// division's reciprocal), and a short FP64 dependency chain.
 // K = polynomial order + 1 (one instantiation per order present).  A warp
 // walks the whole chunk (no block barriers), so the loads of many chunks
 // are in flight per SM.
@@ -1247,16 +1251,21 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
       md[u] = mod[i];
       xf[u] = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
     }
+    float zp[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) zp[k] = 0.0f;
 #pragma unroll
     for (int u = 0; u < CU; u++) {
       if (i0 + 32 * u < hi) {
-        const double y = (double)(fl[u] / md[u]);
+        const float y = fl[u] / md[u];
         float Pk[K];
         legendre<K>(xf[u], Pk);
 #pragma unroll
-        for (int k = 0; k < K; k++) z[k] = fma((double)Pk[k], y, z[k]);
+        for (int k = 0; k < K; k++) zp[k] = fmaf(Pk[k], y, zp[k]);
       }
     }
+#pragma unroll
+    for (int k = 0; k < K; k++) z[k] += (double)zp[k];
   }
 #pragma unroll
   for (int k = 0; k < K; k++) {
@@ -1298,8 +1307,9 @@ __device__ __forceinline__ float poly_eval_r(const float (&coef)[K], float x) {
 // chi2 section of chunk c (continuum_fitting.rs:280-360): chunk 0 alone on
 // [50, start_1); chunk c >= 1 blended with chunk c - 1 (sin^2 factor) on
 // [start_c, stop_{c-1}), then alone up to start_{c+1} (N - 50 for the
-// last).  One warp per section; partial sums in FP64, added in chunk order
-// by k_chunk_final.
+// last).  One warp per section; a lane adds the terms of the pixels it
+// loads together in f32 and those partials in FP64; section sums in FP64,
+// added in chunk order by k_chunk_final.
 template <int K>
 __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b) {
   const int lane = threadIdx.x & 31;
@@ -1332,14 +1342,16 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
         vr[u] = var[i];
         xa[u] = st.xa[i];
       }
+      float part = 0.0f;  // the lane's CU terms in f32, then one FP64 add
 #pragma unroll
       for (int u = 0; u < CU; u++) {
         if (i0 + 32 * u < hi) {
           const float p = poly_eval_r<K>(cc, xa[u]);
           const float r = fl[u] - p * md[u];
-          acc += (double)(r * r / vr[u]);
+          part += r * r / vr[u];
         }
       }
+      acc += (double)part;
     }
   };
   if (c == 0) {
@@ -1359,6 +1371,7 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
         xb[u] = st.xb[i];
         fc[u] = st.fac[i];
       }
+      float part = 0.0f;
 #pragma unroll
       for (int u = 0; u < 2; u++) {
         if (i0 + 32 * u < sp) {
@@ -1366,9 +1379,10 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
           const float cu = poly_eval_r<K>(cc, xb[u]);
           const float p = pv * fc[u] + cu * (1.0f - fc[u]);
           const float r = fl[u] - p * md[u];
-          acc += (double)(r * r / vr[u]);
+          part += r * r / vr[u];
         }
       }
+      acc += (double)part;
     }
     alone(sp, nx);
   }
