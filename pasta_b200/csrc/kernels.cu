@@ -520,7 +520,7 @@ struct FoldStore {
   }
 };
 
-__global__ void __launch_bounds__(FFT_T, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) float br_smem[];
   float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
   // two FFT buffers (BR_STG keeps 16-byte alignment); the stages alternate
@@ -1115,7 +1115,13 @@ void launch_copy_broadened(const DevGrid &G, const EvalBatch &b, float *out, cud
 
 // ------------------------------------------------------------------ chi2
 constexpr int CT = 256, CW = CT / 32;
-constexpr int CU = 4;  // pixels per lane whose loads the chunk kernels issue together
+// pixels per lane whose loads the chunk kernels issue together: 8 up to
+// degree 5 (the Legendre values of 8 pixels fit the 64 registers of 4 CTAs
+// per SM), 4 above
+template <int K>
+__host__ __device__ constexpr int chunk_cu() {
+  return K <= 6 ? 8 : 4;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -1237,6 +1243,7 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
   if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
   const float *mod = model_row(b, P, e), *flux = st.flux;
   const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
+  constexpr int CU = chunk_cu<K>();
   double z[K];
 #pragma unroll
   for (int k = 0; k < K; k++) z[k] = 0.0;
@@ -1330,6 +1337,7 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
     cp[k] = c > 0 ? coef[(c - 1) * MAX_P1 + k] : 0.0f;
   }
   double acc = 0.0;
+  constexpr int CU = chunk_cu<K>();
   // [lo, hi) with chunk c alone; loads of CU pixels before their arithmetic
   auto alone = [&](int lo, int hi) {
     for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
