@@ -57,7 +57,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # profiles/step_launches_dram_1024stars.md): k_broaden includes its
 # block-bound search, chi2 both chunk kernels, the leftover resampling and
 # the final sums
-DRAM_BYTES_PER_EVAL = {"k_interp": 481230, "k_broaden": 608154 + 921, "chi2": 163516 + 149386 + 128 + 259}
+DRAM_BYTES_PER_EVAL = {"k_interp": 480046, "k_broaden": 617963 + 936, "chi2": 163539 + 149358 + 152 + 259}
 
 
 def log(*a):
