@@ -160,3 +160,20 @@ def test_binary_fit_constraints(benv):
     d = r.to_dict()
     r2 = P.BinaryOptimizationResult.from_dict(d)
     assert r2.to_json() == r.to_json()
+
+
+def test_binary_fit_graph_replay_equals_eager(benv, monkeypatch):
+    """Each binary fit captures its per-iteration evaluation once as a CUDA
+    graph and replays it; with PASTA_NO_GRAPH set the same launches run
+    eagerly.  Same kernels in the same order: bit-identical trajectories."""
+    P, star = benv["P"], benv["star"]
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = benv["interp"].get_binary_fitter(benv["d"], cont, P.PSOSettings(16, 6), (0.0, 100.0),
+                                              (-100.0, 100.0))
+    graph = fitter.fit(benv["interp"], benv["cinterp"], star.flux, star.var, seed=31, _trace=True)
+    monkeypatch.setenv("PASTA_NO_GRAPH", "1")
+    eager = fitter.fit(benv["interp"], benv["cinterp"], star.flux, star.var, seed=31, _trace=True)
+    np.testing.assert_array_equal(graph._trace, eager._trace)
+    assert graph.label1.as_list() == eager.label1.as_list() and graph.label2.as_list() == eager.label2.as_list()
+    assert graph.light_ratio == eager.light_ratio and graph.chi2 == eager.chi2
+    np.testing.assert_array_equal(graph.continuum_params, eager.continuum_params)
