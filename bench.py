@@ -473,17 +473,12 @@ def run_ours(args):
         "metric": METRIC, "value": fits_per_s, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (u16 grid, f64 continuum solves)", "data": "synthetic (seeded)",
-        "config": {"workload": "config-1 fits in steady state: %d slots/GPU refilled as fits finish (slots spread "
-                               "over all PSO iterations); grid 60x21x11 x %d px uint16 (%.1f GB), N_obs 10k-60k, "
-                               "vsini 0-300, RV +-150, R=85000, 8 chunks deg 5, PSO %dx%d"
-                               % (n_stars, spec.n_px, spectra.nbytes / 1e9, PARTICLES, ITERS),
-                   "stars_per_gpu": n_stars, "particles": PARTICLES, "iterations": ITERS,
+        "config": {**workload_config(n_stars, spec, spectra.nbytes, world),
                    "evals_per_step": evals_step, "fits_finished_in_timed_steps": fits_done,
                    "host_ms_per_step": {k: (st1[k + "_us"] - st0[k + "_us"]) / 1000.0 / args.steps
                                         for k in ("admit", "device", "retire", "refit")},
                    "step": "one served step: PSO update, chi2 of every active particle, best update, "
                            "admissions and retirements (final refit)",
-                   "parallelism": "replicas x%d (stars sharded, no collective)" % world,
                    "l2": "inputs larger than L2 (%.1f GB grid, ~%.0f GB of interpolation reads per step)"
                          % (spectra.nbytes / 1e9, interp_bytes / 1e9)},
         "evals_per_s": evals_per_s,
@@ -568,6 +563,16 @@ def cpu_baseline(labels, spectra, factors, spec, stars, seeds, budget_s=20.0):
                       "fits/s = evals/s / %d" % (n, PARTICLES, e, t, nthreads, EVALS_PER_FIT)}
 
 
+def workload_config(n_stars, spec, grid_bytes, world):
+    """The workload both arms of the bench name in their `config`."""
+    return {"workload": "config-1 fits in steady state: %d slots/GPU refilled as fits finish (slots spread "
+                        "over all PSO iterations); grid 60x21x11 x %d px uint16 (%.1f GB), N_obs 10k-60k, "
+                        "vsini 0-300, RV +-150, R=85000, 8 chunks deg 5, PSO %dx%d"
+                        % (n_stars, spec.n_px, grid_bytes / 1e9, PARTICLES, ITERS),
+            "stars_per_gpu": n_stars, "particles": PARTICLES, "iterations": ITERS,
+            "parallelism": "replicas x%d (stars sharded, no collective)" % world}
+
+
 def run_reference(args):
     rank, world, local = env_rank()
     if rank != 0:
@@ -603,10 +608,9 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {"workload": "batched fits: grid 60x21x11 x %d px uint16, N_obs 10k-60k, PSO %dx%d, "
-                                   "8 chunks deg 5" % (spec.n_px, PARTICLES, ITERS),
-                       "implementation": "C++ restatement of the reference CPU path (oracle FP32 mirror); the "
-                                         "Rust reference cannot be built here"},
+            "config": workload_config(args.stars, spec, spectra.nbytes, world),
+            "implementation": "C++ restatement of the reference CPU path (oracle FP32 mirror, stars on all host "
+                              "threads like fit_bulk); the Rust reference cannot be built here",
             "evals_per_s": evals_s,
             "cpu_baseline": {"value": value, "unit": "fits/s", "cores": nthreads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
