@@ -52,12 +52,14 @@ BROADEN_BYTES_PER_BLOCK, BROADEN_BYTES_PER_EVAL, BROADEN_BYTES_PER_OBS = 2048 * 
 PATH_BYTES_PER_WIN_PX, PATH_BYTES_PER_OBS = 128, 8
 # nominal FP32 CUDA-core peak of a B200: 148 SMs x 128 FMA/clk x 2 flops x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
-# DRAM bytes per evaluation measured by ncu at full size (dram__bytes_read.sum +
-# dram__bytes_write.sum of one mid-fit step of 65,536 evaluations;
-# profiles/step_launches_dram_1024stars.md): k_broaden includes its
-# block-bound search, chi2 both chunk kernels, the leftover resampling and
-# the final sums
+# DRAM bytes per evaluation (dram__bytes_read.sum + dram__bytes_write.sum)
+# from one ncu capture of a mid-fit step of 16 stars (1,024 evaluations,
+# --clock-control none), divided by its evaluations: the traffic of a launch
+# grows in proportion to the evaluations it runs, so a full launch's traffic
+# is this figure times its evaluations.  k_broaden includes its block-bound
+# search; chi2 is both chunk kernels and the final sums.
 DRAM_BYTES_PER_EVAL = {"k_interp": 480046, "k_broaden": 617963 + 936, "chi2": 163539 + 149358 + 152 + 259}
+DRAM_SOURCE = "ncu capture, mid-fit step of 16 config-1 stars (1,024 evaluations), scaled per evaluation"
 
 
 def log(*a):
@@ -407,8 +409,9 @@ def run_ours(args):
     d2h = int(sum(8 * 8 + 4 * len(r.continuum_params) for r in res))
     err = np.array([np.abs(np.array(r.label.as_list()) - s.label) for r, s in zip(res, stars)])
 
-    # -------- plain one-star-at-a-time GPU path on a sample
+    # -------- plain one-star-at-a-time GPU path on a sample of the workload
     n_plain = min(args.plain_stars, n_stars)
+    torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     plain = P.fit_many(interp, disps[:n_plain], conts[:n_plain], settings, fl[:n_plain], vr[:n_plain],
                        (0.0, 300.0), (-150.0, 150.0), seeds=seeds[:n_plain], mode=1)
@@ -426,49 +429,66 @@ def run_ours(args):
     linear = linear_leg(P, S, args.linear_labels, args.linear_k) if args.linear_labels > 0 and rank == 0 else None
     torch.cuda.synchronize(dev)
 
-    # -------- served time-to-fit: Poisson arrivals, each request its own
-    # continuum settings (4-12 chunks, degree 3-8), stars of the workload
-    lat = serve_latency(P, interp, stars, settings, seeds, rate=args.serve_rate, n_req=args.serve_requests,
-                        seed=4242 + rank) if args.serve_requests > 0 else None
+    # -------- served time-to-fit: Poisson arrivals at each rate, each request
+    # its own continuum settings (4-12 chunks, degree 3-8), stars of the workload
+    lat = None
+    if args.serve_requests > 0:
+        lat = [serve_latency(P, interp, stars, settings, seeds, rate=r, n_req=args.serve_requests,
+                             seed=4242 + rank) for r in args.serve_rates]
     torch.cuda.synchronize(dev)
 
-    # -------- CPU baseline (oracle, rank 0 at N=1)
-    cpu = None
+    # -------- CPU legs (oracle, rank 0 at N=1): the baseline and the label
+    # errors of a sample of the timed workload against the FP64 oracle
+    cpu = replay = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(labels, spectra, factors, spec, stars, seeds, budget_s=args.cpu_seconds)
+        O = _oracle()
+        og = cpu_setup(O, labels, spectra, factors, spec)
+        cpu = cpu_baseline(O, og, stars, seeds, budget_s=args.cpu_seconds)
+        if args.replay_stars > 0:
+            replay = label_replay(O, og, stars[:args.replay_stars], seeds[:args.replay_stars],
+                                  res[:args.replay_stars])
+        del og
 
     if rank != 0:
         return None
     peak, peak_kind = measured_peaks()
     ev = stage["evals"]
+    step_ms = dev_ms / args.steps
 
     def traffic(k):
-        return None if DRAM_BYTES_PER_EVAL[k] is None else DRAM_BYTES_PER_EVAL[k] * ev
+        return DRAM_BYTES_PER_EVAL[k] * ev
 
-    # the dominant kernel: fused broadening (FP32 FFT work; its HBM view beside it)
-    br_s = stage["broaden_ms"] / 1000.0
+    def hbm_view(kernel, bytes_alg, ms, tkey, note=None):
+        """algorithmic rate and measured-DRAM fraction of one kernel (per mid-fit launch)"""
+        s_ = ms / 1000.0
+        tr = traffic(tkey)
+        d = {"bound": "hbm", "kernel": kernel, "achieved": tr / s_ / 1e9, "peak": peak, "unit": "GB/s",
+             "frac": tr / s_ / 1e9 / peak, "traffic": tr, "basis": "measured DRAM bytes per launch / launch time",
+             "peak_kind": peak_kind, "ms": ms, "algorithmic_bytes_per_launch": bytes_alg,
+             "algorithmic_rate": {"value": bytes_alg / s_ / 1e9, "unit": "GB/s",
+                                  "over_peak": bytes_alg / s_ / 1e9 / peak}}
+        if note:
+            d["note"] = note
+        return d
+
+    # the dominant kernel: fused broadening.  Its work is FP32 FFT arithmetic;
+    # its HBM view is measured DRAM bytes (and algorithmic bytes) per launch
     br_flops = stage["broaden_blocks"] * BROADEN_FLOPS_PER_BLOCK
     br_bytes = (stage["broaden_blocks"] * BROADEN_BYTES_PER_BLOCK + ev * BROADEN_BYTES_PER_EVAL
                 + stage["obs_px"] * BROADEN_BYTES_PER_OBS)
-    br_tf = br_flops / br_s / 1e12
-    roofline = {"bound": "fp32", "kernel": "k_broaden", "achieved": br_tf, "peak": FP32_PEAK_TFLOPS,
-                "unit": "TFLOP/s", "frac": br_tf / FP32_PEAK_TFLOPS, "traffic": traffic("k_broaden"),
-                "peak_kind": "nominal FP32 (MEASURED_PEAKS.json holds HBM and bf16 tensor peaks only)",
-                "algorithmic_flops_per_launch": br_flops,
-                "hbm": {"achieved": br_bytes / br_s / 1e9, "peak": peak, "unit": "GB/s",
-                        "frac": br_bytes / br_s / 1e9 / peak, "algorithmic_bytes_per_launch": br_bytes,
-                        "peak_kind": peak_kind}}
-    interp_s = stage["interp_ms"] / 1000.0
+    roofline = hbm_view("k_broaden", br_bytes, stage["broaden_ms"], "k_broaden")
+    br_tf = br_flops / (stage["broaden_ms"] / 1000.0) / 1e12
+    roofline["fp32"] = {"achieved": br_tf, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": br_tf / FP32_PEAK_TFLOPS,
+                        "algorithmic_flops_per_launch": br_flops,
+                        "peak_kind": "nominal FP32 CUDA-core peak (148 SMs x 128 FMA/clk x 1.965 GHz)"}
     interp_bytes = stage["interp_px"] * INTERP_BYTES_PER_PX
-    achieved = interp_bytes / interp_s / 1e9
     # chunk continuum + chi2: per observed pixel the model, flux and chunk
     # coordinate (moments) and the model, flux, var and coordinate (residuals)
     chi2_bytes = stage["obs_px"] * (12 + 16)
-    chi2_gbs = chi2_bytes / (stage["chi2_ms"] / 1000.0) / 1e9
-    # the path as a whole on the per-evaluation byte basis B_eval
+    # the path as a whole on the per-evaluation byte basis B_eval (no reuse)
     path_bytes = stage["interp_px"] * PATH_BYTES_PER_WIN_PX + stage["obs_px"] * PATH_BYTES_PER_OBS
     path_gbs = path_bytes / ev * evals_per_s / 1e9
-    step_ms = dev_ms / args.steps
+    step_dram = sum(DRAM_BYTES_PER_EVAL.values()) * evals_step
     line = {
         "metric": METRIC, "value": fits_per_s, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -489,23 +509,29 @@ def run_ours(args):
         "binary": binary,
         "linear_continuum": linear,
         "plain_gpu": {"fits_per_s": plain_fits, "stars": n_plain, "identical_results": same,
-                      "batched_e2e_over_plain": e2e_fits / (plain_fits * world)},
+                      "what": "plain form: stars 0..%d of the workload one at a time, swarm on the host, "
+                              "eager launches, costs read back every iteration" % (n_plain - 1),
+                      "served_over_plain": fits_per_s / (plain_fits * world),
+                      "batched_e2e_over_plain": e2e_fits / (plain_fits * world),
+                      "served_p99_s": lat[-1]["p99"] if lat else None},
         "label_error_vs_truth": {"median_abs": np.median(err, axis=0).tolist(),
                                  "order": ["teff", "m", "logg", "vsini", "rv"]},
+        "label_error_vs_fp64_oracle": replay,
         "stage_ms": {k: v for k, v in stage.items() if k.endswith("_ms")},
         "roofline": roofline,
-        "roofline_path": {"bound": "hbm", "basis": "B_eval = 128 B x window px + 8 B x observed px per evaluation",
-                          "achieved": path_gbs, "peak": peak, "unit": "GB/s", "frac": path_gbs / peak,
-                          "peak_kind": peak_kind, "bytes_per_eval": path_bytes / ev},
+        "roofline_path": {"basis": "B_eval = 128 B x window px + 8 B x observed px per evaluation (no reuse)",
+                          "algorithmic_rate": {"value": path_gbs, "unit": "GB/s", "over_peak": path_gbs / peak},
+                          "measured_dram": {"value": step_dram / (step_ms / 1000.0) / 1e9, "unit": "GB/s",
+                                            "frac": step_dram / (step_ms / 1000.0) / 1e9 / peak,
+                                            "bytes_per_step": step_dram},
+                          "peak": peak, "peak_kind": peak_kind, "bytes_per_eval": path_bytes / ev},
         "roofline_kernels": [
-            {"bound": "hbm", "kernel": "k_interp", "achieved": achieved, "peak": peak, "unit": "GB/s",
-             "frac": achieved / peak, "traffic": traffic("k_interp"), "peak_kind": peak_kind,
-             "algorithmic_bytes_per_launch": interp_bytes,
-             "note": "neighbour rows shared by a star's particles hit in L2, so the algorithmic rate exceeds HBM"},
-            {"bound": "hbm", "kernel": "k_chunk_moments+k_chunk_resid", "achieved": chi2_gbs, "peak": peak,
-             "unit": "GB/s", "frac": chi2_gbs / peak, "traffic": traffic("chi2"), "peak_kind": peak_kind,
-             "algorithmic_bytes_per_launch": chi2_bytes},
+            hbm_view("k_interp", interp_bytes, stage["interp_ms"], "k_interp",
+                     "neighbour rows shared by a star's particles are read once per group and hit in L2, so the "
+                     "algorithmic rate exceeds the DRAM rate"),
+            hbm_view("k_chunk_moments+k_chunk_resid", chi2_bytes, stage["chi2_ms"], "chi2"),
         ],
+        "dram_source": DRAM_SOURCE,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
@@ -547,9 +573,7 @@ def cpu_sample(O, og, stars, seeds, n_stars, iters, nthreads):
     return time.perf_counter() - t0, evals
 
 
-def cpu_baseline(labels, spectra, factors, spec, stars, seeds, budget_s=20.0):
-    O = _oracle()
-    og = cpu_setup(O, labels, spectra, factors, spec)
+def cpu_baseline(O, og, stars, seeds, budget_s=20.0):
     nthreads = os.cpu_count() or 1
     t1, e1 = cpu_sample(O, og, stars, seeds, 1, 0, 1)  # calibration: one star, initial swarm only
     per_eval = t1 / e1
@@ -561,6 +585,41 @@ def cpu_baseline(labels, spectra, factors, spec, stars, seeds, budget_s=20.0):
             "evals_per_s": evals_s,
             "sample": "%d stars x %d particles (initial swarm evaluation, %d chi2 evals) in %.1fs on %d threads; "
                       "fits/s = evals/s / %d" % (n, PARTICLES, e, t, nthreads, EVALS_PER_FIT)}
+
+
+def label_replay(O, og, stars, seeds, results):
+    """Label errors of the device fits of a sample of the timed workload
+    against the FP64 oracle replayed on the same draw stream (64 x 200, the
+    same seeds), beside the error of the oracle's FP32 mirror of the
+    reference's arithmetic on the same replay.  Tolerance: dTeff <= 1 K,
+    d[M/H], dlogg <= 1e-3, dvsini, dRV <= 0.01 km/s."""
+    tol = np.array([1.0, 1e-3, 1e-3, 0.01, 0.01])
+    st = O.settings(PARTICLES, ITERS, (0.0, 300.0), (-150.0, 150.0))
+    nthreads = os.cpu_count() or 1
+    gpu_err, f32_err, per = [], [], []
+    t0 = time.perf_counter()
+    for s, sd, r in zip(stars, seeds, results):
+        od = O.Disp(og, O.DISP_FIXED, s.wl, RESOLUTION)
+        oc = O.Cont(O.CONT_CHUNK, s.wl, 8, 5, 0.2)
+        r64, rc64 = O.fit(og, od, oc, st, s.flux[None], s.var[None], [sd], O.F64, nthreads=nthreads,
+                          over_stars=False)
+        r32, rc32 = O.fit(og, od, oc, st, s.flux[None], s.var[None], [sd], O.F32, nthreads=nthreads,
+                          over_stars=False)
+        ref = r64[0]["label"]
+        g = np.abs(np.array(r.label.as_list()) - ref)
+        f = np.abs(r32[0]["label"] - ref)
+        gpu_err.append(g)
+        f32_err.append(f)
+        per.append({"gpu": g.tolist(), "fp32_mirror": f.tolist(), "within_tolerance": bool((g <= tol).all()),
+                    "chi2_rel": abs(r.chi2 - r64[0]["chi2"]) / r64[0]["chi2"]})
+    gpu_err, f32_err = np.array(gpu_err), np.array(f32_err)
+    return {"stars": len(stars), "order": ["teff", "m", "logg", "vsini", "rv"],
+            "gpu_max_abs": gpu_err.max(axis=0).tolist(), "fp32_mirror_max_abs": f32_err.max(axis=0).tolist(),
+            "tolerance": tol.tolist(), "gpu_within_tolerance": int(sum(p["within_tolerance"] for p in per)),
+            "per_star": per, "seconds": time.perf_counter() - t0,
+            "what": "stars 0..%d of the timed workload: device fit (fit_many, the e2e run) and the oracle's FP32 "
+                    "mirror of the reference, each against the FP64 oracle on the same seeded draws (64 x 200)"
+                    % (len(stars) - 1)}
 
 
 def workload_config(n_stars, spec, grid_bytes, world):
@@ -624,11 +683,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--stars", type=int, default=1024)
     ap.add_argument("--npx", type=int, default=80000)
-    ap.add_argument("--plain-stars", type=int, default=2)
+    ap.add_argument("--plain-stars", type=int, default=16, help="plain-form leg: stars of the workload")
+    ap.add_argument("--replay-stars", type=int, default=4,
+                    help="label errors against the FP64 oracle: stars of the workload replayed on the CPU (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-rate", type=float, default=30.0, help="served latency run: arrivals per second")
-    ap.add_argument("--serve-requests", type=int, default=300, help="served latency run: requests (0: skip)")
+    ap.add_argument("--serve-rates", type=lambda x: [float(v) for v in x.split(",")], default=[50.0, 500.0, 2000.0],
+                    help="served latency runs: arrivals per second, comma separated")
+    ap.add_argument("--serve-requests", type=int, default=300, help="served latency runs: requests each (0: skip)")
     ap.add_argument("--binary-stars", type=int, default=16, help="binary-fit leg: stars (0: skip)")
     ap.add_argument("--linear-only", action="store_true",
                     help="time chi2 with a linear-model continuum, tensor-core and CUDA-core paths, and print it")
@@ -641,6 +703,18 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torch.distributed.run
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % args.gpus,
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        raise SystemExit(subprocess.call(cmd))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if world != args.gpus:
+        raise SystemExit("--gpus %d but %d ranks were launched" % (args.gpus, world))
     if args.linear_only:
         from pasta_b200 import pasta as P
         from pasta_b200 import synth as S

@@ -213,7 +213,14 @@ int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d,
  * L is rejected with PASTA_E_ARG; calls whose work overlaps on the GPU race
  * on the array.  The first call on a device sets up the array's address and
  * should come before any stream capture.  Nothing is allocated: no
- * cudaMalloc, cudaFree or allocating library routine. */
+ * cudaMalloc, cudaFree or allocating library routine.  L == 0 returns
+ * PASTA_OK with nothing queued.  A CUDA error already pending in the calling
+ * thread is reported (PASTA_E_CUDA) and left pending; a stream of another
+ * device than the grid's is rejected (PASTA_E_ARG).  The calling thread's
+ * current device is the same after the call as before.  Every evaluation
+ * takes the FFT broadening path (blocks sized for the widest 2,048-tap
+ * rotation kernel), so narrow kernels cost more than in pasta_chi2 and
+ * their chi2 carries the FFT path's roundoff. */
 int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d,
                        const pasta_continuum *c, const float *flux,
                        const float *var, int64_t n, const double *labels,
@@ -297,9 +304,17 @@ int pasta_batch_destroy(pasta_batch *b);
  * Continuous batching: requests are admitted into device slots as slots and
  * HBM budget free up, every admitted star advances one PSO iteration per
  * device step, finished stars leave and new ones join without draining.
- * Each request carries its own dispersion and continuum fitter. */
+ * Each request carries its own dispersion and continuum fitter.  No
+ * counterpart in the reference (its fit calls block one star at a time).
+ * hbm_budget_bytes caps the device memory the running requests hold (their
+ * spectra, swarm state and the evaluation workspace of their particles);
+ * 0 = the 40% of the device's memory the evaluation workspace may take (or
+ * PASTA_WORKSPACE_BYTES).  A request waits in the queue while admitting it
+ * would exceed the budget and other requests are running. */
 int pasta_server_create(const pasta_grid *g, int max_slots,
                         int64_t hbm_budget_bytes, pasta_server **out);
+/* the server's HBM budget and the bytes its running requests hold */
+int pasta_server_memory(const pasta_server *s, int64_t *budget, int64_t *used);
 int pasta_server_submit(pasta_server *s, const pasta_dispersion *d,
                         const pasta_continuum *c,
                         const pasta_pso_settings *settings, const float *flux,

@@ -514,10 +514,96 @@ std::vector<float> oa_convolve(const std::vector<float> &in, const std::vector<f
   return y;
 }
 
-// direct linear convolution in double: full-convolution entries [off, off+cnt)
+// Iterative radix-2 complex FFT in double (unnormalised; sign -1 forward,
+// +1 inverse) of size n = 2^k, twiddles from std::cos / std::sin per size.
+struct FftD {
+  int n = 0;
+  std::vector<double> wr, wi;
+  std::vector<int> rev;
+  explicit FftD(int n_) : n(n_), wr(n_ / 2), wi(n_ / 2), rev(n_) {
+    int bits = 0;
+    while ((1 << bits) < n) bits++;
+    for (int k = 0; k < n / 2; k++) {
+      const double ang = -2.0 * M_PI * (double)k / (double)n;
+      wr[k] = std::cos(ang);
+      wi[k] = std::sin(ang);
+    }
+    for (int i = 0; i < n; i++) {
+      int r = 0;
+      for (int b = 0; b < bits; b++)
+        if (i & (1 << b)) r |= 1 << (bits - 1 - b);
+      rev[i] = r;
+    }
+  }
+  void run(double *re, double *im, int sign) const {
+    for (int i = 0; i < n; i++) {
+      const int j = rev[i];
+      if (j > i) {
+        std::swap(re[i], re[j]);
+        std::swap(im[i], im[j]);
+      }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+      const int half = len >> 1, stride = n / len;
+      for (int i = 0; i < n; i += len)
+        for (int j = 0; j < half; j++) {
+          const double cr = wr[j * stride], ci = sign < 0 ? wi[j * stride] : -wi[j * stride];
+          const double ar = re[i + j + half], ai = im[i + j + half];
+          const double vr = ar * cr - ai * ci, vi = ar * ci + ai * cr;
+          const double ur = re[i + j], ui = im[i + j];
+          re[i + j] = ur + vr;
+          im[i + j] = ui + vi;
+          re[i + j + half] = ur - vr;
+          im[i + j + half] = ui - vi;
+        }
+    }
+  }
+};
+
+// Linear convolution in double by overlap-save FFT blocks (two real blocks
+// per complex transform): full-convolution entries [off, off + cnt).  The
+// FP64 mode uses it for wide kernels, where it agrees with the direct sum to
+// ~1e-15 relative and is much faster; it is the same linear convolution.
+std::vector<double> fft_convolve64(const std::vector<double> &in, const std::vector<double> &h, int64_t off,
+                                   int64_t cnt) {
+  const int64_t l = (int64_t)in.size(), m = (int64_t)h.size();
+  int n = 1024;
+  while (n < 4 * m) n <<= 1;
+  const FftD F(n);
+  const int64_t V = n - (m - 1);
+  std::vector<double> hr(n, 0.0), hi(n, 0.0), xr(n), xi(n);
+  for (int64_t k = 0; k < m; k++) hr[k] = h[k];
+  F.run(hr.data(), hi.data(), -1);
+  std::vector<double> y(cnt, 0.0);
+  for (int64_t j0 = off; j0 < off + cnt; j0 += 2 * V) {
+    const int64_t j1 = j0 + V;
+    for (int t = 0; t < n; t++) {
+      const int64_t a = j0 - (m - 1) + t, b = j1 - (m - 1) + t;
+      xr[t] = (a >= 0 && a < l) ? in[a] : 0.0;
+      xi[t] = (b >= 0 && b < l) ? in[b] : 0.0;
+    }
+    F.run(xr.data(), xi.data(), -1);
+    for (int k = 0; k < n; k++) {
+      const double ar = xr[k], ai = xi[k];
+      xr[k] = ar * hr[k] - ai * hi[k];
+      xi[k] = ar * hi[k] + ai * hr[k];
+    }
+    F.run(xr.data(), xi.data(), +1);
+    for (int64_t t = m - 1; t < n; t++) {
+      const int64_t u0 = j0 + t - (m - 1) - off, u1 = j1 + t - (m - 1) - off;
+      if (u0 >= 0 && u0 < cnt && j0 + t - (m - 1) < j1) y[u0] = xr[t] / n;
+      if (u1 >= 0 && u1 < cnt) y[u1] = xi[t] / n;
+    }
+  }
+  return y;
+}
+
+// linear convolution in double: full-convolution entries [off, off+cnt)
+// (direct sums for narrow kernels, FFT blocks in double for wide ones)
 std::vector<double> direct_convolve(const std::vector<double> &in, const std::vector<double> &h,
                                     int64_t off, int64_t cnt) {
   const int64_t l = (int64_t)in.size(), m = (int64_t)h.size();
+  if (m > 48 && cnt > 4096) return fft_convolve64(in, h, off, cnt);
   std::vector<double> y(cnt, 0.0);
   for (int64_t t = 0; t < cnt; t++) {
     int64_t j = off + t;

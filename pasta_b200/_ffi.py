@@ -93,6 +93,7 @@ SIGNATURES = {
     "pasta_server_step": (I, [P]),
     "pasta_server_poll": (I, [P, P, P, P, I64, I, P]),
     "pasta_server_pending": (I, [P, P, P, P]),
+    "pasta_server_memory": (I, [P, P, P]),
     "pasta_server_destroy": (I, [P]),
     "pasta_server_run": (I, [P, I, P]),
     "pasta_server_stats": (I, [P, P]),

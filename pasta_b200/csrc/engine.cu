@@ -2997,7 +2997,17 @@ int pasta_server_create(const pasta_grid *gc, int max_slots, int64_t hbm_budget_
     std::unique_ptr<pasta_server> sv(new pasta_server());
     sv->g = const_cast<pasta_grid *>(gc);
     sv->slots = max_slots;
-    sv->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t)1 << 40;
+    if (hbm_budget_bytes > 0) {
+      sv->budget = hbm_budget_bytes;
+    } else {
+      // default: the device memory the evaluation workspace may take (40% of
+      // the device, or PASTA_WORKSPACE_BYTES), so the admitted requests'
+      // evaluations fit one workspace and a step is never split in sub-batches
+      size_t fr = 0, tot = 0;
+      CK(cudaMemGetInfo(&fr, &tot));
+      sv->budget = (int64_t)(0.4 * (double)tot);
+      if (const char *e = getenv("PASTA_WORKSPACE_BYTES")) sv->budget = atoll(e);
+    }
     sv->slot_req.resize(max_slots);
     sv->slot_flux.resize(max_slots);
     sv->slot_var.resize(max_slots);
@@ -3024,7 +3034,11 @@ int pasta_server_submit(pasta_server *sv, const pasta_dispersion *d, const pasta
     r.var.assign(var, var + n);
     r.t_submit = now_s();
     r.seed = seed;
-    r.bytes = n * 8 + (int64_t)settings->num_particles * 200;
+    // device memory the request holds while it runs: its spectrum and swarm
+    // state, and the evaluation workspace of its particles
+    const int64_t stride = std::max<int64_t>(sv->g->stride, (n + 63) / 64 * 64);
+    r.bytes = n * 8 + (int64_t)settings->num_particles *
+                          (200 + workspace_bytes_per_eval(stride, bnd_stride_for((int)sv->g->npx)));
     sv->queue.push_back(std::move(r));
     if (request_id) *request_id = sv->queue.back().id;
   });
@@ -3082,7 +3096,8 @@ int pasta_server_step(pasta_server *sv) {
         if (sv->slot_req[i]) continue;
         auto &r = sv->queue.front();
         if (r.st.num_particles > sv->Pmax) break;
-        if (sv->used + r.bytes > sv->budget && any_active) break;
+        // a request that alone exceeds the budget still runs when nothing else does
+        if (sv->used + r.bytes > sv->budget && sv->used > 0) break;
         std::unique_ptr<pasta_server::Req> rp(new pasta_server::Req(std::move(r)));
         sv->queue.pop_front();
         sv->used += rp->bytes;
@@ -3318,6 +3333,15 @@ int pasta_server_poll(pasta_server *sv, int64_t *ids, pasta_fit_result *results,
       k++;
     }
     *n_out = k;
+  });
+}
+
+int pasta_server_memory(const pasta_server *sv, int64_t *budget, int64_t *used) {
+  return guard([&] {
+    pasta_server *s = const_cast<pasta_server *>(sv);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (budget) *budget = s->budget;
+    if (used) *used = s->used;
   });
 }
 

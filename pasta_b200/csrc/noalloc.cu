@@ -127,9 +127,28 @@ __global__ void k_noalloc_init(DevStar st, DevStar *dst, int *eval_star, int L) 
 // flux, var [n] f32, labels [L x 5] f64, out [L] f64, status [L] int32 are
 // device pointers; stream is a cudaStream_t (NULL: the legacy default stream).
 // Asynchronous: results are valid once the stream has reached this work.
+// Restores the calling thread's current device on every return path, so a
+// framework that works on another device finds its device unchanged.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c,
                                   const float *flux, const float *var, int64_t n, const double *labels, int64_t L,
                                   double *out, int32_t *status, void *stream) {
+  DeviceGuard keep_device;
+  // an error left by the caller's own earlier work stays the caller's: it is
+  // reported, not consumed, and nothing is launched
+  if (cudaError_t pend = cudaPeekAtLastError(); pend != cudaSuccess) {
+    g_noalloc_err = std::string("a CUDA error was already pending before this call: ") + cudaGetErrorString(pend);
+    return PASTA_E_CUDA;
+  }
   DevGrid G;
   DevStar star;
   int64_t stride = 0;
@@ -144,10 +163,11 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
     g_noalloc_err = "flux, var, labels, out and status must be device pointers";
     return PASTA_E_ARG;
   }
-  if (L < 1) {
-    g_noalloc_err = "at least one label is required";
+  if (L < 0) {
+    g_noalloc_err = "the label count must not be negative";
     return PASTA_E_ARG;
   }
+  if (L == 0) return PASTA_OK;  // nothing to evaluate, like pasta_chi2
   stride = std::max<int64_t>(stride, (n + 63) / 64 * 64);  // rows also hold the model at the observed pixels
   const int bstr = bnd_stride_for(G.npx);
   // the star record, and the group slots of a partly filled last segment
@@ -167,6 +187,13 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   if (e != cudaSuccess) {
     g_noalloc_err = std::string("cudaSetDevice failed: ") + cudaGetErrorString(e);
     return PASTA_E_CUDA;
+  }
+  if (stream) {
+    int sdev = -1;
+    if (cudaStreamGetDevice((cudaStream_t)stream, &sdev) == cudaSuccess && sdev != dev) {
+      g_noalloc_err = "the stream belongs to another device than the grid";
+      return PASTA_E_ARG;
+    }
   }
   DeviceSetup *S = nullptr;
   rc = setup_device(dev, &S);

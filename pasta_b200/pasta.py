@@ -1109,6 +1109,12 @@ class Server:
         return dict(zip(["evals", "steps", "particles_per_slot", "admit_us", "device_us", "retire_us", "refit_us"],
                         out.tolist()))
 
+    def memory(self):
+        """(HBM budget, bytes held by the running requests)."""
+        b, u = C.c_int64(), C.c_int64()
+        check(lib().pasta_server_memory(self._h, C.byref(b), C.byref(u)))
+        return b.value, u.value
+
     def pending(self):
         q, a, d = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().pasta_server_pending(self._h, C.byref(q), C.byref(a), C.byref(d)))

@@ -449,3 +449,48 @@ def test_linear_continuum_fit_params(env):
     assert len(r.continuum_params) == 40
     np.testing.assert_allclose(r.continuum_params, params, rtol=1e-3, atol=1e-4 * np.abs(params).max())
     assert abs(r.chi2 - chi2) <= 1e-4 * chi2
+
+
+def test_server_budget_makes_requests_wait(env):
+    """Admission by HBM budget: with room for two running requests, the third
+    and fourth wait in the queue until earlier ones retire, never more than
+    two run at once, and every result is the one the star gets alone."""
+    P, S, spec = env["P"], env["S"], env["spec"]
+    interp = env["interp"]
+    labs = S.random_labels(spec, 4, seed=19, vsini=(0, 150), rv=(-80, 80))
+    reqs = []
+    for i, l in enumerate(labs):
+        st = S.make_star(spec, l, 8000, 60.0, 85000.0, seed=60 + i)
+        reqs.append((P.FixedResolutionDispersion(st.wl, 85000.0, env["wl"]),
+                     P.ChunkContinuumFitter(st.wl, 5, 4, 0.2), st))
+    settings = P.PSOSettings(16, 6)
+    probe = P.Server(interp, max_slots=4)
+    budget0, used0 = probe.memory()
+    assert budget0 > 0 and used0 == 0
+    d, c, st = reqs[0]
+    probe.submit(d, c, settings, st.flux, st.var, (0.0, 300.0), (-150.0, 150.0), seed=3)
+    probe.step()
+    per_request = probe.memory()[1]
+    assert per_request > 16 * 20000 * 4  # the particles' evaluation workspace is counted
+    del probe
+    srv = P.Server(interp, max_slots=4, hbm_budget_bytes=int(2.5 * per_request))
+    ids = [srv.submit(d, c, settings, st.flux, st.var, (0.0, 300.0), (-150.0, 150.0), seed=300 + i)
+           for i, (d, c, st) in enumerate(reqs)]
+    done, waited, steps = {}, False, 0
+    while len(done) < len(reqs):
+        srv.step()
+        q, a, _ = srv.pending()
+        assert a <= 2
+        waited |= q > 0 and a == 2
+        assert srv.memory()[1] <= int(2.5 * per_request)
+        for rid, status, res in srv.poll():
+            assert status == 0
+            done[rid] = res
+        steps += 1
+        assert steps < 200
+    assert waited
+    for i, (d, c, st) in enumerate(reqs):
+        alone = interp.get_fitter(d, c, settings, (0.0, 300.0), (-150.0, 150.0)).fit(interp, st.flux, st.var,
+                                                                                    seed=300 + i)
+        assert done[ids[i]].label.as_list() == alone.label.as_list()
+        assert done[ids[i]].chi2 == alone.chi2
