@@ -88,6 +88,14 @@ int64_t pasta_kernel_launch_count(void);
  * for the calls and batches started afterwards (no counterpart in the
  * reference; the environment variable PASTA_LINEAR_TC=0 sets the default). */
 int pasta_set_linear_tensor_cores(int on);
+/* Interpolation (GridInterpolator::interpolate, interpolate.rs:930-983) of
+ * 16 or more evaluations of one star that share their 64 neighbour rows (a
+ * contracted swarm) runs as one matrix product on the tensor cores (tcgen05,
+ * rows staged by TMA, f32 accuracy from exact bf16 byte planes and three-part
+ * bf16 weights); 0 keeps every evaluation on the CUDA cores, for the calls
+ * and batches started afterwards (no counterpart in the reference; the
+ * environment variable PASTA_INTERP_TC=0 sets the default). */
+int pasta_set_interp_tensor_cores(int on);
 
 /* ----------------------------------------------------------- the grid
  * Replaces InMemFetcher::new / from_tar_zstd + GridInterpolator::new
@@ -198,6 +206,15 @@ int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d,
                const pasta_continuum *c, const float *flux, const float *var,
                int64_t n, const double *labels, int64_t L, double *out,
                int32_t *status);
+
+/* chi2 of S spectra, each with its own dispersion, continuum fitter, pixel
+ * count and label (labels S x 5), in one batched device pass: the batched
+ * form of InMemInterpolator.chi2_bulk (lib.rs:1297-1338), which evaluates
+ * one spectrum per call there.  out[S] (NaN where status != 0). */
+int pasta_chi2_many(const pasta_grid *g, int64_t S, const pasta_dispersion *const *d,
+                    const pasta_continuum *const *c, const float *const *flux,
+                    const float *const *var, const int64_t *n, const double *labels,
+                    double *out, int32_t *status);
 
 /* pasta_chi2 for callers that cannot allocate device memory: a host
  * framework that gives the GPU's whole memory to its own pool, a real-time

@@ -53,6 +53,7 @@ SIGNATURES = {
     "pasta_set_device": (I, [I]),
     "pasta_kernel_launch_count": (I64, []),
     "pasta_set_linear_tensor_cores": (I, [I]),
+    "pasta_set_interp_tensor_cores": (I, [I]),
     "pasta_grid_create": (I, [P, P, P, I64, I64, I, D, D, P, P]),
     "pasta_grid_destroy": (I, [P]),
     "pasta_grid_direct_max": (I, [P, P]),
@@ -79,6 +80,7 @@ SIGNATURES = {
     "pasta_interpolate_and_convolve": (I, [P, P, P, I64, P, P]),
     "pasta_chi2": (I, [P, P, P, P, P, I64, P, I64, P, P]),
     "pasta_chi2_noalloc": (I, [P, P, P, P, P, I64, P, I64, P, P, P]),
+    "pasta_chi2_many": (I, [P, I64, P, P, P, P, P, P, P, P]),
     "pasta_fit": (I, [P, P, P, P, P, P, I64, I64, P, I, P, P, P]),
     "pasta_fit_many": (I, [P, I64, P, P, P, P, P, P, P, I, P, P]),
     "pasta_compute_uncertainty": (I, [P, P, P, I64, P, P, I64, D, P, P, P, P, P]),

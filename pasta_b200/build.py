@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
           "-I" + os.path.join(ROOT, "include")]
-UNITS = [("prep.cu", ["-fmad=false"]), ("kernels.cu", []), ("binary.cu", ["-fmad=false"]), ("lintc.cu", []),
+UNITS = [("prep.cu", ["-fmad=false"]), ("kernels.cu", []), ("binary.cu", ["-fmad=false"]), ("lintc.cu", []), ("interp_tc.cu", []),
          ("engine.cu", []), ("noalloc.cu", [])]
 DEPS = ["common.cuh", "fft.cuh", "kernels.h"]
 

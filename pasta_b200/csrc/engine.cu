@@ -7,6 +7,7 @@
 // over batches of (star, label) evaluations; drives the particle swarm
 // either fully on the device (batched form, one CUDA graph per PSO step)
 // or with the swarm on the host one star at a time (plain form).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -205,8 +206,10 @@ struct Workspace {
   DBuf<float2> H, HG;
   DBuf<EvalPrep> prep;
   DBuf<int> bnd;       // first observed pixel per broadening block
-  DBuf<GroupRec> grec; // interpolation groups, SEG slots per segment
+  DBuf<GroupRec> grec; // interpolation groups, at each segment's first evaluation
   DBuf<int> gcount;    // groups per segment
+  DBuf<TcGroup> tcrec; // tensor-core interpolation groups, at each segment's first evaluation
+  DBuf<int> tccount;   // tensor-core groups per segment
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
@@ -216,6 +219,7 @@ struct Workspace {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
+    tcrec.release(); tccount.release();
     dlist.release(); dcount.release(); zpart.release();
     cap = 0;
     A.alloc((size_t)want * str);
@@ -225,7 +229,9 @@ struct Workspace {
     prep.alloc((size_t)want);
     bnd.alloc((size_t)want * bstr);
     grec.alloc((size_t)(want + SEG - 1) / SEG * SEG);
-    gcount.alloc((size_t)(want + SEG - 1) / SEG);
+    gcount.alloc((size_t)want);
+    tcrec.alloc((size_t)want);
+    tccount.alloc((size_t)want);
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
     dlist.alloc((size_t)want);
@@ -240,7 +246,8 @@ struct Workspace {
 
 // bytes of workspace one evaluation takes with rows of `stride` floats
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
-  return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)bnd_stride * 4 +
+  return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)sizeof(TcGroup) +
+         8 + (int64_t)bnd_stride * 4 +
          (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8) + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8;
 }
 
@@ -262,6 +269,8 @@ struct pasta_grid {
   std::mutex mu;
   Workspace ws;
   int direct_max = 0;  // combined kernels of at most this many taps are broadened directly (measured)
+  alignas(64) CUtensorMap tmap;  // TMA view of the resident rows (tensor-core interpolation)
+  bool has_tmap = false;
 };
 
 namespace {
@@ -712,6 +721,7 @@ struct EvalArgs {
   const float *given = nullptr;  // model given at observed pixels
   int64_t given_stride = 0;      // floats between the given rows of consecutive evaluations
   int lin_group = 0;             // consecutive evaluations sharing a star (tensor-core linear continua), or 0
+  int star_len = 0;              // consecutive evaluations per star (interpolation segments); 0: one star
   uint32_t lin_kp_mask = 0;      // tensor-core bases present (bit kp / 16)
 };
 
@@ -763,6 +773,21 @@ bool linear_tc_enabled() {
   return v != 0;
 }
 
+// tensor-core interpolation of shared-row groups: on unless
+// PASTA_INTERP_TC=0 or pasta_set_interp_tensor_cores(0) selects the CUDA cores
+std::atomic<int> g_interp_tc{-1};
+bool interp_tc_enabled() {
+  int v = g_interp_tc.load();
+  if (v < 0) {
+    const char *e = getenv("PASTA_INTERP_TC");
+    v = (e && e[0] == '0') ? 0 : 1;
+    int expect = -1;
+    g_interp_tc.compare_exchange_strong(expect, v);
+    v = g_interp_tc.load();
+  }
+  return v != 0;
+}
+
 int width_upper_bound(const pasta_grid *g, double vsini_hi) {
   if (g->d.dvelo <= 0.0 || !(vsini_hi > 0.0)) return 1;
   int w = rotation_width(vsini_hi, g->d.dvelo);
@@ -797,6 +822,13 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.bnd = g->ws.bnd.p;
   b.grec = g->ws.grec.p;
   b.gcount = g->ws.gcount.p;
+  // segments start at star boundaries; a sub-batch that starts inside a star
+  // is cut in plain chunks of SEG
+  b.seg_len = a.star_len > 0 && off % a.star_len == 0 ? a.star_len : 0;
+  const bool tc = interp_tc_enabled() && g->has_tmap;
+  b.tcrec = tc ? g->ws.tcrec.p : nullptr;
+  b.tccount = g->ws.tccount.p;
+  b.tmap = tc ? &g->tmap : nullptr;
   b.bnd_stride = g->ws.bnd_stride;
   b.ccoef = g->ws.ccoef.p;
   b.cpart = g->ws.cpart.p;
@@ -1034,6 +1066,7 @@ void final_refit(pasta_grid *g, StarSet &ss, const std::vector<StarInput> &in, c
   a.max_m = max_m;
   star_kinds(ss.h, a);
   a.lin_group = 1;  // one evaluation per star
+  a.star_len = 1;
   ensure_workspace(g, S, a.max_nobs);
   run_evals(g, a, s);
   std::vector<double> hp((size_t)S * pstride);
@@ -1127,6 +1160,7 @@ void batch_init(Batch &B, pasta_grid *g, const std::vector<StarInput> &in) {
   a.max_m = B.max_m;
   star_kinds(B.ss.h, a);
   a.lin_group = B.Pmax <= 128 ? B.Pmax : 0;  // star s owns evaluations [s Pmax, (s + 1) Pmax)
+  a.star_len = B.Pmax;
   ensure_workspace(g, (int64_t)E, a.max_nobs);
   for (auto &e : B.ev) CK(cudaEventCreate(&e));
   if (!getenv("PASTA_NO_GRAPH")) {
@@ -1194,6 +1228,7 @@ void batch_profile_step(Batch &B, double *out) {
   if (a.max_m > 1) launch_rotker(g->d, b, C.tw.p, s);
   CK(cudaEventRecord(B.ev[3], s));
   launch_group(g->d, b, s);
+  launch_interp_tc(g->d, b, s);
   launch_interp(g->d, b, s);
   CK(cudaEventRecord(B.ev[4], s));
   launch_obs_bounds(g->d, b, s);
@@ -1450,6 +1485,11 @@ struct pasta_server {
 extern "C" {
 
 int pasta_abi_version(void) { return PASTA_B200_ABI_VERSION; }
+int pasta_set_interp_tensor_cores(int on) {
+  g_interp_tc.store(on ? 1 : 0);
+  return PASTA_OK;
+}
+
 int pasta_set_linear_tensor_cores(int on) {
   g_linear_tc.store(on ? 1 : 0);
   return PASTA_OK;
@@ -1626,6 +1666,7 @@ int pasta_grid_create(const double *labels, const uint16_t *spectra, const float
                       cudaMemcpyHostToDevice));
     }
     g->factor.upload(fac);
+    g->has_tmap = make_grid_tensor_map(g->spectra.p, g->n_cols, g->stride, &g->tmap);
     g->dtv.upload(g->tv); g->dmv.upload(g->mv); g->dlv.upload(g->lv);
     g->dllo.upload(g->llo); g->dlhi.upload(g->lhi); g->dcum.upload(g->cum);
     g->wl_kind = wl_kind;
@@ -2074,6 +2115,60 @@ int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d, const pasta_conti
                const float *var, int64_t n, const double *labels, int64_t L, double *out, int32_t *status) {
   if (!d || !c || !flux || !var) { g_last_error = "dispersion, continuum and data required"; return PASTA_E_ARG; }
   return run_label_batch(g, d, c, flux, var, n, labels, 5, L, nullptr, nullptr, out, status, 0, 0);
+}
+
+int pasta_chi2_many(const pasta_grid *g, int64_t S, const pasta_dispersion *const *d, const pasta_continuum *const *c,
+                    const float *const *flux, const float *const *var, const int64_t *n, const double *labels,
+                    double *out, int32_t *status) {
+  return guard([&] {
+    if (S < 0 || (S > 0 && (!d || !c || !flux || !var || !n || !labels || !out)))
+      fail(PASTA_E_ARG, "dispersions, continua, spectra, labels and outputs are required");
+    if (S == 0) return;
+    std::vector<StarInput> in(S);
+    double vmax = 0.0;
+    for (int64_t i = 0; i < S; i++) {
+      if (!d[i] || !c[i] || !flux[i] || !var[i]) fail(PASTA_E_ARG, "spectrum %lld: missing input", (long long)i);
+      in[i] = StarInput{d[i], c[i], nullptr, flux[i], var[i], n[i], 0};
+      validate_star(g, in[i]);
+      if (labels[5 * i + 3] > vmax) vmax = labels[5 * i + 3];
+    }
+    pasta_grid *gg = const_cast<pasta_grid *>(g);
+    std::lock_guard<std::mutex> lk(gg->mu);
+    Ctx &C = ctx();
+    cudaStream_t s = C.stream;
+    StarSet ss;
+    ss.build(in);
+    std::vector<int> star(S);
+    for (int64_t i = 0; i < S; i++) star[i] = (int)i;
+    DBuf<double> lab, cost;
+    DBuf<int> es, st;
+    lab.upload(labels, (size_t)S * 5);
+    es.upload(star);
+    cost.alloc(S);
+    st.alloc(S);
+    EvalArgs a;
+    a.stars = ss.dstars.p;
+    a.labels = lab.p;
+    a.eval_star = es.p;
+    a.E = S;
+    a.cost = cost.p;
+    a.status = st.p;
+    a.need_chi2 = 1;
+    a.max_m = width_upper_bound(g, vmax);
+    star_kinds(ss.h, a);
+    a.lin_group = 1;  // one evaluation per star
+    a.star_len = 1;
+    ensure_workspace(gg, S, a.max_nobs);
+    run_evals(gg, a, s);
+    std::vector<int> hs(S);
+    CK(cudaMemcpyAsync(out, cost.p, (size_t)S * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hs.data(), st.p, (size_t)S * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < S; i++) {
+      if (status) status[i] = hs[i];
+      if (hs[i]) out[i] = std::numeric_limits<double>::quiet_NaN();
+    }
+  });
 }
 
 int pasta_dispersion_convolve(const pasta_dispersion *d, const float *in, int64_t n, float *out) {
@@ -3167,6 +3262,7 @@ int pasta_server_step(pasta_server *sv) {
       a.max_chunks = std::max(a.max_chunks, sv->graph_chunks);
       a.lin_kp_mask |= sv->graph_lin;
       a.lin_group = sv->Pmax <= 128 ? sv->Pmax : 0;
+      a.star_len = sv->Pmax;
     }
     ensure_workspace(g, E, a.max_nobs);
     const bool grown = sv->graph_max_m < sv->max_m || (a.chunk_p1_mask & ~sv->graph_mask) ||

@@ -159,6 +159,63 @@ __device__ __forceinline__ void fft_stage_pp(const float2 *src, float2 *dst, con
   fft_pass<R, NS, INV, SmemLoad, SmemStore, false>(tw, SmemLoad{src}, SmemStore{dst});
 }
 
+// ------------------------------------------------------------------------
+// 2048-point FFT of one 128-thread group, 2048 = 16 x 16 x 8 ("four-step"
+// decomposition, n = 128 n1 + 8 n2 + n3, k = k1 + 16 k2 + 256 k3):
+//   pass 1  thread t = 8 n2 + n3: DFT-16 over n1, times W_2048^(t k1)
+//   pass 2  thread t = 8 k1 + n3: DFT-16 over n2, times W_128^(n3 k2)
+//   pass 3  thread t: for c = t and t + 128 (c = k1 + 16 k2), DFT-8 over n3,
+//           giving X[c + 256 k3]
+// Each thread keeps 16 values in registers through a pass; the passes
+// exchange through shared memory twice.  The inverse runs the same passes
+// backwards (DFT-8, DFT-16, DFT-16 with conjugate twiddles), starting from
+// the spectrum where the forward transform left it, so a spectrum product
+// between them needs no reordering: a round trip costs four exchanges.
+// Exchange 1 rows are padded to F2_XP values and exchange 2 is XOR-swizzled
+// so that every access of a half-warp (64-bit values) touches 16 distinct
+// bank pairs.  Twiddles come from per-CTA tables built from the host's
+// double-precision table.
+constexpr int F2_T = 128;
+constexpr int F2_XP = 136;
+constexpr int F2_S1 = 16 * F2_XP;  // complex values of exchange buffer 1
+constexpr int F2_S2 = 2048;        // complex values of exchange buffer 2
+__device__ __forceinline__ int f2_a2(int c, int n3) { return 8 * c + (n3 ^ ((c >> 1) & 7)); }
+
+// a * w (FWD) or a * conj(w) (INV)
+template <bool INV>
+__device__ __forceinline__ cf cmul_tw(cf a, float2 w) {
+  return INV ? cf{a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y} : cf{a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x};
+}
+
+// DFT-16 of v (natural order in and out) as 4 x 4: n = 4a + b, k = c + 4d
+template <bool INV>
+__device__ __forceinline__ void dft16(cf v[16]) {
+  const float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+#pragma unroll
+  for (int b = 0; b < 4; b++) dft4<INV>(v[b], v[4 + b], v[8 + b], v[12 + b]);
+  // y[b][c] sits in v[4c + b]; times W16^(bc)
+  const float sg = INV ? 1.0f : -1.0f;
+  v[5] = cmul(v[5], cf{c1, sg * s1});     // b1 c1: W^1
+  v[6] = cmul(v[6], cf{h, sg * h});       // b2 c1: W^2
+  v[7] = cmul(v[7], cf{s1, sg * c1});     // b3 c1: W^3
+  v[9] = cmul(v[9], cf{h, sg * h});       // b1 c2: W^2
+  v[10] = rot90<INV>(v[10]);              // b2 c2: W^4
+  v[11] = cmul(v[11], cf{-h, sg * h});    // b3 c2: W^6
+  v[13] = cmul(v[13], cf{s1, sg * c1});   // b1 c3: W^3
+  v[14] = cmul(v[14], cf{-h, sg * h});    // b2 c3: W^6
+  v[15] = cmul(v[15], cf{-c1, -sg * s1}); // b3 c3: W^9
+#pragma unroll
+  for (int c = 0; c < 4; c++) dft4<INV>(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+  // X[c + 4d] sits in v[4c + d]: transpose the 4 x 4 index
+  cf t[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) t[i] = v[i];
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+#pragma unroll
+    for (int d = 0; d < 4; d++) v[c + 4 * d] = t[4 * c + d];
+}
+
 template <bool INV>
 __device__ __forceinline__ void fft2048(float2 *c, const float2 *__restrict__ tw) {
   fft_stage<8, 1, INV>(c, tw);

@@ -1,0 +1,346 @@
+// interp_tc.cu -- cubic interpolation of evaluations that share their 64
+// neighbour rows, on the 5th-generation tensor cores.
+//
+// GridInterpolator::interpolate (interpolate.rs:930-983) computes, per
+// pixel, flux = sum_n w_n * (u16_n * factor_n) over the 64 neighbour models.
+// A particle swarm contracts into one grid cube within a few dozen
+// iterations; from then on its particles share the 64 rows and differ only
+// in their weights, so the swarm's interpolation is one matrix product per
+// tile of 128 pixels:
+//   D [128 pixels x members] = A [128 pixels x 128] . B [128 x members]
+// with A[p][k] = 256 * hi_k(p) and A[p][64 + k] = lo_k(p), the two bytes of
+// row k's u16 value at pixel p (exact in bf16), and B[k][n] = B[64 + k][n]
+// = weight_n,k x factor_k, split into three bf16 parts whose sum is the f32
+// value (8 + 8 + 8 significant bits).  Every product is exact in the f32
+// accumulator; the three parts are three MMA chains into one tensor-memory
+// accumulator.  A member's result depends only on its own weights (each
+// accumulator column is computed on its own), so it does not depend on the
+// other members of the group.
+//
+// Rows are staged by TMA (cp.async.bulk.tensor, one 128-pixel box per row,
+// from the grid resident in this GPU's memory; no multicast), converted to
+// the bf16 byte planes by the CTA's threads, multiplied by tcgen05.mma
+// (kind::f16, M = 128, N = members rounded up to 16, one elected thread
+// issues), and read back from tensor memory by tcgen05.ld for the stores.
+// The last npx % 128 pixels carry the reference's extra 1/65535
+// (interpolate.rs:978) and are computed on the CUDA cores.
+//
+// Every wait on an mbarrier is bounded (about a second); a wait that runs
+// out marks the group's evaluations with an internal error and the CTA still
+// frees its tensor memory.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pb {
+
+namespace {
+
+constexpr int TT = 128;      // threads: pixel p of a tile = thread p
+constexpr int TPX = 128;     // pixels per tile (MMA M)
+constexpr int TK = 128;      // reduction: 64 neighbours x {256 x high byte, low byte}
+constexpr int TSLAB = 16;    // tiles per CTA
+constexpr int S_TC_TIMEOUT = -99;  // PASTA_E_INTERNAL
+
+// shared memory (bytes): three weight parts [64 members][128] bf16 (K-major),
+// two staging tiles [64 rows][128 pixels] u16, the A tile [128 pixels][128]
+// bf16 (K-major), barriers and flags, the members' windows
+constexpr int SB_B = 0;
+constexpr int SB_STG = SB_B + 3 * 64 * TK * 2;
+constexpr int SB_A = SB_STG + 2 * 64 * TPX * 2;
+constexpr int SB_MISC = SB_A + TPX * TK * 2;
+constexpr int SB_WIN = SB_MISC + 64;
+constexpr int SB_TOTAL = SB_WIN + 2 * SEG * 4;
+
+// byte offset of element (row, k) of a K-major bf16 tile with TK elements
+// per row: core matrices of 8 rows x 16 bytes (8 elements), K-adjacent core
+// matrices 128 bytes apart, 8-row groups TK / 8 core matrices apart
+__device__ __forceinline__ int kmaj16(int row, int k) {
+  return ((((row >> 3) * (TK >> 3) + (k >> 3)) << 3) + (row & 7)) * 16 + (k & 7) * 2;
+}
+// shared-memory matrix descriptor of such a tile (no swizzle, version 1)
+__device__ __forceinline__ uint64_t desc16(uint32_t saddr) {
+  const uint64_t lbo = 128, sbo = (TK >> 3) * 128;
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((lbo >> 4) << 16) | ((sbo >> 4) << 32) | (1ull << 46);
+}
+// instruction descriptor: f32 accumulator, bf16 A and B, both K-major
+__device__ __forceinline__ uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > 2000000000ll) return false;
+  }
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// TMA: one box of 128 pixels of grid row y starting at pixel x
+__device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// sixteen consecutive f32 columns of this thread's tensor-memory lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// bf16 bits of x (round to nearest even), as the low 16 bits
+__device__ __forceinline__ uint32_t bf16_bits(float x) {
+  uint32_t r;
+  asm("{\n\t.reg .b16 h;\n\tcvt.rn.bf16.f32 h, %1;\n\tmov.b32 %0, {h, h};\n\t}" : "=r"(r) : "f"(x));
+  return r & 0xFFFFu;
+}
+__device__ __forceinline__ float bf16_val(uint32_t bits) { return __uint_as_float(bits << 16); }
+
+}  // namespace
+
+// One CTA per (segment, tensor-core group, slab of TSLAB tiles).
+__global__ void __launch_bounds__(TT) k_interp_tc(DevGrid G, EvalBatch b, const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int s = blockIdx.x, gi = blockIdx.z, t = threadIdx.x, w = t >> 5;
+  if (gi >= b.tccount[s]) return;
+  int start, len;
+  {
+    const int L = b.seg_len > 0 ? b.seg_len : b.E;
+    const int spb = (L + SEG - 1) / SEG;
+    const int j = s / spb, q = s - j * spb;
+    start = j * L + q * SEG;
+    len = min(min(SEG, L - q * SEG), b.E - start);
+  }
+  if (len <= 0) return;
+  const TcGroup &R = b.tcrec[start + gi];
+  const int nm = R.nmem;
+  // this CTA's pixels: tiles [x0, x1) of the group's window, the tail after
+  // tail_start on the CUDA cores
+  const int slab0 = blockIdx.y * TSLAB * TPX;
+  const int lo = max(R.lo & ~(TPX - 1), slab0), hi = min(R.hi, slab0 + TSLAB * TPX);
+  if (lo >= hi) return;
+  const int tc_hi = min(hi, G.tail_start);
+  const int ntiles = tc_hi > lo ? (tc_hi - lo + TPX - 1) / TPX : 0;
+  const int NP = (nm + 15) & ~15;
+
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t full0 = sbase + SB_MISC, full1 = full0 + 8, mbar_mma = full0 + 16;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + SB_MISC + 24);
+  int *err = reinterpret_cast<int *>(sm + SB_MISC + 28);
+  int *wlo = reinterpret_cast<int *>(sm + SB_WIN), *whi = wlo + SEG;
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar_mma) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    *err = 0;
+  }
+  if (w == 0 && ntiles > 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + SB_MISC + 24),
+                 "r"(64)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  // the members' windows, and the weights: B_j[n][k] = B_j[n][64 + k]
+  if (t < SEG) {
+    const int e = t < nm ? R.member[t] : -1;
+    wlo[t] = e >= 0 ? b.prep[e].i_lo : 0;
+    whi[t] = e >= 0 ? b.prep[e].i_hi : 0;
+  }
+  for (int i = t; i < 64 * 64; i += TT) {
+    const int n = i >> 6, k = i & 63;
+    float wf = 0.0f;
+    if (n < nm && R.col[k] >= 0) wf = b.prep[R.member[n]].w[k] * R.f[k];
+    const uint32_t h0 = bf16_bits(wf);
+    const float r1 = wf - bf16_val(h0);
+    const uint32_t h1 = bf16_bits(r1);
+    const uint32_t h2 = bf16_bits(r1 - bf16_val(h1));
+    const uint32_t hs[3] = {h0, h1, h2};
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      unsigned short *bj = reinterpret_cast<unsigned short *>(sm + SB_B + j * 64 * TK * 2);
+      bj[kmaj16(n, k) >> 1] = (unsigned short)hs[j];
+      bj[kmaj16(n, 64 + k) >> 1] = (unsigned short)hs[j];
+    }
+  }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = ntiles > 0 ? *tslot : 0u;
+  const uint32_t idesc = idesc_bf16(TPX, NP > 0 ? NP : 16);
+  auto issue_tile = [&](int i) {  // TMA of tile i's 64 rows into staging i & 1
+    const uint32_t fb = (i & 1) ? full1 : full0;
+    const uint32_t dst = sbase + SB_STG + (uint32_t)((i & 1) * 64 * TPX * 2);
+    mbar_expect(fb, 64 * TPX * 2);
+    for (int k = 0; k < 64; k++) {
+      const int c = R.col[k] >= 0 ? R.col[k] : 0;  // a missing row has weight 0
+      tma_row(dst + (uint32_t)(k * TPX * 2), &tmap, lo + i * TPX, c, fb);
+    }
+  };
+  if (t == 0) {
+    if (ntiles > 0) issue_tile(0);
+    if (ntiles > 1) issue_tile(1);
+  }
+  bool ok = true;
+  for (int i = 0; i < ntiles && ok; i++) {
+    const int px0 = lo + i * TPX;
+    // rows of tile i staged
+    if (!mbar_wait((i & 1) ? full1 : full0, (uint32_t)((i >> 1) & 1))) atomicOr(err, 1);
+    // convert: pixel t, row k -> A[t][k] = 256 x high byte, A[t][64 + k] = low byte
+    {
+      const unsigned short *stg = reinterpret_cast<const unsigned short *>(sm + SB_STG + (i & 1) * 64 * TPX * 2);
+#pragma unroll
+      for (int k8 = 0; k8 < 64; k8 += 8) {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint32_t u0 = stg[(k8 + 2 * q) * TPX + t], u1 = stg[(k8 + 2 * q + 1) * TPX + t];
+          // exact floats of the byte planes (below 2^23): f = bits(0x4B000000 | x) - 2^23
+          const float2 fh = __fadd2_rn(make_float2(__uint_as_float(0x4B000000u | (u0 & 0xFF00u)),
+                                                   __uint_as_float(0x4B000000u | (u1 & 0xFF00u))),
+                                       make_float2(-8388608.0f, -8388608.0f));
+          const float2 fl = __fadd2_rn(make_float2(__uint_as_float(0x4B000000u | (u0 & 0xFFu)),
+                                                   __uint_as_float(0x4B000000u | (u1 & 0xFFu))),
+                                       make_float2(-8388608.0f, -8388608.0f));
+          // at most 8 significant bits: the bf16 value is the top half of the f32
+          h[q] = __byte_perm(__float_as_uint(fh.x), __float_as_uint(fh.y), 0x7632);
+          l[q] = __byte_perm(__float_as_uint(fl.x), __float_as_uint(fl.y), 0x7632);
+        }
+        *reinterpret_cast<uint4 *>(sm + SB_A + kmaj16(t, k8)) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4 *>(sm + SB_A + kmaj16(t, 64 + k8)) = make_uint4(l[0], l[1], l[2], l[3]);
+      }
+    }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    ok = *err == 0;
+    if (!ok) break;
+    if (t == 0) {
+      // the staging buffer is free again: tile i + 2 streams in
+      if (i + 2 < ntiles) issue_tile(i + 2);
+      const uint64_t da = desc16(sbase + SB_A);
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const uint64_t db = desc16(sbase + SB_B + (uint32_t)(j * 64 * TK * 2));
+#pragma unroll
+        for (int ks = 0; ks < TK / 16; ks++)
+          mma_bf16(tmem, da + (uint64_t)((ks * 256) >> 4), db + (uint64_t)((ks * 256) >> 4), idesc,
+                   (j | ks) ? 1u : 0u);
+      }
+      mma_commit(mbar_mma);
+    }
+    if (!mbar_wait(mbar_mma, (uint32_t)(i & 1))) atomicOr(err, 1);
+    tc_fence_after();
+    // read back: warp w holds pixels 32 w .. 32 w + 31 (tensor-memory lanes)
+    const int px = px0 + t;
+    const uint32_t lane = (uint32_t)(w * 32) << 16;
+    for (int c0 = 0; c0 < NP; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + lane + (uint32_t)c0, v);
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int n = c0 + j;
+        if (n < nm && px >= wlo[n] && px < whi[n] && px < tc_hi) b.bufA[(size_t)R.member[n] * b.stride + px] = v[j];
+      }
+    }
+    tc_fence_before();
+    __syncthreads();  // tensor memory and the A tile are free for the next tile
+    ok = *err == 0;
+  }
+  // tail pixels [tail_start, hi): the reference's extra 1/65535 (interpolate.rs:978)
+  if (ok && hi > G.tail_start) {
+    const int t0 = max(lo, G.tail_start);
+    const int npx = hi - t0;
+    for (int i = t; i < npx * nm; i += TT) {
+      const int n = i / npx, px = t0 + i % npx;
+      if (px < wlo[n] || px >= whi[n]) continue;
+      const EvalPrep &P = b.prep[R.member[n]];
+      float acc = 0.0f;
+      for (int k = 0; k < 64; k++) {
+        const int c = R.col[k];
+        if (c < 0) continue;
+        const float x = (float)G.spectra[(size_t)c * G.stride + px];
+        acc = fmaf(P.w[k], __fmul_rn(__fdiv_rn(x, 65535.0f), R.f[k]), acc);
+      }
+      b.bufA[(size_t)R.member[n] * b.stride + px] = acc;
+    }
+  }
+  if (!ok && t < nm) b.prep[R.member[t]].status = S_TC_TIMEOUT;
+  __syncthreads();
+  if (w == 0 && ntiles > 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64));
+}
+
+void launch_interp_tc(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
+  if (b.E <= 0 || !b.tcrec || !b.tmap) return;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_interp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_TOTAL);
+    attr = true;
+  }
+  const int slabs = (G.npx + TSLAB * TPX - 1) / (TSLAB * TPX);
+  dim3 grid(num_segments(b), slabs, TC_MAX_GROUPS);
+  k_interp_tc<<<grid, TT, SB_TOTAL, s>>>(G, b, *reinterpret_cast<const CUtensorMap *>(b.tmap));
+  count_launch();
+}
+
+// The grid as a 2D uint16 tensor [rows][stride] for TMA, box 128 x 1.
+bool make_grid_tensor_map(const uint16_t *spectra, int64_t rows, int64_t stride, void *out) {
+  typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                               const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return false;
+    fn = reinterpret_cast<EncodeFn>(p);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)stride, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)stride * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TPX, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, (void *)spectra, dims, strides,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace pb

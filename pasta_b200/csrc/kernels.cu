@@ -54,22 +54,50 @@ __device__ __forceinline__ unsigned long long cols_hash(const int *c) {
   return h;
 }
 
-// One CTA per segment of SEG consecutive evaluations: slice 0 (SEG threads)
-// finds the groups, then GROUP_SLICES slices of SEG threads write the group
-// records, one group per slice at a time (thread t of a slice handles
-// neighbour row t).
+// Segment s of a batch: [start, start + len), a chunk of at most SEG
+// evaluations of one star (EvalBatch::seg_len), len <= 0 when empty.
+__device__ __forceinline__ void seg_range(const EvalBatch &b, int s, int &start, int &len) {
+  const int L = b.seg_len > 0 ? b.seg_len : b.E;
+  const int spb = (L + SEG - 1) / SEG;
+  const int j = s / spb, q = s - j * spb;
+  start = j * L + q * SEG;
+  len = min(min(SEG, L - q * SEG), b.E - start);
+}
+int num_segments(const EvalBatch &b) {
+  if (b.E <= 0) return 0;
+  const int L = b.seg_len > 0 ? b.seg_len : b.E;
+  return (b.E + L - 1) / L * ((L + SEG - 1) / SEG);
+}
+
+// One CTA per segment: slice 0 (SEG threads) finds the groups, then
+// GROUP_SLICES slices of SEG threads write the group records, one group per
+// slice at a time (thread t of a slice handles neighbour row t).  Columns
+// shared by TC_MIN_MEMBERS or more evaluations form tensor-core groups
+// (with the tensor-core path on); the others form groups of up to GROUP_MAX.
 constexpr int GROUP_SLICES = 4;
 __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatch b) {
   __shared__ unsigned long long hs[SEG];
-  __shared__ int ok[SEG], lead[SEG], gid[SEG], slot[SEG], open_g[SEG], fill[SEG];
-  __shared__ int ng;
+  __shared__ int ok[SEG], lead[SEG], gid[SEG], slot[SEG], open_g[SEG], fill[SEG], cnt_l[SEG], tcg[SEG];
+  __shared__ int ng, ntc;
   __shared__ int cnt[GROUP_SLICES][2];
   __shared__ int mem[GROUP_SLICES][GROUP_MAX];
-  const int s = blockIdx.x, tid = threadIdx.x, t = tid % SEG, sl = tid / SEG, e = s * SEG + t;
+  const int s = blockIdx.x, tid = threadIdx.x, t = tid % SEG, sl = tid / SEG;
+  int start, len;
+  seg_range(b, s, start, len);
+  if (len <= 0) {
+    if (tid == 0) {
+      b.gcount[s] = 0;
+      if (b.tccount) b.tccount[s] = 0;
+    }
+    return;
+  }
+  const int e = start + t;
   if (sl == 0) {
-    const bool v = e < b.E && b.prep[e].status == 0;
+    const bool v = t < len && b.prep[e].status == 0;
     ok[t] = v;
     hs[t] = v ? cols_hash(b.prep[e].cols) : 0ull;
+    cnt_l[t] = 0;
+    tcg[t] = -1;
   }
   __syncthreads();
   if (sl == 0) {  // leader: the first earlier evaluation with the same columns
@@ -78,7 +106,7 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
       const int *c = b.prep[e].cols;
       for (int u = 0; u < t; u++) {
         if (!ok[u] || hs[u] != hs[t]) continue;
-        const int *cu = b.prep[s * SEG + u].cols;
+        const int *cu = b.prep[start + u].cols;
         bool same = true;
         for (int n = 0; n < 64 && same; n++) same = cu[n] == c[n];
         if (same) {
@@ -86,17 +114,26 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
           break;
         }
       }
+      atomicAdd(&cnt_l[L], 1);
     }
     lead[t] = L;
     open_g[t] = -1;
     fill[t] = 0;
   }
   __syncthreads();
-  if (tid == 0) {  // groups in evaluation order, at most GROUP_MAX members each
+  if (tid == 0) {
+    // tensor-core groups, in leader order
+    int nt = 0;
+    if (b.tcrec)
+      for (int u = 0; u < SEG; u++)
+        if (ok[u] && lead[u] == u && cnt_l[u] >= TC_MIN_MEMBERS && nt < TC_MAX_GROUPS) tcg[u] = nt++;
+    ntc = nt;
+    if (b.tccount) b.tccount[s] = nt;
+    // the other evaluations in groups of at most GROUP_MAX, in evaluation order
     int n = 0;
     for (int u = 0; u < SEG; u++) {
       gid[u] = -1;
-      if (!ok[u]) continue;
+      if (!ok[u] || tcg[lead[u]] >= 0) continue;
       const int l = lead[u];
       if (open_g[l] < 0 || fill[l] == GROUP_MAX) {
         open_g[l] = n++;
@@ -109,15 +146,45 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     b.gcount[s] = n;
   }
   __syncthreads();
+  // tensor-core group records: slice g writes group g (thread t: row t, member t)
+  if (sl < ntc) {
+    int l = -1;
+    for (int u = 0; u < SEG; u++)
+      if (ok[u] && lead[u] == u && tcg[u] == sl) l = u;
+    TcGroup &T = b.tcrec[start + sl];
+    const int c = b.prep[start + l].cols[t];
+    T.col[t] = c;
+    T.f[t] = c >= 0 ? G.factor[c] : 0.0f;
+    // members in evaluation order: the rank of t among the group's members
+    const bool mine = ok[t] && lead[t] == l;
+    const unsigned bal = __ballot_sync(0xffffffffu, mine);
+    const int lane = t & 31;
+    if (lane == 0) cnt[sl][t >> 5] = __popc(bal);
+    __syncwarp();
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + sl), "r"(SEG) : "memory");  // this slice's two warps
+    if (mine) T.member[__popc(bal & ((1u << lane) - 1u)) + ((t >> 5) ? cnt[sl][0] : 0)] = e;
+    if (t == 0) {
+      int lo = 1 << 30, hi = 0;
+      for (int u = 0; u < SEG; u++)
+        if (ok[u] && lead[u] == l) {
+          lo = min(lo, b.prep[start + u].i_lo);
+          hi = max(hi, b.prep[start + u].i_hi);
+        }
+      T.nmem = cnt_l[l];
+      T.lo = lo;
+      T.hi = hi;
+    }
+  }
+  __syncthreads();
   const int lane = tid & 31, wsl = t >> 5;  // warp within the slice
   for (int base = 0; base < ng; base += GROUP_SLICES) {
     const int g = base + sl;
     const bool act = g < ng;
     if (t < GROUP_MAX) mem[sl][t] = -1;
     __syncthreads();
-    if (act && gid[t] == g) mem[sl][slot[t]] = s * SEG + t;
+    if (act && gid[t] == g) mem[sl][slot[t]] = e;
     __syncthreads();
-    GroupRec &R = b.grec[(size_t)s * SEG + (act ? g : 0)];
+    GroupRec &R = b.grec[(size_t)start + (act ? g : 0)];
     int c = -1, nm = 0;
     float f = 0.0f, w[GROUP_MAX], wf[GROUP_MAX];
     unsigned bal = 0u;
@@ -165,7 +232,7 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
 
 void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
-  k_group<<<(b.E + SEG - 1) / SEG, SEG * GROUP_SLICES, 0, s>>>(G, b);
+  k_group<<<num_segments(b), SEG * GROUP_SLICES, 0, s>>>(G, b);
   count_launch();
 }
 
@@ -251,8 +318,10 @@ __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
   const int s = blockIdx.x;
   const int px = blockIdx.y * IT_TILE + threadIdx.x * 8;
   const int ng = b.gcount[s];
+  int start, len;
+  seg_range(b, s, start, len);
   for (int g = blockIdx.z; g < ng; g += gridDim.z) {
-    const float4 *src = reinterpret_cast<const float4 *>(b.grec + (size_t)s * SEG + g);
+    const float4 *src = reinterpret_cast<const float4 *>(b.grec + (size_t)start + g);
     float4 *dst = reinterpret_cast<float4 *>(&R);
     for (int i = threadIdx.x; i < (int)(sizeof(GroupRec) / 16); i += IT_T) dst[i] = src[i];
     __syncthreads();
@@ -268,7 +337,7 @@ __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
 
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
-  const int segs = (b.E + SEG - 1) / SEG, tiles = (G.npx + IT_TILE - 1) / IT_TILE;
+  const int segs = num_segments(b), tiles = (G.npx + IT_TILE - 1) / IT_TILE;
   const int want = num_sms() * 6;  // two waves of the 3 CTAs an SM holds
   const int z = segs * tiles >= want ? 1 : std::min(SEG, (want + segs * tiles - 1) / (segs * tiles));
   dim3 grid(segs, tiles, z);
@@ -364,26 +433,9 @@ __device__ __forceinline__ float instrument(const DevStar &st, int N, int i, int
 }
 
 // ------------------------------------------------------ fused broadening
-// One work item = two blocks of one evaluation.  Block k yields V = 2048 -
-// (m - 1) - 2 hg final outputs starting at s_k = o_lo + k (V - 1): the
-// rotation outputs [s - hg, s + V + hg) come from one overlap-save block of
-// 2048 inputs (the reference uses overlap-add, convolve_rv.rs:121-157; both
-// are the same linear convolution), and the instrument profile is then
-// applied from shared memory.  Block k owns synth pixels [s_k, s_k + V - 1);
-// its last output is the partner j + 1 of its last owned pixel j.  The two
-// real blocks ride in the real and imaginary parts of one complex FFT (the
-// kernel is real, so the two products separate after the inverse).
-// Rotation outputs outside [0, N) are zero, like the reference's cropped
-// segment.  With the identity rotation the FFT is skipped.
-//
-// Epilogue: either the owned synth pixels go to row B, or (chi2 batches,
-// EvalPrep::epi) the block resamples the observed pixels whose left synth
-// pixel it owns (EvalBatch::bnd lists them per block) straight from shared
-// memory and writes the model at the observed pixels to row B; the synth
-// row never reaches memory.
-// Asynchronous 16-byte global -> shared copies (cp.async): the next work
-// item's input streams in while the current one is transformed.  A copy
-// with ok == false reads nothing and fills zeros.
+// Asynchronous 16-byte global -> shared copies (cp.async): the next tile's
+// input streams in while the current one is worked.  A copy with ok ==
+// false reads nothing and fills zeros.
 __device__ __forceinline__ void cp_async16(float *smem, const float *gmem, bool ok) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   const int n = ok ? 16 : 0;
@@ -391,25 +443,6 @@ __device__ __forceinline__ void cp_async16(float *smem, const float *gmem, bool 
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// staging row: synth pixels [a0, a0 + BR_STG) with a0 = j0 rounded down to
-// 4, so a block's 2048 inputs start at offset j0 - a0 in 0..3
-constexpr int BR_STG = 2064;
-// dynamic shared memory of k_broaden (floats): two staging rows, two
-// swizzled FFT arrays (float2; the blocks' outputs reuse one of them), the
-// instrument taps
-constexpr int BR_SMEM_FLOATS = 2 * BR_STG + 2 * FFT_SM + 2 * FFT_SM + 512;
-
-// pixels outside [ilo, ihi) are zero; ilo and ihi are multiples of 8, so
-// every 16-byte chunk is wholly inside or outside
-__device__ __forceinline__ void stage_row(float *stg, const float *row, int j0, int ilo, int ihi) {
-  const int a0 = j0 & ~3;
-  for (int c = threadIdx.x; c < BR_STG / 4; c += FFT_T) {
-    const int g = a0 + 4 * c;
-    const bool ok = g >= ilo && g + 4 <= ihi;
-    cp_async16(stg + 4 * c, ok ? row + g : row + ilo, ok);
-  }
-}
 
 struct BroadenItem {
   int e, pair, m, hg, V, s0, s1, j0, j1;
@@ -466,84 +499,84 @@ struct ItemCursor {
   }
 };
 
-// start the copies of an item's input into the staging rows
-__device__ __forceinline__ void stage_item(const EvalBatch &b, int e, int pair, float *stg0, float *stg1) {
+// The 2 x 16 inputs of this thread for an item: block input j = 128 n1 + t
+// is synth pixel j0 + j of the interpolated row (zero outside [i_lo, i_hi)).
+__device__ __forceinline__ void broaden_inputs(const EvalBatch &b, const ItemCursor &c, float (&x0)[16],
+                                               float (&x1)[16]) {
   BroadenItem w;
-  broaden_item(b, e, pair, w);
-  const EvalPrep &P = b.prep[e];
-  const float *row = b.bufA + (size_t)e * b.stride;
-  stage_row(stg0, row, w.j0, P.i_lo, P.i_hi);
-  if (w.has1) stage_row(stg1, row, w.j1, P.i_lo, P.i_hi);
+  broaden_item(b, c.e, c.pair, w);
+  const EvalPrep &P = b.prep[c.e];
+  const float *row = b.bufA + (size_t)c.e * b.stride;
+  const int ilo = P.i_lo, ihi = P.i_hi;
+#pragma unroll
+  for (int n1 = 0; n1 < 16; n1++) {
+    const int g0 = w.j0 + 128 * n1 + (int)threadIdx.x, g1 = w.j1 + 128 * n1 + (int)threadIdx.x;
+    x0[n1] = (g0 >= ilo && g0 < ihi) ? __ldg(row + g0) : 0.0f;
+    x1[n1] = (w.has1 && g1 >= ilo && g1 < ihi) ? __ldg(row + g1) : 0.0f;
+  }
 }
 
-struct StageLoad {
-  const float *s0, *s1;
-  bool has1;
-  __device__ __forceinline__ cf operator()(int i, int) const { return cf{s0[i], has1 ? s1[i] : 0.0f}; }
-};
-// last forward stage: the spectrum times the kernel spectrum H (1025 bins of
-// a real kernel; bins above 1024 are the conjugates of 2048 - k).  The stage
-// writes output k to the slot it read input k from, so the product takes the
-// place of a separate pass.
-struct SpecStore {
-  float2 *c;
-  const float2 *__restrict__ H;
-  __device__ __forceinline__ void operator()(int k, int a, cf v, int) const {
-    float2 h = __ldg(&H[k <= 1024 ? k : FFTN - k]);
-    if (k > 1024) h.y = -h.y;
-    const cf z = cmul(v, cf{h.x, h.y});
-    c[a] = make_float2(z.x, z.y);
-  }
-};
-// last inverse stage of the unfolded path: rotation output t (data index
-// s - hg + t - base of each block) scaled, zero outside the grid
-struct MaskStore {
-  float2 *c;
-  int base, r0, r1, N;
-  float sc;
-  __device__ __forceinline__ void operator()(int t, int a, cf v, int) const {
-    const int i0 = r0 + (t - base), i1 = r1 + (t - base);
-    c[a] = make_float2((i0 >= 0 && i0 < N) ? v.x * sc : 0.0f, (i1 >= 0 && i1 < N) ? v.y * sc : 0.0f);
-  }
-};
-// last inverse stage of the folded path: FFT index i is output i - lo
-struct FoldStore {
-  float *o0, *o1;
-  int lo, V;
-  float sc;
-  __device__ __forceinline__ void operator()(int i, int, cf v, int) const {
-    const int u = i - lo;
-    if ((unsigned)u < (unsigned)V) {
-      o0[u] = v.x * sc;
-      o1[u] = v.y * sc;
-    }
-  }
-};
+// 8-byte asynchronous global -> shared copy (float indices)
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 
-__global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
-  extern __shared__ __align__(16) float br_smem[];
-  float *stg0 = br_smem, *stg1 = stg0 + BR_STG;
-  // two FFT buffers (BR_STG keeps 16-byte alignment); the stages alternate
-  // between them, so each needs one barrier.  The transform ends in fb; the
-  // outputs then take the other buffer (fa), or fb itself on the folded path
-  float2 *fa = reinterpret_cast<float2 *>(stg1 + BR_STG);
-  float2 *fb = fa + FFT_SM;
-  float *gks = reinterpret_cast<float *>(fb + FFT_SM);  // the fixed instrument kernel of the current item
-  const int N = G.npx;
-  const int p0 = pidx(threadIdx.x);
+constexpr int BT = F2_T;      // threads of k_broaden
+constexpr int BR_FX = 2048;   // float indices of observed pixels prefetched per item
+// dynamic shared memory (bytes): exchange buffers 1 and 2 (buffer 2 also
+// holds the rotation outputs, buffer 1 the outputs of the instrument taps),
+// twiddles of passes 1 and 2, the item's observed float indices, the fixed
+// instrument taps
+constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T1 = BR_S2 + F2_S2 * 8, BR_T2 = BR_T1 + 16 * BT * 8,
+              BR_FXO = BR_T2 + 16 * 8 * 8, BR_GK = BR_FXO + BR_FX * 8, BR_SMEM = BR_GK + 512 * 4;
+
+// One work item = two overlap-save blocks of one evaluation.  Block k yields
+// V = 2048 - (m - 1) - 2 hg final outputs starting at s_k = o_lo + k (V - 1):
+// the rotation outputs [s - hg, s + V + hg) come from one overlap-save block
+// of 2048 inputs (the reference uses overlap-add, convolve_rv.rs:121-157;
+// both are the same linear convolution), and the instrument profile is then
+// applied from shared memory.  Block k owns synth pixels [s_k, s_k + V - 1);
+// its last output is the partner j + 1 of its last owned pixel j.  The two
+// real blocks ride in the real and imaginary parts of one complex FFT (the
+// kernel is real, so the two products separate after the inverse).  Rotation
+// outputs outside [0, N) are zero, like the reference's cropped segment.
+// With the identity rotation the FFT is skipped.  Away from the grid ends
+// the instrument Gaussian acts on rotation outputs that are all inside
+// [0, N), where rotation-then-Gaussian is one convolution with the combined
+// kernel: the spectra are multiplied (H x G) and the taps are skipped.
+//
+// Epilogue: either the owned synth pixels go to row B, or (chi2 batches,
+// EvalPrep::epi) the block resamples the observed pixels whose left synth
+// pixel it owns (EvalBatch::bnd lists them per block) from shared memory and
+// writes the model at the observed pixels to row B; the synth row never
+// reaches memory.  The next item's inputs are loaded into registers and this
+// item's observed float indices copied into shared memory (cp.async) while
+// the transforms run.
+__global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char br_smem[];
+  float2 *S1 = reinterpret_cast<float2 *>(br_smem + BR_S1);
+  float2 *S2 = reinterpret_cast<float2 *>(br_smem + BR_S2);
+  float2 *T1 = reinterpret_cast<float2 *>(br_smem + BR_T1);
+  float2 *T2 = reinterpret_cast<float2 *>(br_smem + BR_T2);
+  double *fxs = reinterpret_cast<double *>(br_smem + BR_FXO);
+  float *gks = reinterpret_cast<float *>(br_smem + BR_GK);
+  const int t = threadIdx.x, N = G.npx;
+  // twiddle tables: T1[k1][t] = W_2048^(t k1), T2[k2][n3] = W_128^(n3 k2)
+  for (int i = t; i < 16 * BT; i += BT) T1[i] = __ldg(&tw[((i & (BT - 1)) * (i >> 7)) & (FFTN - 1)]);
+  for (int i = t; i < 16 * 8; i += BT) T2[i] = __ldg(&tw[(16 * (i & 7) * (i >> 3)) & (FFTN - 1)]);
   ItemCursor cur;
   cur.init(b);
   cur.settle(b);
-  if (!cur.done()) stage_item(b, cur.e, cur.pair, stg0, stg1);
-  cp_async_commit();
+  float in0[16], in1[16];
+  if (!cur.done()) broaden_inputs(b, cur, in0, in1);
+  const int k1p = t >> 3, n3p = t & 7;  // pass-2 role of this thread
   while (!cur.done()) {
     ItemCursor nxt = cur;
     nxt.advance();
     nxt.settle(b);
     BroadenItem w;
     broaden_item(b, cur.e, cur.pair, w);
-    cp_async_wait_all();
-    __syncthreads();  // the item's input is staged; the last item's outputs are written
     const int e = w.e, pair = w.pair, m = w.m, hg = w.hg, V = w.V, s0 = w.s0, s1 = w.s1;
     const bool has1 = w.has1;
     const EvalPrep &P = b.prep[e];
@@ -551,123 +584,202 @@ __global__ void __launch_bounds__(FFT_T, 3) k_broaden(DevGrid G, EvalBatch b, co
     const DevStar &st = b.stars[P.star];
     const bool fixedk = hg > 0 && st.disp_kind == DISP_FIXED;
     const int gw = 2 * hg + 1;
+    int q0 = 0, q1 = 0, q2 = 0;
+    if (P.epi) {
+      const int *bd = b.bnd + (size_t)e * b.bnd_stride + 2 * pair;
+      q0 = bd[0];
+      q1 = bd[1];
+      q2 = has1 ? bd[2] : q1;
+    }
+    __syncthreads();  // the last item's epilogue is done with the shared buffers
+    // this item's observed float indices (uniform grids) and instrument taps
+    const bool pre = P.epi && G.wl_kind != WL_NONUNI;
+    if (pre) {
+      const int nq = min(q2 - q0, BR_FX);
+      for (int i = t; i < nq; i += BT) cp_async8(fxs + i, st.fidx + q0 + i);
+    }
+    cp_async_commit();
     if (fixedk)
-      for (int t = threadIdx.x; t < gw; t += FFT_T) gks[t] = st.gk[t];
-    const StageLoad ld{stg0 + (w.j0 & 3), stg1 + (w.j1 & 3), has1};
-    int base = 0;  // data index of rotation output (s - hg)
-    // Away from the grid ends the Gaussian acts on rotation outputs that are
-    // all inside [0, N), where rotation-then-Gaussian equals one convolution
-    // with the combined kernel: multiply the spectra and skip the taps.
+      for (int k = t; k < gw; k += BT) gks[k] = __ldg(&st.gk[k]);
+    // the next item's inputs stream into registers meanwhile
+    float nx0[16], nx1[16];
+    if (!nxt.done()) broaden_inputs(b, nxt, nx0, nx1);
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
-    float *ob0 = reinterpret_cast<float *>(fold ? fb : fa), *ob1 = ob0 + FFT_SM;
+    const float sc = 1.0f / 2048.0f;
+    float *ob0, *ob1;  // final outputs u in [0, V) of the two blocks
     if (m > 1) {
-      // first stage straight from the staging rows
-      fft_pass<8, 1, false, StageLoad, SmemStore, false>(tw, ld, SmemStore{fa});
-      if (!nxt.done()) stage_item(b, nxt.e, nxt.pair, stg0, stg1);
-      cp_async_commit();
-      fft_stage_pp<8, 8, false>(fa, fb, tw);
-      fft_stage_pp<8, 64, false>(fb, fa, tw);
-      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
-      fft_pass<4, 512, false, SmemLoad, SpecStore, false>(tw, SmemLoad{fa}, SpecStore{fb, H});
-      fft_stage_pp<8, 1, true>(fb, fa, tw);
-      fft_stage_pp<8, 8, true>(fa, fb, tw);
-      fft_stage_pp<8, 64, true>(fb, fa, tw);
-      base = m - 1;
-      const float sc = 1.0f / 2048.0f;
-      if (fold)  // output u sits at base + 2 hg + u
-        fft_pass<4, 512, true, SmemLoad, FoldStore, false>(tw, SmemLoad{fa}, FoldStore{ob0, ob1, base + 2 * hg, V, sc});
-      else
-        fft_pass<4, 512, true, SmemLoad, MaskStore, false>(tw, SmemLoad{fa},
-                                                           MaskStore{fb, base, s0 - hg, s1 - hg, N, sc});
-    } else {  // identity rotation: the staged input is the rotation output
-      for (int t = threadIdx.x; t < FFTN; t += FFT_T) {
-        const cf v = ld(t, 0);
-        fb[p0 + (t - threadIdx.x)] = make_float2(v.x, v.y);
+      cf v[16];
+#pragma unroll
+      for (int n1 = 0; n1 < 16; n1++) v[n1] = cf{in0[n1], in1[n1]};
+      // pass 1: DFT-16 over n1, twiddle, exchange 1
+      dft16<false>(v);
+#pragma unroll
+      for (int k1 = 0; k1 < 16; k1++) {
+        const cf z = k1 ? cmul_tw<false>(v[k1], T1[k1 * BT + t]) : v[k1];
+        S1[k1 * F2_XP + t] = make_float2(z.x, z.y);
       }
       __syncthreads();
-      if (!nxt.done()) stage_item(b, nxt.e, nxt.pair, stg0, stg1);
-      cp_async_commit();
+      // pass 2: DFT-16 over n2, twiddle, exchange 2
+#pragma unroll
+      for (int n2 = 0; n2 < 16; n2++) {
+        const float2 z = S1[k1p * F2_XP + 8 * n2 + n3p];
+        v[n2] = cf{z.x, z.y};
+      }
+      dft16<false>(v);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; k2++) {
+        const cf z = k2 ? cmul_tw<false>(v[k2], T2[k2 * 8 + n3p]) : v[k2];
+        S2[f2_a2(k1p + 16 * k2, n3p)] = make_float2(z.x, z.y);
+      }
+      __syncthreads();
+      // pass 3 (DFT-8 over n3), the spectrum product, and the inverse DFT-8
+      // over k3, for c = t and t + 128; each thread rewrites the slots it read
+      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = t + 128 * h;
+        cf u[8];
+        float2 hk[8];
+#pragma unroll
+        for (int k3 = 0; k3 < 8; k3++) {
+          const int k = c + 256 * k3;
+          hk[k3] = __ldg(&H[k <= 1024 ? k : FFTN - k]);
+          if (k > 1024) hk[k3].y = -hk[k3].y;
+        }
+#pragma unroll
+        for (int n3 = 0; n3 < 8; n3++) {
+          const float2 z = S2[f2_a2(c, n3)];
+          u[n3] = cf{z.x, z.y};
+        }
+        dft8<false>(u);
+#pragma unroll
+        for (int k3 = 0; k3 < 8; k3++) u[k3] = cmul(u[k3], cf{hk[k3].x, hk[k3].y});
+        dft8<true>(u);
+#pragma unroll
+        for (int n3 = 0; n3 < 8; n3++) S2[f2_a2(c, n3)] = make_float2(u[n3].x, u[n3].y);
+      }
+      __syncthreads();
+      // inverse pass 2: conjugate twiddle, DFT-16 over k2, exchange 1
+#pragma unroll
+      for (int k2 = 0; k2 < 16; k2++) {
+        const float2 z = S2[f2_a2(k1p + 16 * k2, n3p)];
+        v[k2] = k2 ? cmul_tw<true>(cf{z.x, z.y}, T2[k2 * 8 + n3p]) : cf{z.x, z.y};
+      }
+      dft16<true>(v);
+#pragma unroll
+      for (int n2 = 0; n2 < 16; n2++) S1[k1p * F2_XP + 8 * n2 + n3p] = make_float2(v[n2].x, v[n2].y);
+      __syncthreads();
+      // inverse pass 1: conjugate twiddle, DFT-16 over k1 -> 2048 x output 128 n1 + t
+#pragma unroll
+      for (int k1 = 0; k1 < 16; k1++) {
+        const float2 z = S1[k1 * F2_XP + t];
+        v[k1] = k1 ? cmul_tw<true>(cf{z.x, z.y}, T1[k1 * BT + t]) : cf{z.x, z.y};
+      }
+      dft16<true>(v);
+      // FFT index i = 128 n1 + t holds rotation output (s - hg) + (i - (m - 1))
+      const int base = m - 1;
+      if (fold) {  // final output u = i - base - 2 hg
+        ob0 = reinterpret_cast<float *>(S2);
+        ob1 = ob0 + 2048;
+#pragma unroll
+        for (int n1 = 0; n1 < 16; n1++) {
+          const int u = 128 * n1 + t - base - 2 * hg;
+          if ((unsigned)u < (unsigned)V) {
+            ob0[u] = v[n1].x * sc;
+            ob1[u] = v[n1].y * sc;
+          }
+        }
+      } else {  // rotation outputs r = i - base, zero outside the grid
+        const int r0 = s0 - hg, r1 = s1 - hg;
+#pragma unroll
+        for (int n1 = 0; n1 < 16; n1++) {
+          const int r = 128 * n1 + t - base;
+          if (r >= 0) {
+            const int i0 = r0 + r, i1 = r1 + r;
+            S2[r] = make_float2((i0 >= 0 && i0 < N) ? v[n1].x * sc : 0.0f, (i1 >= 0 && i1 < N) ? v[n1].y * sc : 0.0f);
+          }
+        }
+      }
+    } else {  // identity rotation: the inputs are the rotation outputs r = j
+#pragma unroll
+      for (int n1 = 0; n1 < 16; n1++) S2[128 * n1 + t] = make_float2(in0[n1], in1[n1]);
     }
-    const float2 *c = fb;  // rotation outputs of the unfolded paths
-    if (!fold) {
-      for (int u = threadIdx.x; u < V; u += FFT_T) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (!fold) {  // instrument taps from the rotation outputs in S2 into buffer 1
+      ob0 = reinterpret_cast<float *>(S1);
+      ob1 = ob0 + 2048;
+      for (int u = t; u < V; u += BT) {
         const int i0 = s0 + u, i1 = s1 + u;
         float v0, v1;
         if (hg == 0) {
-          const float2 x = c[pidx(base + u)];
+          const float2 x = S2[u];
           v0 = x.x;
           v1 = x.y;
-        } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at base + (i - s + hg)
+        } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at i - s + hg
           float a0 = 0.0f, a1 = 0.0f;
           for (int k = 0; k < gw; k++) {
             const float g = gks[k];
-            const float2 x = c[pidx(base + u + 2 * hg - k)];
+            const float2 x = S2[u + 2 * hg - k];
             a0 = fmaf(g, x.x, a0);
             a1 = fmaf(g, x.y, a1);
           }
           v0 = a0;
           v1 = a1;
         } else {
-          v0 = instrument(st, N, i0, hg, [&](int i) { return c[pidx(base + i - (s0 - hg))].x; });
-          v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return c[pidx(base + i - (s1 - hg))].y; }) : 0.0f;
+          v0 = instrument(st, N, i0, hg, [&](int i) { return S2[i - (s0 - hg)].x; });
+          v1 = has1 ? instrument(st, N, i1, hg, [&](int i) { return S2[i - (s1 - hg)].y; }) : 0.0f;
         }
         ob0[u] = v0;
         ob1[u] = v1;
       }
-      __syncthreads();  // (the folded path's last stage ended with one)
+      __syncthreads();
     }
     float *y = b.bufB + (size_t)e * b.stride;
     if (P.epi) {
-      // observed pixels [bnd[2 pair], bnd[2 pair + 2]) have their left synth
-      // pixel in this item's blocks; the boundary between them is bnd[2 pair + 1]
-      const int *bd = b.bnd + (size_t)e * b.bnd_stride + 2 * pair;
-      const int q0 = bd[0], q1 = bd[1], q2 = has1 ? bd[2] : q1;
+      // observed pixels [q0, q2) have their left synth pixel in this item's
+      // blocks; the boundary between them is q1
       const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
-      constexpr int EU = 8;  // observed pixels per thread whose float indices load together
-      for (int i0 = q0 + threadIdx.x; i0 < q2; i0 += FFT_T * EU) {
-        double fx[EU];
-        if (R.kind != WL_NONUNI) {
-#pragma unroll
-          for (int k = 0; k < EU; k++) fx[k] = R.fidx[min(i0 + k * FFT_T, q2 - 1)];
-        }
-#pragma unroll
-        for (int k = 0; k < EU; k++) {
-          const int i = i0 + k * FFT_T;
-          if (i >= q2) break;
-          const ResPos q = R.kind != WL_NONUNI ? R.pos_from_fidx(fx[k]) : R.pos(i);
-          const bool k1 = i >= q1;
-          const float *o = k1 ? ob1 : ob0;
-          const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
-          y[i] = resample_value(q.w, o[u], o[u + 1]);
-        }
+      for (int i = q0 + t; i < q2; i += BT) {
+        ResPos q;
+        if (R.kind == WL_NONUNI) q = R.pos(i);
+        else q = R.pos_from_fidx(i - q0 < BR_FX ? fxs[i - q0] : R.fidx[i]);
+        const bool k1 = i >= q1;
+        const float *o = k1 ? ob1 : ob0;
+        const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
+        y[i] = resample_value(q.w, o[u], o[u + 1]);
       }
     } else {
       // owned pixels; the last block also writes its final output
       const int n0 = 2 * pair + 1 == nblk ? V : V - 1, n1 = 2 * pair + 2 == nblk ? V : V - 1;
-      for (int u = threadIdx.x; u < V; u += FFT_T) {
+      for (int u = t; u < V; u += BT) {
         const int i0 = s0 + u, i1 = s1 + u;
         if (u < n0 && i0 < ohi) y[i0] = ob0[u];
         if (has1 && u < n1 && i1 < ohi) y[i1] = ob1[u];
       }
     }
     cur = nxt;
+#pragma unroll
+    for (int n1 = 0; n1 < 16; n1++) {
+      in0[n1] = nx0[n1];
+      in1[n1] = nx1[n1];
+    }
   }
-  cp_async_wait_all();
 }
 
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cudaStream_t s) {
   if (b.E <= 0 || b.max_pairs <= 0) return;
-  const size_t smem = BR_SMEM_FLOATS * sizeof(float);
+  const size_t smem = BR_SMEM;
   static int per_sm[64] = {};  // resident CTAs per SM, per device
   int dev = 0;
   cudaGetDevice(&dev);
-  int fit = 4;
+  int fit = 3;
   if (dev >= 0 && dev < 64) {
     if (!per_sm[dev]) {
       cudaFuncSetAttribute(k_broaden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       int n = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_broaden, FFT_T, smem) != cudaSuccess || n < 1) n = 1;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_broaden, BT, smem) != cudaSuccess || n < 1) n = 1;
       per_sm[dev] = n;
     }
     fit = per_sm[dev];
@@ -675,7 +787,7 @@ void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cuda
   const long long total = (long long)b.E * b.max_pairs;
   long long grid = (long long)num_sms() * fit;  // persistent: the CTAs that fit at once
   if (grid > total) grid = total;
-  k_broaden<<<(unsigned)grid, FFT_T, smem, s>>>(G, b, tw);
+  k_broaden<<<(unsigned)grid, BT, smem, s>>>(G, b, tw);
   count_launch();
 }
 
@@ -1616,6 +1728,7 @@ void launch_pipeline(const DevGrid &G, const EvalBatch &b, const float2 *tw, con
   else launch_prep(G, b, s);
   if (o.rot) launch_rotker(G, b, tw, s);
   launch_group(G, b, s);
+  launch_interp_tc(G, b, s);
   launch_interp(G, b, s);
   launch_obs_bounds(G, b, s);
   launch_broaden(G, b, tw, s);

@@ -21,6 +21,20 @@ struct __align__(16) GroupRec {
   int nmem, nn;           // members, compacted rows
 };
 
+// Evaluations with identical neighbour columns, TC_MIN_MEMBERS or more of
+// them in one segment, are interpolated together on the tensor cores
+// (interp_tc.cu): the group's rows are staged by TMA and its members'
+// weights are the columns of one matrix product.
+constexpr int TC_MIN_MEMBERS = 16, TC_MAX_GROUPS = SEG / TC_MIN_MEMBERS;
+struct __align__(16) TcGroup {
+  int member[SEG];  // evaluation indices, ascending (first nmem valid)
+  int col[64];      // the shared neighbour columns (-1: missing)
+  float f[64];      // their dequantisation factors (0 for missing)
+  int nmem;
+  int lo, hi;       // union of the members' interpolation windows [i_lo, i_hi)
+  int pad;
+};
+
 constexpr int LIN_MAX_SLICES = 32;  // at most MAX_CHUNKS: the slices' residual sums use EvalBatch::cpart
 
 // Per-launch description of one batch of evaluations.
@@ -50,8 +64,16 @@ struct EvalBatch {
   int bnd_stride;
   float *ccoef;              // [E][MAX_CHUNKS][MAX_P1] chunk polynomial coefficients (f32)
   double *cpart;             // [E][MAX_CHUNKS] chi2 partial sums per chunk section
-  GroupRec *grec;            // [ceil(E / SEG) * SEG] groups of each segment, in order
-  int *gcount;               // [ceil(E / SEG)] groups per segment
+  // Segments: the evaluations of each star (seg_len consecutive ones; 0:
+  // the whole batch is one star) in chunks of at most SEG from the star's
+  // first evaluation, so a star's groups do not depend on the rest of the
+  // batch.  A segment's records sit at its first evaluation's index.
+  int seg_len;
+  GroupRec *grec;            // [E] groups of each segment, in order
+  int *gcount;               // [segments] groups per segment
+  TcGroup *tcrec;            // [E] tensor-core groups of each segment (null: none)
+  int *tccount;              // [segments]
+  const void *tmap;          // host pointer to the grid's TMA tensor map (null: no tensor-core path)
   const float *given;        // model given at the observed pixels (continuum utilities) or null
   int64_t given_stride;      // floats between the given rows of consecutive evaluations
   int direct_max;            // combined kernels of at most this many taps are convolved directly (0: never)
@@ -87,6 +109,13 @@ void launch_rotker(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, 
 // groups of evaluations sharing their neighbour rows (after the preparation)
 void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// tensor-core interpolation of the groups k_group marked (interp_tc.cu)
+void launch_interp_tc(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
+// segments of a batch (see EvalBatch::seg_len)
+int num_segments(const EvalBatch &b);
+// the grid's TMA tensor map: uint16 [rows][stride], box 128 pixels x 1 row
+// (host side; out points to a CUtensorMap); false when the driver lacks it
+bool make_grid_tensor_map(const uint16_t *spectra, int64_t rows, int64_t stride, void *out);
 // first observed pixel of every fused broadening block (chi2 batches)
 void launch_obs_bounds(const DevGrid &G, const EvalBatch &b, cudaStream_t s);
 void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *twiddle, cudaStream_t s);

@@ -655,20 +655,34 @@ class _Interpolator:
     def chi2_bulk(self, observed_wavelength, observed_flux, observed_var, labels, progress=None,
                   allow_nan=None) -> list:
         """Chi2 of many spectra, each with its own wavelengths, a pre-convolved
-        grid and a 5 x 8 x 0.2 chunk fitter (lib.rs:1297-1338)."""
-        out = []
-        for wl, fl, vr, lab in zip(observed_wavelength, observed_flux, observed_var, labels):
-            disp = NoConvolutionDispersion(wl, self.synth_wl)
-            cont = ChunkContinuumFitter(wl, 5, 8, 0.2)
-            lab = self._labels(lab, 5)
-            model, st = self._produce(disp, lab)
-            if st[0]:
-                if allow_nan:
-                    out.append(float("nan"))
-                    continue
-                self._raise_status(st)
-            out.append(cont.fit_and_return_chi2(model[0], fl, vr))
-        return out
+        grid and a 5 x 8 x 0.2 chunk fitter (lib.rs:1297-1338), all in one
+        batched device pass (pasta_chi2_many)."""
+        wls = [f64(w) for w in observed_wavelength]
+        fl = [f32(x) for x in observed_flux]
+        vr = [f32(x) for x in observed_var]
+        S = len(wls)
+        if not (len(fl) == len(vr) == S == len(labels)):
+            raise ValueError("wavelengths, fluxes, variances and labels must have the same count")
+        for w, f, v in zip(wls, fl, vr):
+            if not (len(w) == len(f) == len(v)):
+                raise ValueError("Flux and variance vectors must have the same length")
+        if S == 0:
+            return []
+        disps = [NoConvolutionDispersion(w, self.synth_wl) for w in wls]
+        conts = [ChunkContinuumFitter(w, 5, 8, 0.2) for w in wls]
+        lab = f64(np.asarray(labels, dtype=np.float64).reshape(S, 5))
+        out = np.empty(S)
+        st = np.zeros(S, np.int32)
+        Pp = C.c_void_p
+        dh = (Pp * S)(*[d._h.value for d in disps])
+        ch = (Pp * S)(*[c._h.value for c in conts])
+        fp = (Pp * S)(*[x.ctypes.data for x in fl])
+        vp = (Pp * S)(*[x.ctypes.data for x in vr])
+        n = np.array([len(x) for x in fl], np.int64)
+        check(lib().pasta_chi2_many(self._grid._h, S, dh, ch, fp, vp, ptr(n), ptr(lab), ptr(out), ptr(st)))
+        if not allow_nan:
+            self._raise_status(st, "chi2")
+        return [float(x) for x in out]
 
     def ccf(self, vs, teff, m, logg, dispersion, observed_flux) -> np.ndarray:
         """Cross-correlation of the unbroadened model with the flux (lib.rs:1340-1371)."""
@@ -759,6 +773,48 @@ class _Interpolator:
         return bool(out.value)
 
 
+ZSTD_MAGIC = b"\x28\xb5\x2f\xfd"
+
+
+def _tar_bytes(file_path: str) -> bytes:
+    """The tar archive inside a .tar.zst file (model_fetchers.rs:168-180).  A
+    zstd frame is decoded by the zstandard module or the zstd program; a
+    file that is not zstd-compressed is read as a plain tar archive."""
+    raw = open(file_path, "rb").read()
+    if raw[:4] != ZSTD_MAGIC:
+        return raw
+    try:
+        import zstandard  # type: ignore
+        return zstandard.ZstdDecompressor().decompress(raw, max_output_size=1 << 40)
+    except ImportError:
+        pass
+    import shutil
+    import subprocess
+    exe = shutil.which("zstd") or shutil.which("unzstd")
+    if exe is None:
+        raise RuntimeError("%s is zstd-compressed, and neither the 'zstandard' Python module nor a zstd program is "
+                           "available to decode it; decompress it to a plain .tar (which from_tar_zstd also reads) "
+                           "or install one of them" % file_path)
+    return subprocess.run([exe, "-dc", file_path], check=True, capture_output=True).stdout
+
+
+def _read_tar_models(file_path: str, includes_factor: bool):
+    """(labels, spectra, maxima or None) of the archive's grid models."""
+    labels, specs, maxima = [], [], []
+    with tarfile.open(fileobj=io.BytesIO(_tar_bytes(file_path))) as tf:
+        for mem in tf.getmembers():
+            name = os.path.basename(mem.name)
+            if not mem.isfile() or not name.startswith("l"):
+                continue
+            labels.append(_label_from_filename(name))
+            sp, mx = _split_factor(np.load(io.BytesIO(tf.extractfile(mem).read())), includes_factor)
+            specs.append(sp)
+            maxima.append(mx)
+    if not specs:
+        raise ValueError("no grid models in %r" % file_path)
+    return np.array(labels), np.stack(specs), np.array(maxima, np.float32) if includes_factor else None
+
+
 class InMemInterpolator(_Interpolator):
     """lib.rs:1881-1908: the whole grid resident in HBM."""
 
@@ -768,26 +824,9 @@ class InMemInterpolator(_Interpolator):
     @staticmethod
     def from_tar_zstd(file_path: str, includes_factor: bool, wavelength: WlGrid) -> "InMemInterpolator":
         """model_fetchers.rs:168-226: members starting with 'l' are grid models."""
-        raw = open(file_path, "rb").read()
-        try:
-            import zstandard  # type: ignore
-            data = zstandard.ZstdDecompressor().decompress(raw, max_output_size=1 << 40)
-        except ImportError:
-            import subprocess
-            data = subprocess.run(["zstd", "-dc", file_path], check=True, capture_output=True).stdout
-        labels, specs, maxima = [], [], []
-        with tarfile.open(fileobj=io.BytesIO(data)) as tf:
-            for mem in tf.getmembers():
-                name = os.path.basename(mem.name)
-                if not mem.isfile() or not name.startswith("l"):
-                    continue
-                labels.append(_label_from_filename(name))
-                s, mx = _split_factor(np.load(io.BytesIO(tf.extractfile(mem).read())), includes_factor)
-                specs.append(s)
-                maxima.append(mx)
+        labels, specs, maxima = _read_tar_models(file_path, includes_factor)
         self = InMemInterpolator.__new__(InMemInterpolator)
-        self._init_arrays(np.array(labels), np.stack(specs),
-                          np.array(maxima, np.float32) if includes_factor else None, wavelength)
+        self._init_arrays(labels, specs, maxima, wavelength)
         return self
 
     @staticmethod

@@ -494,3 +494,111 @@ def test_server_budget_makes_requests_wait(env):
                                                                                     seed=300 + i)
         assert done[ids[i]].label.as_list() == alone.label.as_list()
         assert done[ids[i]].chi2 == alone.chi2
+
+
+def test_interpolation_tensor_cores(env):
+    """Labels of one star that share their 64 neighbour rows (16 or more)
+    are interpolated on the tensor cores: each model against the oracle's
+    FP32 mirror (1e-5 of the maximum) and against the CUDA-core path (2e-6),
+    the reference's 1/65535 tail included; a member's result does not depend
+    on the other members of its group; scattered labels stay exact."""
+    from pasta_b200 import _ffi
+    O, S, interp, og, spec = env["O"], env["S"], env["interp"], env["og"], env["spec"]
+    rng = np.random.default_rng(9)
+    cube = np.stack([rng.uniform(7010.0, 7240.0, 40), rng.uniform(0.01, 0.09, 40), rng.uniform(4.01, 4.24, 40)], 1)
+    scat = S.random_labels(spec, 8, seed=3)[:, :3]
+    lab = np.vstack([cube, scat])
+    tc = interp.interpolate_bulk(lab)
+    _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(0))
+    try:
+        cc = interp.interpolate_bulk(lab)
+    finally:
+        _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(1))
+    for i in range(len(lab)):
+        ref = og.interpolate(*lab[i], O.F32)
+        assert relmax(tc[i], ref) <= FLUX_TOL, i
+    assert np.abs(tc - cc).max() <= 2e-6 * np.abs(cc).max()
+    np.testing.assert_array_equal(tc[40:], cc[40:])  # scattered labels: CUDA cores either way
+    half = interp.interpolate_bulk(cube[:20])
+    np.testing.assert_array_equal(half, tc[:20])
+
+
+def test_chi2_bulk_one_batched_pass(env):
+    """chi2_bulk (lib.rs:1297-1338): spectra with their own wavelength grids,
+    a no-convolution dispersion and a 5 x 8 x 0.2 chunk fitter each, in one
+    batched pass; against the FP64 oracle and against each spectrum alone."""
+    O, P, S, spec, interp = env["O"], env["P"], env["S"], env["spec"], env["interp"]
+    labs = np.array([[7130.0, 0.07, 4.02, 30.0, 20.0], [6600.0, -0.3, 3.8, 0.0, -40.0],
+                     [7700.0, 0.3, 4.3, 120.0, 60.0]])
+    stars = [S.make_star(spec, l, n, 90.0, 0.0, seed=70 + i) for i, (l, n) in enumerate(zip(labs, [9000, 12000, 7000]))]
+    got = interp.chi2_bulk([s.wl for s in stars], [s.flux for s in stars], [s.var for s in stars], labs)
+    for i, s in enumerate(stars):
+        od = O.Disp(env["og"], O.DISP_NONE, s.wl)
+        oc = O.Cont(O.CONT_CHUNK, s.wl, 5, 8, 0.2)
+        ref, st = O.chi2(env["og"], od, oc, s.flux, s.var, labs[i][None], O.F64)
+        assert st[0] == 0
+        assert abs(got[i] - ref[0]) <= CHI2_TOL * ref[0]
+        d = P.NoConvolutionDispersion(s.wl, env["wl"])
+        f = interp.get_fitter(d, P.ChunkContinuumFitter(s.wl, 5, 8, 0.2), P.PSOSettings(8, 2), (0, 300), (-150, 150))
+        alone = f.chi2(interp, s.flux, s.var, [labs[i]])[0]
+        assert abs(got[i] - alone) <= 1e-12 * alone
+    bad = labs.copy()
+    bad[1, 0] = 9000.0  # outside the grid
+    out = interp.chi2_bulk([s.wl for s in stars], [s.flux for s in stars], [s.var for s in stars], bad, allow_nan=True)
+    assert np.isnan(out[1]) and np.isfinite(out[0]) and np.isfinite(out[2])
+    with pytest.raises(P.PastaError):
+        interp.chi2_bulk([s.wl for s in stars], [s.flux for s in stars], [s.var for s in stars], bad)
+
+
+def test_grid_ingest_directory_and_tar(env, tmp_path):
+    """InMemInterpolator(dir) / OnDiskInterpolator / CachedInterpolator from a
+    directory of .npy models (model_fetchers.rs:136-166) and from a tar
+    archive (model_fetchers.rs:168-226), with and without the f32 maximum
+    prefix, interpolate exactly like the same grid given as arrays."""
+    import tarfile
+    P, S = env["P"], env["S"]
+    spec = S.config0_grid(n_px=4000)
+    for with_factor in (False, True):
+        spec.includes_factor = with_factor
+        labels, spectra, factors = S.make_grid(spec)
+        d = tmp_path / ("grid%d" % with_factor)
+        S.write_grid_dir(str(d), labels, spectra, factors)
+        wl = P.WlGrid(spec.log_first, spec.log_step, spec.n_px, log=True)
+        ref = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+        tar = tmp_path / ("grid%d.tar" % with_factor)
+        with tarfile.open(tar, "w") as tf:
+            tf.add(str(d), arcname="models")
+        grids = [P.InMemInterpolator(str(d), with_factor, wl), P.OnDiskInterpolator(str(d), with_factor, wl),
+                 P.CachedInterpolator(str(d), with_factor, wl), P.InMemInterpolator.from_tar_zstd(str(tar), with_factor, wl)]
+        tml = [(7130.0, 0.07, 4.02), (6010.0, -0.49, 3.51)]
+        for g in grids:
+            assert g.list_gridpoints() == ref.list_gridpoints()
+            for x in tml:
+                np.testing.assert_array_equal(g.interpolate(*x), ref.interpolate(*x))
+
+
+def test_fit_trace_output(env, tmp_path):
+    """PSOobserver / BestParticleObserver files (fitting.rs:217-296; lib.rs:837-851):
+    one it_<i>.json per iteration with every particle's position and cost, and
+    the best particle after every iteration, consistent with the fit result."""
+    import json
+    P, star = env["P"], env["star"]
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(d, cont, P.PSOSettings(12, 5), (0.0, 300.0), (-150.0, 150.0))
+    tdir = tmp_path / "trace"
+    r = fitter.fit(env["interp"], star.flux, star.var, trace_directory=str(tdir), seed=31)
+    files = sorted(os.listdir(tdir))
+    assert files == ["it_%d.json" % i for i in range(5)]
+    last = json.load(open(tdir / "it_4.json"))
+    assert len(last) == 12 and set(last[0]) == {"position", "cost"} and len(last[0]["position"]) == 5
+    best_file = tmp_path / "best.json"
+    r2 = fitter.fit(env["interp"], star.flux, star.var, best_particle_file=str(best_file), seed=31)
+    hist = json.load(open(best_file))
+    assert len(hist) == 5
+    costs = [h["cost"] for h in hist]
+    assert all(b <= a for a, b in zip(costs, costs[1:]))
+    assert r2.label.as_list() == r.label.as_list()
+    assert abs(costs[-1] - r2.chi2) <= 1e-9 * r2.chi2 or costs[-1] >= r2.chi2
+    with pytest.raises(RuntimeError):
+        fitter.fit(env["interp"], star.flux, star.var, trace_directory=str(tdir), best_particle_file=str(best_file))

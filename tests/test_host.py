@@ -157,3 +157,34 @@ def test_rust_style_u16_cast():
     from pasta_b200.pasta import _as_u16
     x = np.array([-3.0, 0.0, 0.99, 1.0, 65534.9, 65535.0, 70000.0, np.nan, np.inf], np.float32)
     np.testing.assert_array_equal(_as_u16(x), [0, 0, 0, 1, 65534, 65535, 65535, 0, 65535])
+
+
+def test_tar_grid_reader(tmp_path):
+    """Grid archives (model_fetchers.rs:168-226): models are the members whose
+    name starts with 'l'; a plain tar is read directly, and a zstd frame
+    without a decoder installed gives a clear error."""
+    import tarfile
+    from pasta_b200 import pasta as P
+    from pasta_b200 import synth as S
+    spec = S.config0_grid(n_px=256)
+    spec.includes_factor = True
+    labels, spectra, factors = S.make_grid(spec)
+    d = tmp_path / "grid"
+    S.write_grid_dir(str(d), labels[:6], spectra[:6], factors[:6])
+    (d / "readme.txt").write_text("not a model")
+    tar = tmp_path / "grid.tar"
+    with tarfile.open(tar, "w") as tf:
+        tf.add(str(d), arcname="grid")
+    lab, sp, mx = P._read_tar_models(str(tar), True)
+    order = np.lexsort((lab[:, 2], lab[:, 1], lab[:, 0]))
+    ref = np.lexsort((labels[:6, 2], labels[:6, 1], labels[:6, 0]))
+    np.testing.assert_allclose(lab[order], labels[:6][ref])
+    np.testing.assert_array_equal(sp[order], spectra[:6][ref])
+    np.testing.assert_array_equal(mx[order], factors[:6][ref])
+    zst = tmp_path / "grid.tar.zst"
+    zst.write_bytes(P.ZSTD_MAGIC + b"\x00" * 64)
+    import importlib.util
+    import shutil
+    if importlib.util.find_spec("zstandard") is None and not (shutil.which("zstd") or shutil.which("unzstd")):
+        with pytest.raises(RuntimeError, match="zstd"):
+            P._read_tar_models(str(zst), True)
