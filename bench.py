@@ -99,6 +99,36 @@ def make_grid(spec, use_gpu):
     return labels, spectra, None
 
 
+def make_grid_factor_gpu(spec):
+    """includes_factor grid (blackbody x line spectrum, f32 maximum per model) with the products on the GPU
+    (the same model as synth.make_grid)."""
+    import torch
+    from pasta_b200 import synth as S
+    torch.backends.cuda.matmul.allow_tf32 = False
+    labels = S.gridpoints(spec)
+    lm = S.LineModel(spec)
+    wl = spec.wl()
+    prof = torch.from_numpy(lm.profiles(wl, dtype=np.float32)).cuda()
+    wlt = torch.from_numpy(wl).cuda()
+    spectra = np.empty((len(labels), spec.n_px), np.uint16)
+    factors = np.empty(len(labels), np.float32)
+    hc_k = 1.4387769e8
+    for s0 in range(0, len(labels), 1024):
+        lab = labels[s0:s0 + 1024]
+        d = torch.from_numpy(lm.depths(lab).astype(np.float32)).cuda()
+        f = (1.0 - d @ prof).clamp_(min=0.0)
+        t = torch.from_numpy(lab[:, 0]).cuda()[:, None]
+        bb = (1.0 / (wlt[None, :] ** 5 * torch.expm1(hc_k / (wlt[None, :] * t)))).to(torch.float32)
+        f = f * bb
+        mx = f.max(dim=1).values
+        factors[s0:s0 + 1024] = mx.cpu().numpy()
+        q = torch.clamp(torch.round(f / mx[:, None] * 65535.0), 0, 65535).to(torch.int32)
+        spectra[s0:s0 + 1024] = q.cpu().numpy().astype(np.uint16)
+    del prof
+    torch.cuda.empty_cache()
+    return labels, spectra, factors
+
+
 def make_workload(n_stars, seed, spec):
     from pasta_b200 import synth as S
     rng = np.random.default_rng(seed)
@@ -290,6 +320,208 @@ def linear_leg(P, S, n_labels, k, reps=5):
         out[name] = {"chi2_evals_per_s": n_labels / best, "seconds": best}
     _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(1))
     return out
+
+
+def variable_sigma(wl):
+    """R(lambda) linear 60,000 -> 90,000 over the observed range, as the Gaussian
+    sigma in Angstrom the reference's VariableTargetDispersion takes
+    (convolve_rv.rs:363 uses disp as a sigma)."""
+    return (wl / np.linspace(60000.0, 90000.0, len(wl)) / 2.355).astype(np.float32)
+
+
+def precision_leg(args):
+    """Precision study on the config-1 grid: n_stars stars with R(lambda) 60k
+    -> 90k, rotation through the FFT blocks, the FP32 path (compensated f64
+    continuum sums, FP64 Cholesky) against the FP64 oracle over n_labels
+    seeded label vectors (half uniform in the grid and the vsini/RV ranges,
+    half near each star's own labels, as a contracted swarm): model flux
+    (max |d| / max |ref| per label) and chi2 (relative), with the oracle's
+    FP32 mirror of the reference's arithmetic beside it; then label errors of
+    seeded fits (64 x 200) replayed on the FP64 oracle."""
+    import concurrent.futures as cf
+    import torch
+    from pasta_b200 import pasta as P
+    from pasta_b200 import synth as S
+    torch.cuda.set_device(0)
+    O = _oracle()
+    spec = S.config1_grid(n_px=args.npx)
+    labels, spectra, factors = make_grid(spec, use_gpu=True)
+    wl = P.WlGrid(spec.log_first, spec.log_step, spec.n_px, log=True)
+    interp = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+    interp.direct_max = 0  # rotation through the FFT path
+    og = O.Grid(labels, spectra, factors, O.WL_LOGSPACE, spec.log_first, spec.log_step)
+    ns = args.precision_stars
+    stars = make_workload(ns, 2000, spec)
+    rng = np.random.default_rng(2024)
+    per = -(-args.precision_labels // ns)
+    nthreads = os.cpu_count() or 1
+    fl_err, fl_err32, c_err, c_err32, chi_ref = [], [], [], [], []
+    t0 = time.perf_counter()
+    for i, st in enumerate(stars):
+        n_here = min(per, args.precision_labels - i * per)
+        if n_here <= 0:
+            break
+        uni = S.random_labels(spec, n_here - n_here // 2, seed=int(rng.integers(1 << 30)), vsini=(0.0, 300.0),
+                              rv=(-150.0, 150.0))
+        near = st.label + rng.normal(0, 1, (n_here // 2, 5)) * np.array([0.01 * st.label[0], 0.05, 0.05, 5.0, 3.0])
+        near[:, 3] = np.clip(near[:, 3], 0.0, 300.0)
+        lo = [spec.teffs.min(), spec.ms.min(), spec.loggs.min()]
+        hi = [spec.teffs.max(), spec.ms.max(), spec.loggs.max()]
+        near[:, :3] = np.clip(near[:, :3], lo, hi)
+        labs = np.vstack([uni, near])
+        sig = variable_sigma(st.wl)
+        d = P.VariableResolutionDispersion(st.wl, sig, wl)
+        cont = P.ChunkContinuumFitter(st.wl, 8, 5, 0.2)
+        fitter = interp.get_fitter(d, cont, P.PSOSettings(8, 2), (0.0, 300.0), (-150.0, 150.0))
+        gm = interp.produce_model_bulk(d, labs)
+        gc = np.array(fitter.chi2(interp, st.flux, st.var, labs))
+        od = O.Disp(og, O.DISP_VARIABLE, st.wl, disp=sig)
+        oc = O.Cont(O.CONT_CHUNK, st.wl, 8, 5, 0.2)
+        r64, s64 = O.chi2(og, od, oc, st.flux, st.var, labs, O.F64, nthreads=nthreads)
+        r32, s32 = O.chi2(og, od, oc, st.flux, st.var, labs, O.F32, nthreads=nthreads)
+
+        def models(k):
+            m64 = od.produce_model(labs[k], O.F64)
+            m32 = od.produce_model(labs[k], O.F32)
+            mx = np.abs(m64).max()
+            return np.abs(gm[k] - m64).max() / mx, np.abs(m32 - m64).max() / mx
+
+        with cf.ThreadPoolExecutor(nthreads) as ex:
+            for a, b in ex.map(models, range(len(labs))):
+                fl_err.append(a)
+                fl_err32.append(b)
+        ok = (s64 == 0) & np.isfinite(r64)
+        c_err.extend((np.abs(gc[ok] - r64[ok]) / r64[ok]).tolist())
+        c_err32.extend((np.abs(r32[ok] - r64[ok]) / r64[ok]).tolist())
+        chi_ref.extend(r64[ok].tolist())
+        del od, oc
+    t_models = time.perf_counter() - t0
+
+    def stats(x):
+        x = np.asarray(x)
+        return {"max": float(x.max()), "p99": float(np.percentile(x, 99)), "median": float(np.median(x))}
+
+    chi_ref = np.array(chi_ref)
+    c_err, c_err32 = np.array(c_err), np.array(c_err32)
+    good = chi_ref < 10.0
+    out = {"workload": "precision study: config-1 grid (60x21x11 x %d px), %d stars with R(lambda) 60k->90k "
+                       "(VariableResolutionDispersion), rotation by FFT blocks, 8 chunks deg 5; %d label vectors"
+                       % (spec.n_px, ns, len(fl_err)),
+           "model_flux_rel_err": {"gpu_vs_fp64": stats(fl_err), "fp32_mirror_vs_fp64": stats(fl_err32),
+                                  "basis": "max |model - FP64| / max |FP64| per label"},
+           "chi2_rel_err": {"gpu_vs_fp64": stats(c_err), "fp32_mirror_vs_fp64": stats(c_err32),
+                            "gpu_vs_fp64_chi2_below_10": stats(c_err[good]) if good.any() else None,
+                            "labels": int(len(c_err))},
+           "seconds_models_chi2": t_models}
+    if args.replay_stars > 0:
+        k = args.replay_stars
+        disps = [P.VariableResolutionDispersion(s.wl, variable_sigma(s.wl), wl) for s in stars[:k]]
+        conts = [P.ChunkContinuumFitter(s.wl, 8, 5, 0.2) for s in stars[:k]]
+        seeds = [int(77 + i) for i in range(k)]
+        res = P.fit_many(interp, disps, conts, P.PSOSettings(PARTICLES, ITERS), [s.flux for s in stars[:k]],
+                         [s.var for s in stars[:k]], (0.0, 300.0), (-150.0, 150.0), seeds=seeds)
+        out["label_error_vs_fp64_oracle"] = label_replay(
+            O, og, stars[:k], seeds, res, disp=lambda s: O.Disp(og, O.DISP_VARIABLE, s.wl, disp=variable_sigma(s.wl)))
+    return out
+
+
+def config4_leg(args):
+    """Config 4: the includes_factor grid (80 x 26 x 13 models x 120,000 px,
+    6.5 GB u16 + f32 maxima), stars fitted with a 40-column Legendre
+    linear-model continuum (tensor cores) and PSO 128 x 300, served (slots
+    refilled as fits finish, steady state) and batched (fit_many)."""
+    import torch
+    from pasta_b200 import _ffi
+    from pasta_b200 import pasta as P
+    from pasta_b200 import synth as S
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    spec = S.config4_grid(n_px=120000)
+    t = time.time()
+    labels, spectra, factors = make_grid_factor_gpu(spec)
+    wl = P.WlGrid(spec.log_first, spec.log_step, spec.n_px, log=True)
+    interp = P.InMemInterpolator.from_arrays(labels, spectra, factors, wl)
+    log(f"[config4] grid {spectra.shape} in {time.time() - t:.1f}s")
+    ns = args.c4_stars
+    rng = np.random.default_rng(4096)
+    lab = S.random_labels(spec, ns, seed=4096, vsini=(0.0, 300.0), rv=(-150.0, 150.0))
+    t = time.time()
+    stars = S.make_stars(spec, lab, rng.integers(10000, 60001, ns), rng.uniform(20.0, 200.0, ns), RESOLUTION,
+                         seed=4096)
+    log(f"[config4] {ns} stars in {time.time() - t:.1f}s")
+    disps = [P.FixedResolutionDispersion(s.wl, RESOLUTION, wl) for s in stars]
+    conts = [P.LinearModelContinuumFitter(S.legendre_design(s.wl, 40)) for s in stars]
+    Pn, It = 128, 300
+    settings = P.PSOSettings(Pn, It)
+    seeds = [int(11 + i) for i in range(ns)]
+    fl = [s.flux for s in stars]
+    vr = [s.var for s in stars]
+    srv = P.Server(interp, max_slots=ns)
+    per_step = -(-ns // (It + 1))
+    cursor = [0]
+
+    def feed(k):
+        for _ in range(k):
+            i = cursor[0] % ns
+            srv.submit(disps[i], conts[i], settings, fl[i], vr[i], (0.0, 300.0), (-150.0, 150.0),
+                       seed=seeds[i] + 7919 * (cursor[0] // ns))
+            cursor[0] += 1
+
+    t = time.time()
+    for _ in range(It + 1):
+        feed(per_step)
+        srv.step()
+        srv.poll(4096)
+    log(f"[config4] served ramp-up in {time.time() - t:.1f}s")
+    feed(per_step * (args.warmup + 2))
+    srv.run(args.warmup)
+    srv.poll(4096)
+    feed(per_step * (args.steps + 2))
+    torch.cuda.synchronize(dev)
+    st0 = srv.stats()
+    with ClockSampler(0) as clk:
+        ms = srv.run(args.steps)
+    torch.cuda.synchronize(dev)
+    st1 = srv.stats()
+    del srv
+    evals = st1["evals"] - st0["evals"]
+    served = evals / (ms / 1000.0) / (Pn * (It + 1))
+    # stage profile of a batched mid-fit step (roofline of the dominant kernel)
+    nb = min(ns, args.c4_batch)
+    b = P.BatchFit(interp, disps[:nb], conts[:nb], settings, fl[:nb], vr[:nb], (0.0, 300.0), (-150.0, 150.0),
+                   seeds=seeds[:nb])
+    b.step(It // 2)
+    prof = [b.profile_step() for _ in range(3)]
+    stage = {k: float(np.mean([p[k] for p in prof])) for k in prof[0]}
+    b.finish()
+    del b
+    # batched form end to end (fit_many from host arrays) on nb stars
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    res = P.fit_many(interp, disps[:nb], conts[:nb], settings, fl[:nb], vr[:nb], (0.0, 300.0), (-150.0, 150.0),
+                     seeds=seeds[:nb])
+    torch.cuda.synchronize(dev)
+    t_e2e = time.perf_counter() - t0
+    peak, peak_kind = measured_peaks()
+    br_s = stage["broaden_ms"] / 1000.0
+    br_bytes = (stage["broaden_blocks"] * BROADEN_BYTES_PER_BLOCK + stage["evals"] * BROADEN_BYTES_PER_EVAL
+                + stage["obs_px"] * BROADEN_BYTES_PER_OBS)
+    br_tf = stage["broaden_blocks"] * BROADEN_FLOPS_PER_BLOCK / br_s / 1e12
+    err = np.array([np.abs(np.array(r.label.as_list()) - s.label) for r, s in zip(res, stars[:nb])])
+    return {"config4": True, "metric": METRIC, "value": served, "unit": "fits/s",
+            "workload": "config 4: includes_factor grid 80x26x13 x 120000 px (%.1f GB), %d stars served in steady "
+                        "state (slots refilled), 40-column Legendre linear-model continuum, PSO %dx%d, R=85000"
+                        % (spectra.nbytes / 1e9, ns, Pn, It),
+            "served": {"fits_per_s": served, "evals_per_s": evals / (ms / 1000.0), "ms_per_step": ms / args.steps,
+                       "steps": args.steps},
+            "batched_e2e": {"stars": nb, "fits_per_s": nb / t_e2e, "seconds": t_e2e},
+            "stage_ms": {k: v for k, v in stage.items() if k.endswith("_ms")},
+            "roofline": {"bound": "hbm", "kernel": "k_broaden", "algorithmic_rate": br_bytes / br_s / 1e9,
+                         "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+                         "fp32": {"achieved": br_tf, "peak": FP32_PEAK_TFLOPS, "frac": br_tf / FP32_PEAK_TFLOPS}},
+            "label_error_vs_truth": {"median_abs": np.median(err, axis=0).tolist()},
+            "clocks": clk.summary(), "linear_tensor_cores": True,
+            "kernel_launches": int(_ffi.lib().pasta_kernel_launch_count())}
 
 
 def run_ours(args):
@@ -587,7 +819,7 @@ def cpu_baseline(O, og, stars, seeds, budget_s=20.0):
                       "fits/s = evals/s / %d" % (n, PARTICLES, e, t, nthreads, EVALS_PER_FIT)}
 
 
-def label_replay(O, og, stars, seeds, results):
+def label_replay(O, og, stars, seeds, results, disp=None):
     """Label errors of the device fits of a sample of the timed workload
     against the FP64 oracle replayed on the same draw stream (64 x 200, the
     same seeds), beside the error of the oracle's FP32 mirror of the
@@ -599,7 +831,7 @@ def label_replay(O, og, stars, seeds, results):
     gpu_err, f32_err, per = [], [], []
     t0 = time.perf_counter()
     for s, sd, r in zip(stars, seeds, results):
-        od = O.Disp(og, O.DISP_FIXED, s.wl, RESOLUTION)
+        od = disp(s) if disp else O.Disp(og, O.DISP_FIXED, s.wl, RESOLUTION)
         oc = O.Cont(O.CONT_CHUNK, s.wl, 8, 5, 0.2)
         r64, rc64 = O.fit(og, od, oc, st, s.flux[None], s.var[None], [sd], O.F64, nthreads=nthreads,
                           over_stars=False)
@@ -698,6 +930,16 @@ def main():
     ap.add_argument("--linear-k", type=int, default=40)
     ap.add_argument("--binary-only", action="store_true",
                     help="run only the binary-fit leg (with its CPU baseline unless --no-cpu) and print it")
+    ap.add_argument("--precision", action="store_true",
+                    help="run the precision study (R(lambda) 60k->90k, FFT rotation, FP32 path vs the FP64 oracle) "
+                         "and print it")
+    ap.add_argument("--precision-stars", type=int, default=256)
+    ap.add_argument("--precision-labels", type=int, default=10000)
+    ap.add_argument("--config4", action="store_true",
+                    help="run the config-4 workload (includes_factor grid at 120,000 px, 40-column linear-model "
+                         "continuum, PSO 128 x 300) served and batched, and print it")
+    ap.add_argument("--c4-stars", type=int, default=512, help="config-4 leg: served slots (stars)")
+    ap.add_argument("--c4-batch", type=int, default=256, help="config-4 leg: stars in the batched fit")
     ap.add_argument("--stages-only", action="store_true",
                     help="profiling aid: one mid-fit batched step, stage by stage, in an NVTX range 'stages'")
     args = ap.parse_args()
@@ -719,6 +961,12 @@ def main():
         from pasta_b200 import pasta as P
         from pasta_b200 import synth as S
         print(json.dumps(linear_leg(P, S, args.linear_labels, args.linear_k)), flush=True)
+        return
+    if args.precision:
+        print(json.dumps(precision_leg(args)), flush=True)
+        return
+    if args.config4:
+        print(json.dumps(config4_leg(args)), flush=True)
         return
     if args.binary_only:
         from pasta_b200 import pasta as P

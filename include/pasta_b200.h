@@ -117,6 +117,12 @@ int pasta_grid_destroy(pasta_grid *g);
  * reference); set: 0..512, for the batches and fits started afterwards */
 int pasta_grid_direct_max(const pasta_grid *g, int32_t *taps);
 int pasta_grid_set_direct_max(pasta_grid *g, int32_t taps);
+/* the measured group size (evaluations of one star sharing their 64
+ * neighbour rows) from which the interpolation runs on the tensor cores, 65
+ * = never (no counterpart in the reference); set: 8..65, for the batches and
+ * fits started afterwards; PASTA_INTERP_TC_MIN fixes it at grid creation */
+int pasta_grid_tc_min(const pasta_grid *g, int32_t *members);
+int pasta_grid_set_tc_min(pasta_grid *g, int32_t members);
 /* sizes: n_teff, n_m, n_logg, n_px, n_models (lib.rs:1436-1461) */
 int pasta_grid_shape(const pasta_grid *g, int64_t *out5);
 int pasta_grid_axis(const pasta_grid *g, int axis, double *out);

@@ -58,6 +58,8 @@ SIGNATURES = {
     "pasta_grid_destroy": (I, [P]),
     "pasta_grid_direct_max": (I, [P, P]),
     "pasta_grid_set_direct_max": (I, [P, C.c_int32]),
+    "pasta_grid_tc_min": (I, [P, P]),
+    "pasta_grid_set_tc_min": (I, [P, I]),
     "pasta_grid_shape": (I, [P, P]),
     "pasta_grid_axis": (I, [P, I, P]),
     "pasta_grid_logg_limits": (I, [P, P, P]),

@@ -25,6 +25,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/pasta_b200.h"
@@ -210,6 +211,8 @@ struct Workspace {
   DBuf<int> gcount;    // groups per segment
   DBuf<TcGroup> tcrec; // tensor-core interpolation groups, at each segment's first evaluation
   DBuf<int> tccount;   // tensor-core groups per segment
+  DBuf<int> tclist;    // indices of all tensor-core groups, and their count [1]
+  DBuf<int> tclist_count;
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
@@ -219,7 +222,7 @@ struct Workspace {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
-    tcrec.release(); tccount.release();
+    tcrec.release(); tccount.release(); tclist.release(); tclist_count.release();
     dlist.release(); dcount.release(); zpart.release();
     cap = 0;
     A.alloc((size_t)want * str);
@@ -232,6 +235,8 @@ struct Workspace {
     gcount.alloc((size_t)want);
     tcrec.alloc((size_t)want);
     tccount.alloc((size_t)want);
+    tclist.alloc((size_t)want);
+    tclist_count.alloc(1);
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
     dlist.alloc((size_t)want);
@@ -271,6 +276,7 @@ struct pasta_grid {
   int direct_max = 0;  // combined kernels of at most this many taps are broadened directly (measured)
   alignas(64) CUtensorMap tmap;  // TMA view of the resident rows (tensor-core interpolation)
   bool has_tmap = false;
+  int tc_min = 16;  // members from which a shared-row group is interpolated on the tensor cores (measured)
 };
 
 namespace {
@@ -828,7 +834,10 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   const bool tc = interp_tc_enabled() && g->has_tmap;
   b.tcrec = tc ? g->ws.tcrec.p : nullptr;
   b.tccount = g->ws.tccount.p;
+  b.tclist = g->ws.tclist.p;
+  b.tclist_count = g->ws.tclist_count.p;
   b.tmap = tc ? &g->tmap : nullptr;
+  b.tc_min = g->tc_min;
   b.bnd_stride = g->ws.bnd_stride;
   b.ccoef = g->ws.ccoef.p;
   b.cpart = g->ws.cpart.p;
@@ -1594,6 +1603,109 @@ void tune_direct(pasta_grid *g) {
   g->direct_max = best;
 }
 
+// The group size from which the tensor-core interpolation beats the CUDA
+// cores on this device and grid: 16 segments of 64 evaluations, each split
+// into groups of gs evaluations in distinct grid cubes, interpolated with
+// the tensor-core path on and off (CUDA events, best of 3 after a warm-up),
+// for gs on a ladder; the smallest gs at which the tensor cores win, and
+// every larger gs on the ladder, sets the threshold (SEG + 1: never).
+void tune_interp_tc(pasta_grid *g) {
+  g->tc_min = 16;
+  if (const char *ev = getenv("PASTA_INTERP_TC_MIN")) {
+    g->tc_min = std::max(TC_MIN_MEMBERS, std::min(SEG + 1, atoi(ev)));
+    return;
+  }
+  if (!g->has_tmap) return;
+  // label centres of distinct cubes (neighbour columns) around the grid's middle
+  std::vector<std::array<double, 3>> cubes;
+  std::vector<std::vector<int>> seen;
+  const int nt = (int)g->tv.size(), nm = (int)g->mv.size();
+  for (int i = 0; i + 1 < nt && cubes.size() < 64; i++)
+    for (int j = 0; j + 1 < nm && cubes.size() < 64; j++) {
+      const int ti = (nt / 2 + i) % (nt - 1), mj = (nm / 2 + j) % (nm - 1);
+      const double t = 0.5 * (g->tv[ti] + g->tv[ti + 1]), mh = 0.5 * (g->mv[mj] + g->mv[mj + 1]);
+      const int lo = std::max(g->llo[ti], g->llo[ti + 1]), hi = std::min(g->lhi[ti], g->lhi[ti + 1]);
+      if (hi <= lo) continue;
+      const double lg = 0.5 * (g->lv[(lo + hi) / 2] + g->lv[(lo + hi) / 2 + 1]);
+      int cols[64];
+      float w[64];
+      if (local_grid(g->hg, t, mh, lg, cols, w) != 0) continue;
+      std::vector<int> c(cols, cols + 64);
+      if (std::find(seen.begin(), seen.end(), c) != seen.end()) continue;
+      seen.push_back(c);
+      cubes.push_back({t, mh, lg});
+    }
+  if (cubes.size() < 8) return;
+  Ctx &C = ctx();
+  cudaStream_t s = C.stream;
+  const int E = 16 * SEG;
+  DevStar st = make_star(nullptr, nullptr, nullptr, nullptr, 0);
+  st.disp_kind = DISP_NONE;
+  DBuf<DevStar> ds;
+  ds.upload(&st, 1);
+  DBuf<double> dl;
+  dl.alloc((size_t)E * 5);
+  DBuf<int> de;
+  de.upload(std::vector<int>(E, 0));
+  ensure_workspace(g, E, 0);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const double dt = 0.05 * (g->tv[1] - g->tv[0]), dm = 0.05 * (g->mv[1] - g->mv[0]);
+  const int ladder[] = {8, 12, 16, 24, 32, 48};
+  int best = SEG + 1;
+  std::vector<double> lab((size_t)E * 5);
+  for (int gs : ladder) {
+    const int ng = SEG / gs;
+    for (int e = 0; e < E; e++) {
+      const int q = e / SEG, u = e % SEG, gi = std::min(u / gs, ng);
+      const auto &c = cubes[(size_t)(q * (ng + 1) + gi) % cubes.size()];
+      double *x = &lab[(size_t)e * 5];
+      x[0] = c[0] + dt * ((u % gs) % 7 - 3) / 3.0;
+      x[1] = c[1] + dm * ((u % gs) % 5 - 2) / 2.0;
+      x[2] = c[2];
+      x[3] = 0.0;
+      x[4] = 0.0;
+    }
+    CK(cudaMemcpy(dl.p, lab.data(), lab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    EvalArgs a;
+    a.stars = ds.p;
+    a.labels = dl.p;
+    a.eval_star = de.p;
+    a.E = E;
+    a.full_window = 1;
+    a.max_m = 1;
+    star_kinds({st}, a);
+    float tm[2];
+    for (int mode = 0; mode < 2; mode++) {
+      g->tc_min = mode ? gs : SEG + 1;
+      run_evals(g, a, s);
+      float bt = 1e30f;
+      for (int rep = 0; rep < 3; rep++) {
+        CK(cudaEventRecord(e0, s));
+        run_evals(g, a, s);
+        CK(cudaEventRecord(e1, s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        bt = std::min(bt, ms);
+      }
+      tm[mode] = bt;
+    }
+    if (getenv("PASTA_TUNE_VERBOSE"))
+      fprintf(stderr, "pasta_b200 tune: %lld px, groups of %d: CUDA cores %.4f ms, tensor cores %.4f ms\n",
+              (long long)g->npx, gs, tm[0], tm[1]);
+    if (tm[1] < tm[0]) {
+      if (best > SEG) best = gs;
+    } else {
+      best = SEG + 1;  // the tensor cores must win from the threshold on
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g->tc_min = best;
+}
+
 }  // namespace
 
 int pasta_grid_create(const double *labels, const uint16_t *spectra, const float *maxima, int64_t n_models,
@@ -1695,7 +1807,22 @@ int pasta_grid_create(const double *labels, const uint16_t *spectra, const float
     else if (wl_kind == WL_LOG) d.dvelo = M_LN10 * wl_b;
     else d.dvelo = 0.0;
     tune_direct(g.get());
+    tune_interp_tc(g.get());
     *out = g.release();
+  });
+}
+
+int pasta_grid_tc_min(const pasta_grid *g, int32_t *out) {
+  return guard([&] {
+    if (!g || !out) fail(PASTA_E_ARG, "grid and output required");
+    *out = g->tc_min;
+  });
+}
+int pasta_grid_set_tc_min(pasta_grid *g, int32_t members) {
+  return guard([&] {
+    if (!g) fail(PASTA_E_ARG, "grid required");
+    if (members < TC_MIN_MEMBERS || members > SEG + 1) fail(PASTA_E_ARG, "members must be in [%d, %d]", TC_MIN_MEMBERS, SEG + 1);
+    g->tc_min = members;
   });
 }
 

@@ -131,33 +131,29 @@ __device__ __forceinline__ uint32_t bf16_bits(float x) {
 }
 __device__ __forceinline__ float bf16_val(uint32_t bits) { return __uint_as_float(bits << 16); }
 
+// TMA of tile i's 64 rows (pixels lo + 128 i ...) into staging buffer i & 1
+__device__ __forceinline__ void issue_tile(const TcGroup &R, const CUtensorMap *map, uint32_t sbase, uint32_t full0,
+                                           uint32_t full1, int lo, int i) {
+  const uint32_t fb = (i & 1) ? full1 : full0;
+  const uint32_t dst = sbase + SB_STG + (uint32_t)((i & 1) * 64 * TPX * 2);
+  mbar_expect(fb, 64 * TPX * 2);
+  for (int k = 0; k < 64; k++) {
+    const int c = R.col[k] >= 0 ? R.col[k] : 0;  // a missing row has weight 0
+    tma_row(dst + (uint32_t)(k * TPX * 2), map, lo + i * TPX, c, fb);
+  }
+}
+
 }  // namespace
 
-// One CTA per (segment, tensor-core group, slab of TSLAB tiles).
+// Persistent CTAs over the items (tensor-core group, slab of TSLAB tiles)
+// of the groups k_group listed; tensor memory is allocated once per CTA and
+// the barriers' phases run on across items.
 __global__ void __launch_bounds__(TT) k_interp_tc(DevGrid G, EvalBatch b, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int s = blockIdx.x, gi = blockIdx.z, t = threadIdx.x, w = t >> 5;
-  if (gi >= b.tccount[s]) return;
-  int start, len;
-  {
-    const int L = b.seg_len > 0 ? b.seg_len : b.E;
-    const int spb = (L + SEG - 1) / SEG;
-    const int j = s / spb, q = s - j * spb;
-    start = j * L + q * SEG;
-    len = min(min(SEG, L - q * SEG), b.E - start);
-  }
-  if (len <= 0) return;
-  const TcGroup &R = b.tcrec[start + gi];
-  const int nm = R.nmem;
-  // this CTA's pixels: tiles [x0, x1) of the group's window, the tail after
-  // tail_start on the CUDA cores
-  const int slab0 = blockIdx.y * TSLAB * TPX;
-  const int lo = max(R.lo & ~(TPX - 1), slab0), hi = min(R.hi, slab0 + TSLAB * TPX);
-  if (lo >= hi) return;
-  const int tc_hi = min(hi, G.tail_start);
-  const int ntiles = tc_hi > lo ? (tc_hi - lo + TPX - 1) / TPX : 0;
-  const int NP = (nm + 15) & ~15;
-
+  const int t = threadIdx.x, w = t >> 5;
+  const int slabs = (G.npx + TSLAB * TPX - 1) / (TSLAB * TPX);
+  const int nitems = *b.tclist_count * slabs;
+  if ((int)blockIdx.x >= nitems) return;
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
   const uint32_t full0 = sbase + SB_MISC, full1 = full0 + 8, mbar_mma = full0 + 16;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + SB_MISC + 24);
@@ -170,153 +166,188 @@ __global__ void __launch_bounds__(TT) k_interp_tc(DevGrid G, EvalBatch b, const 
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *err = 0;
   }
-  if (w == 0 && ntiles > 0) {
+  if (w == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + SB_MISC + 24),
                  "r"(64)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  // the members' windows, and the weights: B_j[n][k] = B_j[n][64 + k]
-  if (t < SEG) {
-    const int e = t < nm ? R.member[t] : -1;
-    wlo[t] = e >= 0 ? b.prep[e].i_lo : 0;
-    whi[t] = e >= 0 ? b.prep[e].i_hi : 0;
-  }
-  for (int i = t; i < 64 * 64; i += TT) {
-    const int n = i >> 6, k = i & 63;
-    float wf = 0.0f;
-    if (n < nm && R.col[k] >= 0) wf = b.prep[R.member[n]].w[k] * R.f[k];
-    const uint32_t h0 = bf16_bits(wf);
-    const float r1 = wf - bf16_val(h0);
-    const uint32_t h1 = bf16_bits(r1);
-    const uint32_t h2 = bf16_bits(r1 - bf16_val(h1));
-    const uint32_t hs[3] = {h0, h1, h2};
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      unsigned short *bj = reinterpret_cast<unsigned short *>(sm + SB_B + j * 64 * TK * 2);
-      bj[kmaj16(n, k) >> 1] = (unsigned short)hs[j];
-      bj[kmaj16(n, 64 + k) >> 1] = (unsigned short)hs[j];
-    }
-  }
-  proxy_fence();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = ntiles > 0 ? *tslot : 0u;
-  const uint32_t idesc = idesc_bf16(TPX, NP > 0 ? NP : 16);
-  auto issue_tile = [&](int i) {  // TMA of tile i's 64 rows into staging i & 1
-    const uint32_t fb = (i & 1) ? full1 : full0;
-    const uint32_t dst = sbase + SB_STG + (uint32_t)((i & 1) * 64 * TPX * 2);
-    mbar_expect(fb, 64 * TPX * 2);
-    for (int k = 0; k < 64; k++) {
-      const int c = R.col[k] >= 0 ? R.col[k] : 0;  // a missing row has weight 0
-      tma_row(dst + (uint32_t)(k * TPX * 2), &tmap, lo + i * TPX, c, fb);
+  const uint32_t tmem = *tslot;
+  uint32_t uses0 = 0u, uses1 = 0u, uses_mma = 0u;  // completed phases of each barrier
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const TcGroup &R = b.tcrec[b.tclist[item / slabs]];
+    const int nm = R.nmem;
+    // this item's pixels: tiles over [lo, tc_hi) of the group's window, the
+    // tail after tail_start on the CUDA cores
+    const int slab0 = (item % slabs) * TSLAB * TPX;
+    const int lo = max(R.lo & ~(TPX - 1), slab0), hi = min(R.hi, slab0 + TSLAB * TPX);
+    if (lo >= hi) continue;
+    if (*err) {  // a wait ran out earlier in this CTA: fail this group as well
+      if (t < nm) b.prep[R.member[t]].status = S_TC_TIMEOUT;
+      continue;
     }
-  };
-  if (t == 0) {
-    if (ntiles > 0) issue_tile(0);
-    if (ntiles > 1) issue_tile(1);
-  }
-  bool ok = true;
-  for (int i = 0; i < ntiles && ok; i++) {
-    const int px0 = lo + i * TPX;
-    // rows of tile i staged
-    if (!mbar_wait((i & 1) ? full1 : full0, (uint32_t)((i >> 1) & 1))) atomicOr(err, 1);
-    // convert: pixel t, row k -> A[t][k] = 256 x high byte, A[t][64 + k] = low byte
-    {
-      const unsigned short *stg = reinterpret_cast<const unsigned short *>(sm + SB_STG + (i & 1) * 64 * TPX * 2);
-#pragma unroll
-      for (int k8 = 0; k8 < 64; k8 += 8) {
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const uint32_t u0 = stg[(k8 + 2 * q) * TPX + t], u1 = stg[(k8 + 2 * q + 1) * TPX + t];
-          // exact floats of the byte planes (below 2^23): f = bits(0x4B000000 | x) - 2^23
-          const float2 fh = __fadd2_rn(make_float2(__uint_as_float(0x4B000000u | (u0 & 0xFF00u)),
-                                                   __uint_as_float(0x4B000000u | (u1 & 0xFF00u))),
-                                       make_float2(-8388608.0f, -8388608.0f));
-          const float2 fl = __fadd2_rn(make_float2(__uint_as_float(0x4B000000u | (u0 & 0xFFu)),
-                                                   __uint_as_float(0x4B000000u | (u1 & 0xFFu))),
-                                       make_float2(-8388608.0f, -8388608.0f));
-          // at most 8 significant bits: the bf16 value is the top half of the f32
-          h[q] = __byte_perm(__float_as_uint(fh.x), __float_as_uint(fh.y), 0x7632);
-          l[q] = __byte_perm(__float_as_uint(fl.x), __float_as_uint(fl.y), 0x7632);
-        }
-        *reinterpret_cast<uint4 *>(sm + SB_A + kmaj16(t, k8)) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4 *>(sm + SB_A + kmaj16(t, 64 + k8)) = make_uint4(l[0], l[1], l[2], l[3]);
-      }
+    const int tc_hi = min(hi, G.tail_start);
+    const int ntiles = tc_hi > lo ? (tc_hi - lo + TPX - 1) / TPX : 0;
+    const int NP = (nm + 15) & ~15;
+    // the members' windows, and the weights: B_j[n][k] = B_j[n][64 + k]
+    if (t < SEG) {
+      const int e = t < nm ? R.member[t] : -1;
+      wlo[t] = e >= 0 ? b.prep[e].i_lo : 0;
+      whi[t] = e >= 0 ? b.prep[e].i_hi : 0;
+    }
+    for (int i = t; i < 64 * 64; i += TT) {
+      const int n = i >> 6, k = i & 63;
+      float wf = 0.0f;
+      if (n < nm && R.col[k] >= 0) wf = b.prep[R.member[n]].w[k] * R.f[k];
+      const uint32_t h0 = bf16_bits(wf);
+      const float r1 = wf - bf16_val(h0);
+      const uint32_t h1 = bf16_bits(r1);
+      const uint32_t h2 = bf16_bits(r1 - bf16_val(h1));
+      unsigned short *b0 = reinterpret_cast<unsigned short *>(sm + SB_B);
+      unsigned short *b1 = b0 + 64 * TK, *b2 = b1 + 64 * TK;
+      const int o0 = kmaj16(n, k) >> 1, o1 = kmaj16(n, 64 + k) >> 1;
+      b0[o0] = b0[o1] = (unsigned short)h0;
+      b1[o0] = b1[o1] = (unsigned short)h1;
+      b2[o0] = b2[o1] = (unsigned short)h2;
     }
     proxy_fence();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    ok = *err == 0;
-    if (!ok) break;
+    const uint32_t idesc = idesc_bf16(TPX, NP);
     if (t == 0) {
-      // the staging buffer is free again: tile i + 2 streams in
-      if (i + 2 < ntiles) issue_tile(i + 2);
-      const uint64_t da = desc16(sbase + SB_A);
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        const uint64_t db = desc16(sbase + SB_B + (uint32_t)(j * 64 * TK * 2));
-#pragma unroll
-        for (int ks = 0; ks < TK / 16; ks++)
-          mma_bf16(tmem, da + (uint64_t)((ks * 256) >> 4), db + (uint64_t)((ks * 256) >> 4), idesc,
-                   (j | ks) ? 1u : 0u);
-      }
-      mma_commit(mbar_mma);
+      if (ntiles > 0) issue_tile(R, &tmap, sbase, full0, full1, lo, 0);
+      if (ntiles > 1) issue_tile(R, &tmap, sbase, full0, full1, lo, 1);
     }
-    if (!mbar_wait(mbar_mma, (uint32_t)(i & 1))) atomicOr(err, 1);
-    tc_fence_after();
-    // read back: warp w holds pixels 32 w .. 32 w + 31 (tensor-memory lanes)
-    const int px = px0 + t;
-    const uint32_t lane = (uint32_t)(w * 32) << 16;
-    for (int c0 = 0; c0 < NP; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + lane + (uint32_t)c0, v);
+    bool ok = true;
+    for (int i = 0; i < ntiles; i++) {
+      const int px0 = lo + i * TPX;
+      const int sb = i & 1;
+      // rows of tile i staged
+      if (ok && !mbar_wait(sb ? full1 : full0, (sb ? uses1 : uses0) & 1u)) atomicOr(err, 1);
+      if (sb) uses1++;
+      else uses0++;
+      // convert: pixel t, row k -> A[t][k] = 256 x high byte, A[t][64 + k] = low byte
+      {
+        const unsigned short *stg = reinterpret_cast<const unsigned short *>(sm + SB_STG + sb * 64 * TPX * 2);
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int n = c0 + j;
-        if (n < nm && px >= wlo[n] && px < whi[n] && px < tc_hi) b.bufA[(size_t)R.member[n] * b.stride + px] = v[j];
+        for (int k8 = 0; k8 < 64; k8 += 8) {
+          uint32_t h[4], l[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const uint32_t u0 = stg[(k8 + 2 * q) * TPX + t], u1 = stg[(k8 + 2 * q + 1) * TPX + t];
+            // exact floats of the byte planes (below 2^23): f = bits(0x4B000000 | x) - 2^23
+            const float2 fh = __fadd2_rn(make_float2(__uint_as_float(0x4B000000u | (u0 & 0xFF00u)),
+                                                     __uint_as_float(0x4B000000u | (u1 & 0xFF00u))),
+                                         make_float2(-8388608.0f, -8388608.0f));
+            const float2 fl = __fadd2_rn(make_float2(__uint_as_float(0x4B000000u | (u0 & 0xFFu)),
+                                                     __uint_as_float(0x4B000000u | (u1 & 0xFFu))),
+                                         make_float2(-8388608.0f, -8388608.0f));
+            // at most 8 significant bits: the bf16 value is the top half of the f32
+            h[q] = __byte_perm(__float_as_uint(fh.x), __float_as_uint(fh.y), 0x7632);
+            l[q] = __byte_perm(__float_as_uint(fl.x), __float_as_uint(fl.y), 0x7632);
+          }
+          *reinterpret_cast<uint4 *>(sm + SB_A + kmaj16(t, k8)) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4 *>(sm + SB_A + kmaj16(t, 64 + k8)) = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+      }
+      proxy_fence();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      ok = *err == 0;
+      if (t == 0 && ok) {
+        // the staging buffer is free again: tile i + 2 streams in
+        if (i + 2 < ntiles) issue_tile(R, &tmap, sbase, full0, full1, lo, i + 2);
+        const uint64_t da = desc16(sbase + SB_A);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          const uint64_t db = desc16(sbase + SB_B + (uint32_t)(j * 64 * TK * 2));
+#pragma unroll
+          for (int ks = 0; ks < TK / 16; ks++)
+            mma_bf16(tmem, da + (uint64_t)((ks * 256) >> 4), db + (uint64_t)((ks * 256) >> 4), idesc,
+                     (j | ks) ? 1u : 0u);
+        }
+        mma_commit(mbar_mma);
+      }
+      if (ok) {
+        if (!mbar_wait(mbar_mma, uses_mma & 1u)) atomicOr(err, 1);
+        uses_mma++;
+        tc_fence_after();
+        // read back: warp w holds pixels 32 w .. 32 w + 31 (tensor-memory lanes)
+        const int px = px0 + t;
+        const uint32_t lane = (uint32_t)(w * 32) << 16;
+        for (int c0 = 0; c0 < NP; c0 += 16) {
+          float v[16];
+          tmem_ld16(tmem + lane + (uint32_t)c0, v);
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const int n = c0 + j;
+            if (n < nm && px >= wlo[n] && px < whi[n] && px < tc_hi)
+              b.bufA[(size_t)R.member[n] * b.stride + px] = v[j];
+          }
+        }
+        tc_fence_before();
+      }
+      __syncthreads();  // tensor memory and the A tile are free for the next tile
+      ok = *err == 0;
+    }
+    // tail pixels [tail_start, hi): the reference's extra 1/65535 (interpolate.rs:978)
+    if (ok && hi > G.tail_start) {
+      const int t0 = max(lo, G.tail_start);
+      const int npx = hi - t0;
+      for (int i = t; i < npx * nm; i += TT) {
+        const int n = i / npx, px = t0 + i % npx;
+        if (px < wlo[n] || px >= whi[n]) continue;
+        const EvalPrep &P = b.prep[R.member[n]];
+        float acc = 0.0f;
+        for (int k = 0; k < 64; k++) {
+          const int c = R.col[k];
+          if (c < 0) continue;
+          const float x = (float)G.spectra[(size_t)c * G.stride + px];
+          acc = fmaf(P.w[k], __fmul_rn(__fdiv_rn(x, 65535.0f), R.f[k]), acc);
+        }
+        b.bufA[(size_t)R.member[n] * b.stride + px] = acc;
       }
     }
-    tc_fence_before();
-    __syncthreads();  // tensor memory and the A tile are free for the next tile
-    ok = *err == 0;
+    if (!ok && t < nm) b.prep[R.member[t]].status = S_TC_TIMEOUT;
+    __syncthreads();  // the windows and weights are rewritten for the next item
   }
-  // tail pixels [tail_start, hi): the reference's extra 1/65535 (interpolate.rs:978)
-  if (ok && hi > G.tail_start) {
-    const int t0 = max(lo, G.tail_start);
-    const int npx = hi - t0;
-    for (int i = t; i < npx * nm; i += TT) {
-      const int n = i / npx, px = t0 + i % npx;
-      if (px < wlo[n] || px >= whi[n]) continue;
-      const EvalPrep &P = b.prep[R.member[n]];
-      float acc = 0.0f;
-      for (int k = 0; k < 64; k++) {
-        const int c = R.col[k];
-        if (c < 0) continue;
-        const float x = (float)G.spectra[(size_t)c * G.stride + px];
-        acc = fmaf(P.w[k], __fmul_rn(__fdiv_rn(x, 65535.0f), R.f[k]), acc);
-      }
-      b.bufA[(size_t)R.member[n] * b.stride + px] = acc;
-    }
+  // a tile whose barrier wait ran out may still have copies or products in
+  // flight: wait for them once more (bounded) before freeing tensor memory
+  if (*err && t == 0) {
+    mbar_wait(full0, uses0 & 1u);
+    mbar_wait(full1, uses1 & 1u);
+    mbar_wait(mbar_mma, uses_mma & 1u);
   }
-  if (!ok && t < nm) b.prep[R.member[t]].status = S_TC_TIMEOUT;
+  tc_fence_before();
   __syncthreads();
-  if (w == 0 && ntiles > 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64));
+  tc_fence_after();
+  if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64));
 }
 
 void launch_interp_tc(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0 || !b.tcrec || !b.tmap) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_interp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_TOTAL);
-    attr = true;
+  static int per_sm[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int fit = 1;
+  if (dev >= 0 && dev < 64) {
+    if (!per_sm[dev]) {
+      cudaFuncSetAttribute(k_interp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_TOTAL);
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_interp_tc, TT, SB_TOTAL) != cudaSuccess || n < 1) n = 1;
+      per_sm[dev] = n;
+    }
+    fit = per_sm[dev];
   }
-  const int slabs = (G.npx + TSLAB * TPX - 1) / (TSLAB * TPX);
-  dim3 grid(num_segments(b), slabs, TC_MAX_GROUPS);
-  k_interp_tc<<<grid, TT, SB_TOTAL, s>>>(G, b, *reinterpret_cast<const CUtensorMap *>(b.tmap));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // persistent: the CTAs that fit at once; each takes items in grid strides
+  k_interp_tc<<<sms * fit, TT, SB_TOTAL, s>>>(G, b, *reinterpret_cast<const CUtensorMap *>(b.tmap));
   count_launch();
 }
 

@@ -126,9 +126,13 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     int nt = 0;
     if (b.tcrec)
       for (int u = 0; u < SEG; u++)
-        if (ok[u] && lead[u] == u && cnt_l[u] >= TC_MIN_MEMBERS && nt < TC_MAX_GROUPS) tcg[u] = nt++;
+        if (ok[u] && lead[u] == u && cnt_l[u] >= max(b.tc_min, TC_MIN_MEMBERS) && nt < TC_MAX_GROUPS) tcg[u] = nt++;
     ntc = nt;
     if (b.tccount) b.tccount[s] = nt;
+    if (nt > 0) {
+      const int at = atomicAdd(b.tclist_count, nt);
+      for (int k = 0; k < nt; k++) b.tclist[at + k] = start + k;
+    }
     // the other evaluations in groups of at most GROUP_MAX, in evaluation order
     int n = 0;
     for (int u = 0; u < SEG; u++) {
@@ -146,12 +150,13 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     b.gcount[s] = n;
   }
   __syncthreads();
-  // tensor-core group records: slice g writes group g (thread t: row t, member t)
-  if (sl < ntc) {
+  // tensor-core group records: slice sl writes groups sl, sl + GROUP_SLICES,
+  // ... (thread t: row t, member t)
+  for (int tg = sl; tg < ntc; tg += GROUP_SLICES) {
     int l = -1;
     for (int u = 0; u < SEG; u++)
-      if (ok[u] && lead[u] == u && tcg[u] == sl) l = u;
-    TcGroup &T = b.tcrec[start + sl];
+      if (ok[u] && lead[u] == u && tcg[u] == tg) l = u;
+    TcGroup &T = b.tcrec[start + tg];
     const int c = b.prep[start + l].cols[t];
     T.col[t] = c;
     T.f[t] = c >= 0 ? G.factor[c] : 0.0f;
@@ -160,7 +165,6 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     const unsigned bal = __ballot_sync(0xffffffffu, mine);
     const int lane = t & 31;
     if (lane == 0) cnt[sl][t >> 5] = __popc(bal);
-    __syncwarp();
     asm volatile("bar.sync %0, %1;" ::"r"(1 + sl), "r"(SEG) : "memory");  // this slice's two warps
     if (mine) T.member[__popc(bal & ((1u << lane) - 1u)) + ((t >> 5) ? cnt[sl][0] : 0)] = e;
     if (t == 0) {
@@ -174,6 +178,7 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
       T.lo = lo;
       T.hi = hi;
     }
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + sl), "r"(SEG) : "memory");  // cnt[sl] is reused
   }
   __syncthreads();
   const int lane = tid & 31, wsl = t >> 5;  // warp within the slice
@@ -232,6 +237,7 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
 
 void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
+  if (b.tcrec) cudaMemsetAsync(b.tclist_count, 0, sizeof(int), s);
   k_group<<<num_segments(b), SEG * GROUP_SLICES, 0, s>>>(G, b);
   count_launch();
 }

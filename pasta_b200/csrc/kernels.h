@@ -21,11 +21,11 @@ struct __align__(16) GroupRec {
   int nmem, nn;           // members, compacted rows
 };
 
-// Evaluations with identical neighbour columns, TC_MIN_MEMBERS or more of
-// them in one segment, are interpolated together on the tensor cores
-// (interp_tc.cu): the group's rows are staged by TMA and its members'
-// weights are the columns of one matrix product.
-constexpr int TC_MIN_MEMBERS = 16, TC_MAX_GROUPS = SEG / TC_MIN_MEMBERS;
+// Evaluations with identical neighbour columns, EvalBatch::tc_min or more
+// of them in one segment (at least TC_MIN_MEMBERS), are interpolated
+// together on the tensor cores (interp_tc.cu): the group's rows are staged
+// by TMA and its members' weights are the columns of one matrix product.
+constexpr int TC_MIN_MEMBERS = 8, TC_MAX_GROUPS = SEG / TC_MIN_MEMBERS;
 struct __align__(16) TcGroup {
   int member[SEG];  // evaluation indices, ascending (first nmem valid)
   int col[64];      // the shared neighbour columns (-1: missing)
@@ -72,6 +72,9 @@ struct EvalBatch {
   GroupRec *grec;            // [E] groups of each segment, in order
   int *gcount;               // [segments] groups per segment
   TcGroup *tcrec;            // [E] tensor-core groups of each segment (null: none)
+  int *tclist;               // [E] indices into tcrec of all tensor-core groups, in any order
+  int *tclist_count;         // [1] their number (zeroed before k_group)
+  int tc_min;                // members a tensor-core group needs (TC_MIN_MEMBERS .. SEG; larger: none)
   int *tccount;              // [segments]
   const void *tmap;          // host pointer to the grid's TMA tensor map (null: no tensor-core path)
   const float *given;        // model given at the observed pixels (continuum utilities) or null

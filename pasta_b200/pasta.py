@@ -596,6 +596,19 @@ class _Interpolator:
     def direct_max(self, taps: int):
         check(lib().pasta_grid_set_direct_max(self._grid._h, int(taps)))
 
+    @property
+    def tc_min(self) -> int:
+        """Members from which a group of one star's evaluations sharing their 64
+        neighbour rows is interpolated on the tensor cores (65: never); measured
+        on this device when the grid was loaded (no counterpart in the reference)."""
+        v = C.c_int32()
+        check(lib().pasta_grid_tc_min(self._grid._h, C.byref(v)))
+        return int(v.value)
+
+    @tc_min.setter
+    def tc_min(self, members: int):
+        check(lib().pasta_grid_set_tc_min(self._grid._h, int(members)))
+
     def interpolate_linear(self, teff, m, logg) -> np.ndarray:
         """Trilinear interpolation over the 8 surrounding models
         (interpolate.rs:985-1028; lib.rs:1127-1139)."""

@@ -508,19 +508,26 @@ def test_interpolation_tensor_cores(env):
     cube = np.stack([rng.uniform(7010.0, 7240.0, 40), rng.uniform(0.01, 0.09, 40), rng.uniform(4.01, 4.24, 40)], 1)
     scat = S.random_labels(spec, 8, seed=3)[:, :3]
     lab = np.vstack([cube, scat])
-    tc = interp.interpolate_bulk(lab)
-    _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(0))
+    keep = interp.tc_min
+    assert 8 <= keep <= 65
+    interp.tc_min = 16
     try:
-        cc = interp.interpolate_bulk(lab)
+        tc = interp.interpolate_bulk(lab)
+        half = interp.interpolate_bulk(cube[:20])
+        _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(0))
+        try:
+            cc = interp.interpolate_bulk(lab)
+        finally:
+            _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(1))
     finally:
-        _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(1))
+        interp.tc_min = keep
     for i in range(len(lab)):
         ref = og.interpolate(*lab[i], O.F32)
         assert relmax(tc[i], ref) <= FLUX_TOL, i
     assert np.abs(tc - cc).max() <= 2e-6 * np.abs(cc).max()
     np.testing.assert_array_equal(tc[40:], cc[40:])  # scattered labels: CUDA cores either way
-    half = interp.interpolate_bulk(cube[:20])
     np.testing.assert_array_equal(half, tc[:20])
+    print("tensor-core group threshold measured on this device: %d members" % keep)
 
 
 def test_chi2_bulk_one_batched_pass(env):
