@@ -118,7 +118,7 @@ def make_grid_factor_gpu(spec):
         d = torch.from_numpy(lm.depths(lab).astype(np.float32)).cuda()
         f = (1.0 - d @ prof).clamp_(min=0.0)
         t = torch.from_numpy(lab[:, 0]).cuda()[:, None]
-        bb = (1.0 / (wlt[None, :] ** 5 * torch.expm1(hc_k / (wlt[None, :] * t)))).to(torch.float32)
+        bb = (1.0 / (wlt[None, :] ** 5 * torch.expm1(hc_k / (wlt[None, :] * t))) / S.BB_REF).to(torch.float32)
         f = f * bb
         mx = f.max(dim=1).values
         factors[s0:s0 + 1024] = mx.cpu().numpy()

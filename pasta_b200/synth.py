@@ -129,11 +129,16 @@ class LineModel:
         return np.clip(f, 0.0, None)
 
 
+HC_K = 1.4387769e8  # h c / k in Angstrom K
+# Planck's wavelength dependence of a 5772 K blackbody at 5000 A: the unit of
+# blackbody(), so that grid maxima and flux ratios are of order one
+BB_REF = 1.0 / (5000.0 ** 5 * np.expm1(HC_K / (5000.0 * 5772.0)))
+
+
 def blackbody(wl_a: np.ndarray, teff: float) -> np.ndarray:
-    """Planck B_lambda(T) up to a constant, wavelengths in Angstrom."""
-    hc_k = 1.4387769e8  # h c / k in Angstrom K
-    x = hc_k / (wl_a * teff)
-    return 1.0 / (wl_a ** 5 * np.expm1(x))
+    """Planck B_lambda(T) relative to a 5772 K blackbody at 5000 A, wavelengths in Angstrom."""
+    x = HC_K / (wl_a * teff)
+    return 1.0 / (wl_a ** 5 * np.expm1(x)) / BB_REF
 
 
 def gridpoints(spec: GridSpec) -> np.ndarray:
@@ -357,8 +362,7 @@ def make_stars(spec: GridSpec, labels: np.ndarray, n_obs, snr, resolution: float
 def continuum_shape(wl: np.ndarray, teff: float, m: float, logg: float) -> np.ndarray:
     """Unnormalised continuum of a model: the blackbody at Teff relative to a
     5772 K blackbody at 5000 A, scaled smoothly with [M/H] and logg."""
-    ref = blackbody(np.array([5000.0]), 5772.0)[0]
-    return blackbody(wl, teff) / ref * (1.0 + 0.05 * m + 0.02 * (logg - 4.0))
+    return blackbody(wl, teff) * (1.0 + 0.05 * m + 0.02 * (logg - 4.0))
 
 
 def make_continuum_grid(spec: GridSpec):
