@@ -1335,39 +1335,8 @@ void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   count_launch();
 }
 
-// The chunk kernels take evaluations in groups of chunk_cg<K>() consecutive
-// ones: the members of a group that belong to one star (the particles of a
-// swarm) share each pixel's loads of flux, variance and chunk coordinates
-// and its Legendre values; each member keeps its own sums, so its result does
-// not depend on the others.  Members of another star are taken in a further
-// pass of the same warp.
-template <int K>
-__host__ __device__ constexpr int chunk_cg() {
-  return K <= 2 ? 4 : (K <= 8 ? 2 : 1);
-}
-
-// the live members (status 0) of the group starting at e0, as a bit mask
-template <int NG>
-__device__ __forceinline__ unsigned chunk_live(const EvalBatch &b, int e0) {
-  unsigned m = 0u;
-#pragma unroll
-  for (int g = 0; g < NG; g++)
-    if (e0 + g < b.E && b.prep[e0 + g].status == 0) m |= 1u << g;
-  return m;
-}
-// the members of `todo` that share the star of its lowest member
-template <int NG>
-__device__ __forceinline__ unsigned chunk_same_star(const EvalBatch &b, int e0, unsigned todo, int &star) {
-  star = b.prep[e0 + __ffs(todo) - 1].star;
-  unsigned m = 0u;
-#pragma unroll
-  for (int g = 0; g < NG; g++)
-    if ((todo >> g & 1u) && b.prep[e0 + g].star == star) m |= 1u << g;
-  return m;
-}
-
 // ChunkFitter::fit_continuum (continuum_fitting.rs:382-396), one warp per
-// (group of evaluations, chunk): the unweighted least-squares polynomial of
+// (evaluation, chunk): the unweighted least-squares polynomial of
 // flux/model over the chunk (216-226) is the projection onto the chunk's
 // polynomial space; it is solved here in a Legendre basis with the FP64
 // Cholesky factor of its Gram matrix (the same space as the reference's
@@ -1380,97 +1349,80 @@ __device__ __forceinline__ unsigned chunk_same_star(const EvalBatch &b, int e0, 
 // walks the whole chunk (no block barriers), so the loads of many chunks
 // are in flight per SM.
 template <int K>
-__global__ void __launch_bounds__(CT, 2) k_chunk_moments(EvalBatch b) {
-  constexpr int NG = chunk_cg<K>(), CU = 4;
-  const int lane = threadIdx.x & 31;
-  const long long gw = (long long)blockIdx.x * CW + (threadIdx.x >> 5);
-  const int ngr = (b.E + NG - 1) / NG;
-  if (gw >= (long long)ngr * b.max_chunks) return;
-  const int e0 = (int)(gw / b.max_chunks) * NG, c = (int)(gw % b.max_chunks);
-  unsigned todo = chunk_live<NG>(b, e0);
-  while (todo) {
-    int star;
-    const unsigned mask = chunk_same_star<NG>(b, e0, todo, star);
-    todo &= ~mask;
-    const DevStar &st = b.stars[star];
-    if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) continue;
-    const float *flux = st.flux;
-    const float *mod[NG];
+__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch b) {
+  __shared__ double zs[CW][MAX_P1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long gw = (long long)blockIdx.x * CW + warp;
+  if (gw >= (long long)b.E * b.max_chunks) return;
+  const int e = (int)(gw / b.max_chunks), c = (int)(gw % b.max_chunks);
+  const EvalPrep &P = b.prep[e];
+  if (P.status) return;
+  const DevStar &st = b.stars[P.star];
+  if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
+  const float *mod = model_row(b, P, e), *flux = st.flux;
+  const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
+  constexpr int CU = chunk_cu<K>();
+  double z[K];
 #pragma unroll
-    for (int g = 0; g < NG; g++) mod[g] = (mask >> g & 1u) ? model_row(b, b.prep[e0 + g], e0 + g) : nullptr;
-    const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
-    double z[NG][K];
+  for (int k = 0; k < K; k++) z[k] = 0.0;
+  // loads of CU pixels are issued before any arithmetic on them (the f32
+  // division has a slow path the compiler will not schedule loads across)
+  for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
+    float fl[CU], md[CU], xf[CU];
 #pragma unroll
-    for (int g = 0; g < NG; g++)
-#pragma unroll
-      for (int k = 0; k < K; k++) z[g][k] = 0.0;
-    // loads of CU pixels are issued before any arithmetic on them (the f32
-    // division has a slow path the compiler will not schedule loads across)
-    for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
-      float fl[CU], xf[CU], md[NG][CU];
-#pragma unroll
-      for (int u = 0; u < CU; u++) {
-        const int i = min(i0 + 32 * u, hi - 1);
-        fl[u] = flux[i];
-        xf[u] = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
-#pragma unroll
-        for (int g = 0; g < NG; g++) md[g][u] = (mask >> g & 1u) ? mod[g][i] : 1.0f;
-      }
-      float zp[NG][K];
-#pragma unroll
-      for (int g = 0; g < NG; g++)
-#pragma unroll
-        for (int k = 0; k < K; k++) zp[g][k] = 0.0f;
-#pragma unroll
-      for (int u = 0; u < CU; u++) {
-        if (i0 + 32 * u < hi) {
-          float Pk[K];
-          legendre<K>(xf[u], Pk);
-#pragma unroll
-          for (int g = 0; g < NG; g++) {
-            const float y = fl[u] / md[g][u];
-#pragma unroll
-            for (int k = 0; k < K; k++) zp[g][k] = fmaf(Pk[k], y, zp[g][k]);
-          }
-        }
-      }
-#pragma unroll
-      for (int g = 0; g < NG; g++)
-#pragma unroll
-        for (int k = 0; k < K; k++) z[g][k] += (double)zp[g][k];
+    for (int u = 0; u < CU; u++) {
+      const int i = min(i0 + 32 * u, hi - 1);
+      fl[u] = flux[i];
+      md[u] = mod[i];
+      xf[u] = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
     }
-    const double *L = st.chol + (size_t)c * K * K;
+    float zp[K];
 #pragma unroll
-    for (int g = 0; g < NG; g++) {
-      if (!(mask >> g & 1u)) continue;
-      double a[K];
+    for (int k = 0; k < K; k++) zp[k] = 0.0f;
 #pragma unroll
-      for (int k = 0; k < K; k++) a[k] = warp_sum(z[g][k]);
-      if (lane == 0) {  // FP64 Cholesky solve G a = z
-        for (int k = 0; k < K; k++) {
-          double t = a[k];
-          for (int j = 0; j < k; j++) t -= L[k * K + j] * a[j];
-          a[k] = t / L[k * K + k];
-        }
-        for (int k = K - 1; k >= 0; k--) {
-          double t = a[k];
-          for (int j = k + 1; j < K; j++) t -= L[j * K + k] * a[j];
-          a[k] = t / L[k * K + k];
-        }
-        const int e = e0 + g;
-        float *cf = b.ccoef + ((size_t)e * MAX_CHUNKS + c) * MAX_P1;
-        for (int k = 0; k < K; k++) cf[k] = (float)a[k];
-        if (b.params) {
-          double *par = b.params + (size_t)e * b.param_stride + c * K;
-          for (int k = 0; k < K; k++) par[k] = a[k];
-        }
+    for (int u = 0; u < CU; u++) {
+      if (i0 + 32 * u < hi) {
+        const float y = fl[u] / md[u];
+        float Pk[K];
+        legendre<K>(xf[u], Pk);
+#pragma unroll
+        for (int k = 0; k < K; k++) zp[k] = fmaf(Pk[k], y, zp[k]);
       }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) z[k] += (double)zp[k];
+  }
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const double t = warp_sum(z[k]);
+    if (lane == 0) zs[warp][k] = t;
+  }
+  if (lane == 0) {  // FP64 Cholesky solve G a = z, in place
+    double *a = zs[warp];
+    const double *L = st.chol + (size_t)c * K * K;
+    for (int k = 0; k < K; k++) {
+      double t = a[k];
+      for (int j = 0; j < k; j++) t -= L[k * K + j] * a[j];
+      a[k] = t / L[k * K + k];
+    }
+    for (int k = K - 1; k >= 0; k--) {
+      double t = a[k];
+      for (int j = k + 1; j < K; j++) t -= L[j * K + k] * a[j];
+      a[k] = t / L[k * K + k];
+    }
+    float *cf = b.ccoef + ((size_t)e * MAX_CHUNKS + c) * MAX_P1;
+    for (int k = 0; k < K; k++) cf[k] = (float)a[k];
+    if (b.params) {
+      double *par = b.params + (size_t)e * b.param_stride + c * K;
+      for (int k = 0; k < K; k++) par[k] = a[k];
     }
   }
 }
 
 template <int K>
-__device__ __forceinline__ float poly_eval_r(const float (&coef)[K], const float (&P)[K]) {
+__device__ __forceinline__ float poly_eval_r(const float (&coef)[K], float x) {
+  float P[K];
+  legendre<K>(x, P);
   float s = 0.0f;
 #pragma unroll
   for (int k = 0; k < K; k++) s = fmaf(coef[k], P[k], s);
@@ -1480,124 +1432,88 @@ __device__ __forceinline__ float poly_eval_r(const float (&coef)[K], const float
 // chi2 section of chunk c (continuum_fitting.rs:280-360): chunk 0 alone on
 // [50, start_1); chunk c >= 1 blended with chunk c - 1 (sin^2 factor) on
 // [start_c, stop_{c-1}), then alone up to start_{c+1} (N - 50 for the
-// last).  One warp per (group of evaluations, section); a lane adds each
-// member's terms of the pixels it loads together in f32 and those partials
-// in FP64; section sums in FP64, added in chunk order by k_chunk_final.
+// last).  One warp per section; a lane adds the terms of the pixels it
+// loads together in f32 and those partials in FP64; section sums in FP64,
+// added in chunk order by k_chunk_final.
 template <int K>
-__global__ void __launch_bounds__(CT, 2) k_chunk_resid(EvalBatch b) {
-  constexpr int NG = chunk_cg<K>(), CU = 4;
+__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b) {
   const int lane = threadIdx.x & 31;
   const long long gw = (long long)blockIdx.x * CW + (threadIdx.x >> 5);
-  const int ngr = (b.E + NG - 1) / NG;
-  if (gw >= (long long)ngr * b.max_chunks) return;
-  const int e0 = (int)(gw / b.max_chunks) * NG, c = (int)(gw % b.max_chunks);
-  unsigned todo = chunk_live<NG>(b, e0);
-  while (todo) {
-    int star;
-    const unsigned mask = chunk_same_star<NG>(b, e0, todo, star);
-    todo &= ~mask;
-    const DevStar &st = b.stars[star];
-    if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) continue;
-    const int N = st.n_obs, nc = st.n_chunks;
-    const float *flux = st.flux, *var = st.var;
-    const float *mod[NG];
-    float cc[NG][K], cp[NG][K];
+  if (gw >= (long long)b.E * b.max_chunks) return;
+  const int e = (int)(gw / b.max_chunks), c = (int)(gw % b.max_chunks);
+  const EvalPrep &P = b.prep[e];
+  if (P.status) return;
+  const DevStar &st = b.stars[P.star];
+  if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
+  const int N = st.n_obs, nc = st.n_chunks;
+  const float *mod = model_row(b, P, e), *flux = st.flux, *var = st.var;
+  const float *coef = b.ccoef + (size_t)e * MAX_CHUNKS * MAX_P1;
+  float cc[K], cp[K];
 #pragma unroll
-    for (int g = 0; g < NG; g++) {
-      const bool on = mask >> g & 1u;
-      mod[g] = on ? model_row(b, b.prep[e0 + g], e0 + g) : nullptr;
-      const float *coef = b.ccoef + (size_t)(e0 + g) * MAX_CHUNKS * MAX_P1;
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        cc[g][k] = on ? coef[c * MAX_P1 + k] : 0.0f;
-        cp[g][k] = (on && c > 0) ? coef[(c - 1) * MAX_P1 + k] : 0.0f;
-      }
-    }
-    double acc[NG];
-#pragma unroll
-    for (int g = 0; g < NG; g++) acc[g] = 0.0;
-    // [lo, hi) with chunk c alone; loads of CU pixels before their arithmetic
-    auto alone = [&](int lo, int hi) {
-      for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
-        float fl[CU], vr[CU], xa[CU], md[NG][CU];
-#pragma unroll
-        for (int u = 0; u < CU; u++) {
-          const int i = min(i0 + 32 * u, hi - 1);
-          fl[u] = flux[i];
-          vr[u] = var[i];
-          xa[u] = st.xa[i];
-#pragma unroll
-          for (int g = 0; g < NG; g++) md[g][u] = (mask >> g & 1u) ? mod[g][i] : 0.0f;
-        }
-        float part[NG];  // each member's CU terms in f32, then one FP64 add
-#pragma unroll
-        for (int g = 0; g < NG; g++) part[g] = 0.0f;
-#pragma unroll
-        for (int u = 0; u < CU; u++) {
-          if (i0 + 32 * u < hi) {
-            float Pk[K];
-            legendre<K>(xa[u], Pk);
-#pragma unroll
-            for (int g = 0; g < NG; g++) {
-              const float p = poly_eval_r<K>(cc[g], Pk);
-              const float r = fl[u] - p * md[g][u];
-              part[g] += r * r / vr[u];
-            }
-          }
-        }
-#pragma unroll
-        for (int g = 0; g < NG; g++) acc[g] += (double)part[g];
-      }
-    };
-    if (c == 0) {
-      alone(50, st.cstart[1]);
-    } else {
-      const int s0 = st.cstart[c], sp = st.cstop[c - 1];
-      const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
-      for (int i0 = s0 + lane; i0 < sp; i0 += 32 * 2) {  // overlap: blend previous and current
-        float fl[2], vr[2], xa[2], xb[2], fc[2], md[NG][2];
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const int i = min(i0 + 32 * u, sp - 1);
-          fl[u] = flux[i];
-          vr[u] = var[i];
-          xa[u] = st.xa[i];
-          xb[u] = st.xb[i];
-          fc[u] = st.fac[i];
-#pragma unroll
-          for (int g = 0; g < NG; g++) md[g][u] = (mask >> g & 1u) ? mod[g][i] : 0.0f;
-        }
-        float part[NG];
-#pragma unroll
-        for (int g = 0; g < NG; g++) part[g] = 0.0f;
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-          if (i0 + 32 * u < sp) {
-            float Pa[K], Pb[K];
-            legendre<K>(xa[u], Pa);
-            legendre<K>(xb[u], Pb);
-#pragma unroll
-            for (int g = 0; g < NG; g++) {
-              const float pv = poly_eval_r<K>(cp[g], Pa);
-              const float cu = poly_eval_r<K>(cc[g], Pb);
-              const float p = pv * fc[u] + cu * (1.0f - fc[u]);
-              const float r = fl[u] - p * md[g][u];
-              part[g] += r * r / vr[u];
-            }
-          }
-        }
-#pragma unroll
-        for (int g = 0; g < NG; g++) acc[g] += (double)part[g];
-      }
-      alone(sp, nx);
-    }
-#pragma unroll
-    for (int g = 0; g < NG; g++) {
-      if (!(mask >> g & 1u)) continue;
-      const double t = warp_sum(acc[g]);
-      if (lane == 0) b.cpart[(size_t)(e0 + g) * MAX_CHUNKS + c] = t;
-    }
+  for (int k = 0; k < K; k++) {
+    cc[k] = coef[c * MAX_P1 + k];
+    cp[k] = c > 0 ? coef[(c - 1) * MAX_P1 + k] : 0.0f;
   }
+  double acc = 0.0;
+  constexpr int CU = chunk_cu<K>();
+  // [lo, hi) with chunk c alone; loads of CU pixels before their arithmetic
+  auto alone = [&](int lo, int hi) {
+    for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
+      float fl[CU], md[CU], vr[CU], xa[CU];
+#pragma unroll
+      for (int u = 0; u < CU; u++) {
+        const int i = min(i0 + 32 * u, hi - 1);
+        fl[u] = flux[i];
+        md[u] = mod[i];
+        vr[u] = var[i];
+        xa[u] = st.xa[i];
+      }
+      float part = 0.0f;  // the lane's CU terms in f32, then one FP64 add
+#pragma unroll
+      for (int u = 0; u < CU; u++) {
+        if (i0 + 32 * u < hi) {
+          const float p = poly_eval_r<K>(cc, xa[u]);
+          const float r = fl[u] - p * md[u];
+          part += r * r / vr[u];
+        }
+      }
+      acc += (double)part;
+    }
+  };
+  if (c == 0) {
+    alone(50, st.cstart[1]);
+  } else {
+    const int s0 = st.cstart[c], sp = st.cstop[c - 1];
+    const int nx = c == nc - 1 ? N - 50 : st.cstart[c + 1];
+    for (int i0 = s0 + lane; i0 < sp; i0 += 32 * 2) {  // overlap: blend previous and current
+      float fl[2], md[2], vr[2], xa[2], xb[2], fc[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int i = min(i0 + 32 * u, sp - 1);
+        fl[u] = flux[i];
+        md[u] = mod[i];
+        vr[u] = var[i];
+        xa[u] = st.xa[i];
+        xb[u] = st.xb[i];
+        fc[u] = st.fac[i];
+      }
+      float part = 0.0f;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (i0 + 32 * u < sp) {
+          const float pv = poly_eval_r<K>(cp, xa[u]);
+          const float cu = poly_eval_r<K>(cc, xb[u]);
+          const float p = pv * fc[u] + cu * (1.0f - fc[u]);
+          const float r = fl[u] - p * md[u];
+          part += r * r / vr[u];
+        }
+      }
+      acc += (double)part;
+    }
+    alone(sp, nx);
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) b.cpart[(size_t)e * MAX_CHUNKS + c] = acc;
 }
 
 // chi2 = sum of the section partials in chunk order / (N - 100); errors as NaN
@@ -1696,7 +1612,7 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b) {
 
 template <int K>
 static void launch_chunk(const EvalBatch &b, cudaStream_t s) {
-  const long long warps = (long long)((b.E + chunk_cg<K>() - 1) / chunk_cg<K>()) * b.max_chunks;
+  const long long warps = (long long)b.E * b.max_chunks;
   const unsigned grid = (unsigned)((warps + CW - 1) / CW);
   k_chunk_moments<K><<<grid, CT, 0, s>>>(b);
   k_chunk_resid<K><<<grid, CT, 0, s>>>(b);
