@@ -532,10 +532,21 @@ constexpr int BT = F2_T;      // threads of k_broaden
 constexpr int BR_FX = 2048;   // float indices of observed pixels prefetched per item
 // dynamic shared memory (bytes): exchange buffers 1 and 2 (buffer 2 also
 // holds the rotation outputs, buffer 1 the outputs of the instrument taps),
-// twiddles of passes 1 and 2, the item's observed float indices, the fixed
+// twiddles of pass 2, the item's observed float indices, the fixed
 // instrument taps
-constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T1 = BR_S2 + F2_S2 * 8, BR_T2 = BR_T1 + 16 * BT * 8,
-              BR_FXO = BR_T2 + 16 * 8 * 8, BR_GK = BR_FXO + BR_FX * 8, BR_SMEM = BR_GK + 512 * 4;
+constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T2 = BR_S2 + F2_S2 * 8, BR_FXO = BR_T2 + 16 * 8 * 8,
+              BR_GK = BR_FXO + BR_FX * 8, BR_SMEM = BR_GK + 512 * 4;
+
+// the pass-1 twiddle W_2048^(t k1) of this thread from W^t, W^2t, W^4t and
+// W^8t (table values, computed in double on the host) by at most three
+// products
+__device__ __forceinline__ cf tw_pass1(int k1, const cf &w1, const cf &w2, const cf &w4, const cf &w8) {
+  cf r = (k1 & 1) ? w1 : cf{1.0f, 0.0f};
+  if (k1 & 2) r = (k1 & 1) ? cmul(r, w2) : w2;
+  if (k1 & 4) r = (k1 & 3) ? cmul(r, w4) : w4;
+  if (k1 & 8) r = (k1 & 7) ? cmul(r, w8) : w8;
+  return r;
+}
 
 // One work item = two overlap-save blocks of one evaluation.  Block k yields
 // V = 2048 - (m - 1) - 2 hg final outputs starting at s_k = o_lo + k (V - 1):
@@ -559,23 +570,28 @@ constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T1 = BR_S2 + F2_S2 * 8, B
 // reaches memory.  The next item's inputs are loaded into registers and this
 // item's observed float indices copied into shared memory (cp.async) while
 // the transforms run.
-__global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) unsigned char br_smem[];
   float2 *S1 = reinterpret_cast<float2 *>(br_smem + BR_S1);
   float2 *S2 = reinterpret_cast<float2 *>(br_smem + BR_S2);
-  float2 *T1 = reinterpret_cast<float2 *>(br_smem + BR_T1);
   float2 *T2 = reinterpret_cast<float2 *>(br_smem + BR_T2);
   double *fxs = reinterpret_cast<double *>(br_smem + BR_FXO);
   float *gks = reinterpret_cast<float *>(br_smem + BR_GK);
   const int t = threadIdx.x, N = G.npx;
-  // twiddle tables: T1[k1][t] = W_2048^(t k1), T2[k2][n3] = W_128^(n3 k2)
-  for (int i = t; i < 16 * BT; i += BT) T1[i] = __ldg(&tw[((i & (BT - 1)) * (i >> 7)) & (FFTN - 1)]);
+  // twiddles: T2[k2][n3] = W_128^(n3 k2) in shared memory; W_2048^(t k1)
+  // from the four powers of two of W^t in registers
   for (int i = t; i < 16 * 8; i += BT) T2[i] = __ldg(&tw[(16 * (i & 7) * (i >> 3)) & (FFTN - 1)]);
+  cf tw1, tw2, tw4, tw8;
+  {
+    const float2 a = __ldg(&tw[t]), c = __ldg(&tw[2 * t]), d = __ldg(&tw[4 * t]), f = __ldg(&tw[8 * t]);
+    tw1 = cf{a.x, a.y};
+    tw2 = cf{c.x, c.y};
+    tw4 = cf{d.x, d.y};
+    tw8 = cf{f.x, f.y};
+  }
   ItemCursor cur;
   cur.init(b);
   cur.settle(b);
-  float in0[16], in1[16];
-  if (!cur.done()) broaden_inputs(b, cur, in0, in1);
   const int k1p = t >> 3, n3p = t & 7;  // pass-2 role of this thread
   while (!cur.done()) {
     ItemCursor nxt = cur;
@@ -598,7 +614,10 @@ __global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const
       q2 = has1 ? bd[2] : q1;
     }
     __syncthreads();  // the last item's epilogue is done with the shared buffers
-    // this item's observed float indices (uniform grids) and instrument taps
+    // this item's inputs, observed float indices (uniform grids, cp.async)
+    // and instrument taps
+    float in0[16], in1[16];
+    broaden_inputs(b, cur, in0, in1);
     const bool pre = P.epi && G.wl_kind != WL_NONUNI;
     if (pre) {
       const int nq = min(q2 - q0, BR_FX);
@@ -607,9 +626,6 @@ __global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const
     cp_async_commit();
     if (fixedk)
       for (int k = t; k < gw; k += BT) gks[k] = __ldg(&st.gk[k]);
-    // the next item's inputs stream into registers meanwhile
-    float nx0[16], nx1[16];
-    if (!nxt.done()) broaden_inputs(b, nxt, nx0, nx1);
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     const float sc = 1.0f / 2048.0f;
@@ -622,7 +638,7 @@ __global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const
       dft16<false>(v);
 #pragma unroll
       for (int k1 = 0; k1 < 16; k1++) {
-        const cf z = k1 ? cmul_tw<false>(v[k1], T1[k1 * BT + t]) : v[k1];
+        const cf z = k1 ? cmul(v[k1], tw_pass1(k1, tw1, tw2, tw4, tw8)) : v[k1];
         S1[k1 * F2_XP + t] = make_float2(z.x, z.y);
       }
       __syncthreads();
@@ -680,7 +696,10 @@ __global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const
 #pragma unroll
       for (int k1 = 0; k1 < 16; k1++) {
         const float2 z = S1[k1 * F2_XP + t];
-        v[k1] = k1 ? cmul_tw<true>(cf{z.x, z.y}, T1[k1 * BT + t]) : cf{z.x, z.y};
+        v[k1] = k1 ? cmul_tw<true>(cf{z.x, z.y}, [&] {
+          const cf q = tw_pass1(k1, tw1, tw2, tw4, tw8);
+          return make_float2(q.x, q.y);
+        }()) : cf{z.x, z.y};
       }
       dft16<true>(v);
       // FFT index i = 128 n1 + t holds rotation output (s - hg) + (i - (m - 1))
@@ -766,11 +785,6 @@ __global__ void __launch_bounds__(BT, 3) k_broaden(DevGrid G, EvalBatch b, const
       }
     }
     cur = nxt;
-#pragma unroll
-    for (int n1 = 0; n1 < 16; n1++) {
-      in0[n1] = nx0[n1];
-      in1[n1] = nx1[n1];
-    }
   }
 }
 
@@ -780,7 +794,7 @@ void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cuda
   static int per_sm[64] = {};  // resident CTAs per SM, per device
   int dev = 0;
   cudaGetDevice(&dev);
-  int fit = 3;
+  int fit = 4;
   if (dev >= 0 && dev < 64) {
     if (!per_sm[dev]) {
       cudaFuncSetAttribute(k_broaden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

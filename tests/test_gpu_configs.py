@@ -249,8 +249,9 @@ def test_config4_linear_continuum_tensor_cores(c4):
         _ffi.check(_ffi.lib().pasta_set_linear_tensor_cores(1))
     ref, st = O.chi2(c4["og"], od, oc, star.flux, star.var, labs, O.F64)
     assert (st == 0).all()
-    np.testing.assert_allclose(gpu, cc, rtol=5e-6)
     np.testing.assert_allclose(gpu, ref, rtol=CHI2_TOL)
+    np.testing.assert_allclose(cc, ref, rtol=CHI2_TOL)
+    np.testing.assert_allclose(gpu, cc, rtol=CHI2_TOL)
 
 
 # ------------------------------------------------------------ staircase
