@@ -764,6 +764,10 @@ def run_ours(args):
             hbm_view("k_chunk_moments+k_chunk_resid", chi2_bytes, stage["chi2_ms"], "chi2"),
         ],
         "dram_source": DRAM_SOURCE,
+        "tuned": {"direct_max_taps": interp.direct_max, "interp_tc_min_members": interp.tc_min,
+                  "what": "measured on this device at grid load: widest combined broadening kernel convolved "
+                          "directly, and the group size from which the interpolation runs on the tensor cores "
+                          "(65: never, the CUDA cores win at every size)"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
