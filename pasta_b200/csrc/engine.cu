@@ -213,8 +213,6 @@ struct Workspace {
   DBuf<int> tccount;   // tensor-core groups per segment
   DBuf<int> tclist;    // indices of all tensor-core groups, and their count [1]
   DBuf<int> tclist_count;
-  DBuf<int> glist;     // indices of all CUDA-core groups, and their count [1]
-  DBuf<int> glist_count;
   DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
@@ -224,8 +222,7 @@ struct Workspace {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
-    tcrec.release(); tccount.release(); tclist.release(); tclist_count.release(); glist.release();
-    glist_count.release();
+    tcrec.release(); tccount.release(); tclist.release(); tclist_count.release();
     dlist.release(); dcount.release(); zpart.release();
     cap = 0;
     A.alloc((size_t)want * str);
@@ -240,8 +237,6 @@ struct Workspace {
     tccount.alloc((size_t)want);
     tclist.alloc((size_t)want);
     tclist_count.alloc(1);
-    glist.alloc((size_t)want);
-    glist_count.alloc(1);
     ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
     dlist.alloc((size_t)want);
@@ -257,7 +252,7 @@ struct Workspace {
 // bytes of workspace one evaluation takes with rows of `stride` floats
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
   return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)sizeof(TcGroup) +
-         12 + (int64_t)bnd_stride * 4 +
+         8 + (int64_t)bnd_stride * 4 +
          (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8) + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8;
 }
 
@@ -841,8 +836,6 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.tccount = g->ws.tccount.p;
   b.tclist = g->ws.tclist.p;
   b.tclist_count = g->ws.tclist_count.p;
-  b.glist = g->ws.glist.p;
-  b.glist_count = g->ws.glist_count.p;
   b.tmap = tc ? &g->tmap : nullptr;
   b.tc_min = g->tc_min;
   b.bnd_stride = g->ws.bnd_stride;

@@ -148,10 +148,6 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     }
     ng = n;
     b.gcount[s] = n;
-    if (b.glist && n > 0) {
-      const int at = atomicAdd(b.glist_count, n);
-      for (int k = 0; k < n; k++) b.glist[at + k] = start + k;
-    }
   }
   __syncthreads();
   // tensor-core group records: slice sl writes groups sl, sl + GROUP_SLICES,
@@ -242,7 +238,6 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
 void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
   if (b.tcrec) cudaMemsetAsync(b.tclist_count, 0, sizeof(int), s);
-  if (b.glist) cudaMemsetAsync(b.glist_count, 0, sizeof(int), s);
   k_group<<<num_segments(b), SEG * GROUP_SLICES, 0, s>>>(G, b);
   count_launch();
 }
@@ -324,10 +319,10 @@ __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch
 // stays in L2; z = slice of the segment's groups (groups z, z + Z, ...), more
 // than one only for batches too small to fill the GPU otherwise.  Groups have
 // disjoint members, so the slicing does not change any result.
-__global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b, int y0) {
+__global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
   __shared__ GroupRec R;
   const int s = blockIdx.x;
-  const int px = (blockIdx.y + y0) * IT_TILE + threadIdx.x * 8;
+  const int px = blockIdx.y * IT_TILE + threadIdx.x * 8;
   const int ng = b.gcount[s];
   int start, len;
   seg_range(b, s, start, len);
@@ -346,184 +341,13 @@ __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b, int 
   }
 }
 
-// ------------------------------------------ staged CUDA-core interpolation
-// The same groups and arithmetic as k_interp, with the rows streamed into
-// shared memory by bulk copies (cp.async.bulk, the TMA unit) in chunks of
-// IS_CH rows x IT_TILE pixels, IS_NST chunks in flight ahead of the
-// arithmetic, across the items of a CTA: the loads are off the threads'
-// critical path, which k_interp spends waiting on them.  Items are (group of
-// the list k_group wrote, tile of IT_TILE pixels) in grid strides; only
-// tiles wholly below tail_start (the last tiles keep k_interp).
-constexpr int IS_CH = 8, IS_NST = 3;
-constexpr int IS_STAGE = IS_CH * IT_TILE * 2;  // bytes of one chunk
-constexpr int IS_SMEM = IS_NST * IS_STAGE + 8 * IS_NST + 16;
-
-__device__ __forceinline__ void bulk_copy(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(mbar)
-               : "memory");
-}
-__device__ __forceinline__ bool is_wait(uint32_t mbar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (clock64() - t0 > 2000000000ll) return false;
-  }
-}
-
-// the chunk producer (warp 0): the CTA's items in order, each item's chunks
-struct ChunkProducer {
-  int item, chunk, nitems, tiles;
-  uint32_t issued;
-  // issue the next chunk into stage issued % IS_NST; false when none is left
-  __device__ __forceinline__ bool next(const DevGrid &G, const EvalBatch &b, uint32_t sbase, uint32_t bar0,
-                                       int lane) {
-    while (item < nitems) {
-      const GroupRec &Rg = b.grec[b.glist[item / tiles]];
-      if (chunk < Rg.nn / IS_CH) {
-        const uint32_t st = issued % IS_NST, mbar = bar0 + 8 * st;
-        const int px0 = (item % tiles) * IT_TILE;
-        if (lane == 0)
-          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(IS_STAGE) : "memory");
-        __syncwarp();
-        if (lane < IS_CH)
-          bulk_copy(sbase + st * IS_STAGE + (uint32_t)(lane * IT_TILE * 2),
-                    G.spectra + (size_t)Rg.col[chunk * IS_CH + lane] * G.stride + px0, IT_TILE * 2, mbar);
-        chunk++;
-        issued++;
-        return true;
-      }
-      item += gridDim.x;
-      chunk = 0;
-    }
-    return false;
-  }
-};
-
-template <int NM>
-__device__ __forceinline__ void staged_item(const EvalBatch &b, const GroupRec &R, const int (&wlo)[GROUP_MAX],
-                                            const int (&whi)[GROUP_MAX], int px, const unsigned char *stg,
-                                            uint32_t bar0, uint32_t &consumed, ChunkProducer &pr, const DevGrid &G,
-                                            uint32_t sbase, int *err) {
-  const int t = threadIdx.x, lane = t & 31;
-  bool in[NM], any = false;
-#pragma unroll
-  for (int m = 0; m < NM; m++) {
-    in[m] = px >= wlo[m] && px < whi[m];
-    any |= in[m];
-  }
-  float2 acc[NM][4];
-#pragma unroll
-  for (int m = 0; m < NM; m++)
-#pragma unroll
-    for (int k = 0; k < 4; k++) acc[m][k] = make_float2(0.0f, 0.0f);
-  const float2 bias = make_float2(-8388608.0f, -8388608.0f);
-  const int nch = R.nn / IS_CH;
-  for (int c = 0; c < nch; c++) {
-    const uint32_t st = consumed % IS_NST;
-    if (!is_wait(bar0 + 8 * st, (consumed / IS_NST) & 1u)) atomicOr(err, 1);
-    if (any) {
-      const unsigned char *rows = stg + st * IS_STAGE + t * 16;
-#pragma unroll
-      for (int r = 0; r < IS_CH; r++) {
-        const uint4 q = *reinterpret_cast<const uint4 *>(rows + r * IT_TILE * 2);
-        const float4 w4 = R.wf[c * IS_CH + r];
-        const float ws[4] = {w4.x, w4.y, w4.z, w4.w};
-        const uint32_t u[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          float2 v = make_float2(__int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7410)),
-                                 __int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7432)));
-          v = __fadd2_rn(v, bias);  // exact u16 -> f32
-#pragma unroll
-          for (int m = 0; m < NM; m++) acc[m][k] = __ffma2_rn(make_float2(ws[m], ws[m]), v, acc[m][k]);
-        }
-      }
-    }
-    consumed++;
-    __syncthreads();  // the stage is free: the producer refills it
-    if ((t >> 5) == 0) pr.next(G, b, sbase, bar0, lane);
-  }
-#pragma unroll
-  for (int m = 0; m < NM; m++) {
-    if (!in[m]) continue;
-    float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)R.member[m] * b.stride + px);
-    out[0] = make_float4(acc[m][0].x, acc[m][0].y, acc[m][1].x, acc[m][1].y);
-    out[1] = make_float4(acc[m][2].x, acc[m][2].y, acc[m][3].x, acc[m][3].y);
-  }
-}
-
-__global__ void __launch_bounds__(IT_T, 2) k_interp_staged(DevGrid G, EvalBatch b, int tiles) {
-  extern __shared__ __align__(128) unsigned char ism[];
-  __shared__ GroupRec R;
-  __shared__ int wlo[GROUP_MAX], whi[GROUP_MAX];
-  const int t = threadIdx.x;
-  const int nitems = *b.glist_count * tiles;
-  if ((int)blockIdx.x >= nitems) return;
-  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(ism);
-  const uint32_t bar0 = sbase + IS_NST * IS_STAGE;
-  int *err = reinterpret_cast<int *>(ism + IS_NST * IS_STAGE + 8 * IS_NST);
-  if (t == 0) {
-    for (int k = 0; k < IS_NST; k++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8 * k) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    *err = 0;
-  }
-  __syncthreads();
-  ChunkProducer pr{(int)blockIdx.x, 0, nitems, tiles, 0u};
-  if ((t >> 5) == 0)
-    for (int k = 0; k < IS_NST; k++) pr.next(G, b, sbase, bar0, t & 31);
-  uint32_t consumed = 0;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int gi = b.glist[item / tiles];
-    const int px = (item % tiles) * IT_TILE + t * 8;
-    __syncthreads();  // the last item is done with the group record
-    {
-      const float4 *src = reinterpret_cast<const float4 *>(b.grec + gi);
-      float4 *dst = reinterpret_cast<float4 *>(&R);
-      for (int i = t; i < (int)(sizeof(GroupRec) / 16); i += IT_T) dst[i] = src[i];
-      if (t < GROUP_MAX) {
-        const int e = b.grec[gi].member[t];
-        wlo[t] = e >= 0 ? b.prep[e].i_lo : 0;
-        whi[t] = e >= 0 ? b.prep[e].i_hi : 0;
-      }
-    }
-    __syncthreads();
-    switch (R.nmem) {
-      case 1: staged_item<1>(b, R, wlo, whi, px, ism, bar0, consumed, pr, G, sbase, err); break;
-      case 2: staged_item<2>(b, R, wlo, whi, px, ism, bar0, consumed, pr, G, sbase, err); break;
-      case 3: staged_item<3>(b, R, wlo, whi, px, ism, bar0, consumed, pr, G, sbase, err); break;
-      default: staged_item<4>(b, R, wlo, whi, px, ism, bar0, consumed, pr, G, sbase, err); break;
-    }
-    if (*err && t < GROUP_MAX && R.member[t] >= 0) b.prep[R.member[t]].status = -99;  // a copy never arrived
-  }
-}
-
 void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
   const int segs = num_segments(b), tiles = (G.npx + IT_TILE - 1) / IT_TILE;
-  // tiles wholly below tail_start: staged kernel (when the group list is kept)
-  const int staged = b.glist ? G.tail_start / IT_TILE : 0;
-  if (staged > 0) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_interp_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, IS_SMEM);
-      attr = true;
-    }
-    k_interp_staged<<<num_sms() * 2, IT_T, IS_SMEM, s>>>(G, b, staged);
-    count_launch();
-  }
-  if (staged >= tiles) return;
-  const int rest = tiles - staged;
   const int want = num_sms() * 6;  // two waves of the 3 CTAs an SM holds
-  const int z = segs * rest >= want ? 1 : std::min(SEG, (want + segs * rest - 1) / (segs * rest));
-  dim3 grid(segs, rest, z);
-  k_interp<<<grid, IT_T, 0, s>>>(G, b, staged);
+  const int z = segs * tiles >= want ? 1 : std::min(SEG, (want + segs * tiles - 1) / (segs * tiles));
+  dim3 grid(segs, tiles, z);
+  k_interp<<<grid, IT_T, 0, s>>>(G, b);
   count_launch();
 }
 

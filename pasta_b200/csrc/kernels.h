@@ -72,8 +72,6 @@ struct EvalBatch {
   GroupRec *grec;            // [E] groups of each segment, in order
   int *gcount;               // [segments] groups per segment
   TcGroup *tcrec;            // [E] tensor-core groups of each segment (null: none)
-  int *glist;                // [E] indices into grec of all CUDA-core groups, in any order (null: none kept)
-  int *glist_count;          // [1] their number (zeroed before k_group)
   int *tclist;               // [E] indices into tcrec of all tensor-core groups, in any order
   int *tclist_count;         // [1] their number (zeroed before k_group)
   int tc_min;                // members a tensor-core group needs (TC_MIN_MEMBERS .. SEG; larger: none)
