@@ -171,15 +171,14 @@ __device__ __forceinline__ void fft_stage_pp(const float2 *src, float2 *dst, con
 // backwards (DFT-8, DFT-16, DFT-16 with conjugate twiddles), starting from
 // the spectrum where the forward transform left it, so a spectrum product
 // between them needs no reordering: a round trip costs four exchanges.
-// Both exchanges are XOR-swizzled so that every access of a half-warp
-// (64-bit values) touches 16 distinct bank pairs.  Twiddles come from per-CTA tables built from the host's
+// Exchange 1 rows are padded to F2_XP values and exchange 2 is XOR-swizzled
+// so that every access of a half-warp (64-bit values) touches 16 distinct
+// bank pairs.  Twiddles come from per-CTA tables built from the host's
 // double-precision table.
 constexpr int F2_T = 128;
-constexpr int F2_S1 = 2048;  // complex values of exchange buffer 1
-constexpr int F2_S2 = 2048;  // complex values of exchange buffer 2
-// exchange 1: row k1 (0..15), column j = 8 n2 + n3 (0..127)
-__device__ __forceinline__ int f2_a1(int k1, int j) { return 128 * k1 + (j ^ ((k1 & 1) << 3)); }
-// exchange 2: c = k1 + 16 k2 (0..255), n3 (0..7)
+constexpr int F2_XP = 136;
+constexpr int F2_S1 = 16 * F2_XP;  // complex values of exchange buffer 1
+constexpr int F2_S2 = 2048;        // complex values of exchange buffer 2
 __device__ __forceinline__ int f2_a2(int c, int n3) { return 8 * c + (n3 ^ ((c >> 1) & 7)); }
 
 // a * w (FWD) or a * conj(w) (INV)

@@ -529,13 +529,13 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 }
 
 constexpr int BT = F2_T;      // threads of k_broaden
-constexpr int BR_FX = 1536;   // float indices of observed pixels prefetched per item
+constexpr int BR_FX = 2048;   // float indices of observed pixels prefetched per item
 // dynamic shared memory (bytes): exchange buffers 1 and 2 (buffer 2 also
 // holds the rotation outputs, buffer 1 the outputs of the instrument taps),
-// twiddles of pass 2, the item's kernel half spectrum (1025 bins), the
-// item's observed float indices
-constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T2 = BR_S2 + F2_S2 * 8, BR_H = BR_T2 + 16 * 8 * 8,
-              BR_FXO = BR_H + 1040 * 8, BR_SMEM = BR_FXO + BR_FX * 8;
+// twiddles of pass 2, the item's observed float indices, the fixed
+// instrument taps
+constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T2 = BR_S2 + F2_S2 * 8, BR_FXO = BR_T2 + 16 * 8 * 8,
+              BR_GK = BR_FXO + BR_FX * 8, BR_SMEM = BR_GK + 512 * 4;
 
 // the pass-1 twiddle W_2048^(t k1) of this thread from W^t, W^2t, W^4t and
 // W^8t (table values, computed in double on the host) by at most three
@@ -575,8 +575,8 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
   float2 *S1 = reinterpret_cast<float2 *>(br_smem + BR_S1);
   float2 *S2 = reinterpret_cast<float2 *>(br_smem + BR_S2);
   float2 *T2 = reinterpret_cast<float2 *>(br_smem + BR_T2);
-  float2 *Hs = reinterpret_cast<float2 *>(br_smem + BR_H);
   double *fxs = reinterpret_cast<double *>(br_smem + BR_FXO);
+  float *gks = reinterpret_cast<float *>(br_smem + BR_GK);
   const int t = threadIdx.x, N = G.npx;
   // twiddles: T2[k2][n3] = W_128^(n3 k2) in shared memory; W_2048^(t k1)
   // from the four powers of two of W^t in registers
@@ -593,10 +593,6 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
   cur.init(b);
   cur.settle(b);
   const int k1p = t >> 3, n3p = t & 7;  // pass-2 role of this thread
-  // an item's inputs are loaded into registers while the item before it is
-  // resampled (they are not needed in between)
-  float in0[16], in1[16];
-  if (!cur.done()) broaden_inputs(b, cur, in0, in1);
   while (!cur.done()) {
     ItemCursor nxt = cur;
     nxt.advance();
@@ -617,21 +613,21 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
       q1 = bd[1];
       q2 = has1 ? bd[2] : q1;
     }
-    const int e_last = min((has1 ? s1 : s0) + V, ohi);
-    const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     __syncthreads();  // the last item's epilogue is done with the shared buffers
-    // this item's kernel half spectrum and observed float indices (uniform
-    // grids) stream into shared memory while the first passes run
-    if (m > 1) {
-      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
-      for (int k = t; k < 1025; k += BT) cp_async8(Hs + k, H + k);
-    }
+    // this item's inputs, observed float indices (uniform grids, cp.async)
+    // and instrument taps
+    float in0[16], in1[16];
+    broaden_inputs(b, cur, in0, in1);
     const bool pre = P.epi && G.wl_kind != WL_NONUNI;
     if (pre) {
       const int nq = min(q2 - q0, BR_FX);
       for (int i = t; i < nq; i += BT) cp_async8(fxs + i, st.fidx + q0 + i);
     }
     cp_async_commit();
+    if (fixedk)
+      for (int k = t; k < gw; k += BT) gks[k] = __ldg(&st.gk[k]);
+    const int e_last = min((has1 ? s1 : s0) + V, ohi);
+    const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     const float sc = 1.0f / 2048.0f;
     float *ob0, *ob1;  // final outputs u in [0, V) of the two blocks
     if (m > 1) {
@@ -643,13 +639,13 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
 #pragma unroll
       for (int k1 = 0; k1 < 16; k1++) {
         const cf z = k1 ? cmul(v[k1], tw_pass1(k1, tw1, tw2, tw4, tw8)) : v[k1];
-        S1[f2_a1(k1, t)] = make_float2(z.x, z.y);
+        S1[k1 * F2_XP + t] = make_float2(z.x, z.y);
       }
       __syncthreads();
       // pass 2: DFT-16 over n2, twiddle, exchange 2
 #pragma unroll
       for (int n2 = 0; n2 < 16; n2++) {
-        const float2 z = S1[f2_a1(k1p, 8 * n2 + n3p)];
+        const float2 z = S1[k1p * F2_XP + 8 * n2 + n3p];
         v[n2] = cf{z.x, z.y};
       }
       dft16<false>(v);
@@ -658,10 +654,10 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
         const cf z = k2 ? cmul_tw<false>(v[k2], T2[k2 * 8 + n3p]) : v[k2];
         S2[f2_a2(k1p + 16 * k2, n3p)] = make_float2(z.x, z.y);
       }
-      cp_async_wait_all();  // the kernel spectrum (and float indices) of this item
       __syncthreads();
       // pass 3 (DFT-8 over n3), the spectrum product, and the inverse DFT-8
       // over k3, for c = t and t + 128; each thread rewrites the slots it read
+      const float2 *H = (fold ? b.HG : b.H) + (size_t)e * 1025;
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int c = t + 128 * h;
@@ -670,7 +666,7 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
 #pragma unroll
         for (int k3 = 0; k3 < 8; k3++) {
           const int k = c + 256 * k3;
-          hk[k3] = Hs[k <= 1024 ? k : FFTN - k];
+          hk[k3] = __ldg(&H[k <= 1024 ? k : FFTN - k]);
           if (k > 1024) hk[k3].y = -hk[k3].y;
         }
 #pragma unroll
@@ -694,12 +690,12 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
       }
       dft16<true>(v);
 #pragma unroll
-      for (int n2 = 0; n2 < 16; n2++) S1[f2_a1(k1p, 8 * n2 + n3p)] = make_float2(v[n2].x, v[n2].y);
+      for (int n2 = 0; n2 < 16; n2++) S1[k1p * F2_XP + 8 * n2 + n3p] = make_float2(v[n2].x, v[n2].y);
       __syncthreads();
       // inverse pass 1: conjugate twiddle, DFT-16 over k1 -> 2048 x output 128 n1 + t
 #pragma unroll
       for (int k1 = 0; k1 < 16; k1++) {
-        const float2 z = S1[f2_a1(k1, t)];
+        const float2 z = S1[k1 * F2_XP + t];
         v[k1] = k1 ? cmul_tw<true>(cf{z.x, z.y}, [&] {
           const cf q = tw_pass1(k1, tw1, tw2, tw4, tw8);
           return make_float2(q.x, q.y);
@@ -736,9 +732,6 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
     }
     cp_async_wait_all();
     __syncthreads();
-    // the next item's inputs stream into registers during the taps and the
-    // resampling (this item's inputs are consumed)
-    if (!nxt.done()) broaden_inputs(b, nxt, in0, in1);
     if (!fold) {  // instrument taps from the rotation outputs in S2 into buffer 1
       ob0 = reinterpret_cast<float *>(S1);
       ob1 = ob0 + 2048;
@@ -752,7 +745,7 @@ __global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const
         } else if (fixedk) {  // g[i] = sum_k gk[k] r[i + hg - k]; r[i] sits at i - s + hg
           float a0 = 0.0f, a1 = 0.0f;
           for (int k = 0; k < gw; k++) {
-            const float g = __ldg(&st.gk[k]);
+            const float g = gks[k];
             const float2 x = S2[u + 2 * hg - k];
             a0 = fmaf(g, x.x, a0);
             a1 = fmaf(g, x.y, a1);
