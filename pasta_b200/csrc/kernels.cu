@@ -212,16 +212,18 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     if (act) {
       const int pos = __popc(bal & ((1u << lane) - 1u)) + (wsl ? cnt[sl][0] : 0);
       if (keep) {
-        R.wf[pos] = make_float4(wf[0], wf[1], wf[2], wf[3]);
-        R.w[pos] = make_float4(w[0], w[1], w[2], w[3]);
+        R.wf[pos][0] = make_float4(wf[0], wf[1], wf[2], wf[3]);
+        R.wf[pos][1] = make_float4(wf[4], wf[5], wf[6], wf[7]);
+        R.w[pos][0] = make_float4(w[0], w[1], w[2], w[3]);
+        R.w[pos][1] = make_float4(w[4], w[5], w[6], w[7]);
         R.col[pos] = c;
         R.f[pos] = f;
       }
       const int kept = cnt[sl][0] + cnt[sl][1];
       const int padded = (kept + 7) & ~7;
       if (t >= kept && t < padded) {  // zero-weight padding rows (add exactly 0)
-        R.wf[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        R.w[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        R.wf[t][0] = R.wf[t][1] = R.w[t][0] = R.w[t][1] = z4;
         R.col[t] = 0;
         R.f[t] = 0.0f;
       }
@@ -242,37 +244,48 @@ void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   count_launch();
 }
 
-constexpr int IT_T = 256, IT_TILE = IT_T * 8;
+constexpr int IT_T = 256, IT_PX = 4, IT_TILE = IT_T * IT_PX;
 
-// the NM members of a group on this thread's 8 pixels (one 128-bit load per row)
+// member m's weight (x factor when wf) of compacted row n
+__device__ __forceinline__ float grp_w(const float4 (&v)[2], int m) {
+  const float4 q = v[m >> 2];
+  const int k = m & 3;
+  return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
+}
+
+// the NM members of a group on this thread's 4 pixels (one 64-bit load per row)
 template <int NM>
 __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch &b, const GroupRec &R, int px) {
-  int e[NM];
-  bool in[NM], any = false;
+  // member m's window holds px (re-evaluated at the stores, so that the
+  // members' indices need no registers across the row loop)
+  auto inside = [&](int m) {
+    const EvalPrep &P = b.prep[R.member[m]];
+    return px >= P.i_lo && px < P.i_hi;
+  };
+  bool any = false;
 #pragma unroll
-  for (int m = 0; m < NM; m++) {
-    e[m] = R.member[m];
-    const EvalPrep &P = b.prep[e[m]];
-    in[m] = px >= P.i_lo && px < P.i_hi;
-    any |= in[m];
-  }
+  for (int m = 0; m < NM; m++) any |= inside(m);
   if (!any) return;
   const int nn = R.nn;
-  if (px + 8 <= G.tail_start) {
-    float2 acc[NM][4];
+  if (px + IT_PX <= G.tail_start) {
+    float2 acc[NM][2];
 #pragma unroll
-    for (int m = 0; m < NM; m++)
-#pragma unroll
-      for (int k = 0; k < 4; k++) acc[m][k] = make_float2(0.0f, 0.0f);
+    for (int m = 0; m < NM; m++) acc[m][0] = acc[m][1] = make_float2(0.0f, 0.0f);
     const float2 bias = make_float2(-8388608.0f, -8388608.0f);
-#pragma unroll 8  // 8 row loads in flight per thread (19.5 -> 19.1 ms per step against 4)
+    constexpr int UNR = NM > 4 ? 4 : 8;  // row loads in flight per thread (with their weights in registers)
+#pragma unroll UNR
     for (int n = 0; n < nn; n++) {
-      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
-      const float4 w4 = R.wf[n];
-      const float ws[4] = {w4.x, w4.y, w4.z, w4.w};
-      const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+      const uint2 q = __ldg(reinterpret_cast<const uint2 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
+      float ws[8];
+      const float4 w0 = R.wf[n][0];
+      ws[0] = w0.x; ws[1] = w0.y; ws[2] = w0.z; ws[3] = w0.w;
+      if (NM > 4) {
+        const float4 w1 = R.wf[n][1];
+        ws[4] = w1.x; ws[5] = w1.y; ws[6] = w1.z; ws[7] = w1.w;
+      }
+      const uint32_t u[2] = {q.x, q.y};
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < 2; k++) {
         float2 v = make_float2(__int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7410)),
                                __int_as_float(__byte_perm(u[k], 0x4B000000u, 0x7432)));
         v = __fadd2_rn(v, bias);  // exact u16 -> f32
@@ -282,39 +295,36 @@ __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch
     }
 #pragma unroll
     for (int m = 0; m < NM; m++) {
-      if (!in[m]) continue;
-      float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e[m] * b.stride + px);
-      out[0] = make_float4(acc[m][0].x, acc[m][0].y, acc[m][1].x, acc[m][1].y);
-      out[1] = make_float4(acc[m][2].x, acc[m][2].y, acc[m][3].x, acc[m][3].y);
+      if (!inside(m)) continue;
+      *reinterpret_cast<float4 *>(b.bufA + (size_t)R.member[m] * b.stride + px) =
+          make_float4(acc[m][0].x, acc[m][0].y, acc[m][1].x, acc[m][1].y);
     }
     return;
   }
   // last tile: the final npx % 128 pixels carry an extra 1/65535 (interpolate.rs:978)
 #pragma unroll
   for (int m = 0; m < NM; m++) {
-    if (!in[m]) continue;
-    float acc[8];
+    if (!inside(m)) continue;
+    float acc[IT_PX];
 #pragma unroll
-    for (int k = 0; k < 8; k++) acc[k] = 0.0f;
+    for (int k = 0; k < IT_PX; k++) acc[k] = 0.0f;
     for (int n = 0; n < nn; n++) {
-      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
-      const float4 w4 = R.w[n];
-      const float wn = m == 0 ? w4.x : m == 1 ? w4.y : m == 2 ? w4.z : w4.w, fn = R.f[n];
-      const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+      const uint2 q = __ldg(reinterpret_cast<const uint2 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
+      const float wn = grp_w(R.w[n], m), fn = R.f[n];
+      const uint32_t u[2] = {q.x, q.y};
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
+      for (int k = 0; k < IT_PX; k++) {
         const float x = (float)((u[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
         const float v = px + k >= G.tail_start ? __fmul_rn(__fdiv_rn(x, 65535.0f), fn) : __fmul_rn(x, fn);
         acc[k] = fmaf(wn, v, acc[k]);
       }
     }
-    float4 *out = reinterpret_cast<float4 *>(b.bufA + (size_t)e[m] * b.stride + px);
-    out[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-    out[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+    *reinterpret_cast<float4 *>(b.bufA + (size_t)R.member[m] * b.stride + px) =
+        make_float4(acc[0], acc[1], acc[2], acc[3]);
   }
 }
 
-// Grid: x = segment, y = 2048-pixel tile, so CTAs that run together read
+// Grid: x = segment, y = tile of IT_TILE pixels, so CTAs that run together read
 // the same tile slab of the resident grid (57 MB for 13,860 x 80,000), which
 // stays in L2; z = slice of the segment's groups (groups z, z + Z, ...), more
 // than one only for batches too small to fill the GPU otherwise.  Groups have
@@ -322,7 +332,7 @@ __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch
 __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
   __shared__ GroupRec R;
   const int s = blockIdx.x;
-  const int px = blockIdx.y * IT_TILE + threadIdx.x * 8;
+  const int px = blockIdx.y * IT_TILE + threadIdx.x * IT_PX;
   const int ng = b.gcount[s];
   int start, len;
   seg_range(b, s, start, len);
@@ -335,7 +345,11 @@ __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
       case 1: interp_members<1>(G, b, R, px); break;
       case 2: interp_members<2>(G, b, R, px); break;
       case 3: interp_members<3>(G, b, R, px); break;
-      default: interp_members<4>(G, b, R, px); break;
+      case 4: interp_members<4>(G, b, R, px); break;
+      case 5: interp_members<5>(G, b, R, px); break;
+      case 6: interp_members<6>(G, b, R, px); break;
+      case 7: interp_members<7>(G, b, R, px); break;
+      default: interp_members<8>(G, b, R, px); break;
     }
     __syncthreads();
   }

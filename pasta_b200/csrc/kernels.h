@@ -11,14 +11,15 @@ namespace pb {
 // particles of one star in the batched engine), with the rows they use in
 // reference order (zero-weight rows of every member dropped, padded to a
 // multiple of 8 with zero weights).
-constexpr int GROUP_MAX = 4, SEG = 64;
+constexpr int GROUP_MAX = 8, SEG = 64;
 struct __align__(16) GroupRec {
-  float4 wf[64];          // per member weight x dequantisation factor (0: padding / not a member)
-  float4 w[64];           // per member weight (the exact tail path)
+  float4 wf[64][2];       // per member (8) weight x dequantisation factor (0: padding / not a member)
+  float4 w[64][2];        // per member weight (the exact tail path)
   int col[64];            // grid row of compacted neighbour n
   float f[64];            // its dequantisation factor
   int member[GROUP_MAX];  // evaluation indices (-1: unused)
   int nmem, nn;           // members, compacted rows
+  int pad[2];
 };
 
 // Evaluations with identical neighbour columns, EvalBatch::tc_min or more
