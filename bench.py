@@ -53,13 +53,13 @@ PATH_BYTES_PER_WIN_PX, PATH_BYTES_PER_OBS = 128, 8
 # nominal FP32 CUDA-core peak of a B200: 148 SMs x 128 FMA/clk x 2 flops x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # DRAM bytes per evaluation (dram__bytes_read.sum + dram__bytes_write.sum)
-# from one ncu capture of a mid-fit step of 16 stars (1,024 evaluations,
+# from one ncu capture of a mid-fit step of 256 stars (16,384 evaluations,
 # --clock-control none), divided by its evaluations: the traffic of a launch
 # grows in proportion to the evaluations it runs, so a full launch's traffic
 # is this figure times its evaluations.  k_broaden includes its block-bound
 # search; chi2 is both chunk kernels and the final sums.
-DRAM_BYTES_PER_EVAL = {"k_interp": 480046, "k_broaden": 617963 + 936, "chi2": 163539 + 149358 + 152 + 259}
-DRAM_SOURCE = "ncu capture, mid-fit step of 16 config-1 stars (1,024 evaluations), scaled per evaluation"
+DRAM_BYTES_PER_EVAL = {"k_interp": 459082, "k_broaden": 534001 + 852, "chi2": 154226 + 143807 + 154 + 259}
+DRAM_SOURCE = "ncu capture, mid-fit step of 256 config-1 stars (16,384 evaluations), scaled per evaluation"
 
 
 def log(*a):

@@ -543,7 +543,7 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 }
 
 constexpr int BT = F2_T;      // threads of k_broaden
-constexpr int BR_FX = 2048;   // float indices of observed pixels prefetched per item
+constexpr int BR_FX = 1024;   // float indices of observed pixels prefetched per item (5 CTAs/SM)
 // dynamic shared memory (bytes): exchange buffers 1 and 2 (buffer 2 also
 // holds the rotation outputs, buffer 1 the outputs of the instrument taps),
 // twiddles of pass 2, the item's observed float indices, the fixed
@@ -584,7 +584,7 @@ __device__ __forceinline__ cf tw_pass1(int k1, const cf &w1, const cf &w2, const
 // reaches memory.  The next item's inputs are loaded into registers and this
 // item's observed float indices copied into shared memory (cp.async) while
 // the transforms run.
-__global__ void __launch_bounds__(BT, 4) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
   extern __shared__ __align__(16) unsigned char br_smem[];
   float2 *S1 = reinterpret_cast<float2 *>(br_smem + BR_S1);
   float2 *S2 = reinterpret_cast<float2 *>(br_smem + BR_S2);
@@ -808,7 +808,7 @@ void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cuda
   static int per_sm[64] = {};  // resident CTAs per SM, per device
   int dev = 0;
   cudaGetDevice(&dev);
-  int fit = 4;
+  int fit = 5;
   if (dev >= 0 && dev < 64) {
     if (!per_sm[dev]) {
       cudaFuncSetAttribute(k_broaden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
