@@ -1652,7 +1652,7 @@ void tune_interp_tc(pasta_grid *g) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   const double dt = 0.05 * (g->tv[1] - g->tv[0]), dm = 0.05 * (g->mv[1] - g->mv[0]);
-  const int ladder[] = {8, 12, 16, 24, 32, 48};
+  const int ladder[] = {8, 12, 16, 24, 32, 48, 64};
   int best = SEG + 1;
   std::vector<double> lab((size_t)E * 5);
   for (int gs : ladder) {

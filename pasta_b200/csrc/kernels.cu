@@ -780,14 +780,25 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
       // observed pixels [q0, q2) have their left synth pixel in this item's
       // blocks; the boundary between them is q1
       const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
-      for (int i = q0 + t; i < q2; i += BT) {
-        ResPos q;
-        if (R.kind == WL_NONUNI) q = R.pos(i);
-        else q = R.pos_from_fidx(i - q0 < BR_FX ? fxs[i - q0] : R.fidx[i]);
-        const bool k1 = i >= q1;
-        const float *o = k1 ? ob1 : ob0;
-        const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
-        y[i] = resample_value(q.w, o[u], o[u + 1]);
+      constexpr int EU = 4;  // observed pixels per thread and round, their loads first
+      for (int i0 = q0 + t; i0 < q2; i0 += EU * BT) {
+        double fx[EU];
+#pragma unroll
+        for (int r = 0; r < EU; r++) {
+          const int i = min(i0 + r * BT, q2 - 1);
+          fx[r] = R.kind == WL_NONUNI ? 0.0 : (i - q0 < BR_FX ? fxs[i - q0] : R.fidx[i]);
+        }
+#pragma unroll
+        for (int r = 0; r < EU; r++) {
+          const int i = i0 + r * BT;
+          if (i < q2) {
+            const ResPos q = R.kind == WL_NONUNI ? R.pos(i) : R.pos_from_fidx(fx[r]);
+            const bool k1 = i >= q1;
+            const float *o = k1 ? ob1 : ob0;
+            const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
+            y[i] = resample_value(q.w, o[u], o[u + 1]);
+          }
+        }
       }
     } else {
       // owned pixels; the last block also writes its final output
