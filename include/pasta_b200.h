@@ -213,6 +213,16 @@ int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d,
                int64_t n, const double *labels, int64_t L, double *out,
                int32_t *status);
 
+/* InMemInterpolator.ccf (lib.rs:1340-1371): the model at (teff, m, logg),
+ * interpolated once, shifted to each velocity vs[i] and resampled onto the
+ * dispersion's wavelengths (shift_and_resample, convolve_rv.rs:532-604; no
+ * broadening), dotted with flux (n = the dispersion's length).  out[V]; the
+ * dot products are summed in FP64 on the device and rounded to f32 (the
+ * reference sums in f32).  Status per velocity; NaN where it is non-zero. */
+int pasta_ccf(const pasta_grid *g, const pasta_dispersion *d, const double *vs,
+              int64_t V, double teff, double m, double logg, const float *flux,
+              int64_t n, float *out, int32_t *status);
+
 /* chi2 of S spectra, each with its own dispersion, continuum fitter, pixel
  * count and label (labels S x 5), in one batched device pass: the batched
  * form of InMemInterpolator.chi2_bulk (lib.rs:1297-1338), which evaluates

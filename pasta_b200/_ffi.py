@@ -83,6 +83,7 @@ SIGNATURES = {
     "pasta_chi2": (I, [P, P, P, P, P, I64, P, I64, P, P]),
     "pasta_chi2_noalloc": (I, [P, P, P, P, P, I64, P, I64, P, P, P]),
     "pasta_chi2_many": (I, [P, I64, P, P, P, P, P, P, P, P]),
+    "pasta_ccf": (I, [P, P, P, I64, D, D, D, P, I64, P, P]),
     "pasta_fit": (I, [P, P, P, P, P, P, I64, I64, P, I, P, P, P]),
     "pasta_fit_many": (I, [P, I64, P, P, P, P, P, P, P, I, P, P]),
     "pasta_compute_uncertainty": (I, [P, P, P, I64, P, P, I64, D, P, P, P, P, P]),

@@ -2149,7 +2149,7 @@ int pasta_continuum_build(const pasta_continuum *c, const float *params, int64_t
 static int run_label_batch(const pasta_grid *gc, const pasta_dispersion *d, const pasta_continuum *c,
                            const float *flux, const float *var, int64_t n, const double *labels, int ncols,
                            int64_t L, float *out_obs, float *out_synth, double *out_chi2, int32_t *status,
-                           int full_window, int no_rotation) {
+                           int full_window, int no_rotation, const float *dot_with = nullptr) {
   return guard([&] {
     pasta_grid *g = const_cast<pasta_grid *>(gc);
     if (L < 0) fail(PASTA_E_ARG, "negative label count");
@@ -2211,7 +2211,14 @@ static int run_label_batch(const pasta_grid *gc, const pasta_dispersion *d, cons
     CK(cudaStreamSynchronize(s));
     if (status)
       for (int64_t i = 0; i < L; i++) status[i] = hst[i];
-    if (out_obs) {
+    if (out_obs && dot_with) {  // the models stay on the device: out_obs receives L dot products
+      DBuf<float> dx, dd;
+      dx.upload(dot_with, nobs);
+      dd.alloc(L);
+      launch_dot_rows(dout.p, nobs, (int)nobs, dx.p, dst.p, dd.p, (int)L, s);
+      CK(cudaMemcpyAsync(out_obs, dd.p, (size_t)L * sizeof(float), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    } else if (out_obs) {
       CK(cudaMemcpyAsync(out_obs, dout.p, (size_t)L * nobs * sizeof(float), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       for (int64_t i = 0; i < L; i++)
@@ -2237,6 +2244,22 @@ int pasta_produce_model(const pasta_grid *g, const pasta_dispersion *d, const do
                         int32_t *status) {
   if (!d) { g_last_error = "dispersion required"; return PASTA_E_ARG; }
   return run_label_batch(g, d, nullptr, nullptr, nullptr, 0, labels, 5, L, out, nullptr, nullptr, status, 0, 0);
+}
+int pasta_ccf(const pasta_grid *g, const pasta_dispersion *d, const double *vs, int64_t V, double teff, double m,
+              double logg, const float *flux, int64_t n, float *out, int32_t *status) {
+  if (!d || !flux || !out || (V > 0 && !vs)) { g_last_error = "dispersion, velocities, flux and output required"; return PASTA_E_ARG; }
+  if (n != (int64_t)d->wl.size()) { g_last_error = "Dispersion and observed flux must have the same length."; return PASTA_E_ARG; }
+  // no broadening: the dispersion's wavelengths only (the reference resamples the unbroadened model)
+  if (d->kind != PASTA_DISP_NONE) { g_last_error = "ccf needs a no-convolution dispersion on the observed wavelengths"; return PASTA_E_ARG; }
+  std::vector<double> lab((size_t)std::max<int64_t>(V, 0) * 5);
+  for (int64_t i = 0; i < V; i++) {
+    lab[(size_t)i * 5 + 0] = teff;
+    lab[(size_t)i * 5 + 1] = m;
+    lab[(size_t)i * 5 + 2] = logg;
+    lab[(size_t)i * 5 + 3] = 0.0;
+    lab[(size_t)i * 5 + 4] = vs[i];
+  }
+  return run_label_batch(g, d, nullptr, nullptr, nullptr, 0, lab.data(), 5, V, out, nullptr, nullptr, status, 0, 0, flux);
 }
 int pasta_chi2(const pasta_grid *g, const pasta_dispersion *d, const pasta_continuum *c, const float *flux,
                const float *var, int64_t n, const double *labels, int64_t L, double *out, int32_t *status) {

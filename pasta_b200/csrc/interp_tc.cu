@@ -83,7 +83,7 @@ constexpr int B_SFULL = 0, B_SEMPTY = B_SFULL + NSTG, B_AFULL = B_SEMPTY + NSTG,
               B_DFULL = B_AEMPTY + NA, B_DEMPTY = B_DFULL + ND, B_BFULL = B_DEMPTY + ND, B_BEMPTY = B_BFULL + 2,
               B_DRAIN = B_BEMPTY + 2, NBAR = B_DRAIN + 1;
 constexpr int SB_MISC = SB_BAR + NBAR * 8;  // tensor-memory address, error flag
-constexpr int SB_EPI = (SB_MISC + 16 + 15) & ~15;  // per member: row offset (8 B), window lo, hi
+constexpr int SB_EPI = (SB_MISC + 16 + 15) & ~15;  // per member: row pointer (8 B), window lo, hi
 constexpr int SB_TOTAL = SB_EPI + 64 * 16;
 static_assert(SB_A % 1024 == 0 && SB_B % 1024 == 0 && SB_BAR % 8 == 0, "shared layout");
 static_assert(SB_TOTAL <= 227 * 1024, "shared memory of one CTA");
@@ -180,6 +180,13 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
                : "r"(taddr));
 #pragma unroll
   for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+// store v to p when ok, as one predicated instruction (no branch).  No
+// memory clobber: the interpolated rows are not read in this kernel, so the
+// loads of the next row pointers may move above these stores.
+__device__ __forceinline__ void st_if(float *p, float v, bool ok) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.global.f32 [%0], %1;\n\t}\n" ::"l"(p), "f"(v),
+               "r"((int)ok));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(TT, 1) k_interp_tc(DevGrid G, EvalBatch b, con
     // -------------------------------------------------------- epilogue
     const int e = t - 32 * W_EP;  // 0 .. 127
     const int q = w & 3;          // tensor-memory lanes 32 q .. 32 q + 31
-    long long *rowoff = reinterpret_cast<long long *>(sm + SB_EPI);
+    float **rowp = reinterpret_cast<float **>(sm + SB_EPI);
     int *wlo = reinterpret_cast<int *>(sm + SB_EPI + 64 * 8), *whi = wlo + 64;
     long long g = 0;
     bool stop = false;  // uniform within a warp; made uniform over the epilogue warps at each item
@@ -420,7 +427,7 @@ __global__ void __launch_bounds__(TT, 1) k_interp_tc(DevGrid G, EvalBatch b, con
       if (ep_any(stop || *err != 0)) break;
       if (e < 64) {
         const int m = e < I.nm ? I.R->member[e] : -1;
-        rowoff[e] = m >= 0 ? (long long)m * b.stride : 0;
+        rowp[e] = m >= 0 ? b.bufA + (size_t)m * b.stride : b.bufA;
         wlo[e] = m >= 0 ? b.prep[m].i_lo : 0;
         whi[e] = m >= 0 ? b.prep[m].i_hi : 0;
       }
@@ -448,12 +455,27 @@ __global__ void __launch_bounds__(TT, 1) k_interp_tc(DevGrid G, EvalBatch b, con
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(bar(B_DEMPTY + d));
+        // straight-line predicated stores, 8 columns per (uniform) step; a
+        // warp whose pixels all lie inside every member's window tests only
+        // the member count
         const int px = I.lo + i * TPX + 32 * q + lane;
-        const bool inside = px >= all_lo && px < all_hi;
+        if (__all_sync(0xffffffffu, px >= all_lo && px < all_hi)) {
 #pragma unroll
-        for (int n = 0; n < DCOLS; n++) {
-          if (n < I.nm && (inside || (px >= wlo[n] && px < whi[n] && px < I.tc_hi)))
-            b.bufA[rowoff[n] + px] = v[n];
+          for (int c0 = 0; c0 < DCOLS; c0 += 8)
+            if (c0 < I.NP) {
+#pragma unroll
+              for (int j = 0; j < 8; j++) st_if(rowp[c0 + j] + px, v[c0 + j], c0 + j < I.nm);
+            }
+        } else {
+#pragma unroll
+          for (int c0 = 0; c0 < DCOLS; c0 += 8)
+            if (c0 < I.NP) {
+#pragma unroll
+              for (int j = 0; j < 8; j++) {
+                const int n = c0 + j;
+                st_if(rowp[n] + px, v[n], n < I.nm && px >= wlo[n] && px < whi[n] && px < I.tc_hi);
+              }
+            }
         }
       }
       // tail pixels [tail_start, hi): the reference's extra 1/65535 (interpolate.rs:978)
@@ -471,7 +493,7 @@ __global__ void __launch_bounds__(TT, 1) k_interp_tc(DevGrid G, EvalBatch b, con
             const float x = (float)G.spectra[(size_t)col * G.stride + px];
             acc = fmaf(P.w[k], __fmul_rn(__fdiv_rn(x, 65535.0f), I.R->f[k]), acc);
           }
-          b.bufA[rowoff[n] + px] = acc;
+          rowp[n][px] = acc;
         }
       }
     }

@@ -1286,6 +1286,34 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Dot product of each row with x (InMemInterpolator.ccf, lib.rs:1340-1371):
+// one CTA per row, FP64 sums, rounded to f32 once; NaN for a failed row.
+__global__ void __launch_bounds__(256) k_dot_rows(const float *rows, int64_t stride, int n, const float *x,
+                                                   const int *status, float *out) {
+  __shared__ double ws[8];
+  const int r = blockIdx.x, t = threadIdx.x;
+  const bool ok = status[r] == 0;
+  double acc = 0.0;
+  if (ok) {
+    const float *row = rows + (size_t)r * stride;
+    for (int i = t; i < n; i += 256) acc = fma((double)row[i], (double)x[i], acc);
+  }
+  acc = warp_sum(acc);
+  if ((t & 31) == 0) ws[t >> 5] = acc;
+  __syncthreads();
+  if (t == 0) {
+    double tot = 0.0;
+    for (int k = 0; k < 8; k++) tot += ws[k];
+    out[r] = ok ? (float)tot : __int_as_float(0x7fc00000);
+  }
+}
+void launch_dot_rows(const float *rows, int64_t stride, int n, const float *x, const int *status, float *out, int L,
+                     cudaStream_t s) {
+  if (L <= 0) return;
+  k_dot_rows<<<L, 256, 0, s>>>(rows, stride, n, x, status, out);
+  count_launch();
+}
+
 // block sum of K per-thread doubles into out[0..K)
 template <int K>
 __device__ __forceinline__ void block_sum_vec(const double (&v)[K], double (*ws)[MAX_P1], double *out) {

@@ -136,6 +136,9 @@ void launch_linear_tc(const EvalBatch &b, cudaStream_t s);
 // copy the preparation status to b.status (batches without chi2)
 void launch_prep_status(const EvalBatch &b, cudaStream_t s);
 // model at the observed pixels: out [E][out_stride]
+// out[r] = rows[r] . x (n values, FP64 sums), NaN where status[r] != 0
+void launch_dot_rows(const float *rows, int64_t stride, int n, const float *x, const int *status, float *out, int L,
+                     cudaStream_t s);
 void launch_resample_out(const DevGrid &G, const EvalBatch &b, float *out, int64_t out_stride,
                          cudaStream_t s);
 // broadened synth spectrum (before resampling): out [E][npx]

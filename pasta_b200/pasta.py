@@ -703,10 +703,14 @@ class _Interpolator:
         if len(dispersion.wl) != len(flux):
             raise ValueError("Dispersion and observed flux must have the same length.")
         nd = NoConvolutionDispersion(dispersion.wl, self.synth_wl)
-        lab = np.array([[teff, m, logg, 0.0, v] for v in vs], np.float64)
-        models, st = self._produce(nd, lab)
+        v = np.ascontiguousarray(vs, np.float64).reshape(-1)
+        out = np.empty(len(v), np.float32)
+        st = np.zeros(len(v), np.int32)
+        # the shifted models stay on the device; their dot products with the flux are summed there
+        check(lib().pasta_ccf(self._grid._h, nd._h, ptr(v), len(v), float(teff), float(m), float(logg), ptr(flux),
+                              len(flux), ptr(out), ptr(st)))
         self._raise_status(st)
-        return (models * flux[None, :]).sum(axis=1, dtype=np.float32)
+        return out
 
     # ---- grid getters (lib.rs:1373-1465)
     def clamp_1d(self, teff, m, logg, index) -> float:

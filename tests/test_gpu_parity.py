@@ -530,6 +530,26 @@ def test_interpolation_tensor_cores(env):
     print("tensor-core group threshold measured on this device: %d members" % keep)
 
 
+def test_ccf_matches_oracle(env):
+    """ccf (lib.rs:1340-1371): the unbroadened model shifted to each velocity
+    and resampled onto the observed wavelengths, dotted with the flux on the
+    device; against the oracle's FP64 model at each velocity and an FP64 dot
+    product (1e-5), a failing velocity raises, and the length check."""
+    O, P, star, og = env["O"], env["P"], env["star"], env["og"]
+    vs = np.linspace(-120.0, 120.0, 25)
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    got = env["interp"].ccf(vs, 7130.0, 0.07, 4.02, d, star.flux)
+    od = O.Disp(og, O.DISP_NONE, star.wl)
+    ref = np.array([np.dot(od.produce_model([7130.0, 0.07, 4.02, 0.0, v], O.F64).astype(np.float64),
+                           star.flux.astype(np.float64)) for v in vs])
+    np.testing.assert_allclose(got, ref, rtol=1e-5)
+    assert np.argmax(got) == np.argmax(ref)
+    with pytest.raises(ValueError):
+        env["interp"].ccf(vs, 7130.0, 0.07, 4.02, d, star.flux[:-1])
+    with pytest.raises(P.PastaError):
+        env["interp"].ccf([0.0, 5.0e5], 7130.0, 0.07, 4.02, d, star.flux)
+
+
 def test_chi2_bulk_one_batched_pass(env):
     """chi2_bulk (lib.rs:1297-1338): spectra with their own wavelength grids,
     a no-convolution dispersion and a 5 x 8 x 0.2 chunk fitter each, in one
