@@ -21,9 +21,10 @@
 // One persistent CTA per SM, its warps specialised and handing tiles on
 // through mbarriers, so that staging, conversion, products and stores of
 // different tiles overlap:
-//   warp 0      TMA producer: the 64 rows of a tile (one 128-pixel box per
-//               row, from the grid resident in this GPU's memory; no
-//               multicast) into a ring of NSTG staging buffers;
+//   warp 0      TMA producer: the 64 rows of a tile (16 tile::gather4
+//               loads of four 128-pixel rows each, from the grid resident in
+//               this GPU's memory; no multicast) into a ring of NSTG staging
+//               buffers;
 //   warp 1      one thread issues the 24 tcgen05.mma of a tile (kind::f16,
 //               M = 128, N = members rounded up to 16) into one of ND
 //               tensor-memory accumulators;
@@ -160,12 +161,11 @@ __device__ __forceinline__ bool ep_any(bool pred) {
   return r != 0;
 }
 
-// TMA: one box of 128 pixels of grid row y starting at pixel x
-__device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t mbar) {
+// TMA gather of four rows (one 128-pixel box each) into four consecutive boxes
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map, int x, const int (&y)[4], uint32_t mbar) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
-          "r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];\n" ::
+          "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]), "r"(mbar)
       : "memory");
 }
 __device__ __forceinline__ void mbar_expect(uint32_t mbar, uint32_t bytes) {
@@ -277,9 +277,15 @@ __global__ void __launch_bounds__(TT, 1) k_interp_tc(DevGrid G, EvalBatch b, con
     for (int item = blockIdx.x; item < nitems && !stop; item += gridDim.x) {
       TcItem I;
       if (!tc_item(G, b, item, slabs, I)) continue;
-      // the rows of this group (a missing row has weight 0: row 0 stands in)
-      const int c0 = I.R->col[lane], c1 = I.R->col[lane + 32];
-      const int r0 = c0 >= 0 ? c0 : 0, r1 = c1 >= 0 ? c1 : 0;
+      // the rows of this group (a missing row has weight 0: row 0 stands in);
+      // lane l < 16 gathers rows 4l .. 4l + 3
+      const int k0 = 4 * (lane & 15);
+      int rr[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int c = I.R->col[k0 + j];
+        rr[j] = c >= 0 ? c : 0;
+      }
       for (int i = 0; i < I.ntiles; i++, g++) {
         const int s = (int)(g % NSTG);
         const long long u = g / NSTG;
@@ -289,8 +295,7 @@ __global__ void __launch_bounds__(TT, 1) k_interp_tc(DevGrid G, EvalBatch b, con
         __syncwarp();
         const uint32_t dst = sbase + SB_STG + (uint32_t)(s * SZ_STG);
         const int x = I.lo + i * TPX;
-        tma_row(dst + (uint32_t)(lane * TPX * 2), &tmap, x, r0, bar(B_SFULL + s));
-        tma_row(dst + (uint32_t)((lane + 32) * TPX * 2), &tmap, x, r1, bar(B_SFULL + s));
+        if (lane < 16) tma_gather4(dst + (uint32_t)(k0 * TPX * 2), &tmap, x, rr, bar(B_SFULL + s));
       }
     }
     // every issued copy has landed before the CTA leaves (bounded)

@@ -530,6 +530,35 @@ def test_interpolation_tensor_cores(env):
     print("tensor-core group threshold measured on this device: %d members" % keep)
 
 
+def test_tensor_core_groups_with_own_windows(env):
+    """A 64-member tensor-core group (one star's whole swarm in one grid cube)
+    whose members have their own RV shifts and so their own interpolation
+    windows: each model against the CUDA-core path (2e-6 of the maximum) and
+    the oracle (1e-5), the window edges included."""
+    from pasta_b200 import _ffi
+    O, P, star, og, interp = env["O"], env["P"], env["star"], env["og"], env["interp"]
+    rng = np.random.default_rng(21)
+    lab = np.stack([rng.uniform(7010.0, 7240.0, 64), rng.uniform(0.01, 0.09, 64), rng.uniform(4.01, 4.24, 64),
+                    rng.uniform(0.0, 60.0, 64), rng.uniform(-140.0, 140.0, 64)], 1)
+    d = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    keep = interp.tc_min
+    interp.tc_min = 16
+    try:
+        tc = interp.produce_model_bulk(d, lab)
+        _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(0))
+        try:
+            cc = interp.produce_model_bulk(d, lab)
+        finally:
+            _ffi.check(_ffi.lib().pasta_set_interp_tensor_cores(1))
+    finally:
+        interp.tc_min = keep
+    assert np.abs(tc - cc).max() <= 2e-6 * np.abs(cc).max()
+    od = O.Disp(og, O.DISP_FIXED, star.wl, resolution=85000.0)
+    for i in range(0, 64, 7):
+        ref = od.produce_model(lab[i], O.F32)
+        assert relmax(tc[i], ref) <= FLUX_TOL, i
+
+
 def test_ccf_matches_oracle(env):
     """ccf (lib.rs:1340-1371): the unbroadened model shifted to each velocity
     and resampled onto the observed wavelengths, dotted with the flux on the
