@@ -464,6 +464,17 @@ __device__ __forceinline__ void cp_async16(float *smem, const float *gmem, bool 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Bulk prefetch of floats [lo, hi) of a row into L2 (one instruction, issued
+// by one thread; a hint, nothing waits for it).  The row must start on a
+// 16-byte boundary and hold hi rounded up to 4 floats.
+__device__ __forceinline__ void prefetch_row_l2(const float *row, int lo, int hi) {
+  lo &= ~3;
+  hi = (hi + 3) & ~3;
+  if (hi <= lo) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(row + lo), "r"((unsigned)(hi - lo) * 4u)
+               : "memory");
+}
+
 struct BroadenItem {
   int e, pair, m, hg, V, s0, s1, j0, j1;
   bool has1;
@@ -519,15 +530,23 @@ struct ItemCursor {
   }
 };
 
-// The 2 x 16 inputs of this thread for an item: block input j = 128 n1 + t
+// The 2 x 16 inputs of this thread for item w: block input j = 128 n1 + t
 // is synth pixel j0 + j of the interpolated row (zero outside [i_lo, i_hi)).
-__device__ __forceinline__ void broaden_inputs(const EvalBatch &b, const ItemCursor &c, float (&x0)[16],
-                                               float (&x1)[16]) {
-  BroadenItem w;
-  broaden_item(b, c.e, c.pair, w);
-  const EvalPrep &P = b.prep[c.e];
-  const float *row = b.bufA + (size_t)c.e * b.stride;
+// Interior item pairs (both blocks inside the window, the common case) load
+// without per-element bounds tests.
+__device__ __forceinline__ void broaden_inputs(const EvalBatch &b, const BroadenItem &w, const EvalPrep &P,
+                                               float (&x0)[16], float (&x1)[16]) {
+  const float *row = b.bufA + (size_t)w.e * b.stride;
   const int ilo = P.i_lo, ihi = P.i_hi;
+  if (w.has1 && w.j0 >= ilo && w.j1 + FFTN <= ihi) {
+    const float *r0 = row + w.j0 + (int)threadIdx.x, *r1 = row + w.j1 + (int)threadIdx.x;
+#pragma unroll
+    for (int n1 = 0; n1 < 16; n1++) {
+      x0[n1] = __ldg(r0 + 128 * n1);
+      x1[n1] = __ldg(r1 + 128 * n1);
+    }
+    return;
+  }
 #pragma unroll
   for (int n1 = 0; n1 < 16; n1++) {
     const int g0 = w.j0 + 128 * n1 + (int)threadIdx.x, g1 = w.j1 + 128 * n1 + (int)threadIdx.x;
@@ -631,7 +650,7 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
     // this item's inputs, observed float indices (uniform grids, cp.async)
     // and instrument taps
     float in0[16], in1[16];
-    broaden_inputs(b, cur, in0, in1);
+    broaden_inputs(b, w, P, in0, in1);
     const bool pre = P.epi && G.wl_kind != WL_NONUNI;
     if (pre) {
       const int nq = min(q2 - q0, BR_FX);
@@ -677,11 +696,20 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
         const int c = t + 128 * h;
         cf u[8];
         float2 hk[8];
+        // bins k = c + 256 k3 (c < 256): k < 1024 below k3 = 4, k > 1024
+        // above it (conjugate of bin 2048 - k); k3 = 4 is bin 1024 for c = 0
 #pragma unroll
         for (int k3 = 0; k3 < 8; k3++) {
           const int k = c + 256 * k3;
-          hk[k3] = __ldg(&H[k <= 1024 ? k : FFTN - k]);
-          if (k > 1024) hk[k3].y = -hk[k3].y;
+          if (k3 < 4) {
+            hk[k3] = __ldg(&H[k]);
+          } else if (k3 > 4) {
+            hk[k3] = __ldg(&H[FFTN - k]);
+            hk[k3].y = -hk[k3].y;
+          } else {
+            hk[k3] = __ldg(&H[c == 0 ? 1024 : FFTN - k]);
+            if (c != 0) hk[k3].y = -hk[k3].y;
+          }
         }
 #pragma unroll
         for (int n3 = 0; n3 < 8; n3++) {
@@ -723,8 +751,8 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
         ob1 = ob0 + 2048;
 #pragma unroll
         for (int n1 = 0; n1 < 16; n1++) {
-          const int u = 128 * n1 + t - base - 2 * hg;
-          if ((unsigned)u < (unsigned)V) {
+          const int u = 128 * n1 + t - base - 2 * hg;  // at most 2047 - base - 2 hg = V - 1
+          if (u >= 0) {
             ob0[u] = v[n1].x * sc;
             ob1[u] = v[n1].y * sc;
           }
@@ -1415,25 +1443,20 @@ void launch_resample_obs(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
 // K = polynomial order + 1 (one instantiation per order present).  A warp
 // walks the whole chunk (no block barriers), so the loads of many chunks
 // are in flight per SM.
+// Moments of chunk c walked by one warp; lane 0 then solves G a = z with the
+// chunk's FP64 Cholesky factor, leaving the Legendre coefficients in a[0..K)
+// (and the reference's parameters in b.params when requested).
 template <int K>
-__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch b) {
-  __shared__ double zs[CW][MAX_P1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long gw = (long long)blockIdx.x * CW + warp;
-  if (gw >= (long long)b.E * b.max_chunks) return;
-  const int e = (int)(gw / b.max_chunks), c = (int)(gw % b.max_chunks);
-  const EvalPrep &P = b.prep[e];
-  if (P.status) return;
-  const DevStar &st = b.stars[P.star];
-  if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
-  const float *mod = model_row(b, P, e), *flux = st.flux;
+__device__ __forceinline__ void chunk_solve_warp(const EvalBatch &b, const DevStar &st, const float *mod, int e,
+                                                 int c, int lane, double *a) {
+  const float *flux = st.flux;
   const int lo = st.cstart[c], hi = st.cstop[c], prev = c > 0 ? st.cstop[c - 1] : -1;
+  if (lane == 0 && !b.given) prefetch_row_l2(mod, lo, hi);  // the walk below then reads from L2
   constexpr int CU = chunk_cu<K>();
   double z[K];
 #pragma unroll
   for (int k = 0; k < K; k++) z[k] = 0.0;
-  // loads of CU pixels are issued before any arithmetic on them (the f32
-  // division has a slow path the compiler will not schedule loads across)
+  // loads of CU pixels are issued before any arithmetic on them
   for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
     float fl[CU], md[CU], xf[CU];
 #pragma unroll
@@ -1449,7 +1472,9 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
 #pragma unroll
     for (int u = 0; u < CU; u++) {
       if (i0 + 32 * u < hi) {
-        const float y = fl[u] / md[u];
+        // flux / model as x * rcp(y) (at most 2 ulp; the moments are sums
+        // of thousands of such terms, accumulated in FP64)
+        const float y = __fdividef(fl[u], md[u]);
         float Pk[K];
         legendre<K>(xf[u], Pk);
 #pragma unroll
@@ -1462,10 +1487,9 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
 #pragma unroll
   for (int k = 0; k < K; k++) {
     const double t = warp_sum(z[k]);
-    if (lane == 0) zs[warp][k] = t;
+    if (lane == 0) a[k] = t;
   }
   if (lane == 0) {  // FP64 Cholesky solve G a = z, in place
-    double *a = zs[warp];
     const double *L = st.chol + (size_t)c * K * K;
     for (int k = 0; k < K; k++) {
       double t = a[k];
@@ -1477,8 +1501,6 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_moments(EvalBatch 
       for (int j = k + 1; j < K; j++) t -= L[j * K + k] * a[j];
       a[k] = t / L[k * K + k];
     }
-    float *cf = b.ccoef + ((size_t)e * MAX_CHUNKS + c) * MAX_P1;
-    for (int k = 0; k < K; k++) cf[k] = (float)a[k];
     if (b.params) {
       double *par = b.params + (size_t)e * b.param_stride + c * K;
       for (int k = 0; k < K; k++) par[k] = a[k];
@@ -1496,31 +1518,17 @@ __device__ __forceinline__ float poly_eval_r(const float (&coef)[K], float x) {
   return s;
 }
 
-// chi2 section of chunk c (continuum_fitting.rs:280-360): chunk 0 alone on
-// [50, start_1); chunk c >= 1 blended with chunk c - 1 (sin^2 factor) on
-// [start_c, stop_{c-1}), then alone up to start_{c+1} (N - 50 for the
-// last).  One warp per section; a lane adds the terms of the pixels it
-// loads together in f32 and those partials in FP64; section sums in FP64,
-// added in chunk order by k_chunk_final.
+// chi2 section of chunk c (continuum_fitting.rs:280-360) walked by one
+// warp: chunk 0 alone on [50, start_1); chunk c >= 1 blended with chunk
+// c - 1 (sin^2 factor) on [start_c, stop_{c-1}), then alone up to
+// start_{c+1} (N - 50 for the last).  A lane adds the terms of the pixels
+// it loads together in f32 and those partials in FP64; the warp's sum is
+// returned to lane 0.
 template <int K>
-__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = (long long)blockIdx.x * CW + (threadIdx.x >> 5);
-  if (gw >= (long long)b.E * b.max_chunks) return;
-  const int e = (int)(gw / b.max_chunks), c = (int)(gw % b.max_chunks);
-  const EvalPrep &P = b.prep[e];
-  if (P.status) return;
-  const DevStar &st = b.stars[P.star];
-  if (st.cont_kind != CONT_CHUNK || st.p1 != K || st.cont_bad || c >= st.n_chunks) return;
+__device__ __forceinline__ double chunk_resid_warp(const DevStar &st, const float *mod, int c, int lane,
+                                                   const float (&cc)[K], const float (&cp)[K]) {
   const int N = st.n_obs, nc = st.n_chunks;
-  const float *mod = model_row(b, P, e), *flux = st.flux, *var = st.var;
-  const float *coef = b.ccoef + (size_t)e * MAX_CHUNKS * MAX_P1;
-  float cc[K], cp[K];
-#pragma unroll
-  for (int k = 0; k < K; k++) {
-    cc[k] = coef[c * MAX_P1 + k];
-    cp[k] = c > 0 ? coef[(c - 1) * MAX_P1 + k] : 0.0f;
-  }
+  const float *flux = st.flux, *var = st.var;
   double acc = 0.0;
   constexpr int CU = chunk_cu<K>();
   // [lo, hi) with chunk c alone; loads of CU pixels before their arithmetic
@@ -1541,7 +1549,7 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
         if (i0 + 32 * u < hi) {
           const float p = poly_eval_r<K>(cc, xa[u]);
           const float r = fl[u] - p * md[u];
-          part += r * r / vr[u];
+          part += __fdividef(r * r, vr[u]);
         }
       }
       acc += (double)part;
@@ -1572,34 +1580,68 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_resid(EvalBatch b)
           const float cu = poly_eval_r<K>(cc, xb[u]);
           const float p = pv * fc[u] + cu * (1.0f - fc[u]);
           const float r = fl[u] - p * md[u];
-          part += r * r / vr[u];
+          part += __fdividef(r * r, vr[u]);
         }
       }
       acc += (double)part;
     }
     alone(sp, nx);
   }
-  acc = warp_sum(acc);
-  if (lane == 0) b.cpart[(size_t)e * MAX_CHUNKS + c] = acc;
+  return warp_sum(acc);
 }
 
-// chi2 = sum of the section partials in chunk order / (N - 100); errors as NaN
-__global__ void k_chunk_final(EvalBatch b) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= b.E) return;
+// ChunkFitter::fit_continuum + compute_chi2_from_chunks
+// (continuum_fitting.rs:216-226, 280-360, 382-396) for one evaluation per
+// CTA: warp w takes chunks w, w + 8, ...  First every chunk's moments and
+// FP64 solve: the unweighted least-squares polynomial of flux/model over
+// the chunk is the projection onto the chunk's polynomial space, solved here
+// in a Legendre basis with the Cholesky factor of its Gram matrix (the same
+// space as the reference's monomial SVD, far better conditioned).  After a
+// CTA barrier every chunk section's chi2 from the coefficients in shared
+// memory, reading the model row a second time while it is still in L2;
+// then the sections added in chunk order in FP64 / (N - 100).  Errors give
+// NaN with the evaluation's status.  K = polynomial order + 1 (one
+// instantiation per order present; other orders return at once).
+template <int K>
+__global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_fit(EvalBatch b) {
+  __shared__ double zs[MAX_CHUNKS][MAX_P1];
+  __shared__ float cfs[MAX_CHUNKS][MAX_P1];
+  __shared__ double part[MAX_CHUNKS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int e = blockIdx.x;
   const EvalPrep &P = b.prep[e];
   const DevStar &st = b.stars[P.star];
-  if (st.cont_kind != CONT_CHUNK) return;
+  if (st.cont_kind != CONT_CHUNK || st.p1 != K) return;
   int status = P.status;
   if (!status && st.cont_bad) status = S_CONTINUUM;
-  double chi2 = 0.0;
-  if (!status) {
-    const double *pt = b.cpart + (size_t)e * MAX_CHUNKS;
-    for (int c = 0; c < st.n_chunks; c++) chi2 += pt[c];
-    chi2 /= (double)(st.n_obs - 100);
+  if (status) {
+    write_result(b, e, 0.0, status);
+    return;
   }
-  b.cost[e] = status ? __longlong_as_double(0x7FF8000000000000ll) : chi2;
-  b.status[e] = status;
+  const float *mod = model_row(b, P, e);
+  const int nc = st.n_chunks;
+  for (int c = warp; c < nc; c += CW) {
+    chunk_solve_warp<K>(b, st, mod, e, c, lane, zs[c]);
+    if (lane == 0)
+      for (int k = 0; k < K; k++) cfs[c][k] = (float)zs[c][k];
+  }
+  __syncthreads();
+  for (int c = warp; c < nc; c += CW) {
+    float cc[K], cp[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      cc[k] = cfs[c][k];
+      cp[k] = c > 0 ? cfs[c - 1][k] : 0.0f;
+    }
+    const double acc = chunk_resid_warp<K>(st, mod, c, lane, cc, cp);
+    if (lane == 0) part[c] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double chi2 = 0.0;
+    for (int c = 0; c < nc; c++) chi2 += part[c];
+    write_result(b, e, chi2 / (double)(st.n_obs - 100), 0);
+  }
 }
 
 // LinearModelFitter (continuum_fitting.rs:68-95): projection onto the design
@@ -1679,11 +1721,8 @@ __global__ void __launch_bounds__(CT) k_chi2_other(DevGrid G, EvalBatch b) {
 
 template <int K>
 static void launch_chunk(const EvalBatch &b, cudaStream_t s) {
-  const long long warps = (long long)b.E * b.max_chunks;
-  const unsigned grid = (unsigned)((warps + CW - 1) / CW);
-  k_chunk_moments<K><<<grid, CT, 0, s>>>(b);
-  k_chunk_resid<K><<<grid, CT, 0, s>>>(b);
-  count_launch(2);
+  k_chunk_fit<K><<<b.E, CT, 0, s>>>(b);
+  count_launch();
 }
 
 // chi2 of every evaluation from the model at its observed pixels
@@ -1708,8 +1747,6 @@ void launch_chi2(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
     if (m & (1u << 14)) launch_chunk<14>(b, s);
     if (m & (1u << 15)) launch_chunk<15>(b, s);
     if (m & (1u << 16)) launch_chunk<16>(b, s);
-    k_chunk_final<<<(b.E + 255) / 256, 256, 0, s>>>(b);
-    count_launch();
   }
   if (b.other_cont) {
     if (b.lin_group > 0) launch_linear_tc(b, s);
