@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "fft.cuh"
@@ -500,26 +501,35 @@ __device__ __forceinline__ bool broaden_item(const EvalBatch &b, int e, int pair
   return true;
 }
 
-// The items of a CTA, item = e * max_pairs + pair for item = blockIdx.x,
-// blockIdx.x + gridDim.x, ...: stepping (e, pair) by the precomputed
-// quotient and remainder of gridDim.x needs no division per item.
+// The items of a CTA (item = e * max_pairs + pair) come in runs of ic
+// consecutive items (mostly neighbouring block pairs of one evaluation, so
+// their metadata and the overlap of their inputs are still in cache): run r
+// of the CTA is items [ic R, ic R + ic) with R = blockIdx.x + r gridDim.x.
 struct ItemCursor {
-  int e, pair;
-  int de, dp, mp, E;
-  __device__ __forceinline__ void init(const EvalBatch &b) {
+  int e, pair, k, ic, mp, E;
+  long long run;
+  __device__ __forceinline__ void set_run() {
+    const long long item = run * ic;
+    e = (int)(item / mp);
+    pair = (int)(item % mp);
+    k = 0;
+  }
+  __device__ __forceinline__ void init(const EvalBatch &b, int run_len) {
     mp = b.max_pairs;
     E = b.E;
-    e = (int)blockIdx.x / mp;
-    pair = (int)blockIdx.x % mp;
-    de = (int)gridDim.x / mp;
-    dp = (int)gridDim.x % mp;
+    ic = run_len;
+    run = blockIdx.x;
+    set_run();
   }
   __device__ __forceinline__ void advance() {
-    pair += dp;
-    e += de;
-    if (pair >= mp) {
-      pair -= mp;
-      e++;
+    if (++k < ic) {
+      if (++pair >= mp) {
+        pair = 0;
+        e++;
+      }
+    } else {
+      run += gridDim.x;
+      set_run();
     }
   }
   __device__ __forceinline__ bool done() const { return e >= E; }
@@ -555,20 +565,47 @@ __device__ __forceinline__ void broaden_inputs(const EvalBatch &b, const Broaden
   }
 }
 
-// 8-byte asynchronous global -> shared copy (float indices)
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-
 constexpr int BT = F2_T;      // threads of k_broaden
-constexpr int BR_FX = 1024;   // float indices of observed pixels prefetched per item (5 CTAs/SM)
+constexpr int BR_RUN = 8;     // longest run of consecutive items a CTA takes
 // dynamic shared memory (bytes): exchange buffers 1 and 2 (buffer 2 also
 // holds the rotation outputs, buffer 1 the outputs of the instrument taps),
-// twiddles of pass 2, the item's observed float indices, the fixed
-// instrument taps
-constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T2 = BR_S2 + F2_S2 * 8, BR_FXO = BR_T2 + 16 * 8 * 8,
-              BR_GK = BR_FXO + BR_FX * 8, BR_SMEM = BR_GK + 512 * 4;
+// twiddles of pass 2, the fixed instrument taps
+constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T2 = BR_S2 + F2_S2 * 8, BR_GK = BR_T2 + 16 * 8 * 8,
+              BR_SMEM = BR_GK + 512 * 4;
+
+// Resampling of an item's observed pixels [q0, q2) (the left synth pixel of
+// [q0, q1) in block 0, of [q1, q2) in block 1) from the final outputs in
+// shared memory, with the wavelength kind fixed at compile time.  The float
+// indices come from the star's table (a star's particles share it, so it
+// is read from L2); each thread issues the loads of EU pixels before their
+// arithmetic.
+template <int KIND>
+__device__ __forceinline__ void resample_item(const Resampler &R, float *y, const float *ob0,
+                                              const float *ob1, int q0, int q1, int q2, int s0, int s1, int V) {
+  constexpr int EU = 4;
+  for (int i0 = q0 + (int)threadIdx.x; i0 < q2; i0 += EU * BT) {
+    double fx[EU];
+#pragma unroll
+    for (int r = 0; r < EU; r++) {
+      const int i = min(i0 + r * BT, q2 - 1);
+      fx[r] = KIND == WL_NONUNI ? 0.0 : __ldg(&R.fidx[i]);
+    }
+#pragma unroll
+    for (int r = 0; r < EU; r++) {
+      const int i = i0 + r * BT;
+      if (i < q2) {
+        ResPos q;
+        if (KIND == WL_LOG) q = R.from_index(fx[r] + R.shift_log);
+        else if (KIND == WL_LIN) q = R.from_index(__dadd_rn(__dmul_rn(R.shift_factor, fx[r]), R.lin_offset));
+        else q = R.pos(i);
+        const bool k1 = i >= q1;
+        const float *o = k1 ? ob1 : ob0;
+        const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
+        y[i] = resample_value(q.w, o[u], o[u + 1]);
+      }
+    }
+  }
+}
 
 // the pass-1 twiddle W_2048^(t k1) of this thread from W^t, W^2t, W^4t and
 // W^8t (table values, computed in double on the host) by at most three
@@ -603,12 +640,11 @@ __device__ __forceinline__ cf tw_pass1(int k1, const cf &w1, const cf &w2, const
 // reaches memory.  The next item's inputs are loaded into registers and this
 // item's observed float indices copied into shared memory (cp.async) while
 // the transforms run.
-__global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw, int run_len) {
   extern __shared__ __align__(16) unsigned char br_smem[];
   float2 *S1 = reinterpret_cast<float2 *>(br_smem + BR_S1);
   float2 *S2 = reinterpret_cast<float2 *>(br_smem + BR_S2);
   float2 *T2 = reinterpret_cast<float2 *>(br_smem + BR_T2);
-  double *fxs = reinterpret_cast<double *>(br_smem + BR_FXO);
   float *gks = reinterpret_cast<float *>(br_smem + BR_GK);
   const int t = threadIdx.x, N = G.npx;
   // twiddles: T2[k2][n3] = W_128^(n3 k2) in shared memory; W_2048^(t k1)
@@ -623,9 +659,10 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
     tw8 = cf{f.x, f.y};
   }
   ItemCursor cur;
-  cur.init(b);
+  cur.init(b, run_len);
   cur.settle(b);
   const int k1p = t >> 3, n3p = t & 7;  // pass-2 role of this thread
+  int gk_star = -1;                       // star whose instrument taps are in gks
   while (!cur.done()) {
     ItemCursor nxt = cur;
     nxt.advance();
@@ -651,16 +688,12 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
     // and instrument taps
     float in0[16], in1[16];
     broaden_inputs(b, w, P, in0, in1);
-    const bool pre = P.epi && G.wl_kind != WL_NONUNI;
-    if (pre) {
-      const int nq = min(q2 - q0, BR_FX);
-      for (int i = t; i < nq; i += BT) cp_async8(fxs + i, st.fidx + q0 + i);
-    }
-    cp_async_commit();
-    if (fixedk)
-      for (int k = t; k < gw; k += BT) gks[k] = __ldg(&st.gk[k]);
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
+    if (fixedk && !fold && P.star != gk_star) {  // the taps are applied from shared memory (edge blocks)
+      for (int k = t; k < gw; k += BT) gks[k] = __ldg(&st.gk[k]);
+      gk_star = P.star;
+    }
     const float sc = 1.0f / 2048.0f;
     float *ob0, *ob1;  // final outputs u in [0, V) of the two blocks
     if (m > 1) {
@@ -772,7 +805,6 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
 #pragma unroll
       for (int n1 = 0; n1 < 16; n1++) S2[128 * n1 + t] = make_float2(in0[n1], in1[n1]);
     }
-    cp_async_wait_all();
     __syncthreads();
     if (!fold) {  // instrument taps from the rotation outputs in S2 into buffer 1
       ob0 = reinterpret_cast<float *>(S1);
@@ -808,26 +840,9 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
       // observed pixels [q0, q2) have their left synth pixel in this item's
       // blocks; the boundary between them is q1
       const Resampler R = make_resampler(G, st, P, nullptr, nullptr);
-      constexpr int EU = 4;  // observed pixels per thread and round, their loads first
-      for (int i0 = q0 + t; i0 < q2; i0 += EU * BT) {
-        double fx[EU];
-#pragma unroll
-        for (int r = 0; r < EU; r++) {
-          const int i = min(i0 + r * BT, q2 - 1);
-          fx[r] = R.kind == WL_NONUNI ? 0.0 : (i - q0 < BR_FX ? fxs[i - q0] : R.fidx[i]);
-        }
-#pragma unroll
-        for (int r = 0; r < EU; r++) {
-          const int i = i0 + r * BT;
-          if (i < q2) {
-            const ResPos q = R.kind == WL_NONUNI ? R.pos(i) : R.pos_from_fidx(fx[r]);
-            const bool k1 = i >= q1;
-            const float *o = k1 ? ob1 : ob0;
-            const int u = min(max(q.j - (k1 ? s1 : s0), 0), V - 2);  // in range by construction of bnd
-            y[i] = resample_value(q.w, o[u], o[u + 1]);
-          }
-        }
-      }
+      if (R.kind == WL_LOG) resample_item<WL_LOG>(R, y, ob0, ob1, q0, q1, q2, s0, s1, V);
+      else if (R.kind == WL_LIN) resample_item<WL_LIN>(R, y, ob0, ob1, q0, q1, q2, s0, s1, V);
+      else resample_item<WL_NONUNI>(R, y, ob0, ob1, q0, q1, q2, s0, s1, V);
     } else {
       // owned pixels; the last block also writes its final output
       const int n0 = 2 * pair + 1 == nblk ? V : V - 1, n1 = 2 * pair + 2 == nblk ? V : V - 1;
@@ -860,7 +875,11 @@ void launch_broaden(const DevGrid &G, const EvalBatch &b, const float2 *tw, cuda
   const long long total = (long long)b.E * b.max_pairs;
   long long grid = (long long)num_sms() * fit;  // persistent: the CTAs that fit at once
   if (grid > total) grid = total;
-  k_broaden<<<(unsigned)grid, BT, smem, s>>>(G, b, tw);
+  // runs of up to BR_RUN consecutive items, as long as every CTA still gets
+  // 16 runs or more (small batches keep single items spread over all CTAs)
+  int run_len = (int)std::min<long long>(BR_RUN, std::max<long long>(1, total / (grid * 16)));
+  if (const char *rl = getenv("PASTA_BR_RUN")) run_len = std::max(1, atoi(rl));
+  k_broaden<<<(unsigned)grid, BT, smem, s>>>(G, b, tw, run_len);
   count_launch();
 }
 

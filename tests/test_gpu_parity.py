@@ -666,3 +666,28 @@ def test_fit_trace_output(env, tmp_path):
     assert abs(costs[-1] - r2.chi2) <= 1e-9 * r2.chi2 or costs[-1] >= r2.chi2
     with pytest.raises(RuntimeError):
         fitter.fit(env["interp"], star.flux, star.var, trace_directory=str(tdir), best_particle_file=str(best_file))
+
+
+@pytest.mark.parametrize("run_len", ["1", "3", "16"])
+def test_broadening_independent_of_item_runs(env, monkeypatch, run_len):
+    """k_broaden hands each CTA runs of consecutive block pairs (their length
+    is chosen from the batch size; PASTA_BR_RUN fixes it).  Every block pair
+    is computed and resampled by exactly one CTA whatever the runs, so chi2
+    and the models are bit-identical for every run length."""
+    P, star = env["P"], env["star"]
+    disp = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(disp, cont, P.PSOSettings(16, 5), (0.0, 300.0), (-150.0, 150.0))
+    rng = np.random.default_rng(23)
+    n = 300
+    lab = np.stack([rng.uniform(6050, 7950, n), rng.uniform(-0.45, 0.45, n), rng.uniform(3.55, 4.45, n),
+                    rng.uniform(0, 300, n), rng.uniform(-140, 140, n)], axis=1)
+    monkeypatch.setenv("PASTA_BR_RUN", "1")
+    c_ref = np.array(fitter.chi2(env["interp"], star.flux, star.var, lab.tolist()))
+    m_ref = env["interp"].produce_model_bulk(disp, lab[:40])
+    monkeypatch.setenv("PASTA_BR_RUN", run_len)
+    c = np.array(fitter.chi2(env["interp"], star.flux, star.var, lab.tolist()))
+    m = env["interp"].produce_model_bulk(disp, lab[:40])
+    assert np.isfinite(c_ref).all()
+    np.testing.assert_array_equal(c, c_ref)
+    np.testing.assert_array_equal(m, m_ref)
