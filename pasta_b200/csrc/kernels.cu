@@ -576,13 +576,13 @@ constexpr int BR_S1 = 0, BR_S2 = BR_S1 + F2_S1 * 8, BR_T2 = BR_S2 + F2_S2 * 8, B
 // Resampling of an item's observed pixels [q0, q2) (the left synth pixel of
 // [q0, q1) in block 0, of [q1, q2) in block 1) from the final outputs in
 // shared memory, with the wavelength kind fixed at compile time.  The float
-// indices come from the star's table (a star's particles share it, so it
-// is read from L2); each thread issues the loads of EU pixels before their
-// arithmetic.
+// indices come from the star's table (a star's particles share it; the
+// item prefetched its range into L1 before the transforms); each thread
+// issues the loads of EU pixels before their arithmetic.
 template <int KIND>
 __device__ __forceinline__ void resample_item(const Resampler &R, float *y, const float *ob0,
                                               const float *ob1, int q0, int q1, int q2, int s0, int s1, int V) {
-  constexpr int EU = 4;
+  constexpr int EU = 8;
   for (int i0 = q0 + (int)threadIdx.x; i0 < q2; i0 += EU * BT) {
     double fx[EU];
 #pragma unroll
@@ -684,10 +684,13 @@ __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const
       q2 = has1 ? bd[2] : q1;
     }
     __syncthreads();  // the last item's epilogue is done with the shared buffers
-    // this item's inputs, observed float indices (uniform grids, cp.async)
-    // and instrument taps
+    // this item's inputs and instrument taps
     float in0[16], in1[16];
     broaden_inputs(b, w, P, in0, in1);
+    if (P.epi && G.wl_kind != WL_NONUNI) {  // the float indices the resampling reads: into L1 meanwhile
+      const double *fq = st.fidx + q0;
+      for (int l = t; l * 16 < q2 - q0; l += BT) asm volatile("prefetch.global.L1 [%0];" ::"l"(fq + 16 * l));
+    }
     const int e_last = min((has1 ? s1 : s0) + V, ohi);
     const bool fold = fixedk && m > 1 && st.gspec != nullptr && b.HG != nullptr && s0 - hg >= 0 && e_last + hg <= N;
     if (fixedk && !fold && P.star != gk_star) {  // the taps are applied from shared memory (edge blocks)
@@ -1527,14 +1530,40 @@ __device__ __forceinline__ void chunk_solve_warp(const EvalBatch &b, const DevSt
   }
 }
 
+// Monomial coefficients of the Legendre polynomials, T[k][j] = coefficient
+// of x^j in P_k, from (k + 1) P_{k+1} = (2k + 1) x P_k - k P_{k-1} (dyadic
+// rationals, exact in double up to degree 15).
+struct LegMono {
+  double c[MAX_P1][MAX_P1];
+};
+constexpr LegMono make_leg_mono() {
+  LegMono t{};
+  t.c[0][0] = 1.0;
+  t.c[1][1] = 1.0;
+  for (int k = 1; k + 1 < MAX_P1; k++)
+    for (int j = 0; j < MAX_P1; j++)
+      t.c[k + 1][j] = ((2 * k + 1) * (j > 0 ? t.c[k][j - 1] : 0.0) - k * t.c[k - 1][j]) / (k + 1);
+  return t;
+}
+__constant__ LegMono c_leg_mono = make_leg_mono();
+
+// the chunk polynomial sum_k a_k P_k(x) as monomial coefficients (FP64),
+// rounded to f32 for Horner evaluation
 template <int K>
-__device__ __forceinline__ float poly_eval_r(const float (&coef)[K], float x) {
-  float P[K];
-  legendre<K>(x, P);
-  float s = 0.0f;
+__device__ __forceinline__ void legendre_to_monomial(const double *a, float *m) {
+  for (int j = 0; j < K; j++) {
+    double s = 0.0;
+    for (int k = j; k < K; k++) s = fma(a[k], c_leg_mono.c[k][j], s);
+    m[j] = (float)s;
+  }
+}
+
+template <int K>
+__device__ __forceinline__ float horner(const float (&a)[K], float x) {
+  float p = a[K - 1];
 #pragma unroll
-  for (int k = 0; k < K; k++) s = fmaf(coef[k], P[k], s);
-  return s;
+  for (int j = K - 2; j >= 0; j--) p = fmaf(p, x, a[j]);
+  return p;
 }
 
 // chi2 section of chunk c (continuum_fitting.rs:280-360) walked by one
@@ -1566,7 +1595,7 @@ __device__ __forceinline__ double chunk_resid_warp(const DevStar &st, const floa
 #pragma unroll
       for (int u = 0; u < CU; u++) {
         if (i0 + 32 * u < hi) {
-          const float p = poly_eval_r<K>(cc, xa[u]);
+          const float p = horner<K>(cc, xa[u]);
           const float r = fl[u] - p * md[u];
           part += __fdividef(r * r, vr[u]);
         }
@@ -1595,8 +1624,8 @@ __device__ __forceinline__ double chunk_resid_warp(const DevStar &st, const floa
 #pragma unroll
       for (int u = 0; u < 2; u++) {
         if (i0 + 32 * u < sp) {
-          const float pv = poly_eval_r<K>(cp, xa[u]);
-          const float cu = poly_eval_r<K>(cc, xb[u]);
+          const float pv = horner<K>(cp, xa[u]);
+          const float cu = horner<K>(cc, xb[u]);
           const float p = pv * fc[u] + cu * (1.0f - fc[u]);
           const float r = fl[u] - p * md[u];
           part += __fdividef(r * r, vr[u]);
@@ -1641,8 +1670,7 @@ __global__ void __launch_bounds__(CT, K <= 8 ? 4 : 2) k_chunk_fit(EvalBatch b) {
   const int nc = st.n_chunks;
   for (int c = warp; c < nc; c += CW) {
     chunk_solve_warp<K>(b, st, mod, e, c, lane, zs[c]);
-    if (lane == 0)
-      for (int k = 0; k < K; k++) cfs[c][k] = (float)zs[c][k];
+    if (lane == 0) legendre_to_monomial<K>(zs[c], cfs[c]);
   }
   __syncthreads();
   for (int c = warp; c < nc; c += CW) {
