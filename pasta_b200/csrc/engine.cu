@@ -213,7 +213,6 @@ struct Workspace {
   DBuf<int> tccount;   // tensor-core groups per segment
   DBuf<int> tclist;    // indices of all tensor-core groups, and their count [1]
   DBuf<int> tclist_count;
-  DBuf<float> ccoef;   // chunk coefficients [cap][MAX_CHUNKS][MAX_P1]
   DBuf<double> cpart;  // chunk chi2 partials [cap][MAX_CHUNKS]
   DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
   DBuf<double> zpart;  // tensor-core linear continua: partial coefficients [cap][LIN_MAX_SLICES][64]
@@ -221,7 +220,7 @@ struct Workspace {
   void ensure(int64_t want, int64_t str, int bstr) {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
-    bnd.release(); ccoef.release(); cpart.release(); grec.release(); gcount.release();
+    bnd.release(); cpart.release(); grec.release(); gcount.release();
     tcrec.release(); tccount.release(); tclist.release(); tclist_count.release();
     dlist.release(); dcount.release(); zpart.release();
     cap = 0;
@@ -237,7 +236,6 @@ struct Workspace {
     tccount.alloc((size_t)want);
     tclist.alloc((size_t)want);
     tclist_count.alloc(1);
-    ccoef.alloc((size_t)want * MAX_CHUNKS * MAX_P1);
     cpart.alloc((size_t)want * MAX_CHUNKS);
     dlist.alloc((size_t)want);
     zpart.alloc((size_t)want * LIN_MAX_SLICES * 64);
@@ -253,7 +251,7 @@ struct Workspace {
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
   return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)sizeof(TcGroup) +
          8 + (int64_t)bnd_stride * 4 +
-         (int64_t)MAX_CHUNKS * (MAX_P1 * 4 + 8) + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8;
+         (int64_t)MAX_CHUNKS * 8 + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8;
 }
 
 struct pasta_grid {
@@ -839,7 +837,6 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.tmap = tc ? &g->tmap : nullptr;
   b.tc_min = g->tc_min;
   b.bnd_stride = g->ws.bnd_stride;
-  b.ccoef = g->ws.ccoef.p;
   b.cpart = g->ws.cpart.p;
   b.given = a.given ? a.given + (size_t)off * a.given_stride : nullptr;
   b.given_stride = a.given_stride;
@@ -2071,11 +2068,8 @@ int pasta_continuum_fit(const pasta_continuum *c, const float *model, const floa
     b.chunk_p1_mask = st.cont_kind == CONT_CHUNK ? 1u << st.p1 : 0u;
     b.max_chunks = st.cont_kind == CONT_CHUNK ? st.n_chunks : 0;
     b.other_cont = st.cont_kind == CONT_CHUNK ? 0 : 1;
-    DBuf<float> dcoef;
     DBuf<double> dpart;
-    dcoef.alloc((size_t)MAX_CHUNKS * MAX_P1);
     dpart.alloc(MAX_CHUNKS);
-    b.ccoef = dcoef.p;
     b.cpart = dpart.p;
     b.given = dm.p;
     DevGrid G{};
@@ -2489,7 +2483,6 @@ void run_binary(pasta_grid *g, const pasta_grid *gc, const DevStar *dstar, const
       cb.lin_group = linear_tc_enabled() ? 128 : 0;  // every label belongs to the one star
       cb.lin_kp_mask = a.lin_kp_mask;
       set_lin_slices(g, cb);
-      cb.ccoef = g->ws.ccoef.p;
       cb.cpart = g->ws.cpart.p;
       cb.given = bb.model;
       cb.given_stride = nobs;

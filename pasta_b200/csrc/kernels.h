@@ -63,7 +63,6 @@ struct EvalBatch {
   int obs_epi;               // chi2 batches: resample inside k_broaden, synth rows are not kept
   int *bnd;                  // [E][bnd_stride] first observed pixel of every broadening block
   int bnd_stride;
-  float *ccoef;              // [E][MAX_CHUNKS][MAX_P1] chunk polynomial coefficients (f32)
   double *cpart;             // [E][MAX_CHUNKS] chi2 partial sums per chunk section
   // Segments: the evaluations of each star (seg_len consecutive ones; 0:
   // the whole batch is one star) in chunks of at most SEG from the star's

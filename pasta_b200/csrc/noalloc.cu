@@ -72,11 +72,11 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // bytes of scratch one label needs: prep record, rotation half spectra
 // (alone and times the instrument spectrum),
 // eval->star index, the two spectrum rows, the broadening block bounds and
-// the chunk coefficients and partial sums
+// the partial chi2 sums
 size_t per_label_bytes(int64_t stride, int bnd_stride) {
   return align256(sizeof(EvalPrep)) + 2 * align256(1025 * sizeof(float2)) + align256(sizeof(int)) +
          2 * align256((size_t)stride * sizeof(float)) + align256((size_t)bnd_stride * sizeof(int)) +
-         align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float)) + align256((size_t)MAX_CHUNKS * sizeof(double)) +
+         align256((size_t)MAX_CHUNKS * sizeof(double)) +
          align256(sizeof(GroupRec)) + align256(sizeof(int));
 }
 
@@ -216,8 +216,6 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   p += align256((size_t)stride * sizeof(float) * (size_t)L);
   int *bnd = (int *)p;
   p += align256((size_t)bstr * sizeof(int) * (size_t)L);
-  float *ccoef = (float *)p;
-  p += align256((size_t)MAX_CHUNKS * MAX_P1 * sizeof(float) * (size_t)L);
   double *cpart = (double *)p;
   p += align256((size_t)MAX_CHUNKS * sizeof(double) * (size_t)L);
   // SEG group slots per segment of SEG labels: L rounded up to SEG
@@ -253,7 +251,6 @@ extern "C" int pasta_chi2_noalloc(const pasta_grid *g, const pasta_dispersion *d
   b.obs_epi = 1;
   b.bnd = bnd;
   b.bnd_stride = bstr;
-  b.ccoef = ccoef;
   b.cpart = cpart;
   b.grec = grec;
   b.gcount = gcount;
