@@ -56,9 +56,11 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # from one ncu capture of a mid-fit step of 256 stars (16,384 evaluations,
 # --clock-control none), divided by its evaluations: the traffic of a launch
 # grows in proportion to the evaluations it runs, so a full launch's traffic
-# is this figure times its evaluations.  k_broaden includes its block-bound
-# search; chi2 is both chunk kernels and the final sums.
-DRAM_BYTES_PER_EVAL = {"k_interp": 459082, "k_broaden": 534001 + 852, "chi2": 154226 + 143807 + 154 + 259}
+# is this figure times its evaluations.  The interpolation is the
+# tensor-core kernel plus the CUDA-core kernel (groups below the tuned
+# size); k_broaden includes its block-bound search; chi2 is k_chunk_fit.
+DRAM_BYTES_PER_EVAL = {"k_interp": 142447 + 308582 + 23127 + 2459, "k_broaden": 387851 + 133902 + 852,
+                       "chi2": 246046 + 5488}
 DRAM_SOURCE = "ncu capture, mid-fit step of 256 config-1 stars (16,384 evaluations), scaled per evaluation"
 
 
@@ -758,10 +760,10 @@ def run_ours(args):
                                             "bytes_per_step": step_dram},
                           "peak": peak, "peak_kind": peak_kind, "bytes_per_eval": path_bytes / ev},
         "roofline_kernels": [
-            hbm_view("k_interp", interp_bytes, stage["interp_ms"], "k_interp",
+            hbm_view("k_interp_tc+k_interp", interp_bytes, stage["interp_ms"], "k_interp",
                      "neighbour rows shared by a star's particles are read once per group and hit in L2, so the "
                      "algorithmic rate exceeds the DRAM rate"),
-            hbm_view("k_chunk_moments+k_chunk_resid", chi2_bytes, stage["chi2_ms"], "chi2"),
+            hbm_view("k_chunk_fit", chi2_bytes, stage["chi2_ms"], "chi2"),
         ],
         "dram_source": DRAM_SOURCE,
         "tuned": {"direct_max_taps": interp.direct_max, "interp_tc_min_members": interp.tc_min,
