@@ -637,9 +637,8 @@ __device__ __forceinline__ cf tw_pass1(int k1, const cf &w1, const cf &w2, const
 // EvalPrep::epi) the block resamples the observed pixels whose left synth
 // pixel it owns (EvalBatch::bnd lists them per block) from shared memory and
 // writes the model at the observed pixels to row B; the synth row never
-// reaches memory.  The next item's inputs are loaded into registers and this
-// item's observed float indices copied into shared memory (cp.async) while
-// the transforms run.
+// reaches memory.  An item's float indices are prefetched into L1 before its
+// transforms; a CTA takes runs of consecutive items (ItemCursor).
 __global__ void __launch_bounds__(BT, 5) k_broaden(DevGrid G, EvalBatch b, const float2 *__restrict__ tw, int run_len) {
   extern __shared__ __align__(16) unsigned char br_smem[];
   float2 *S1 = reinterpret_cast<float2 *>(br_smem + BR_S1);
@@ -1478,34 +1477,41 @@ __device__ __forceinline__ void chunk_solve_warp(const EvalBatch &b, const DevSt
   double z[K];
 #pragma unroll
   for (int k = 0; k < K; k++) z[k] = 0.0;
-  // loads of CU pixels are issued before any arithmetic on them
-  for (int i0 = lo + lane; i0 < hi; i0 += 32 * CU) {
-    float fl[CU], md[CU], xf[CU];
+  // pixels [a0, a1) with chunk coordinates xs (the upper-chunk coordinate
+  // below the previous chunk's stop); loads of CU pixels are issued before
+  // any arithmetic on them
+  auto walk = [&](int a0, int a1, const float *__restrict__ xs) {
+    for (int i0 = a0 + lane; i0 < a1; i0 += 32 * CU) {
+      float fl[CU], md[CU], xf[CU];
 #pragma unroll
-    for (int u = 0; u < CU; u++) {
-      const int i = min(i0 + 32 * u, hi - 1);
-      fl[u] = flux[i];
-      md[u] = mod[i];
-      xf[u] = (c > 0 && i < prev) ? st.xb[i] : st.xa[i];
-    }
-    float zp[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) zp[k] = 0.0f;
-#pragma unroll
-    for (int u = 0; u < CU; u++) {
-      if (i0 + 32 * u < hi) {
-        // flux / model as x * rcp(y) (at most 2 ulp; the moments are sums
-        // of thousands of such terms, accumulated in FP64)
-        const float y = __fdividef(fl[u], md[u]);
-        float Pk[K];
-        legendre<K>(xf[u], Pk);
-#pragma unroll
-        for (int k = 0; k < K; k++) zp[k] = fmaf(Pk[k], y, zp[k]);
+      for (int u = 0; u < CU; u++) {
+        const int i = min(i0 + 32 * u, a1 - 1);
+        fl[u] = flux[i];
+        md[u] = mod[i];
+        xf[u] = xs[i];
       }
-    }
+      float zp[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) z[k] += (double)zp[k];
-  }
+      for (int k = 0; k < K; k++) zp[k] = 0.0f;
+#pragma unroll
+      for (int u = 0; u < CU; u++) {
+        if (i0 + 32 * u < a1) {
+          // flux / model as x * rcp(y) (at most 2 ulp; the moments are sums
+          // of thousands of such terms, accumulated in FP64)
+          const float y = __fdividef(fl[u], md[u]);
+          float Pk[K];
+          legendre<K>(xf[u], Pk);
+#pragma unroll
+          for (int k = 0; k < K; k++) zp[k] = fmaf(Pk[k], y, zp[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) z[k] += (double)zp[k];
+    }
+  };
+  const int split = c > 0 ? min(max(prev, lo), hi) : lo;
+  walk(lo, split, st.xb);
+  walk(split, hi, st.xa);
 #pragma unroll
   for (int k = 0; k < K; k++) {
     const double t = warp_sum(z[k]);
