@@ -51,7 +51,13 @@ constexpr int G2_BH = 65536, G2_BL = 81920;                            // Q^T ti
 constexpr int LT_MISC = 98304;                                         // barrier, tensor-memory slot, flags
 constexpr int LT_RED = LT_MISC + 64;                                   // 128 doubles: half-1 residual sums
 constexpr int LT_RFAIL = LT_RED + LT_M * 8;                            // 128 ints: half-1 failure flags
-constexpr int LT_SMEM = LT_RFAIL + LT_M * 4;
+constexpr int LT_ROWS = LT_RFAIL + LT_M * 4;                           // 128 model-row pointers (null: no row)
+constexpr int LT_SMEM = LT_ROWS + LT_M * 8;
+// GEMM2: the ratio tile flux/model of 128 evaluations x 32 pixels, rows
+// 0-63 and 64-127 in the unused halves of the two Q^T tile buffers, each
+// row's 32 values XOR-swizzled by the row (conflict-free column reads)
+constexpr int G2_Y0 = G2_BH + 8192, G2_Y1 = G2_BL + 8192;
+static_assert(G2_Y1 + 8192 <= LT_MISC, "ratio tile");
 
 // byte offset of element (row, k) in a K-major tile with kt elements per
 // row: core matrix (row / 8, k / 4) of 8 rows x 16 bytes, row-group stride
@@ -135,6 +141,36 @@ __device__ __forceinline__ const float *lt_model_row(const EvalBatch &b, const E
   return (P.mobs_in_b ? b.bufB : b.bufA) + (size_t)e * b.stride;
 }
 
+// flux / model of the 16 (row, pixel) elements of a 128 x 32 stage this
+// thread loads: warp w takes rows 16 w .. 16 w + 15, and one warp
+// instruction covers 8 rows x 4 consecutive pixels (lane = 4 row + pixel),
+// so a row's pixels are read in 16-byte pieces by neighbouring lanes and the
+// K-major shared-memory stores of one instruction hit 32 distinct banks.
+// Element j: row 16 w + 8 (j >> 3) + (lane >> 2), pixel 4 (j & 7) + (lane & 3).
+// Rows without a model (null) and pixels at or past x1 give 0.
+__device__ __forceinline__ void load_ratio_tile(const float *const *rows, const float *flux, int i0, int x1,
+                                                float (&y)[16]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rr = lane >> 2, kk = lane & 3;
+  float fx[8];
+#pragma unroll
+  for (int pg = 0; pg < 8; pg++) {
+    const int i = i0 + 4 * pg + kk;
+    fx[pg] = i < x1 ? flux[i] : 0.0f;
+  }
+#pragma unroll
+  for (int rg = 0; rg < 2; rg++) {
+    const float *row = rows[16 * w + 8 * rg + rr];
+#pragma unroll
+    for (int pg = 0; pg < 8; pg++) {
+      const int i = i0 + 4 * pg + kk;
+      y[8 * rg + pg] = (row && i < x1) ? fx[pg] / row[i] : 0.0f;
+    }
+  }
+}
+__device__ __forceinline__ int ratio_row(int j) { return 16 * (threadIdx.x >> 5) + 8 * (j >> 3) + ((threadIdx.x & 31) >> 2); }
+__device__ __forceinline__ int ratio_px(int j) { return 4 * (j & 7) + (threadIdx.x & 3); }
+
 }  // namespace
 
 // One CTA per (group of b.lin_group consecutive evaluations of one star whose
@@ -172,6 +208,8 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + LT_MISC + 8);
   int *err = reinterpret_cast<int *>(sm + LT_MISC + 16);
   double *red = reinterpret_cast<double *>(sm + LT_RED);
+  const float **rows = reinterpret_cast<const float **>(sm + LT_ROWS);
+  if (t < LT_M) rows[t] = mod;  // t = p, h = 0
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -203,11 +241,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
     const int r = t >> 2, kq = 8 * (t & 3);  // Q stage: basis row r, pixels kq .. kq + 8
     float av[16], qv[8];
     auto load_stage = [&](int i0) {
-#pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int i = i0 + 16 * h + j;
-        av[j] = (live && i < x1) ? flux[i] / mod[i] : 0.0f;
-      }
+      load_ratio_tile(rows, flux, i0, x1, av);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const int i = i0 + kq + j;
@@ -217,9 +251,13 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
     if (x0 < x1) load_stage(x0);
     for (int i0 = x0; i0 < x1 && ok; i0 += LT_TK) {
 #pragma unroll
-      for (int g = 0; g < 4; g++)
-        store_split4(sm, G1_AH + kmaj(p, 16 * h + 4 * g, LT_TK), G1_AL + kmaj(p, 16 * h + 4 * g, LT_TK),
-                     make_float4(av[4 * g], av[4 * g + 1], av[4 * g + 2], av[4 * g + 3]));
+      for (int j = 0; j < 16; j++) {
+        float hi, lo;
+        split_tf32(av[j], hi, lo);
+        const int o = kmaj(ratio_row(j), ratio_px(j), LT_TK);
+        *reinterpret_cast<float *>(sm + G1_AH + o) = hi;
+        *reinterpret_cast<float *>(sm + G1_AL + o) = lo;
+      }
       if (r < KP) {
 #pragma unroll
         for (int g = 0; g < 2; g++)
@@ -300,8 +338,19 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
         qv[g] = (i < x1 && kq + 4 * g < KP) ? *reinterpret_cast<const float4 *>(qt + (size_t)i * KP + kq + 4 * g)
                                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     };
-    if (x0 < x1) load_tile(x0);
+    // ratio tile element (row, pixel) in shared memory
+    auto yslot = [&](int row, int k) -> float * {
+      return reinterpret_cast<float *>(sm + (row < 64 ? G2_Y0 : G2_Y1)) + (row & 63) * 32 + (k ^ (row & 31));
+    };
+    float yv[16];  // this thread's part of the next ratio tile (coalesced loads)
+    if (x0 < x1) {
+      load_tile(x0);
+      load_ratio_tile(rows, flux, x0, x1, yv);
+    }
     for (int i0 = x0; i0 < x1 && ok; i0 += LT_TN) {
+      if (i0 > x0) __syncthreads();  // every thread is done with the previous ratio tile
+#pragma unroll
+      for (int j = 0; j < 16; j++) *yslot(ratio_row(j), ratio_px(j)) = yv[j];
 #pragma unroll
       for (int g = 0; g < 2; g++)
         if (kq + 4 * g < KP) store_split4(sm, G2_BH + kmaj(r, kq + 4 * g, KP), G2_BL + kmaj(r, kq + 4 * g, KP), qv[g]);
@@ -321,14 +370,16 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
         }
         mma_commit(mbar);
       }
-      // while the MMAs run: the next tile's basis and this tile's ratios and variances
-      if (i0 + LT_TN < x1) load_tile(i0 + LT_TN);
-      float bb[16], vv[16];
+      // while the MMAs run: the next tile's basis and ratios, this tile's variances
+      if (i0 + LT_TN < x1) {
+        load_tile(i0 + LT_TN);
+        load_ratio_tile(rows, flux, i0 + LT_TN, x1, yv);
+      }
+      float vv[16];
 #pragma unroll
       for (int j = 0; j < 16; j++) {
         const int i = i0 + 16 * h + j;
         const bool use = live && i >= 50 && i < N - 50 && i < x1;
-        bb[j] = use ? flux[i] / mod[i] : 0.0f;
         vv[j] = use ? var[i] : 0.0f;
       }
       if (!mbar_wait(mbar, phase)) atomicOr(err, 1);
@@ -355,7 +406,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
           for (int j = 0; j < 8; j++) {
             const int i = i0 + 16 * h + c + j;
             if (i >= 50 && i < N - 50 && i < x1) {
-              const float rr = (float)f[j] - bb[c + j];
+              const float rr = (float)f[j] - *yslot(p, 16 * h + c + j);
               acc += (double)(rr / vv[c + j] * rr);
             }
           }
