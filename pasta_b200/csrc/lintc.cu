@@ -52,7 +52,8 @@ constexpr int LT_MISC = 98304;                                         // barrie
 constexpr int LT_RED = LT_MISC + 64;                                   // 128 doubles: half-1 residual sums
 constexpr int LT_RFAIL = LT_RED + LT_M * 8;                            // 128 ints: half-1 failure flags
 constexpr int LT_ROWS = LT_RFAIL + LT_M * 4;                           // 128 model-row pointers (null: no row)
-constexpr int LT_SMEM = LT_ROWS + LT_M * 8;
+constexpr int LT_VAR = LT_ROWS + LT_M * 8;                             // GEMM2: the tile's 32 variances
+constexpr int LT_SMEM = LT_VAR + LT_TN * 4;
 // GEMM2: the ratio tile flux/model of 128 evaluations x 32 pixels, rows
 // 0-63 and 64-127 in the unused halves of the two Q^T tile buffers, each
 // row's 32 values XOR-swizzled by the row (conflict-free column reads)
@@ -305,14 +306,13 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
   } else {
     // ---------------------------------------------- GEMM2 + residual epilogue over the slice
     bool zfail = false;
-    if (live) {
-      for (int s2 = 0; s2 < S; s2++)
+    if (live) {  // slot 0 holds the slices' partial coefficients added in slice order (k_linear_zsum)
 #pragma unroll
-        for (int c = 0; c < HALF; c++) {
-          const double v = zp[(size_t)s2 * 64 + h * HALF + c];
-          zfail |= v == LT_FAILED;
-          z[c] += v;
-        }
+      for (int c = 0; c < HALF; c++) {
+        const double v = zp[h * HALF + c];
+        zfail |= v == LT_FAILED;
+        z[c] = v;
+      }
       if (b.params && sl == 0) {
         double *par = b.params + (size_t)e * b.param_stride;
 #pragma unroll
@@ -342,6 +342,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
     auto yslot = [&](int row, int k) -> float * {
       return reinterpret_cast<float *>(sm + (row < 64 ? G2_Y0 : G2_Y1)) + (row & 63) * 32 + (k ^ (row & 31));
     };
+    float *svar = reinterpret_cast<float *>(sm + LT_VAR);
     float yv[16];  // this thread's part of the next ratio tile (coalesced loads)
     if (x0 < x1) {
       load_tile(x0);
@@ -351,6 +352,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
       if (i0 > x0) __syncthreads();  // every thread is done with the previous ratio tile
 #pragma unroll
       for (int j = 0; j < 16; j++) *yslot(ratio_row(j), ratio_px(j)) = yv[j];
+      if (t < LT_TN) svar[t] = i0 + t < x1 ? var[i0 + t] : 1.0f;
 #pragma unroll
       for (int g = 0; g < 2; g++)
         if (kq + 4 * g < KP) store_split4(sm, G2_BH + kmaj(r, kq + 4 * g, KP), G2_BL + kmaj(r, kq + 4 * g, KP), qv[g]);
@@ -370,17 +372,10 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
         }
         mma_commit(mbar);
       }
-      // while the MMAs run: the next tile's basis and ratios, this tile's variances
+      // while the MMAs run: the next tile's basis and ratios
       if (i0 + LT_TN < x1) {
         load_tile(i0 + LT_TN);
         load_ratio_tile(rows, flux, i0 + LT_TN, x1, yv);
-      }
-      float vv[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int i = i0 + 16 * h + j;
-        const bool use = live && i >= 50 && i < N - 50 && i < x1;
-        vv[j] = use ? var[i] : 0.0f;
       }
       if (!mbar_wait(mbar, phase)) atomicOr(err, 1);
       phase ^= 1u;
@@ -407,7 +402,7 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
             const int i = i0 + 16 * h + c + j;
             if (i >= 50 && i < N - 50 && i < x1) {
               const float rr = (float)f[j] - *yslot(p, 16 * h + c + j);
-              acc += (double)(rr / vv[c + j] * rr);
+              acc += (double)(rr / svar[16 * h + c + j] * rr);
             }
           }
         }
@@ -430,6 +425,27 @@ __global__ void __launch_bounds__(LT_T) k_linear_tc(EvalBatch b) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(LT_TMEM_COLS) : "memory");
   }
+}
+
+// The slices' partial coefficients of every evaluation added in slice order
+// into slot 0 (one thread per evaluation and basis column; a failed slice
+// fails the sum), so that each residual-pass CTA reads 64 values instead of
+// 64 per slice.
+__global__ void k_linear_zsum(EvalBatch b, int kp) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)b.E * 64) return;
+  const int e = (int)(i >> 6), c = (int)(i & 63);
+  const DevStar &st = b.stars[b.prep[(e / b.lin_group) * b.lin_group].star];  // the group's star
+  if (st.cont_kind != CONT_LINEAR || st.kp != kp) return;
+  double *zp = b.lin_zpart + (size_t)e * LIN_MAX_SLICES * 64 + c;
+  double acc = 0.0;
+  bool fail = false;
+  for (int s = 0; s < b.lin_slices; s++) {
+    const double v = zp[(size_t)s * 64];
+    fail |= v == LT_FAILED;
+    acc += v;
+  }
+  zp[0] = fail ? LT_FAILED : acc;
 }
 
 // chi2 = the slices' residual sums in slice order / N, and the statuses, of
@@ -463,6 +479,10 @@ static void launch_kp(const EvalBatch &b, dim3 grid, cudaStream_t s) {
   cudaFuncSetAttribute(k_linear_tc<KP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
   cudaFuncSetAttribute(k_linear_tc<KP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, LT_SMEM);
   k_linear_tc<KP, 0><<<grid, LT_T, LT_SMEM, s>>>(b);
+  if (grid.y > 1) {
+    k_linear_zsum<<<(unsigned)(((long long)b.E * 64 + 255) / 256), 256, 0, s>>>(b, KP);
+    count_launch();
+  }
   k_linear_tc<KP, 1><<<grid, LT_T, LT_SMEM, s>>>(b);
   count_launch(2);
 }
