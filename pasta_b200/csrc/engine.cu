@@ -199,6 +199,14 @@ double now_s() {
 }  // namespace
 
 // =================================================================== grid
+// slots of the table that merges evaluations alone in their segment: a power
+// of two, at least twice the evaluations (at most half full)
+int merge_table_slots(int64_t evals) {
+  int64_t n = 1024;
+  while (n < 2 * evals) n *= 2;
+  return (int)n;
+}
+
 struct Workspace {
   int64_t cap = 0, stride = 0;
   int bnd_stride = 0;
@@ -217,12 +225,18 @@ struct Workspace {
   DBuf<int> dlist;     // evaluations on the direct broadening path [cap], and their count [1]
   DBuf<double> zpart;  // tensor-core linear continua: partial coefficients [cap][LIN_MAX_SLICES][64]
   DBuf<int> dcount;
+  // merging of evaluations alone in their segment (EvalBatch::mkey)
+  int mtab = 0;
+  DBuf<unsigned long long> mkey;
+  DBuf<int> mcnt, mmem, mslot, erec, mrcount;
+  DBuf<GroupRec> mrec;
   void ensure(int64_t want, int64_t str, int bstr) {
     if (want <= cap && str == stride && bstr == bnd_stride) return;
     A.release(); B.release(); H.release(); HG.release(); prep.release();
     bnd.release(); cpart.release(); grec.release(); gcount.release();
     tcrec.release(); tccount.release(); tclist.release(); tclist_count.release();
     dlist.release(); dcount.release(); zpart.release();
+    mkey.release(); mcnt.release(); mmem.release(); mslot.release(); erec.release(); mrec.release(); mrcount.release();
     cap = 0;
     A.alloc((size_t)want * str);
     B.alloc((size_t)want * str);
@@ -240,6 +254,14 @@ struct Workspace {
     dlist.alloc((size_t)want);
     zpart.alloc((size_t)want * LIN_MAX_SLICES * 64);
     dcount.alloc(1);
+    mtab = merge_table_slots(want);
+    mkey.alloc((size_t)mtab);
+    mcnt.alloc((size_t)mtab);
+    mmem.alloc((size_t)mtab * MERGE_CAP);
+    mslot.alloc((size_t)mtab + 1);
+    erec.alloc((size_t)want);
+    mrec.alloc((size_t)(want + 1) / 2);
+    mrcount.alloc(1);
     cap = want;
     stride = str;
     bnd_stride = bstr;
@@ -251,7 +273,9 @@ struct Workspace {
 int64_t workspace_bytes_per_eval(int64_t stride, int bnd_stride) {
   return stride * 8 + 2 * 1025 * 8 + (int64_t)sizeof(EvalPrep) + (int64_t)sizeof(GroupRec) + (int64_t)sizeof(TcGroup) +
          8 + (int64_t)bnd_stride * 4 +
-         (int64_t)MAX_CHUNKS * 8 + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8;
+         (int64_t)MAX_CHUNKS * 8 + 4 + (int64_t)LIN_MAX_SLICES * 64 * 8 +
+         // merge table (up to 4 slots per evaluation), own-record index, merged records
+         4 * (8 + 4 + 4 * MERGE_CAP + 4) + 4 + (int64_t)sizeof(GroupRec) / 2;
 }
 
 struct pasta_grid {
@@ -792,6 +816,13 @@ bool interp_tc_enabled() {
   return v != 0;
 }
 
+// evaluations alone in their segment merged across segments: on unless
+// PASTA_INTERP_MERGE=0
+bool interp_merge_enabled() {
+  const char *e = getenv("PASTA_INTERP_MERGE");
+  return !(e && e[0] == '0');
+}
+
 int width_upper_bound(const pasta_grid *g, double vsini_hi) {
   if (g->d.dvelo <= 0.0 || !(vsini_hi > 0.0)) return 1;
   int w = rotation_width(vsini_hi, g->d.dvelo);
@@ -836,6 +867,16 @@ EvalBatch make_batch(pasta_grid *g, const EvalArgs &a, int64_t off, int64_t cnt)
   b.tclist_count = g->ws.tclist_count.p;
   b.tmap = tc ? &g->tmap : nullptr;
   b.tc_min = g->tc_min;
+  if (interp_merge_enabled()) {
+    b.mkey = g->ws.mkey.p;
+    b.mcnt = g->ws.mcnt.p;
+    b.mmem = g->ws.mmem.p;
+    b.mslot = g->ws.mslot.p;
+    b.mtab = g->ws.mtab;
+    b.erec = g->ws.erec.p;
+    b.mrec = g->ws.mrec.p;
+    b.mrcount = g->ws.mrcount.p;
+  }
   b.bnd_stride = g->ws.bnd_stride;
   b.cpart = g->ws.cpart.p;
   b.given = a.given ? a.given + (size_t)off * a.given_stride : nullptr;

@@ -151,6 +151,20 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
     b.gcount[s] = n;
   }
   __syncthreads();
+  if (sl == 0 && b.mkey && ok[t] && tcg[lead[t]] < 0 && cnt_l[lead[t]] == 1) {
+    // alone in its segment: offer it to the batch-wide table of column sets
+    const unsigned long long key = hs[t] | 1ull;
+    unsigned slot = (unsigned)(key ^ (key >> 31)) & (unsigned)(b.mtab - 1);
+    for (int probe = 0; probe < b.mtab; probe++) {  // the table is at most half full
+      const unsigned long long old = atomicCAS(&b.mkey[slot], 0ull, key);
+      if (old == 0ull || old == key) break;
+      slot = (slot + 1) & (unsigned)(b.mtab - 1);
+    }
+    const int r = atomicAdd(&b.mcnt[slot], 1);
+    if (r < MERGE_CAP) b.mmem[(size_t)slot * MERGE_CAP + r] = e;
+    if (r == 1) b.mslot[1 + atomicAdd(&b.mslot[0], 1)] = (int)slot;
+    b.erec[e] = start + gid[t];
+  }
   // tensor-core group records: slice sl writes groups sl, sl + GROUP_SLICES,
   // ... (thread t: row t, member t)
   for (int tg = sl; tg < ntc; tg += GROUP_SLICES) {
@@ -238,11 +252,104 @@ __global__ void __launch_bounds__(SEG *GROUP_SLICES) k_group(DevGrid G, EvalBatc
   }
 }
 
+// One 64-thread CTA per listed table slot (two or more evaluations alone in
+// their segments chose it): the evaluations whose columns equal the first
+// one's (a hash collision leaves the others alone) become group records of
+// up to GROUP_MAX members like k_group's (rows any member weighs, in
+// reference order), and their own single-member records are switched off
+// (nmem 0).
+__global__ void __launch_bounds__(SEG) k_merge(DevGrid G, EvalBatch b) {
+  __shared__ int mem[MERGE_CAP];
+  __shared__ int nmem_s, cnt[2];
+  const int t = threadIdx.x, lane = t & 31, wv = t >> 5;
+  static_assert(MERGE_CAP == SEG, "one thread per listed evaluation");
+  const int nlist = b.mslot[0];
+  for (int j = blockIdx.x; j < nlist; j += gridDim.x) {
+    const int slot = b.mslot[1 + j];
+    const int nc = min(b.mcnt[slot], MERGE_CAP);
+    int e = -1;
+    if (t < nc) {
+      e = b.mmem[(size_t)slot * MERGE_CAP + t];
+      const int *c0 = b.prep[b.mmem[(size_t)slot * MERGE_CAP]].cols, *c = b.prep[e].cols;
+      bool same = true;
+      for (int n = 0; n < 64 && same; n++) same = c[n] == c0[n];
+      if (!same) e = -1;
+    }
+    // compact the matching evaluations, keeping their order
+    const unsigned bm = __ballot_sync(0xffffffffu, e >= 0);
+    if (lane == 0) cnt[wv] = __popc(bm);
+    __syncthreads();
+    if (e >= 0) mem[__popc(bm & ((1u << lane) - 1u)) + (wv ? cnt[0] : 0)] = e;
+    if (t == 0) nmem_s = cnt[0] + cnt[1];
+    __syncthreads();
+    const int nt = nmem_s;
+    if (nt >= 2) {
+      for (int g0 = 0; g0 < nt; g0 += GROUP_MAX) {
+        const int nm = min(GROUP_MAX, nt - g0);
+        __shared__ int rec;
+        if (t == 0) rec = atomicAdd(b.mrcount, 1);
+        __syncthreads();
+        GroupRec &R = b.mrec[rec];
+        // row t of the group: kept when any member weighs it
+        const int c = b.prep[mem[g0]].cols[t];
+        const float f = c >= 0 ? G.factor[c] : 0.0f;
+        float w[GROUP_MAX], wf[GROUP_MAX];
+        bool keep = false;
+#pragma unroll
+        for (int m = 0; m < GROUP_MAX; m++) {
+          w[m] = (m < nm && c >= 0) ? b.prep[mem[g0 + m]].w[t] : 0.0f;
+          wf[m] = w[m] * f;
+          keep |= wf[m] != 0.0f;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        __syncthreads();  // cnt is reused
+        if (lane == 0) cnt[wv] = __popc(bal);
+        __syncthreads();
+        const int pos = __popc(bal & ((1u << lane) - 1u)) + (wv ? cnt[0] : 0);
+        if (keep) {
+          R.wf[pos][0] = make_float4(wf[0], wf[1], wf[2], wf[3]);
+          R.wf[pos][1] = make_float4(wf[4], wf[5], wf[6], wf[7]);
+          R.w[pos][0] = make_float4(w[0], w[1], w[2], w[3]);
+          R.w[pos][1] = make_float4(w[4], w[5], w[6], w[7]);
+          R.col[pos] = c;
+          R.f[pos] = f;
+        }
+        const int kept = cnt[0] + cnt[1];
+        const int padded = (kept + 7) & ~7;
+        if (t >= kept && t < padded) {  // zero-weight padding rows (add exactly 0)
+          const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          R.wf[t][0] = R.wf[t][1] = R.w[t][0] = R.w[t][1] = z4;
+          R.col[t] = 0;
+          R.f[t] = 0.0f;
+        }
+        if (t < GROUP_MAX) R.member[t] = t < nm ? mem[g0 + t] : -1;
+        if (t == 0) {
+          R.nmem = nm;
+          R.nn = padded;
+        }
+        if (t < nm) b.grec[b.erec[mem[g0 + t]]].nmem = 0;  // interpolated here instead
+        __syncthreads();
+      }
+    }
+    __syncthreads();
+  }
+}
+
 void launch_group(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   if (b.E <= 0) return;
   if (b.tcrec) cudaMemsetAsync(b.tclist_count, 0, sizeof(int), s);
+  if (b.mkey) {
+    cudaMemsetAsync(b.mkey, 0, (size_t)b.mtab * sizeof(unsigned long long), s);
+    cudaMemsetAsync(b.mcnt, 0, (size_t)b.mtab * sizeof(int), s);
+    cudaMemsetAsync(b.mslot, 0, sizeof(int), s);
+    cudaMemsetAsync(b.mrcount, 0, sizeof(int), s);
+  }
   k_group<<<num_segments(b), SEG * GROUP_SLICES, 0, s>>>(G, b);
   count_launch();
+  if (b.mkey) {
+    k_merge<<<num_sms() * 8, SEG, 0, s>>>(G, b);
+    count_launch();
+  }
 }
 
 constexpr int IT_T = 256, IT_PX = 4, IT_TILE = IT_T * IT_PX;
@@ -325,6 +432,21 @@ __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch
   }
 }
 
+// one group record on this thread's pixels (nmem 0: a record switched off)
+__device__ __forceinline__ void interp_group(const DevGrid &G, const EvalBatch &b, const GroupRec &R, int px) {
+  switch (R.nmem) {
+    case 0: break;
+    case 1: interp_members<1>(G, b, R, px); break;
+    case 2: interp_members<2>(G, b, R, px); break;
+    case 3: interp_members<3>(G, b, R, px); break;
+    case 4: interp_members<4>(G, b, R, px); break;
+    case 5: interp_members<5>(G, b, R, px); break;
+    case 6: interp_members<6>(G, b, R, px); break;
+    case 7: interp_members<7>(G, b, R, px); break;
+    default: interp_members<8>(G, b, R, px); break;
+  }
+}
+
 // Grid: x = segment, y = tile of IT_TILE pixels, so CTAs that run together read
 // the same tile slab of the resident grid (57 MB for 13,860 x 80,000), which
 // stays in L2; z = slice of the segment's groups (groups z, z + Z, ...), more
@@ -342,16 +464,25 @@ __global__ void __launch_bounds__(IT_T, 3) k_interp(DevGrid G, EvalBatch b) {
     float4 *dst = reinterpret_cast<float4 *>(&R);
     for (int i = threadIdx.x; i < (int)(sizeof(GroupRec) / 16); i += IT_T) dst[i] = src[i];
     __syncthreads();
-    switch (R.nmem) {
-      case 1: interp_members<1>(G, b, R, px); break;
-      case 2: interp_members<2>(G, b, R, px); break;
-      case 3: interp_members<3>(G, b, R, px); break;
-      case 4: interp_members<4>(G, b, R, px); break;
-      case 5: interp_members<5>(G, b, R, px); break;
-      case 6: interp_members<6>(G, b, R, px); break;
-      case 7: interp_members<7>(G, b, R, px); break;
-      default: interp_members<8>(G, b, R, px); break;
-    }
+    interp_group(G, b, R, px);
+    __syncthreads();
+  }
+}
+
+// Groups merged across segments (k_merge), in work items (record, tile)
+// taken tile by tile, so that CTAs that run together read the same tile
+// slab of the grid; their number is known on the device only.
+__global__ void __launch_bounds__(IT_T, 3) k_interp_merged(DevGrid G, EvalBatch b) {
+  __shared__ GroupRec R;
+  const int nrec = *b.mrcount;
+  const long long work = (long long)nrec * ((G.npx + IT_TILE - 1) / IT_TILE);
+  for (long long w = blockIdx.x; w < work; w += gridDim.x) {
+    const int tile = (int)(w / nrec), rec = (int)(w - (long long)tile * nrec);
+    const float4 *src = reinterpret_cast<const float4 *>(b.mrec + rec);
+    float4 *dst = reinterpret_cast<float4 *>(&R);
+    for (int i = threadIdx.x; i < (int)(sizeof(GroupRec) / 16); i += IT_T) dst[i] = src[i];
+    __syncthreads();
+    interp_group(G, b, R, tile * IT_TILE + threadIdx.x * IT_PX);
     __syncthreads();
   }
 }
@@ -364,6 +495,10 @@ void launch_interp(const DevGrid &G, const EvalBatch &b, cudaStream_t s) {
   dim3 grid(segs, tiles, z);
   k_interp<<<grid, IT_T, 0, s>>>(G, b);
   count_launch();
+  if (b.mkey) {
+    k_interp_merged<<<num_sms() * 6, IT_T, 0, s>>>(G, b);
+    count_launch();
+  }
 }
 
 // ------------------------------------------------------------ resampling

@@ -12,6 +12,7 @@ namespace pb {
 // reference order (zero-weight rows of every member dropped, padded to a
 // multiple of 8 with zero weights).
 constexpr int GROUP_MAX = 8, SEG = 64;
+constexpr int MERGE_CAP = 64;  // evaluations one merge-table slot takes (in groups of GROUP_MAX)
 struct __align__(16) GroupRec {
   float4 wf[64][2];       // per member (8) weight x dequantisation factor (0: padding / not a member)
   float4 w[64][2];        // per member weight (the exact tail path)
@@ -76,6 +77,19 @@ struct EvalBatch {
   int *tclist_count;         // [1] their number (zeroed before k_group)
   int tc_min;                // members a tensor-core group needs (TC_MIN_MEMBERS .. SEG; larger: none)
   int *tccount;              // [segments]
+  // Evaluations that end up alone in their segment (spread swarms: the early
+  // iterations of a fit) are merged across segments with the others that
+  // have the same neighbour columns, in groups of up to GROUP_MAX, when mkey
+  // is set (null: off).  Merging changes no result: every member keeps its
+  // own accumulators and row order.
+  unsigned long long *mkey;  // [mtab] hash of the columns per table slot (0: empty); zeroed before k_group
+  int *mcnt;                 // [mtab] evaluations that chose each slot; zeroed before k_group
+  int *mmem;                 // [mtab][MERGE_CAP] the first MERGE_CAP of them
+  int *mslot;                // [1 + mtab] number of slots with two or more evaluations, then the slots
+  int mtab;                  // table slots (a power of two, at least 2 E)
+  int *erec;                 // [E] record index of the evaluation's own (alone) group
+  GroupRec *mrec;            // [(E + 1) / 2] merged group records (at most half the evaluations)
+  int *mrcount;              // [1] their number
   const void *tmap;          // host pointer to the grid's TMA tensor map (null: no tensor-core path)
   const float *given;        // model given at the observed pixels (continuum utilities) or null
   int64_t given_stride;      // floats between the given rows of consecutive evaluations

@@ -691,3 +691,38 @@ def test_broadening_independent_of_item_runs(env, monkeypatch, run_len):
     assert np.isfinite(c_ref).all()
     np.testing.assert_array_equal(c, c_ref)
     np.testing.assert_array_equal(m, m_ref)
+
+
+def test_merged_interpolation_groups_are_bit_identical(env, monkeypatch):
+    """Evaluations alone in their segment (chunks of 64 labels) but with the
+    same neighbour columns as evaluations of other segments are interpolated
+    together (k_merge / k_interp_merged).  Every member keeps its own
+    accumulators and row order, so chi2 and the models are bit-identical with
+    the merging switched off (PASTA_INTERP_MERGE=0), and match the oracle."""
+    O, P, star = env["O"], env["P"], env["star"]
+    disp = P.FixedResolutionDispersion(star.wl, 85000.0, env["wl"])
+    cont = P.ChunkContinuumFitter(star.wl, 5, 8, 0.2)
+    fitter = env["interp"].get_fitter(disp, cont, P.PSOSettings(16, 5), (0.0, 300.0), (-150.0, 150.0))
+    rng = np.random.default_rng(31)
+    n = 512
+    lab = np.stack([rng.uniform(6050, 7950, n), rng.uniform(-0.45, 0.45, n), rng.uniform(3.55, 4.45, n),
+                    rng.uniform(0, 300, n), rng.uniform(-140, 140, n)], axis=1)
+    # one label per segment in the same grid cell (and a second cell), the rest spread
+    for k in range(8):
+        lab[64 * k + 5] = [7130.0 + 10 * k, 0.07 - 0.01 * k, 4.02 + 0.01 * k, 50.0 + k, 20.0 - k]
+        lab[64 * k + 9, :3] = [6310.0 + 5 * k, -0.31, 3.66]
+    monkeypatch.setenv("PASTA_INTERP_MERGE", "0")
+    c_off = np.array(fitter.chi2(env["interp"], star.flux, star.var, lab.tolist()))
+    m_off = env["interp"].produce_model_bulk(disp, lab[:192])
+    monkeypatch.setenv("PASTA_INTERP_MERGE", "1")
+    c_on = np.array(fitter.chi2(env["interp"], star.flux, star.var, lab.tolist()))
+    m_on = env["interp"].produce_model_bulk(disp, lab[:192])
+    assert np.isfinite(c_on).all()
+    np.testing.assert_array_equal(c_on, c_off)
+    np.testing.assert_array_equal(m_on, m_off)
+    og = env["og"]
+    od = O.Disp(og, O.DISP_FIXED, star.wl, 85000.0)
+    oc = O.Cont(O.CONT_CHUNK, star.wl, 5, 8, 0.2)
+    idx = [5, 69, 133]
+    ref = O.chi2(og, od, oc, star.flux, star.var, lab[idx], O.F64)[0]
+    np.testing.assert_allclose(c_on[idx], ref, rtol=CHI2_TOL)
