@@ -380,7 +380,7 @@ __device__ __forceinline__ void interp_members(const DevGrid &G, const EvalBatch
 #pragma unroll
     for (int m = 0; m < NM; m++) acc[m][0] = acc[m][1] = make_float2(0.0f, 0.0f);
     const float2 bias = make_float2(-8388608.0f, -8388608.0f);
-    constexpr int UNR = NM > 4 ? 4 : 8;  // row loads in flight per thread (with their weights in registers)
+    constexpr int UNR = NM > 4 ? 4 : NM > 2 ? 8 : 16;  // row loads in flight per thread (with their weights in registers)
 #pragma unroll UNR
     for (int n = 0; n < nn; n++) {
       const uint2 q = __ldg(reinterpret_cast<const uint2 *>(G.spectra + (size_t)R.col[n] * G.stride + px));
