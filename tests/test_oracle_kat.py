@@ -291,3 +291,78 @@ def test_binary_fit_is_deterministic_and_bounded(binary_small):
     np.testing.assert_array_equal(r1["label1"], r2["label1"])
     assert r1["light_ratio"] == 0.6
     assert 0.0 <= r1["label1"][3] <= 100.0 and -100.0 <= r1["label2"][4] <= 100.0
+
+
+def _oa_convolve_numpy32(x, k):
+    """convolve_rv.rs:121-157 restated with numpy's float32 FFT (pocketfft), an
+    FFT implementation independent of the oracle's own radix-2 transform:
+    overlap-add blocks of 2048 - (m - 1) inputs, forward real FFT, product
+    with the kernel's spectrum, inverse, summed into the output."""
+    n, m = 2048, len(k)
+    step, L = n - (m - 1), len(x)
+    nx = -(-L // step) * step
+    pad = np.zeros(n, np.float32)
+    pad[:m] = k
+    H = np.fft.rfft(pad)
+    y = np.zeros(nx + m - 1 + n, np.float32)
+    for pos in range(0, nx, step):
+        ln = min(step, L - pos)
+        pad = np.zeros(n, np.float32)
+        pad[:ln] = x[pos:pos + ln]
+        r = np.fft.irfft(np.fft.rfft(pad) * H, n).astype(np.float32)
+        y[pos:pos + n] += r
+    return y
+
+
+@pytest.mark.parametrize("vsini", [8.0, 60.0, 300.0])
+def test_fft_substitution_matches_an_independent_float32_fft(small, vsini):
+    """The oracle's FP32 mirror replaces rustfft/realfft by its own radix-2
+    real FFT with the reference's overlap-add blocking.  The same blocking
+    with numpy's float32 FFT (an independent implementation, as rustfft is)
+    agrees with it to float32 roundoff, and both sit at the same distance
+    from the FP64 (direct) convolution."""
+    spec, labels, spectra, g = small
+    x = g.interpolate(7000.0, 0.0, 4.0, O.F32)
+    k = O.rotation_kernel(vsini, np.log(10.0) * spec.log_step).astype(np.float32)
+    start = len(k) // 2
+    ref_np = _oa_convolve_numpy32(x.astype(np.float32), k)[start:start + len(x)].astype(np.float64)
+    y32 = g.convolve_rotation(x, vsini, O.F32)
+    y64 = g.convolve_rotation(x, vsini, O.F64)
+    scale = np.abs(y64).max()
+    # measured: 3-5e-7 of the maximum between the two float32 FFTs, and 2-5e-7 from FP64 for each
+    assert np.abs(y32 - ref_np).max() <= 1e-6 * scale
+    e_oracle, e_numpy = np.abs(y32 - y64).max() / scale, np.abs(ref_np - y64).max() / scale
+    assert e_oracle <= 1e-6 and e_numpy <= 1e-6
+
+
+def test_qr_substitution_matches_svd_least_squares(small):
+    """The oracle's FP32 mirror solves each chunk's unweighted least squares
+    (continuum_fitting.rs:216-226) by Householder QR instead of nalgebra's f32
+    SVD.  LAPACK's float32 SVD least squares (numpy lstsq, sgelsd) on the same
+    float32 design matrix and ratios gives the same chunk continua within
+    5e-6 of their maximum (degree 8: measured up to 2.3e-6, all of it the QR
+    mirror's own roundoff: sgelsd lands within 1e-7 of the FP64 solution).
+    How close nalgebra's f32 SVD lands is not known here; the model tolerance
+    of the parity tests (1e-5) covers either."""
+    spec, labels, spectra, g = small
+    star = S.make_star(spec, [7130.0, 0.07, 4.02, 50.0, 20.0], 3000, 100.0, 85000.0, seed=4)
+    d = O.Disp(g, O.DISP_FIXED, star.wl, 85000.0)
+    model = d.produce_model(star.label, O.F64)
+    p = 8
+    c = O.Cont(O.CONT_CHUNK, star.wl, 5, p, 0.2)
+    par32, _ = c.fit(star.flux, star.var, model.astype(np.float32), O.F32)
+    par64, _ = c.fit(star.flux, star.var, model, O.F64)
+    y32 = (star.flux.astype(np.float32) / model.astype(np.float32)).astype(np.float32)
+    for ch, (s0, e0) in enumerate(c.chunk_bounds()):
+        wl = star.wl[s0:e0]
+        xx = -1.0 + 2.0 * (wl - wl[0]) / (wl[-1] - wl[0])
+        A64 = np.vander(xx, p + 1, increasing=True)
+        A32 = A64.astype(np.float32)
+        sol_np = np.linalg.lstsq(A32, y32[s0:e0], rcond=None)[0].astype(np.float64)
+        c_np = A64 @ sol_np
+        c_32 = A64 @ par32[ch * (p + 1):(ch + 1) * (p + 1)]
+        c_64 = A64 @ par64[ch * (p + 1):(ch + 1) * (p + 1)]
+        scale = np.abs(c_64).max()
+        assert np.abs(c_32 - c_np).max() <= 5e-6 * scale
+        assert np.abs(c_32 - c_64).max() <= 5e-6 * scale
+        assert np.abs(c_np - c_64).max() <= 3e-7 * scale
