@@ -23,7 +23,7 @@
 // different tiles overlap:
 //   warp 0      TMA producer: the 64 rows of a tile (16 tile::gather4
 //               loads of four 128-pixel rows each, from the grid resident in
-//               this GPU's memory; no multicast) into a ring of NSTG staging
+//               this GPU's own memory, each CTA loading for itself) into a ring of NSTG staging
 //               buffers;
 //   warp 1      one thread issues the 24 tcgen05.mma of a tile (kind::f16,
 //               M = 128, N = members rounded up to 16) into one of ND
